@@ -1,0 +1,212 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle (``liboracle_rrtmg.so``, sources beside this file) restates WRF-JAX's
+RRTMG LW/SW radiation path in plain C with the reference's binary32 rounding.
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
+it, as the checker; the product path never imports this module.
+
+``lwrad(**kw)`` / ``swrad(**kw)`` take the reference's keyword arguments
+(``rrtmg_lwrad_wrf_columns``, module_ra_rrtmg_lw.py:6789;
+``rrtmg_swrad_wrf_columns``, module_ra_rrtmg_sw.py:2386) in the WRF runtime
+layout and return dicts keyed by the reference's result field names.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle_rrtmg.so"
+
+_F = ctypes.POINTER(ctypes.c_float)
+
+
+class _In(ctypes.Structure):
+    _fields_ = [("ncol", ctypes.c_int), ("nk", ctypes.c_int)] + [
+        (n, _F) for n in ("p3d", "pi3d", "t3d", "qv", "qc", "qi", "qs", "cldfra", "o3",
+                          "re_cloud", "re_ice", "re_snow", "p8w", "t8w", "tsk", "emiss",
+                          "albedo", "coszr", "xland", "xice", "snow")
+    ] + [("p_top", ctypes.c_double)] + [
+        (n, ctypes.c_float) for n in ("co2", "n2o", "ch4", "cfc11", "cfc12", "solcon")
+    ] + [(n, ctypes.c_int) for n in ("has_reqc", "has_reqi", "has_reqs", "icloud", "cldovrlp")]
+
+
+_OUT_FIELDS = ("rthraten", "rthratenc", "up_top", "upc_top", "dn_top", "dnc_top", "up_sfc",
+               "upc_sfc", "dn_sfc", "dnc_sfc", "swddir", "swddni", "swddif", "swddirc",
+               "swddnic", "taug", "fracs_or_taur", "cldfmc", "taucmc", "uflx", "dflx", "uflxc",
+               "dflxc", "hr", "hrc")
+
+
+class _Out(ctypes.Structure):
+    _fields_ = [(n, _F) for n in _OUT_FIELDS]
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with its Makefile (gcc, no GPU needed)."""
+    srcs = [HERE / n for n in ("oracle_common.c", "oracle_lw.c", "oracle_sw.c", "oracle.h",
+                                "oracle_internal.h")]
+    if force or not LIB_PATH.exists() or any(s.stat().st_mtime > LIB_PATH.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE), "liboracle_rrtmg.so"], check=True)
+    return LIB_PATH
+
+
+class Oracle:
+    """Loaded oracle library plus one table blob."""
+
+    def __init__(self, blob_path: str | os.PathLike, nthreads: int | None = None):
+        self.lib = ctypes.CDLL(str(build()))
+        self.lib.ora_tables_load.restype = ctypes.c_void_p
+        self.lib.ora_tables_load.argtypes = [ctypes.c_char_p]
+        self.lib.ora_tables_free.argtypes = [ctypes.c_void_p]
+        for name in ("ora_lw_columns", "ora_sw_columns"):
+            fn = getattr(self.lib, name)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(_In), ctypes.POINTER(_Out), ctypes.c_int]
+        self.lib.ora_lw_nlayers.restype = ctypes.c_int
+        self.lib.ora_lw_nlayers.argtypes = [ctypes.c_double, ctypes.c_int]
+        self.tables = self.lib.ora_tables_load(str(blob_path).encode())
+        if not self.tables:
+            raise RuntimeError(f"oracle could not load table blob {blob_path}")
+        self.nthreads = nthreads or os.cpu_count() or 1
+
+    def __del__(self):
+        tables = getattr(self, "tables", None)
+        if tables:
+            self.lib.ora_tables_free(tables)
+            self.tables = None
+
+    # ------------------------------------------------------------------
+    @staticmethod
+    def _columns(a):  # (nx, nz, ny) -> (ncol, nz), column index = i*ny + j
+        a = np.asarray(a, np.float32)
+        return np.ascontiguousarray(np.swapaxes(a, 1, 2).reshape(-1, a.shape[1]))
+
+    @staticmethod
+    def _flat2d(a):
+        return np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1))
+
+    def _inputs(self, kw):
+        t3d = np.asarray(kw["t3d"])
+        nx, nk, ny = t3d.shape
+        ncol = nx * ny
+        keep = {}
+
+        def ptr(a):
+            keep[id(a)] = a
+            return a.ctypes.data_as(_F)
+
+        s = _In()
+        s.ncol, s.nk = ncol, nk
+        for name, key in (("p3d", "p3d"), ("pi3d", "pi3d"), ("t3d", "t3d"), ("qv", "qv3d"),
+                          ("qc", "qc3d"), ("qi", "qi3d"), ("qs", "qs3d"), ("cldfra", "cldfra3d"),
+                          ("o3", "o33d"), ("re_cloud", "re_cloud"), ("re_ice", "re_ice"),
+                          ("re_snow", "re_snow"), ("p8w", "p8w"), ("t8w", "t8w")):
+            setattr(s, name, ptr(self._columns(kw[key])))
+        zeros2 = np.zeros(ncol, np.float32)
+        for name in ("tsk", "emiss", "albedo", "coszr", "xland", "xice", "snow"):
+            setattr(s, name, ptr(self._flat2d(kw[name]) if name in kw else zeros2))
+        s.p_top = float(kw.get("p_top", 5000.0))
+        s.co2 = np.float32(kw["co2vmr"])
+        s.n2o = np.float32(kw["n2ovmr"])
+        s.ch4 = np.float32(kw["ch4vmr"])
+        s.cfc11 = np.float32(kw.get("cfc11vmr", 0.0))
+        s.cfc12 = np.float32(kw.get("cfc12vmr", 0.0))
+        s.solcon = np.float32(kw.get("solcon", 0.0))
+        s.has_reqc = int(kw.get("has_reqc", 1))
+        s.has_reqi = int(kw.get("has_reqi", 1))
+        s.has_reqs = int(kw.get("has_reqs", 1))
+        s.icloud = int(kw.get("icloud", 1))
+        s.cldovrlp = int(kw.get("cldovrlp", 2))
+        return s, keep, (nx, nk, ny)
+
+    def _outputs(self, ncol, nk, nlay, ngpt, diagnostics):
+        bufs = {}
+        o = _Out()
+        sizes = dict(rthraten=ncol * nk, rthratenc=ncol * nk)
+        for n in ("up_top", "upc_top", "dn_top", "dnc_top", "up_sfc", "upc_sfc", "dn_sfc",
+                  "dnc_sfc", "swddir", "swddni", "swddif", "swddirc", "swddnic"):
+            sizes[n] = ncol
+        if diagnostics:
+            sizes.update(taug=ncol * nlay * ngpt, fracs_or_taur=ncol * nlay * ngpt,
+                         cldfmc=ncol * ngpt * nlay, taucmc=ncol * ngpt * nlay,
+                         uflx=ncol * (nlay + 1), dflx=ncol * (nlay + 1), uflxc=ncol * (nlay + 1),
+                         dflxc=ncol * (nlay + 1), hr=ncol * nlay, hrc=ncol * nlay)
+        for n, size in sizes.items():
+            bufs[n] = np.zeros(size, np.float32)
+            setattr(o, n, bufs[n].ctypes.data_as(_F))
+        return o, bufs
+
+    @staticmethod
+    def _unflat3(a, nx, ny):
+        return np.swapaxes(a.reshape(nx, ny, -1), 1, 2)
+
+    # ------------------------------------------------------------------
+    def lwrad(self, diagnostics: bool = False, **kw) -> dict:
+        s, keep, (nx, nk, ny) = self._inputs(kw)
+        ncol = nx * ny
+        nlay = self.lib.ora_lw_nlayers(float(kw.get("p_top", 5000.0)), nk)
+        o, b = self._outputs(ncol, nk, nlay, 140, diagnostics)
+        rc = self.lib.ora_lw_columns(self.tables, ctypes.byref(s), ctypes.byref(o), self.nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle LW failed with status {rc}")
+        two = lambda a: a.reshape(nx, ny)
+        zeros = np.zeros((nx, ny), np.float32)
+        out = dict(
+            rthratenlw=self._unflat3(b["rthraten"], nx, ny),
+            rthratenlwc=self._unflat3(b["rthratenc"], nx, ny),
+            lwupt=two(b["up_top"]), lwuptc=two(b["upc_top"]), lwuptcln=zeros,
+            lwdnt=two(b["dn_top"]), lwdntc=two(b["dnc_top"]), lwdntcln=zeros,
+            lwupb=two(b["up_sfc"]), lwupbc=two(b["upc_sfc"]), lwupbcln=zeros,
+            lwdnb=two(b["dn_sfc"]), lwdnbc=two(b["dnc_sfc"]), lwdnbcln=zeros,
+            glw=two(b["dn_sfc"]), olr=two(b["up_top"]),
+            lwcf=two(b["upc_top"] - b["up_top"]),
+        )
+        if diagnostics:
+            out["diag"] = dict(
+                taug=b["taug"].reshape(ncol, nlay, 140), fracs=b["fracs_or_taur"].reshape(ncol, nlay, 140),
+                cldfmc=b["cldfmc"].reshape(ncol, 140, nlay), taucmc=b["taucmc"].reshape(ncol, 140, nlay),
+                uflx=b["uflx"].reshape(ncol, nlay + 1), dflx=b["dflx"].reshape(ncol, nlay + 1),
+                uflxc=b["uflxc"].reshape(ncol, nlay + 1), dflxc=b["dflxc"].reshape(ncol, nlay + 1),
+                hr=b["hr"].reshape(ncol, nlay), hrc=b["hrc"].reshape(ncol, nlay))
+        return out
+
+    def swrad(self, diagnostics: bool = False, **kw) -> dict:
+        s, keep, (nx, nk, ny) = self._inputs(kw)
+        ncol = nx * ny
+        nlay = nk + 1
+        o, b = self._outputs(ncol, nk, nlay, 112, diagnostics)
+        rc = self.lib.ora_sw_columns(self.tables, ctypes.byref(s), ctypes.byref(o), self.nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle SW failed with status {rc}")
+        two = lambda a: a.reshape(nx, ny)
+        zeros = np.zeros((nx, ny), np.float32)
+        coszr = self._flat2d(kw["coszr"])
+        day = coszr > 0.0
+        up_t, upc_t, dn_t, dnc_t = b["up_top"], b["upc_top"], b["dn_top"], b["dnc_top"]
+        swcf = np.where(day, (dn_t - up_t) - (dnc_t - upc_t), 0.0).astype(np.float32)
+        gsw = np.where(day, b["dn_sfc"] - b["up_sfc"], 0.0).astype(np.float32)
+        out = dict(
+            rthratensw=self._unflat3(b["rthraten"], nx, ny),
+            rthratenswc=self._unflat3(b["rthratenc"], nx, ny),
+            swupt=two(up_t), swuptc=two(upc_t), swuptcln=zeros,
+            swdnt=two(dn_t), swdntc=two(dnc_t), swdntcln=zeros,
+            swupb=two(b["up_sfc"]), swupbc=two(b["upc_sfc"]), swupbcln=zeros,
+            swdnb=two(b["dn_sfc"]), swdnbc=two(b["dnc_sfc"]), swdnbcln=zeros,
+            swcf=two(swcf), gsw=two(gsw),
+            swddir=two(b["swddir"]), swddni=two(b["swddni"]), swddif=two(b["swddif"]),
+            swdownc=two(b["dnc_sfc"]), swddnic=two(b["swddnic"]), swddirc=two(b["swddirc"]),
+            coszr=two(coszr),
+        )
+        if diagnostics:
+            out["diag"] = dict(
+                taug=b["taug"].reshape(ncol, nlay, 112), taur=b["fracs_or_taur"].reshape(ncol, nlay, 112),
+                cldfmc=b["cldfmc"].reshape(ncol, 112, nlay), taucmc=b["taucmc"].reshape(ncol, 112, nlay),
+                uflx=b["uflx"].reshape(ncol, nlay + 1), dflx=b["dflx"].reshape(ncol, nlay + 1),
+                uflxc=b["uflxc"].reshape(ncol, nlay + 1), dflxc=b["dflxc"].reshape(ncol, nlay + 1),
+                hr=b["hr"].reshape(ncol, nlay), hrc=b["hrc"].reshape(ncol, nlay))
+        return out

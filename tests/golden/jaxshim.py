@@ -23,11 +23,16 @@ Nothing in the product imports this file.
 
 from __future__ import annotations
 
+import ctypes
+import ctypes.util
 import sys
 import types
-from collections import namedtuple
 
 import numpy as np
+
+_LIBM = ctypes.CDLL(ctypes.util.find_library("m"))
+_LIBM.expf.restype = ctypes.c_float
+_LIBM.expf.argtypes = [ctypes.c_float]
 
 
 # ----------------------------------------------------------------------------
@@ -49,6 +54,12 @@ class Arr(np.ndarray):
     def __getitem__(self, idx):
         # JAX gathers clamp out-of-range integer-array indices instead of raising.
         return super().__getitem__(_clamp_index(idx, self.shape))
+
+    def __pow__(self, other):
+        # ``x ** n`` with a Python int is lax.integer_pow (repeated squaring).
+        if isinstance(other, int) and not isinstance(other, bool):
+            return _integer_pow(self.view(np.ndarray), other)
+        return super().__pow__(other)
 
 
 def _clamp_index(idx, shape):
@@ -430,6 +441,18 @@ def _make_jnp():
 
     jnp.max = max_
     jnp.amax = max_
+
+    def exp(x):
+        arr = np.asarray(_plain(x))
+        if arr.dtype == np.float32:
+            # XLA's binary32 exp is not available here; use glibc expf, the
+            # libm the reference emulates everywhere else on this path.
+            flat = arr.reshape(-1)
+            out = np.fromiter((_LIBM.expf(float(v)) for v in flat), dtype=np.float32, count=flat.size)
+            return wrap(out.reshape(arr.shape))
+        return wrap(np.exp(arr))
+
+    jnp.exp = exp
 
     def _getattr(name):
         f = getattr(np, name)
