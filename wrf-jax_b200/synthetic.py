@@ -100,14 +100,15 @@ def _qsat(t: np.ndarray, p_pa: np.ndarray) -> np.ndarray:
 def make_columns(nx: int, ny: int, nk: int, *, seed: int = 0, t_noise: float = 2.0,
                  rh_lo: float = 0.2, cloud_p: float | tuple = 0.3,
                  night_fraction: float = 0.3, has_req: bool = False,
+                 fractional_clouds: bool = False, p_top: float = P_TOP_PA,
                  julian: float = 172.5, yr: int = 2024) -> ColumnState:
     """Generate one domain of nx x ny columns with nk mass levels."""
     rng = np.random.Generator(np.random.PCG64(seed))
     ncol = nx * ny
     psfc = rng.uniform(950.0e2, 1030.0e2, size=ncol)
     eta = _eta_interfaces(nk)
-    p8w = P_TOP_PA + eta[None, :] * (psfc[:, None] - P_TOP_PA)        # (ncol, nk+1) Pa
-    p8w[:, nk] = P_TOP_PA
+    p8w = p_top + eta[None, :] * (psfc[:, None] - p_top)              # (ncol, nk+1) Pa
+    p8w[:, nk] = p_top
     p3d = 0.5 * (p8w[:, :-1] + p8w[:, 1:])                              # (ncol, nk)
 
     def t_profile(p_pa):
@@ -133,6 +134,8 @@ def make_columns(nx: int, ny: int, nk: int, *, seed: int = 0, t_noise: float = 2
         col_p = np.full((ncol, 1), float(cloud_p))
     cloudy = (rng.uniform(size=(ncol, nk)) < col_p) & (p3d > 300.0e2)
     cldfra = cloudy.astype(np.float64)
+    if fractional_clouds:
+        cldfra = np.where(cloudy, rng.uniform(0.05, 1.0, size=(ncol, nk)), 0.0)
     qc = np.where(cloudy, rng.uniform(0.0, 5.0e-4, size=(ncol, nk)), 0.0)
     qi = np.where(cloudy, rng.uniform(0.0, 2.0e-4, size=(ncol, nk)), 0.0)
     qs = np.zeros((ncol, nk))
@@ -170,7 +173,7 @@ def make_columns(nx: int, ny: int, nk: int, *, seed: int = 0, t_noise: float = 2
         re_ice=to3d(re_ice), re_snow=to3d(re_snow),
     )
     h = 1 if has_req else 0
-    scalars = dict(p_top=P_TOP_PA, yr=yr, julian=julian,
+    scalars = dict(p_top=float(p_top), yr=yr, julian=julian,
                    solcon=float(np.float32(1370.0) * np.float32(eccentricity_factor(julian))),
                    has_reqc=h, has_reqi=h, has_reqs=h, **GASES)
     return ColumnState(fields=fields, scalars=scalars, nx=nx, ny=ny, nk=nk)
