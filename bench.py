@@ -1,0 +1,309 @@
+"""Benchmark: LW+SW RRTMG radiation columns per second on B200.
+
+One step = one rrtmg_lwrad + one rrtmg_swrad call over the whole 425 x 425 x 50
+domain (180,625 columns, the plain-kernel workload) with inputs resident in
+HBM.  `e2e` repeats the step through the public Python API with host (numpy)
+buffers, so the host->device copies of the inputs and the device->host copies
+of every output are inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs its own 425x425x50
+domain (weak scaling; columns are independent, so there is no collective on the
+data path) and the time is the maximum over ranks.
+
+`--impl reference` times the CPU restatement of the reference's algorithm
+(oracle/, the reference itself needs jax/jaxlib which are not installed) on the
+host cores, on a bounded sample of the same workload per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+WORKLOAD = dict(name="plain_425x425x50", nx=425, ny=425, nk=50, seed=0)
+METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0.2 K/day"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _package():
+    if "wrf_jax_b200" in sys.modules:
+        return sys.modules["wrf_jax_b200"]
+    root = REPO / "wrf-jax_b200"
+    spec = importlib.util.spec_from_file_location(
+        "wrf_jax_b200", root / "__init__.py", submodule_search_locations=[str(root)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["wrf_jax_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+        else:
+            self.lines = []
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(ncols_sample: int, threads: int | None = None, reps: int = 1):
+    """Time the oracle (CPU restatement, 'port') on a bounded sample of the workload."""
+    _package()
+    from wrf_jax_b200 import synthetic, tables
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle
+
+    threads = threads or os.cpu_count() or 1
+    ny = WORKLOAD["ny"]
+    nx = max(1, ncols_sample // ny)
+    st = synthetic.make_columns(WORKLOAD["nx"], ny, WORKLOAD["nk"], seed=WORKLOAD["seed"])
+    kw_lw, kw_sw = st.lw_kwargs(), st.sw_kwargs()
+    for kw in (kw_lw, kw_sw):
+        for k, v in list(kw.items()):
+            if isinstance(v, np.ndarray):
+                kw[k] = np.ascontiguousarray(v[:nx])
+    ora = oracle.Oracle(tables.DEFAULT_BLOB, nthreads=threads)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ora.lwrad(**kw_lw)
+        ora.swrad(**kw_sw)
+        times.append(time.perf_counter() - t0)
+    cols = nx * ny
+    return cols / min(times), threads, f"{nx}x{ny}x{WORKLOAD['nk']} rows of the 425x425x50 domain ({cols} columns)", min(times)
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    sample = int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", "4250"))
+    threads = os.cpu_count() or 1
+    times = []
+    for _ in range(args.warmup):
+        cpu_baseline(sample, threads)
+    for _ in range(args.steps):
+        v, th, desc, dt = cpu_baseline(sample, threads)
+        times.append(dt)
+    dt = statistics.median(times)
+    ncols = (sample // WORKLOAD["ny"]) * WORKLOAD["ny"]
+    value = ncols / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD["name"], "columns_per_step": ncols, "nk": WORKLOAD["nk"]},
+        "cpu_baseline": {"value": value, "unit": "columns/s", "cores": threads, "kind": "port",
+                         "sample": f"{ncols} columns of the 425x425x50 domain per step; C restatement "
+                                   "of the reference path (jax/jaxlib are not installed, so the "
+                                   "reference's own JAX code cannot run on this host)"},
+        "e2e": {"value": value, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    _package()
+    from wrf_jax_b200 import rrtmg, synthetic
+
+    st = synthetic.make_columns(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nk"], seed=WORKLOAD["seed"] + rank)
+    ncol = st.nx * st.ny
+    lw_host, sw_host = st.lw_kwargs(), st.sw_kwargs()
+    dev = lambda kw: {k: (torch.from_numpy(v).cuda() if isinstance(v, np.ndarray) else v) for k, v in kw.items()}
+    lw_dev, sw_dev = dev(lw_host), dev(sw_host)
+    ctx = rrtmg.default_context()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        a = rrtmg.rrtmg_lwrad_wrf_columns(**lw_dev, context=ctx)
+        b = rrtmg.rrtmg_swrad_wrf_columns(**sw_dev, context=ctx)
+        return a, b
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier()
+    # per-kernel timing of the dominant kernels (events on the launching stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
+    with ClockSampler(local) as clocks:
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        lw_ms, sw_ms = [], []
+        t0.record(stream)
+        for s in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e2 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rrtmg.rrtmg_lwrad_wrf_columns(**lw_dev, context=ctx)
+            e1.record(stream)
+            rrtmg.rrtmg_swrad_wrf_columns(**sw_dev, context=ctx)
+            e2.record(stream)
+            lw_ms.append((e0, e1))
+            sw_ms.append((e1, e2))
+        t1.record(stream)
+        barrier()
+    elapsed = t0.elapsed_time(t1) / 1e3
+    lw_t = statistics.median(a.elapsed_time(b) for a, b in lw_ms) / 1e3
+    sw_t = statistics.median(a.elapsed_time(b) for a, b in sw_ms) / 1e3
+    if dist is not None:
+        tt = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    value = ws * ncol * args.steps / elapsed
+
+    # end-to-end through the public API with host buffers
+    e2e_steps = max(1, min(args.steps, 5))
+    h2d = sum(v.nbytes for v in lw_host.values() if isinstance(v, np.ndarray)) + \
+        sum(v.nbytes for v in sw_host.values() if isinstance(v, np.ndarray))
+    barrier()
+    t_e2e = time.perf_counter()
+    d2h = 0
+    for _ in range(e2e_steps):
+        a = rrtmg.rrtmg_lwrad_wrf_columns(**lw_host, context=ctx)
+        b = rrtmg.rrtmg_swrad_wrf_columns(**sw_host, context=ctx)
+        d2h = sum(x.nbytes for x in a) + sum(x.nbytes for x in b)
+    barrier()
+    t_e2e = time.perf_counter() - t_e2e
+    if dist is not None:
+        tt = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = ws * ncol * e2e_steps / t_e2e
+
+    hbm, bf16, peak_kind = _peaks()
+    nk = WORKLOAD["nk"]
+    # compulsory HBM bytes per column: LW reads 17 (nx,nk,ny)/(nx,nk+1,ny) fields
+    # and 5 2-D fields, writes 2 3-D + 15 2-D; SW reads 18 3-D-like + 6 2-D, writes 2 3-D + 23 2-D
+    lw_bytes = 4 * (15 * nk + 2 * (nk + 1) + 5 + 2 * nk + 15)
+    sw_bytes = 4 * (15 * nk + 2 * (nk + 1) + 6 + 2 * nk + 23)
+    dom = "lw" if lw_t >= sw_t else "sw"
+    dom_t = lw_t if dom == "lw" else sw_t
+    dom_bytes = (lw_bytes if dom == "lw" else sw_bytes) * ncol
+    achieved = dom_bytes / dom_t / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": WORKLOAD["name"], "nx": WORKLOAD["nx"], "ny": WORKLOAD["ny"], "nk": nk,
+                   "columns_per_gpu": ncol, "path": "plain RRTMG LW+SW (surrogate not built)",
+                   "l2": "inputs larger than L2 (%.0f MB per step)" % (h2d / 1e6),
+                   "lw_ms": lw_t * 1e3, "sw_ms": sw_t * 1e3},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "kernel": f"{dom}_kernel",
+                     "peak_source": peak_kind,
+                     "note": "fused per-column kernel: compulsory HBM bytes / time; the kernel is "
+                             "FP32-issue bound, see profiles/"},
+        "gpu_launches": 4 * args.steps,
+        "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", "4250")))
+        line["cpu_baseline"] = {"value": v, "unit": "columns/s", "cores": th, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

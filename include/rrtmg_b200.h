@@ -1,0 +1,120 @@
+/*
+ * rrtmg_b200: C-ABI of the B200 RRTMG longwave + shortwave radiation path.
+ *
+ * Drop-in for the two jitted column kernels WRF-JAX's radiation stage calls:
+ *   rrtmg_lwrad_wrf_columns  (src/wrf_jax/physics/module_ra_rrtmg_lw.py:6789)
+ *   rrtmg_swrad_wrf_columns  (src/wrf_jax/physics/module_ra_rrtmg_sw.py:2386)
+ * dispatched from _run_radiation_sides / _run_paired_rrtmg
+ * (src/wrf_jax/runtime.py:5422, :433, jitted at runtime.py:406-414).
+ *
+ * Conventions
+ *   - Arrays are float32 in the WRF-JAX runtime layout: 3-D fields
+ *     (west_east, bottom_top, south_north) = (nx, nk, ny) row-major, level-
+ *     interface fields (nx, nk+1, ny), 2-D fields (nx, ny).  Column c = i*ny + j.
+ *     (module_ra_rrtmg_sw.py:2435-2438, module_ra_rrtmg_lw.py:6572-6589)
+ *   - Every array pointer is a DEVICE pointer the caller owns; outputs are
+ *     written in place, inputs are never modified (the reference's calls are
+ *     pure functions returning new arrays).
+ *   - The library owns the lookup tables (uploaded once by rrtmg_create) and
+ *     its per-call scratch (stream-ordered allocations on the call's stream).
+ *   - Calls are asynchronous on the given cudaStream_t (passed as void*; NULL =
+ *     legacy default stream).  One context may serve several streams and host
+ *     threads concurrently.
+ *   - Status codes are ordered: OK < BAD_ARG < UNSUPPORTED_OPTION < CUDA < TIMEOUT.
+ *     Option combinations the reference rejects with NotImplementedError
+ *     (module_ra_rrtmg_lw.py:5750-5753, module_ra_rrtmg_sw.py:1438-1441) return
+ *     RRTMG_UNSUPPORTED_OPTION.
+ */
+#ifndef RRTMG_B200_H
+#define RRTMG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RRTMG_OK = 0,
+    RRTMG_BAD_ARG = 1,
+    RRTMG_UNSUPPORTED_OPTION = 2,
+    RRTMG_CUDA = 3,
+    RRTMG_TIMEOUT = 4
+} rrtmg_status;
+
+typedef struct rrtmg_ctx rrtmg_ctx;
+
+/* Static keywords and scalars of one call (runtime.py:383-404 lists the
+ * reference's static keywords; the gas scalars are runtime.py:5627-5664). */
+typedef struct {
+    int nx, ny, nk;          /* domain: nx*ny columns, nk mass levels */
+    double p_top;            /* model top pressure, Pa (LW buffer layers) */
+    float co2vmr, n2ovmr, ch4vmr, cfc11vmr, cfc12vmr;   /* volume mixing ratios */
+    float solcon;            /* solar constant, W m-2 (SW) */
+    int has_reqc, has_reqi, has_reqs;                   /* effective-radius inputs present */
+    int icloud;              /* 0: no cloud microphysics radii (SW runs clear) */
+    int cldovrlp;            /* 0 clear, >= 1 McICA maximum-random overlap */
+} rrtmg_config;
+
+/* Keyword arrays of rrtmg_lwrad_wrf_columns (module_ra_rrtmg_lw.py:6789-6822).
+ * dz8w is accepted for signature parity and not read (the reference deletes it). */
+typedef struct {
+    const float *p3d, *p8w, *pi3d, *t3d, *t8w, *tsk, *dz8w;
+    const float *qv3d, *qc3d, *qi3d, *qs3d, *cldfra3d, *o33d;
+    const float *emiss, *xland, *xice, *snow;
+    const float *re_cloud, *re_ice, *re_snow;
+} rrtmg_lw_in;
+
+/* Fields of RrtmgLwWrfColumnResult (module_ra_rrtmg_lw.py:499-518). */
+typedef struct {
+    float *rthratenlw, *rthratenlwc;                       /* (nx, nk, ny) K/s of theta */
+    float *lwupt, *lwuptc, *lwuptcln, *lwdnt, *lwdntc, *lwdntcln;
+    float *lwupb, *lwupbc, *lwupbcln, *lwdnb, *lwdnbc, *lwdnbcln;
+    float *glw, *olr, *lwcf;                               /* (nx, ny) W m-2 */
+} rrtmg_lw_out;
+
+/* Keyword arrays of rrtmg_swrad_wrf_columns (module_ra_rrtmg_sw.py:2386-2420).
+ * Albedo fields for sf_surface_physics == 8 are not part of this path. */
+typedef struct {
+    const float *p3d, *p8w, *pi3d, *t3d, *t8w, *tsk, *dz8w;
+    const float *qv3d, *qc3d, *qi3d, *qs3d, *cldfra3d, *o33d;
+    const float *albedo, *coszr, *xland, *xice, *snow;
+    const float *re_cloud, *re_ice, *re_snow;
+} rrtmg_sw_in;
+
+/* Fields of RrtmgSwWrfColumnResult (module_ra_rrtmg_sw.py:617-642). */
+typedef struct {
+    float *rthratensw, *rthratenswc;                       /* (nx, nk, ny) */
+    float *swupt, *swuptc, *swuptcln, *swdnt, *swdntc, *swdntcln;
+    float *swupb, *swupbc, *swupbcln, *swdnb, *swdnbc, *swdnbcln;
+    float *swcf, *gsw, *swddir, *swddni, *swddif, *swdownc, *swddnic, *swddirc;
+    float *coszr;                                          /* (nx, ny) */
+} rrtmg_sw_out;
+
+/* Build a context on `device` from a table blob written by the package's
+ * tables.py (replaces the lru-cached table loaders runtime.py:441-466). */
+rrtmg_status rrtmg_create(const char *table_blob_path, int device, rrtmg_ctx **out);
+rrtmg_status rrtmg_create_from_memory(const void *blob, size_t nbytes, int device, rrtmg_ctx **out);
+void rrtmg_destroy(rrtmg_ctx *ctx);
+
+/* LW: replaces _rrtmg_lwrad_wrf_columns_jit (runtime.py:406-409). */
+rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in,
+                         rrtmg_lw_out *out, void *stream);
+/* SW: replaces _rrtmg_swrad_wrf_columns_jit (runtime.py:410-414). */
+rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in,
+                         rrtmg_sw_out *out, void *stream);
+
+/* Number of LW layers used for a model top and level count
+ * (rrtmg_lw_nlayers, module_ra_rrtmg_common.py:1243-1247). */
+int rrtmg_lw_nlayers(double p_top, int nk);
+
+/* Human-readable text of the last error recorded on this context (or of the
+ * last failed rrtmg_create when ctx is NULL). */
+const char *rrtmg_last_error(const rrtmg_ctx *ctx);
+const char *rrtmg_status_string(rrtmg_status status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RRTMG_B200_H */

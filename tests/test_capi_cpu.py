@@ -1,0 +1,57 @@
+"""C-ABI checks that need no GPU: the library loads and exports every symbol
+declared in include/rrtmg_b200.h; host-side helpers agree with the reference."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+
+import pytest
+
+from conftest import REPO
+
+
+def _declared_symbols():
+    text = (REPO / "include" / "rrtmg_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)  # declarations only, not comments
+    return sorted(set(re.findall(r"\b(rrtmg_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = _declared_symbols()
+    assert {"rrtmg_create", "rrtmg_lwrad", "rrtmg_swrad", "rrtmg_destroy"} <= set(names)
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    from wrf_jax_b200 import _capi, build
+    if not _capi.LIB_PATH.exists():
+        build.build_library()
+    lib = ctypes.CDLL(str(_capi.LIB_PATH))
+    for name in _declared_symbols():
+        assert hasattr(lib, name), name
+    assert set(_capi.EXPORTS) == set(_declared_symbols())
+
+
+@pytest.mark.parametrize("p_top,nk", [(5000.0, 44), (5000.0, 50), (1000.0, 30), (2000.0, 24), (0.0, 10)])
+def test_lw_layer_count_matches_reference_formula(pkg, p_top, nk):
+    from wrf_jax_b200 import _capi
+    lib = _capi.load()
+    # rrtmg_lw_nlayers (module_ra_rrtmg_common.py:1243-1247)
+    expected = (nk + 1) + int(float(p_top) * 0.01 / 4.0 + 0.5) - 1
+    assert lib.rrtmg_lw_nlayers(p_top, nk) == expected
+
+
+def test_status_strings(pkg):
+    from wrf_jax_b200 import _capi
+    lib = _capi.load()
+    assert lib.rrtmg_status_string(0) == b"ok"
+    assert lib.rrtmg_status_string(2) == b"unsupported option"
+
+
+def test_create_rejects_missing_blob(pkg):
+    from wrf_jax_b200 import _capi
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    st = lib.rrtmg_create(b"/nonexistent/blob.bin", 0, ctypes.byref(h))
+    assert st == 1  # RRTMG_BAD_ARG, before any CUDA call
+    assert b"cannot open" in lib.rrtmg_last_error(None)

@@ -1,0 +1,94 @@
+"""ctypes binding of librrtmg_b200.so (the C-ABI in include/rrtmg_b200.h)."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "librrtmg_b200.so"
+
+_F = ctypes.c_void_p  # device pointers
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nk", ctypes.c_int),
+                ("p_top", ctypes.c_double),
+                ("co2vmr", ctypes.c_float), ("n2ovmr", ctypes.c_float), ("ch4vmr", ctypes.c_float),
+                ("cfc11vmr", ctypes.c_float), ("cfc12vmr", ctypes.c_float), ("solcon", ctypes.c_float),
+                ("has_reqc", ctypes.c_int), ("has_reqi", ctypes.c_int), ("has_reqs", ctypes.c_int),
+                ("icloud", ctypes.c_int), ("cldovrlp", ctypes.c_int)]
+
+
+LW_IN_FIELDS = ("p3d", "p8w", "pi3d", "t3d", "t8w", "tsk", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d",
+                "cldfra3d", "o33d", "emiss", "xland", "xice", "snow", "re_cloud", "re_ice", "re_snow")
+LW_OUT_FIELDS = ("rthratenlw", "rthratenlwc", "lwupt", "lwuptc", "lwuptcln", "lwdnt", "lwdntc",
+                 "lwdntcln", "lwupb", "lwupbc", "lwupbcln", "lwdnb", "lwdnbc", "lwdnbcln", "glw",
+                 "olr", "lwcf")
+SW_IN_FIELDS = ("p3d", "p8w", "pi3d", "t3d", "t8w", "tsk", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d",
+                "cldfra3d", "o33d", "albedo", "coszr", "xland", "xice", "snow", "re_cloud", "re_ice",
+                "re_snow")
+SW_OUT_FIELDS = ("rthratensw", "rthratenswc", "swupt", "swuptc", "swuptcln", "swdnt", "swdntc",
+                 "swdntcln", "swupb", "swupbc", "swupbcln", "swdnb", "swdnbc", "swdnbcln", "swcf",
+                 "gsw", "swddir", "swddni", "swddif", "swdownc", "swddnic", "swddirc", "coszr")
+
+
+class LwIn(ctypes.Structure):
+    _fields_ = [(n, _F) for n in LW_IN_FIELDS]
+
+
+class LwOut(ctypes.Structure):
+    _fields_ = [(n, _F) for n in LW_OUT_FIELDS]
+
+
+class SwIn(ctypes.Structure):
+    _fields_ = [(n, _F) for n in SW_IN_FIELDS]
+
+
+class SwOut(ctypes.Structure):
+    _fields_ = [(n, _F) for n in SW_OUT_FIELDS]
+
+
+STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
+          4: "RRTMG_TIMEOUT"}
+
+EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
+           "rrtmg_lw_nlayers", "rrtmg_last_error", "rrtmg_status_string")
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
+    """Load librrtmg_b200.so and declare its signatures (raises if it is missing)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(
+            f"{p} is missing: build the CUDA library first (__graft_entry__.build() or "
+            "python -m wrf_jax_b200 build); there is no CPU fallback")
+    lib = ctypes.CDLL(str(p))
+    lib.rrtmg_create.restype = ctypes.c_int
+    lib.rrtmg_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.rrtmg_create_from_memory.restype = ctypes.c_int
+    lib.rrtmg_create_from_memory.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_void_p)]
+    lib.rrtmg_destroy.restype = None
+    lib.rrtmg_destroy.argtypes = [ctypes.c_void_p]
+    lib.rrtmg_lwrad.restype = ctypes.c_int
+    lib.rrtmg_lwrad.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(LwIn),
+                                ctypes.POINTER(LwOut), ctypes.c_void_p]
+    lib.rrtmg_swrad.restype = ctypes.c_int
+    lib.rrtmg_swrad.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(SwIn),
+                                ctypes.POINTER(SwOut), ctypes.c_void_p]
+    lib.rrtmg_lw_nlayers.restype = ctypes.c_int
+    lib.rrtmg_lw_nlayers.argtypes = [ctypes.c_double, ctypes.c_int]
+    lib.rrtmg_last_error.restype = ctypes.c_char_p
+    lib.rrtmg_last_error.argtypes = [ctypes.c_void_p]
+    lib.rrtmg_status_string.restype = ctypes.c_char_p
+    lib.rrtmg_status_string.argtypes = [ctypes.c_int]
+    if path is None:
+        _lib = lib
+    return lib

@@ -1,0 +1,587 @@
+// C-ABI of librrtmg_b200.so: context creation (table upload), the LW and SW
+// radiation calls, and error reporting.  See include/rrtmg_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/rrtmg_b200.h"
+#include "rrtmg_device.cuh"
+#include "rrtmg_kernels.h"
+
+using namespace rrtmg;
+
+namespace {
+
+struct Entry {
+  uint32_t dtype, ndim, shape[4];
+  uint64_t offset, nbytes;
+};
+
+std::mutex g_create_mutex;
+std::string g_create_error;
+
+}  // namespace
+
+struct rrtmg_ctx {
+  int device = 0;
+  std::vector<unsigned char> host_blob;
+  std::map<std::string, Entry> entries;
+  void *dev_blob = nullptr;
+  Tables tables{};
+  std::mutex mutex;
+  std::string last_error;
+  // KISS jump tables keyed by (nlay, nsub, skip); never freed before destroy
+  std::map<std::tuple<int, int, int>, KissJump *> jumps;
+};
+
+namespace {
+
+rrtmg_status fail(rrtmg_ctx *ctx, rrtmg_status st, const std::string &msg) {
+  if (ctx) {
+    std::lock_guard<std::mutex> lk(ctx->mutex);
+    ctx->last_error = msg;
+  } else {
+    std::lock_guard<std::mutex> lk(g_create_mutex);
+    g_create_error = msg;
+  }
+  return st;
+}
+
+rrtmg_status cuda_fail(rrtmg_ctx *ctx, cudaError_t e, const char *what) {
+  return fail(ctx, RRTMG_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+bool parse_blob(rrtmg_ctx *ctx, std::string &err) {
+  const auto &raw = ctx->host_blob;
+  if (raw.size() < 16 || std::memcmp(raw.data(), "RRTMGB2\0", 8) != 0) {
+    err = "not an RRTMG table blob";
+    return false;
+  }
+  uint32_t version, count;
+  std::memcpy(&version, raw.data() + 8, 4);
+  std::memcpy(&count, raw.data() + 12, 4);
+  if (version != 1) {
+    err = "unsupported table blob version";
+    return false;
+  }
+  size_t pos = 16;
+  for (uint32_t i = 0; i < count; ++i, pos += 88) {
+    if (pos + 88 > raw.size()) {
+      err = "truncated table blob header";
+      return false;
+    }
+    char name[49] = {0};
+    std::memcpy(name, raw.data() + pos, 48);
+    Entry e;
+    std::memcpy(&e.dtype, raw.data() + pos + 48, 4);
+    std::memcpy(&e.ndim, raw.data() + pos + 52, 4);
+    std::memcpy(e.shape, raw.data() + pos + 56, 16);
+    std::memcpy(&e.offset, raw.data() + pos + 72, 8);
+    std::memcpy(&e.nbytes, raw.data() + pos + 80, 8);
+    if (e.offset + e.nbytes > raw.size()) {
+      err = std::string("table entry out of range: ") + name;
+      return false;
+    }
+    ctx->entries[name] = e;
+  }
+  return true;
+}
+
+template <typename T>
+const T *dev_ptr(rrtmg_ctx *ctx, const std::string &name, int *count = nullptr) {
+  auto it = ctx->entries.find(name);
+  if (it == ctx->entries.end()) {
+    if (count) *count = 0;
+    return nullptr;
+  }
+  if (count) *count = static_cast<int>(it->second.nbytes / sizeof(T));
+  return reinterpret_cast<const T *>(static_cast<const unsigned char *>(ctx->dev_blob) + it->second.offset);
+}
+
+template <typename T>
+const T *host_ptr(rrtmg_ctx *ctx, const std::string &name, int *count = nullptr) {
+  auto it = ctx->entries.find(name);
+  if (it == ctx->entries.end()) {
+    if (count) *count = 0;
+    return nullptr;
+  }
+  if (count) *count = static_cast<int>(it->second.nbytes / sizeof(T));
+  return reinterpret_cast<const T *>(ctx->host_blob.data() + it->second.offset);
+}
+
+// Ozone climatology work profile (module_ra_rrtmg_common.py:343-372), binary32.
+void o3_work_profile(rrtmg_ctx *ctx, float *o3wrk, float *ppwrkh) {
+  const float *o3sum = host_ptr<float>(ctx, "o3sum");
+  const float *ppsum = host_ptr<float>(ctx, "ppsum");
+  const float *o3win = host_ptr<float>(ctx, "o3win");
+  const float *ppwin = host_ptr<float>(ctx, "ppwin");
+  volatile float t;
+  o3wrk[0] = 0.5f * (o3sum[0] + o3win[0]);
+  for (int i = 0; i < 30; ++i) {
+    t = (o3win[i + 1] - o3win[i]) / (ppwin[i + 1] - ppwin[i]);
+    const float slope = t;
+    t = slope * (ppsum[i + 1] - ppwin[i]);
+    const float prod = t;
+    const float interp = o3win[i] + prod;
+    o3wrk[i + 1] = 0.5f * (interp + o3sum[i + 1]);
+  }
+  ppwrkh[0] = 1100.0f;
+  for (int i = 0; i < 30; ++i) ppwrkh[i + 1] = 0.5f * (ppsum[i + 1] + ppsum[i]);
+  ppwrkh[31] = 0.0f;
+}
+
+bool fill_tables(rrtmg_ctx *ctx, std::string &err) {
+  Tables &T = ctx->tables;
+  static const int lw_ngc[16] = {10, 12, 16, 14, 16, 8, 12, 8, 12, 6, 8, 8, 4, 2, 2, 2};
+  static const int sw_ngc[14] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};
+  for (int b = 0; b < kLwBands; ++b) {
+    const std::string p = "lw" + std::to_string(b + 1) + ".";
+    LwBand &B = T.lw[b];
+    int n = 0;
+    B.ka = dev_ptr<float>(ctx, p + "ka", &n);
+    B.ka_rows = n / lw_ngc[b];
+    B.kb = dev_ptr<float>(ctx, p + "kb", &n);
+    B.kb_rows = B.kb ? n / lw_ngc[b] : 0;
+    B.fracrefa = dev_ptr<float>(ctx, p + "fracrefa");
+    B.fracrefb = dev_ptr<float>(ctx, p + "fracrefb");
+    B.selfref = dev_ptr<float>(ctx, p + "selfref");
+    B.forref = dev_ptr<float>(ctx, p + "forref");
+    B.ka_mn2 = dev_ptr<float>(ctx, p + "ka_mn2");
+    B.kb_mn2 = dev_ptr<float>(ctx, p + "kb_mn2");
+    B.ka_mn2o = dev_ptr<float>(ctx, p + "ka_mn2o");
+    B.kb_mn2o = dev_ptr<float>(ctx, p + "kb_mn2o");
+    B.ka_mo3 = dev_ptr<float>(ctx, p + "ka_mo3");
+    B.kb_mo3 = dev_ptr<float>(ctx, p + "kb_mo3");
+    B.ka_mco2 = dev_ptr<float>(ctx, p + "ka_mco2");
+    B.kb_mco2 = dev_ptr<float>(ctx, p + "kb_mco2");
+    B.ka_mco = dev_ptr<float>(ctx, p + "ka_mco");
+    B.ka_mo2 = dev_ptr<float>(ctx, p + "ka_mo2");
+    B.kb_mo2 = dev_ptr<float>(ctx, p + "kb_mo2");
+    B.ccl4 = dev_ptr<float>(ctx, p + "ccl4");
+    B.cfc11adj = dev_ptr<float>(ctx, p + "cfc11adj");
+    B.cfc12 = dev_ptr<float>(ctx, p + "cfc12");
+    B.cfc22adj = dev_ptr<float>(ctx, p + "cfc22adj");
+    if (!B.ka || !B.fracrefa || !B.selfref || !B.forref) {
+      err = "table blob lacks longwave band " + std::to_string(b + 1);
+      return false;
+    }
+  }
+  for (int b = 0; b < kSwBands; ++b) {
+    const std::string p = "sw" + std::to_string(b + 16) + ".";
+    SwBand &B = T.sw[b];
+    int n = 0;
+    B.ka = dev_ptr<float>(ctx, p + "ka");
+    B.kb = dev_ptr<float>(ctx, p + "kb");
+    B.selfref = dev_ptr<float>(ctx, p + "selfref");
+    B.forref = dev_ptr<float>(ctx, p + "forref", &n);
+    B.forref_rows = B.forref ? n / sw_ngc[b] : 0;
+    B.sfluxref = dev_ptr<float>(ctx, p + "sfluxref", &n);
+    B.sflux_cols = B.sfluxref ? n / sw_ngc[b] : 0;
+    B.rayla = dev_ptr<float>(ctx, p + "rayla");
+    B.raylb = dev_ptr<float>(ctx, p + "raylb");
+    B.absch4 = dev_ptr<float>(ctx, p + "absch4");
+    B.abso3a = dev_ptr<float>(ctx, p + "abso3a");
+    B.abso3b = dev_ptr<float>(ctx, p + "abso3b");
+    B.absh2o = dev_ptr<float>(ctx, p + "absh2o");
+    B.absco2 = dev_ptr<float>(ctx, p + "absco2");
+    const float *rayl = host_ptr<float>(ctx, p + "rayl", &n);
+    if (rayl && n == 1) {
+      B.rayl = rayl[0];
+      B.rayl_g = nullptr;
+    } else {
+      B.rayl = 0.0f;
+      B.rayl_g = dev_ptr<float>(ctx, p + "rayl");
+    }
+    auto scalar = [&](const char *f) {
+      const float *v = host_ptr<float>(ctx, p + f);
+      return v ? v[0] : 0.0f;
+    };
+    B.strrat = scalar("strrat");
+    B.strrat1 = scalar("strrat1");
+    B.givfac = scalar("givfac");
+    B.scalekur = scalar("scalekur");
+    const int32_t *lr = host_ptr<int32_t>(ctx, p + "layreffr");
+    B.layreffr = lr ? lr[0] : 0;
+    if (!B.sfluxref) {
+      err = "table blob lacks shortwave band " + std::to_string(b + 16);
+      return false;
+    }
+  }
+  T.lw_preflog = dev_ptr<float>(ctx, "lw.preflog");
+  T.lw_tref = dev_ptr<float>(ctx, "lw.tref");
+  T.chi_mls = dev_ptr<float>(ctx, "lw.chi_mls");
+  T.totplnk = dev_ptr<float>(ctx, "lw.totplnk");
+  T.absice3 = dev_ptr<float>(ctx, "lw.absice3");
+  T.absliq1 = dev_ptr<float>(ctx, "lw.absliq1");
+  int n = 0;
+  T.lw_pade_tau = dev_ptr<float>(ctx, "lw.pade_tau_tbl", &n);
+  T.lw_ntbl = n - 1;
+  T.lw_pade_exp = dev_ptr<float>(ctx, "lw.pade_exp_tbl");
+  T.lw_pade_tfn = dev_ptr<float>(ctx, "lw.pade_tfn_tbl");
+  const float *bp = host_ptr<float>(ctx, "lw.pade_bpade");
+  T.lw_bpade = bp ? bp[0] : 0.0f;
+  T.sw_preflog = dev_ptr<float>(ctx, "sw.preflog");
+  T.sw_tref = dev_ptr<float>(ctx, "sw.tref");
+  T.extliq1 = dev_ptr<float>(ctx, "sw.extliq1");
+  T.ssaliq1 = dev_ptr<float>(ctx, "sw.ssaliq1");
+  T.asyliq1 = dev_ptr<float>(ctx, "sw.asyliq1");
+  T.extice3 = dev_ptr<float>(ctx, "sw.extice3");
+  T.ssaice3 = dev_ptr<float>(ctx, "sw.ssaice3");
+  T.asyice3 = dev_ptr<float>(ctx, "sw.asyice3");
+  T.fdlice3 = dev_ptr<float>(ctx, "sw.fdlice3");
+  T.sw_pade_exp = dev_ptr<float>(ctx, "sw.pade_exp_tbl", &n);
+  T.sw_ntbl = n - 1;
+  const float *sbp = host_ptr<float>(ctx, "sw.pade_bpade");
+  T.sw_bpade = sbp ? sbp[0] : 0.0f;
+  T.retab = dev_ptr<float>(ctx, "retab");
+  T.pprof = dev_ptr<float>(ctx, "lw_buffer_pprof", &n);
+  T.nprof = n;
+  T.tprof = dev_ptr<float>(ctx, "lw_buffer_tprof");
+  o3_work_profile(ctx, T.o3wrk, T.ppwrkh);
+  T.logf_tab = dev_ptr<double>(ctx, "glibc.logf_invc_logc");
+  const double *lp = host_ptr<double>(ctx, "glibc.logf_ln2_poly");
+  T.expf_tab = dev_ptr<unsigned long long>(ctx, "glibc.expf_tab");
+  const double *ep = host_ptr<double>(ctx, "glibc.expf_invln2n_poly");
+  if (!T.lw_preflog || !T.chi_mls || !T.totplnk || !T.absice3 || !T.absliq1 || !T.lw_pade_tau ||
+      !T.sw_preflog || !T.extliq1 || !T.extice3 || !T.sw_pade_exp || !T.retab || !T.pprof || !T.tprof ||
+      !T.logf_tab || !lp || !T.expf_tab || !ep || !host_ptr<float>(ctx, "o3sum")) {
+    err = "table blob is missing required tables";
+    return false;
+  }
+  T.logf_ln2 = lp[0];
+  T.logf_a0 = lp[1];
+  T.logf_a1 = lp[2];
+  T.logf_a2 = lp[3];
+  T.expf_invln2n = ep[0];
+  T.expf_c0 = ep[1];
+  T.expf_c1 = ep[2];
+  T.expf_c2 = ep[3];
+  return true;
+}
+
+// Jump of `k` KISS steps (module_ra_rrtmg_common.py:1008-1064).
+KissJump make_jump(uint64_t k) {
+  KissJump J{};
+  uint32_t mul = 1, add = 0;
+  uint32_t basis[32];
+  for (int b = 0; b < 32; ++b) basis[b] = 1u << b;
+  for (uint64_t s = 0; s < k; ++s) {
+    mul = 69069u * mul;
+    add = 69069u * add + 1327217885u;
+    for (int b = 0; b < 32; ++b) {
+      uint32_t x = basis[b];
+      x ^= x << 13;
+      x ^= x >> 17;
+      x ^= x << 5;
+      basis[b] = x;
+    }
+  }
+  J.lcg_mul = mul;
+  J.lcg_add = add;
+  for (int b = 0; b < 32; ++b) J.xs[b] = basis[b];
+  auto powmod = [](uint64_t a, uint64_t e, uint64_t m) {
+    uint64_t r = 1 % m, base = a % m;
+    while (e) {
+      if (e & 1) r = (r * base) % m;
+      base = (base * base) % m;
+      e >>= 1;
+    }
+    return r;
+  };
+  const uint64_t e = k >= 2 ? k - 2 : 0;
+  J.mwc3_pow = static_cast<uint32_t>(powmod(18000, e, 18000ull * 65536 - 1));
+  J.mwc4_pow = static_cast<uint32_t>(powmod(30903, e, 30903ull * 65536 - 1));
+  J.steps = static_cast<uint32_t>(k);
+  return J;
+}
+
+rrtmg_status get_jumps(rrtmg_ctx *ctx, int nlay, int nsub, int skip, const KissJump **out) {
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  auto key = std::make_tuple(nlay, nsub, skip);
+  auto it = ctx->jumps.find(key);
+  if (it != ctx->jumps.end()) {
+    *out = it->second;
+    return RRTMG_OK;
+  }
+  // offsets skip + g * nlay, built incrementally
+  std::vector<KissJump> host(nsub);
+  for (int g = 0; g < nsub; ++g) host[g] = make_jump(static_cast<uint64_t>(skip) + static_cast<uint64_t>(g) * nlay);
+  KissJump *dev = nullptr;
+  cudaError_t e = cudaMalloc(&dev, sizeof(KissJump) * nsub);
+  if (e != cudaSuccess) {
+    ctx->last_error = std::string("cudaMalloc(jump table): ") + cudaGetErrorString(e);
+    return RRTMG_CUDA;
+  }
+  e = cudaMemcpy(dev, host.data(), sizeof(KissJump) * nsub, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    ctx->last_error = std::string("cudaMemcpy(jump table): ") + cudaGetErrorString(e);
+    return RRTMG_CUDA;
+  }
+  ctx->jumps[key] = dev;
+  *out = dev;
+  return RRTMG_OK;
+}
+
+rrtmg_status finish_create(rrtmg_ctx *ctx, int device, rrtmg_ctx **out) {
+  std::string err;
+  if (!parse_blob(ctx, err)) {
+    delete ctx;
+    return fail(nullptr, RRTMG_BAD_ARG, err);
+  }
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return cuda_fail(nullptr, e, "cudaSetDevice");
+  }
+  ctx->device = device;
+  e = cudaMalloc(&ctx->dev_blob, ctx->host_blob.size());
+  if (e != cudaSuccess) {
+    delete ctx;
+    return cuda_fail(nullptr, e, "cudaMalloc(tables)");
+  }
+  e = cudaMemcpy(ctx->dev_blob, ctx->host_blob.data(), ctx->host_blob.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(ctx->dev_blob);
+    delete ctx;
+    return cuda_fail(nullptr, e, "cudaMemcpy(tables)");
+  }
+  if (!fill_tables(ctx, err)) {
+    cudaFree(ctx->dev_blob);
+    delete ctx;
+    return fail(nullptr, RRTMG_BAD_ARG, err);
+  }
+  *out = ctx;
+  return RRTMG_OK;
+}
+
+void cloud_flags(const rrtmg_config *c, int *inflg, int *iceflg, int *liqflg) {
+  *inflg = 2;
+  *iceflg = 3;
+  *liqflg = 1;
+  if (c->icloud != 0) {
+    if (c->has_reqc) *inflg = 3;
+    if (c->has_reqi) { *inflg = 4; *iceflg = 4; }
+    if (c->has_reqs) { *inflg = 5; *iceflg = 5; }
+    if (!c->has_reqs && c->has_reqi && c->has_reqc) { *inflg = 5; *iceflg = 5; }
+  }
+}
+
+rrtmg_status check_config(rrtmg_ctx *ctx, const rrtmg_config *cfg) {
+  if (!ctx || !cfg) return fail(ctx, RRTMG_BAD_ARG, "null context or config");
+  if (cfg->nx <= 0 || cfg->ny <= 0) return fail(ctx, RRTMG_BAD_ARG, "nx and ny must be positive");
+  if (cfg->nk < 4) return fail(ctx, RRTMG_BAD_ARG, "nk must be at least 4 (McICA seeds read four layers)");
+  if (static_cast<long long>(cfg->nx) * cfg->ny > (1ll << 30))
+    return fail(ctx, RRTMG_BAD_ARG, "too many columns in one call");
+  return RRTMG_OK;
+}
+
+ColumnInputs common_inputs(const float *p3d, const float *p8w, const float *pi3d, const float *t3d, const float *t8w,
+                           const float *tsk, const float *qv, const float *qc, const float *qi, const float *qs,
+                           const float *cldfra, const float *o3, const float *xland, const float *xice,
+                           const float *snow, const float *rec, const float *rei, const float *res) {
+  ColumnInputs in{};
+  in.p3d = p3d; in.p8w = p8w; in.pi3d = pi3d; in.t3d = t3d; in.t8w = t8w; in.tsk = tsk;
+  in.qv = qv; in.qc = qc; in.qi = qi; in.qs = qs; in.cldfra = cldfra; in.o3 = o3;
+  in.xland = xland; in.xice = xice; in.snow = snow;
+  in.re_cloud = rec; in.re_ice = rei; in.re_snow = res;
+  return in;
+}
+
+bool any_null(std::initializer_list<const void *> ptrs) {
+  for (const void *p : ptrs)
+    if (!p) return true;
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rrtmg_lw_nlayers(double p_top, int nk) {
+  const double layers_above = p_top * 0.01 / 4.0;
+  return (nk + 1) + static_cast<int>(layers_above + 0.5) - 1;
+}
+
+rrtmg_status rrtmg_create_from_memory(const void *blob, size_t nbytes, int device, rrtmg_ctx **out) {
+  if (!blob || !out || nbytes < 16) return fail(nullptr, RRTMG_BAD_ARG, "null blob or output pointer");
+  auto *ctx = new rrtmg_ctx();
+  ctx->host_blob.assign(static_cast<const unsigned char *>(blob), static_cast<const unsigned char *>(blob) + nbytes);
+  return finish_create(ctx, device, out);
+}
+
+rrtmg_status rrtmg_create(const char *path, int device, rrtmg_ctx **out) {
+  if (!path || !out) return fail(nullptr, RRTMG_BAD_ARG, "null path or output pointer");
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(nullptr, RRTMG_BAD_ARG, std::string("cannot open table blob ") + path);
+  auto *ctx = new rrtmg_ctx();
+  ctx->host_blob.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+  return finish_create(ctx, device, out);
+}
+
+void rrtmg_destroy(rrtmg_ctx *ctx) {
+  if (!ctx) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  for (auto &kv : ctx->jumps) cudaFree(kv.second);
+  cudaFree(ctx->dev_blob);
+  cudaSetDevice(prev);
+  delete ctx;
+}
+
+const char *rrtmg_last_error(const rrtmg_ctx *ctx) {
+  if (!ctx) return g_create_error.c_str();
+  return ctx->last_error.c_str();
+}
+
+const char *rrtmg_status_string(rrtmg_status s) {
+  switch (s) {
+    case RRTMG_OK: return "ok";
+    case RRTMG_BAD_ARG: return "bad argument";
+    case RRTMG_UNSUPPORTED_OPTION: return "unsupported option";
+    case RRTMG_CUDA: return "CUDA error";
+    case RRTMG_TIMEOUT: return "timeout";
+  }
+  return "unknown status";
+}
+
+rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
+                         void *stream_ptr) {
+  rrtmg_status st = check_config(ctx, cfg);
+  if (st != RRTMG_OK) return st;
+  if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
+  if (any_null({in->p3d, in->p8w, in->pi3d, in->t3d, in->t8w, in->tsk, in->qv3d, in->qc3d, in->qi3d, in->qs3d,
+                in->cldfra3d, in->o33d, in->emiss, in->xland, in->xice, in->snow, in->re_cloud, in->re_ice,
+                in->re_snow}))
+    return fail(ctx, RRTMG_BAD_ARG, "a required LW input pointer is null");
+  if (any_null({out->rthratenlw, out->rthratenlwc, out->lwupt, out->lwuptc, out->lwuptcln, out->lwdnt, out->lwdntc,
+                out->lwdntcln, out->lwupb, out->lwupbc, out->lwupbcln, out->lwdnb, out->lwdnbc, out->lwdnbcln,
+                out->glw, out->olr, out->lwcf}))
+    return fail(ctx, RRTMG_BAD_ARG, "a required LW output pointer is null");
+  const int nlay = rrtmg_lw_nlayers(cfg->p_top, cfg->nk);
+  if (nlay > kMaxLay || nlay - cfg->nk > kMaxBuf || nlay < cfg->nk)
+    return fail(ctx, RRTMG_BAD_ARG, "too many layers (nk and p_top exceed the kernel's layer capacity)");
+  int inflg, iceflg, liqflg;
+  cloud_flags(cfg, &inflg, &iceflg, &liqflg);
+  const int icld = cfg->cldovrlp;
+  if (icld >= 1 && (inflg < 2 || iceflg < 3 || liqflg != 1))
+    return fail(ctx, RRTMG_UNSUPPORTED_OPTION, "cloud optics option not supported by cldprmc_lw");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const int ncol = cfg->nx * cfg->ny;
+  const KissJump *jumps = nullptr;
+  st = get_jumps(ctx, nlay, kLwGpts, 150, &jumps);
+  if (st != RRTMG_OK) return st;
+  uint32_t *mask = nullptr;
+  const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
+  e = cudaMallocAsync(reinterpret_cast<void **>(&mask), mask_bytes, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocAsync(mcica mask)");
+
+  McicaArgs m{};
+  m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kLwGpts; m.words = kLwMaskWords;
+  m.enabled = icld >= 1;
+  m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
+  e = launch_mcica(m, stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(mask, stream);
+    return cuda_fail(ctx, e, "mcica kernel launch");
+  }
+  LwArgs a{};
+  a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
+  a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.cfc11 = cfg->cfc11vmr; a.cfc12 = cfg->cfc12vmr;
+  a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
+  a.icld = icld; a.inflg = inflg; a.iceflg = iceflg; a.liqflg = liqflg;
+  a.in = common_inputs(in->p3d, in->p8w, in->pi3d, in->t3d, in->t8w, in->tsk, in->qv3d, in->qc3d, in->qi3d,
+                       in->qs3d, in->cldfra3d, in->o33d, in->xland, in->xice, in->snow, in->re_cloud, in->re_ice,
+                       in->re_snow);
+  a.in.emiss = in->emiss;
+  a.mask = mask;
+  a.rthraten = out->rthratenlw; a.rthratenc = out->rthratenlwc;
+  a.upt = out->lwupt; a.uptc = out->lwuptc; a.dnt = out->lwdnt; a.dntc = out->lwdntc;
+  a.upb = out->lwupb; a.upbc = out->lwupbc; a.dnb = out->lwdnb; a.dnbc = out->lwdnbc;
+  a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
+  a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
+  e = launch_lw(ctx->tables, a, stream);
+  cudaError_t ef = cudaFreeAsync(mask, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(mcica mask)");
+  return RRTMG_OK;
+}
+
+rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
+                         void *stream_ptr) {
+  rrtmg_status st = check_config(ctx, cfg);
+  if (st != RRTMG_OK) return st;
+  if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
+  if (any_null({in->p3d, in->p8w, in->pi3d, in->t3d, in->t8w, in->tsk, in->qv3d, in->qc3d, in->qi3d, in->qs3d,
+                in->cldfra3d, in->o33d, in->albedo, in->coszr, in->xland, in->xice, in->snow, in->re_cloud,
+                in->re_ice, in->re_snow}))
+    return fail(ctx, RRTMG_BAD_ARG, "a required SW input pointer is null");
+  if (any_null({out->rthratensw, out->rthratenswc, out->swupt, out->swuptc, out->swuptcln, out->swdnt, out->swdntc,
+                out->swdntcln, out->swupb, out->swupbc, out->swupbcln, out->swdnb, out->swdnbc, out->swdnbcln,
+                out->swcf, out->gsw, out->swddir, out->swddni, out->swddif, out->swdownc, out->swddnic, out->swddirc,
+                out->coszr}))
+    return fail(ctx, RRTMG_BAD_ARG, "a required SW output pointer is null");
+  const int nlay = cfg->nk + 1;
+  if (nlay > kMaxLay) return fail(ctx, RRTMG_BAD_ARG, "too many layers for the kernel's layer capacity");
+  int inflg, iceflg, liqflg;
+  cloud_flags(cfg, &inflg, &iceflg, &liqflg);
+  const int icld = cfg->icloud == 0 ? 0 : cfg->cldovrlp;
+  if (icld >= 1 && (inflg < 2 || iceflg < 3 || liqflg != 1))
+    return fail(ctx, RRTMG_UNSUPPORTED_OPTION, "cloud optics option not supported by cldprmc_sw");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const int ncol = cfg->nx * cfg->ny;
+  const KissJump *jumps = nullptr;
+  st = get_jumps(ctx, nlay, kSwGpts, 1, &jumps);
+  if (st != RRTMG_OK) return st;
+  uint32_t *mask = nullptr;
+  const size_t mask_bytes = static_cast<size_t>(nlay) * kSwMaskWords * ncol * sizeof(uint32_t);
+  e = cudaMallocAsync(reinterpret_cast<void **>(&mask), mask_bytes, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocAsync(mcica mask)");
+  McicaArgs m{};
+  m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kSwGpts; m.words = kSwMaskWords;
+  m.enabled = icld >= 1;
+  m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
+  e = launch_mcica(m, stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(mask, stream);
+    return cuda_fail(ctx, e, "mcica kernel launch");
+  }
+  SwArgs a{};
+  a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
+  a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.solcon = cfg->solcon;
+  a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
+  a.icld = icld; a.inflg = inflg; a.iceflg = iceflg; a.liqflg = liqflg;
+  a.in = common_inputs(in->p3d, in->p8w, in->pi3d, in->t3d, in->t8w, in->tsk, in->qv3d, in->qc3d, in->qi3d,
+                       in->qs3d, in->cldfra3d, in->o33d, in->xland, in->xice, in->snow, in->re_cloud, in->re_ice,
+                       in->re_snow);
+  a.in.albedo = in->albedo;
+  a.in.coszr = in->coszr;
+  a.mask = mask;
+  a.rthraten = out->rthratensw; a.rthratenc = out->rthratenswc;
+  a.upt = out->swupt; a.uptc = out->swuptc; a.dnt = out->swdnt; a.dntc = out->swdntc;
+  a.upb = out->swupb; a.upbc = out->swupbc; a.dnb = out->swdnb; a.dnbc = out->swdnbc;
+  a.swcf = out->swcf; a.gsw = out->gsw; a.swddir = out->swddir; a.swddni = out->swddni; a.swddif = out->swddif;
+  a.swdownc = out->swdownc; a.swddnic = out->swddnic; a.swddirc = out->swddirc; a.coszr_out = out->coszr;
+  a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
+  e = launch_sw(ctx->tables, a, stream);
+  cudaError_t ef = cudaFreeAsync(mask, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sw kernel launch");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(mcica mask)");
+  return RRTMG_OK;
+}
+
+}  // extern "C"

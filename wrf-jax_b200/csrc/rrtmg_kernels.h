@@ -1,0 +1,54 @@
+// Kernel argument blocks and launchers (internal to librrtmg_b200.so).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "rrtmg_device.cuh"
+
+namespace rrtmg {
+
+struct McicaArgs {
+  int ncol, ny, nk, nlay, nsub, words, enabled;
+  const float *p3d, *cldfra;
+  const KissJump *jumps;  // one per subcolumn
+  uint32_t *mask;         // (nlay, words, ncol)
+};
+
+// Per-column inputs shared by LW and SW (WRF layout, device pointers).
+struct ColumnInputs {
+  const float *p3d, *p8w, *pi3d, *t3d, *t8w, *tsk;
+  const float *qv, *qc, *qi, *qs, *cldfra, *o3;
+  const float *emiss, *albedo, *coszr, *xland, *xice, *snow;
+  const float *re_cloud, *re_ice, *re_snow;
+};
+
+struct LwArgs {
+  int nx, ny, nk, nlay, ncol;
+  float co2, n2o, ch4, cfc11, cfc12;
+  int has_reqc, has_reqi, has_reqs, icloud, icld;
+  int inflg, iceflg, liqflg;
+  ColumnInputs in;
+  const uint32_t *mask;
+  float *rthraten, *rthratenc;
+  float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc, *glw, *olr, *lwcf;
+  float *zero2[4];  // *cln fields, written as zeros
+};
+
+struct SwArgs {
+  int nx, ny, nk, nlay, ncol;
+  float co2, n2o, ch4, solcon;
+  int has_reqc, has_reqi, has_reqs, icloud, icld;
+  int inflg, iceflg, liqflg;
+  ColumnInputs in;
+  const uint32_t *mask;
+  float *rthraten, *rthratenc;
+  float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc;
+  float *swcf, *gsw, *swddir, *swddni, *swddif, *swdownc, *swddnic, *swddirc, *coszr_out;
+  float *zero2[4];
+};
+
+cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
+cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream);
+cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream);
+
+}  // namespace rrtmg

@@ -1,0 +1,912 @@
+// RRTMG shortwave on the GPU: one thread per column, fused from the WRF adapter
+// to the theta tendencies and the 2-D surface/TOA fields.
+//
+// Reference call: rrtmg_swrad_wrf_columns (src/wrf_jax/physics/module_ra_rrtmg_sw.py:2386)
+// and below it: inatm_sw (sw:1250), cldprmc_sw (sw:1409), setcoef_sw (sw:7101),
+// taumol16..29 (sw:4043-6675), spcvmc (sw:6788-7094) with reftra (sw:3490-3601)
+// and vrtqdr (sw:3604-3720), heating (sw:2285-2301), day mask (sw:2667-2719).
+// The adapter passes rounding_token=None, so every statement is one binary32
+// operation in the order written.
+//
+// Schedule.  Night columns (coszr <= 0) write zeros and exit: the reference
+// masks every output of such columns.  For a day column the thread walks the
+// 14 bands; per band it evaluates the band's gas optics for all layers once
+// (thread-local tables of taug/taur and the band's cloud optics), then for each
+// g-point runs a top-down pass (delta-Eddington layer reflectance and
+// transmittance, direct beam, downward adding recurrence) and a bottom-up pass
+// (upward adding recurrence, level fluxes) that accumulates the spectral sums
+// in g-point order.
+#include "rrtmg_device.cuh"
+#include "rrtmg_kernels.h"
+
+namespace rrtmg {
+namespace {
+
+constexpr int kNgc[kSwBands] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};
+constexpr int kGofs[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
+constexpr int kMaxNgc = 12;
+constexpr int kMaxLev = kMaxLay + 1;
+constexpr float kOneMinus = 1.0f - 1.0e-6f;
+
+struct Col {
+  int i, j, nk, nlay, ny;
+  float o3top, adjflux, mu, coszen, albedo;
+  int laytrop;
+  int inflg, iceflg, has_reqc, has_reqi, has_reqs, icloud;
+  float co2, n2o, ch4;
+};
+
+struct SLayer {
+  float pavel, tavel, pdp;
+  int jp, jt, jt1, indself, indfor, trop;
+  float fac00, fac01, fac10, fac11;
+  float colh2o, colco2, colo3, colch4, colo2, colmol;
+  float selffac, selffrac, forfac, forfrac;
+  float cldfrac, clwp, ciwp, cswp, rel, rei, res;
+};
+
+__device__ __forceinline__ float in3(const float *p, const Col &C, int k) {
+  return ld(p + (static_cast<size_t>(C.i) * C.nk + k) * C.ny + C.j);
+}
+__device__ __forceinline__ float in3w(const float *p, const Col &C, int k) {
+  return ld(p + (static_cast<size_t>(C.i) * (C.nk + 1) + k) * C.ny + C.j);
+}
+
+__device__ float o3data_layer(const Tables &T, float pa, float pb) {
+  float total = 0.0f;
+#pragma unroll 4
+  for (int b = 0; b < 31; ++b) {
+    const float pb1 = fmaxf(pa - T.ppwrkh[b], 0.0f);
+    const float pb2 = fmaxf(pa - T.ppwrkh[b + 1], 0.0f);
+    const float pt1 = fmaxf(pb - T.ppwrkh[b], 0.0f);
+    const float pt2 = fmaxf(pb - T.ppwrkh[b + 1], 0.0f);
+    const float overlap = ((pb2 - pb1) - pt2) + pt1;
+    total = total + overlap * T.o3wrk[b];
+  }
+  return total / (pa - pb);
+}
+
+__device__ float retab_interp(const Tables &T, float temp, int hi) {
+  const int tint = static_cast<int>(temp);
+  const int index = clampi(static_cast<int>(temp - 179.0f), 1, hi);
+  const float corr = temp - static_cast<float>(tint);
+  return ld(T.retab + index - 1) * (1.0f - corr) + ld(T.retab + index) * corr;
+}
+
+// Layer quantities: adapter extension, inatm_sw, cloud paths, setcoef_sw.
+__device__ SLayer make_layer(const Tables &T, const SwArgs &a, const Col &C, int l) {
+  SLayer L;
+  const int nk = C.nk;
+  const float plev0 = pa_to_hpa(in3w(a.in.p8w, C, l));
+  const float plev1 = l + 1 <= nk ? pa_to_hpa(in3w(a.in.p8w, C, l + 1)) : 1.0e-5f;
+  L.pavel = l < nk ? pa_to_hpa(in3(a.in.p3d, C, l)) : 0.5f * pa_to_hpa(in3w(a.in.p8w, C, nk));
+  L.tavel = l < nk ? in3(a.in.t3d, C, l) : in3w(a.in.t8w, C, nk);
+  const int kq = l < nk ? l : nk - 1;
+  const float h2o = fmaxf(in3(a.in.qv, C, kq), 1.0e-12f) * 1.607793f;
+  const float o3 = l < nk ? in3(a.in.o3, C, l) : C.o3top;
+  // inatm_sw (sw:1286-1320)
+  const float amd = 28.9660f, amw = 18.0160f, avogad = 6.02214199e23f, grav = 9.8066f;
+  L.pdp = plev0 - plev1;
+  const float amm = (1.0f - h2o) * amd + h2o * amw;
+  const float num = (L.pdp * 1.0e3f) * avogad;
+  const float den = ((1.0e2f * grav) * amm) * (1.0f + h2o);
+  const float coldry = num / den;
+  const float wk0 = h2o * coldry, wk1 = C.co2 * coldry, wk2 = o3 * coldry, wk3 = C.n2o * coldry;
+  const float wk5 = C.ch4 * coldry, wk6 = 0.209488f * coldry;
+  // setcoef_sw (sw:7101-7306)
+  const float stpfac = 296.0f / 1013.0f;
+  const float plog = glibc_logf(T, L.pavel);
+  const int jp = clampi(static_cast<int>(36.0f - 5.0f * (plog + 0.04f)), 1, 58);
+  const float fp = 5.0f * (ld(T.sw_preflog + jp - 1) - plog);
+  const float tf = (L.tavel - ld(T.sw_tref + jp - 1)) / 15.0f;
+  const int jt = clampi(static_cast<int>(3.0f + tf), 1, 4);
+  const float ft = tf - static_cast<float>(jt - 3);
+  const float tf1 = (L.tavel - ld(T.sw_tref + jp)) / 15.0f;
+  const int jt1 = clampi(static_cast<int>(3.0f + tf1), 1, 4);
+  const float ft1 = tf1 - static_cast<float>(jt1 - 3);
+  const float water = wk0 / coldry;
+  const float scalefac = (L.pavel * stpfac) / L.tavel;
+  const int trop = plog > 4.56f;
+  L.trop = l < C.laytrop;
+  const float forfac = scalefac / (1.0f + water);
+  const float ftf = (332.0f - L.tavel) / 36.0f;
+  const int indfor_t = clampi(static_cast<int>(ftf), 1, 2);
+  const float forfrac_t = ftf - static_cast<float>(indfor_t);
+  const float fsf = (L.tavel - 188.0f) / 36.0f;
+  L.indfor = trop ? indfor_t : 3;
+  L.forfrac = trop ? forfrac_t : fsf - 1.0f;
+  const float selffac_t = water * forfac;
+  const float fself = (L.tavel - 188.0f) / 7.2f;
+  const int indself_t = clampi(static_cast<int>(fself) - 7, 1, 9);
+  const float selffrac_t = fself - static_cast<float>(indself_t + 7);
+  L.indself = trop ? indself_t : 0;
+  L.selffac = trop ? selffac_t : 0.0f;
+  L.selffrac = trop ? selffrac_t : 0.0f;
+  L.forfac = forfac;
+  const float cs = 1.0e-20f;
+  L.colh2o = cs * wk0;
+  L.colco2 = cs * wk1;
+  L.colo3 = cs * wk2;
+  const float coln2o0 = cs * wk3;
+  L.colch4 = cs * wk5;
+  L.colo2 = cs * wk6;
+  L.colmol = cs * coldry + L.colh2o;
+  const float fallback = 1.0e-32f * coldry;
+  if (L.colco2 == 0.0f) L.colco2 = fallback;
+  (void)coln2o0;
+  if (L.colch4 == 0.0f) L.colch4 = fallback;
+  if (L.colo2 == 0.0f) L.colo2 = fallback;
+  const float compfp = 1.0f - fp;
+  L.fac10 = compfp * ft;
+  L.fac00 = compfp * (1.0f - ft);
+  L.fac11 = fp * ft1;
+  L.fac01 = fp * (1.0f - ft1);
+  L.jp = jp;
+  L.jt = jt;
+  L.jt1 = jt1;
+  // cloud radii and paths (common:801-961); zero in the extra top layer
+  L.cldfrac = 0.0f; L.clwp = 0.0f; L.ciwp = 0.0f; L.cswp = 0.0f;
+  L.rel = 10.0f; L.rei = 10.0f; L.res = 10.0f;
+  if (l < nk) {
+    const float t = L.tavel;
+    const float cldfra = in3(a.in.cldfra, C, l);
+    float qc = fmaxf(in3(a.in.qc, C, l), 0.0f), qi = fmaxf(in3(a.in.qi, C, l), 0.0f);
+    float qs = fmaxf(in3(a.in.qs, C, l), 0.0f);
+    const int c2 = C.i * C.ny + C.j;
+    const float xland = ld(a.in.xland + c2);
+    float recloud = 5.0f, reice = 10.0f, resnow = 10.0f;
+    if (C.icloud != 0) {
+      if (C.has_reqc) {
+        recloud = fmaxf(2.5f, in3(a.in.re_cloud, C, l) * 1.0e6f);
+        const int cloudy_min = (recloud <= 2.5f) && (cldfra > 0.0f);
+        if (cloudy_min && (xland - 1.5f > 0.0f)) recloud = 10.5f;
+        if (cloudy_min && (xland - 1.5f < 0.0f)) recloud = 7.5f;
+      }
+      if (C.has_reqi) {
+        reice = fmaxf(5.0f, in3(a.in.re_ice, C, l) * 1.0e6f);
+        if ((reice <= 5.0f) && (cldfra > 0.0f)) reice = fmaxf(retab_interp(T, t, 75), 5.0f);
+      }
+      if (C.has_reqs) resnow = fmaxf(10.0f, in3(a.in.re_snow, C, l) * 1.0e6f);
+      if (!C.has_reqs && C.has_reqi && C.has_reqc) {
+        resnow = fmaxf(10.0f, in3(a.in.re_ice, C, l) * 1.0e6f);
+        qs = qi;
+        qi = 0.0f;
+        reice = 10.0f;
+      }
+    }
+    const float dp = L.pdp;
+    const float denom = fmaxf(0.01f, cldfra);
+    float gicewp = (qi + qs) * dp * 100.0f / grav * 1000.0f;
+    const float gliqwp = qc * dp * 100.0f / grav * 1000.0f;
+    float cicewp = gicewp / denom;
+    const float cliqwp = gliqwp / denom;
+    if (C.iceflg >= 4) {
+      gicewp = qi * dp * 100.0f / grav * 1000.0f;
+      cicewp = gicewp / denom;
+    }
+    float csnowp = 0.0f, res_adj = resnow;
+    if (C.iceflg == 5) {
+      float smf = 0.99f;
+      if (res_adj > 130.0f) {
+        const float lim = (130.0f / res_adj) * (130.0f / res_adj);
+        smf = fminf(0.99f, lim);
+        res_adj = 130.0f;
+      }
+      const float gsnowp = qs * smf * dp * 100.0f / grav * 1000.0f;
+      csnowp = gsnowp / denom;
+    }
+    const float xice = ld(a.in.xice + c2), snow = ld(a.in.snow + c2);
+    const float landm = 2.0f - xland, snowh = 0.001f * snow;
+    const float rocean = 14.0f, rland = 8.0f, rice = 14.0f;
+    float rel = rland + (rocean - rland) * fminf(1.0f, fmaxf(0.0f, (273.16f - t) * 0.05f));
+    rel = rel + (rocean - rel) * fminf(1.0f, fmaxf(0.0f, snowh * 10.0f));
+    rel = rel + (rocean - rel) * fminf(1.0f, fmaxf(0.0f, 1.0f - landm));
+    rel = rel + (rice - rel) * fminf(1.0f, fmaxf(0.0f, xice));
+    float rei = retab_interp(T, t, 94);
+    if (C.inflg >= 3) rel = recloud;
+    if (C.iceflg >= 4) rei = reice;
+    if (C.iceflg == 3) rei = fminf(140.0f, rei * 1.0315f);
+    L.cldfrac = cldfra;
+    L.clwp = cliqwp;
+    L.ciwp = cicewp;
+    L.cswp = (C.inflg == 5) ? csnowp : 0.0f;
+    L.rel = rel;
+    L.rei = rei;
+    L.res = (C.inflg == 5) ? res_adj : 10.0f;
+  }
+  return L;
+}
+
+// ---------------------------------------------------------------------------
+// taumol16..29 helpers
+// ---------------------------------------------------------------------------
+struct SwSpec {
+  float sc, fs, f[8];
+  int js0;
+};
+
+__device__ __forceinline__ SwSpec sw_species(float primary, float ratio_secondary, const SLayer &L, float scale, int cap) {
+  SwSpec s;
+  s.sc = primary + ratio_secondary;
+  const float q = primary / s.sc;
+  const float sp = q > kOneMinus ? kOneMinus : q;
+  const float sm = scale * sp;
+  const int js = 1 + static_cast<int>(sm);
+  s.fs = sm - floorf(sm);
+  const float comp = 1.0f - s.fs;
+  s.js0 = clampi(js - 1, 0, cap);
+  s.f[0] = comp * L.fac00;
+  s.f[1] = s.fs * L.fac00;
+  s.f[2] = comp * L.fac10;
+  s.f[3] = s.fs * L.fac10;
+  s.f[4] = comp * L.fac01;
+  s.f[5] = s.fs * L.fac01;
+  s.f[6] = comp * L.fac11;
+  s.f[7] = s.fs * L.fac11;
+  return s;
+}
+
+__device__ __forceinline__ float k8(const float *tab, int ngc, int ns, int js0, int jt0, int jt10, int jp0, int jp1,
+                                    const float *f, int g) {
+  auto R = [&](int js, int jt, int jp) { return ld(tab + (((jp) * 5 + (jt)) * ns + (js)) * ngc + g); };
+  float s = f[0] * R(js0, jt0, jp0);
+  s = s + f[1] * R(js0 + 1, jt0, jp0);
+  s = s + f[2] * R(js0, jt0 + 1, jp0);
+  s = s + f[3] * R(js0 + 1, jt0 + 1, jp0);
+  s = s + f[4] * R(js0, jt10, jp1);
+  s = s + f[5] * R(js0 + 1, jt10, jp1);
+  s = s + f[6] * R(js0, jt10 + 1, jp1);
+  s = s + f[7] * R(js0 + 1, jt10 + 1, jp1);
+  return s;
+}
+
+__device__ __forceinline__ float k4(const float *tab, int ngc, int jt0, int jt10, int jp0, int jp1, const SLayer &L, int g) {
+  float s = L.fac00 * ld(tab + (jp0 * 5 + jt0) * ngc + g);
+  s = s + L.fac10 * ld(tab + (jp0 * 5 + jt0 + 1) * ngc + g);
+  s = s + L.fac01 * ld(tab + (jp1 * 5 + jt10) * ngc + g);
+  s = s + L.fac11 * ld(tab + (jp1 * 5 + jt10 + 1) * ngc + g);
+  return s;
+}
+
+__device__ __forceinline__ float self_interp(const SwBand &B, int ngc, const SLayer &L, int g) {
+  const int i0 = clampi(L.indself - 1, 0, 8);
+  const float s0 = ld(B.selfref + i0 * ngc + g);
+  return s0 + L.selffrac * (ld(B.selfref + (i0 + 1) * ngc + g) - s0);
+}
+
+__device__ __forceinline__ float for_interp(const SwBand &B, int ngc, const SLayer &L, int g, int cap) {
+  const int i0 = clampi(L.indfor - 1, 0, cap);
+  const int i1 = jrow(i0 + 1, B.forref_rows);
+  const float f0 = ld(B.forref + i0 * ngc + g);
+  return f0 + L.forfrac * (ld(B.forref + i1 * ngc + g) - f0);
+}
+
+// Gas optical depth and Rayleigh depth of band B (0 = band 16) at one layer.
+// The species weights returned in sp8/sp4 feed the solar-source rules.
+template <int B>
+__device__ __forceinline__ void sw_taumol(const Tables &T, const SLayer &L, float *taug, float *taur, SwSpec &sp8, SwSpec &sp4) {
+  constexpr int ngc = kNgc[B];
+  constexpr int bn = B + 16;
+  const SwBand &K = T.sw[B];
+  const bool trop = L.trop;
+  const int jp = L.jp;
+  const int jt0 = clampi(L.jt - 1, 0, 3), jt10 = clampi(L.jt1 - 1, 0, 3);
+  const int jp0 = clampi(jp - 1, 0, 11), jp1 = jp0 + 1;
+  const int kjp0 = clampi(jp - 13, 0, 45), kjp1 = clampi(jp - 12, 0, 46);
+  const float colh2o = L.colh2o, colmol = L.colmol;
+  if constexpr (bn == 16) sp8 = sw_species(colh2o, K.strrat1 * L.colch4, L, 8.0f, 7);
+  if constexpr (bn == 17 || bn == 19 || bn == 21) sp8 = sw_species(colh2o, K.strrat * L.colco2, L, 8.0f, 7);
+  if constexpr (bn == 18) sp8 = sw_species(colh2o, K.strrat * L.colch4, L, 8.0f, 7);
+  if constexpr (bn == 22) sp8 = sw_species(colh2o, (1.6f * K.strrat) * L.colo2, L, 8.0f, 7);
+  if constexpr (bn == 24) sp8 = sw_species(colh2o, K.strrat * L.colo2, L, 8.0f, 7);
+  if constexpr (bn == 28) sp8 = sw_species(L.colo3, K.strrat * L.colo2, L, 8.0f, 7);
+  if constexpr (bn == 17 || bn == 21) sp4 = sw_species(colh2o, K.strrat * L.colco2, L, 4.0f, 3);
+  if constexpr (bn == 28) sp4 = sw_species(L.colo3, K.strrat * L.colo2, L, 4.0f, 3);
+#pragma unroll
+  for (int g = 0; g < ngc; ++g) {
+    float tg = 0.0f, tr = 0.0f;
+    if constexpr (bn == 16) {
+      if (trop) {
+        const float ta = k8(K.ka, ngc, 9, sp8.js0, jt0, jt10, jp0, jp1, sp8.f, g);
+        const float cont = colh2o * (L.selffac * self_interp(K, ngc, L, g) + L.forfac * for_interp(K, ngc, L, g, 1));
+        tg = sp8.sc * ta + cont;
+      } else {
+        tg = L.colch4 * k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+      }
+      tr = colmol * K.rayl;
+    } else if constexpr (bn == 17 || bn == 21) {
+      if (trop) {
+        const float ta = k8(K.ka, ngc, 9, sp8.js0, jt0, jt10, jp0, jp1, sp8.f, g);
+        const float cont = colh2o * (L.selffac * self_interp(K, ngc, L, g) + L.forfac * for_interp(K, ngc, L, g, 2));
+        tg = sp8.sc * ta + cont;
+      } else {
+        const float sa = k8(K.kb, ngc, 5, sp4.js0, jt0, jt10, kjp0, kjp1, sp4.f, g);
+        const float cont = (colh2o * L.forfac) * for_interp(K, ngc, L, g, 2);
+        tg = sp8.sc * sa + cont;
+      }
+      tr = colmol * K.rayl;
+    } else if constexpr (bn == 18 || bn == 19) {
+      if (trop) {
+        const float ta = k8(K.ka, ngc, 9, sp8.js0, jt0, jt10, jp0, jp1, sp8.f, g);
+        const float cont = colh2o * (L.selffac * self_interp(K, ngc, L, g) + L.forfac * for_interp(K, ngc, L, g, 2));
+        tg = sp8.sc * ta + cont;
+      } else {
+        const float col = bn == 18 ? L.colch4 : L.colco2;
+        tg = col * k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+      }
+      tr = colmol * K.rayl;
+    } else if constexpr (bn == 20) {
+      if (trop) {
+        const float ta = k4(K.ka, ngc, jt0, jt10, jp0, jp1, L, g);
+        const float inner = (ta + L.selffac * self_interp(K, ngc, L, g)) + L.forfac * for_interp(K, ngc, L, g, 2);
+        tg = colh2o * inner + L.colch4 * ld(K.absch4 + g);
+      } else {
+        const float sa = k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+        const float inner = sa + L.forfac * for_interp(K, ngc, L, g, 2);
+        tg = colh2o * inner + L.colch4 * ld(K.absch4 + g);
+      }
+      tr = colmol * K.rayl;
+    } else if constexpr (bn == 22) {
+      const float o2cont = (4.35e-4f * L.colo2) / (350.0f * 2.0f);
+      if (trop) {
+        const float ta = k8(K.ka, ngc, 9, sp8.js0, jt0, jt10, jp0, jp1, sp8.f, g);
+        const float cont = colh2o * (L.selffac * self_interp(K, ngc, L, g) + L.forfac * for_interp(K, ngc, L, g, 2));
+        tg = (sp8.sc * ta + cont) + o2cont;
+      } else {
+        const float sa = k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+        tg = (L.colo2 * 1.6f) * sa + o2cont;
+      }
+      tr = colmol * K.rayl;
+    } else if constexpr (bn == 23) {
+      if (trop) {
+        const float ta = k4(K.ka, ngc, jt0, jt10, jp0, jp1, L, g);
+        const float sum = (K.givfac * ta + L.selffac * self_interp(K, ngc, L, g)) + L.forfac * for_interp(K, ngc, L, g, 1);
+        tg = colh2o * sum;
+      }
+      tr = colmol * ld(K.rayl_g + g);
+    } else if constexpr (bn == 24) {
+      if (trop) {
+        const float ta = k8(K.ka, ngc, 9, sp8.js0, jt0, jt10, jp0, jp1, sp8.f, g);
+        const float cont = colh2o * (L.selffac * self_interp(K, ngc, L, g) + L.forfac * for_interp(K, ngc, L, g, 1));
+        tg = (sp8.sc * ta + L.colo3 * ld(K.abso3a + g)) + cont;
+        const float r0 = ld(K.rayla + g * 9 + sp8.js0), r1 = ld(K.rayla + g * 9 + sp8.js0 + 1);
+        tr = colmol * (r0 + sp8.fs * (r1 - r0));
+      } else {
+        const float sa = k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+        tg = L.colo2 * sa + L.colo3 * ld(K.abso3b + g);
+        tr = colmol * ld(K.raylb + g);
+      }
+    } else if constexpr (bn == 25) {
+      if (trop) {
+        const float ta = k4(K.ka, ngc, jt0, jt10, jp0, jp1, L, g);
+        tg = colh2o * ta + L.colo3 * ld(K.abso3a + g);
+      } else {
+        tg = L.colo3 * ld(K.abso3b + g);
+      }
+      tr = colmol * ld(K.rayl_g + g);
+    } else if constexpr (bn == 26) {
+      tg = 0.0f;
+      tr = colmol * ld(K.rayl_g + g);
+    } else if constexpr (bn == 27) {
+      const float ab = trop ? k4(K.ka, ngc, jt0, jt10, jp0, jp1, L, g) : k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+      tg = L.colo3 * ab;
+      tr = colmol * ld(K.rayl_g + g);
+    } else if constexpr (bn == 28) {
+      if (trop) tg = sp8.sc * k8(K.ka, ngc, 9, sp8.js0, jt0, jt10, jp0, jp1, sp8.f, g);
+      else tg = sp8.sc * k8(K.kb, ngc, 5, sp4.js0, jt0, jt10, kjp0, kjp1, sp4.f, g);
+      tr = colmol * K.rayl;
+    } else {  // 29
+      if (trop) {
+        const float ta = k4(K.ka, ngc, jt0, jt10, jp0, jp1, L, g);
+        const float wat = (ta + L.selffac * self_interp(K, ngc, L, g)) + L.forfac * for_interp(K, ngc, L, g, 2);
+        tg = colh2o * wat + L.colco2 * ld(K.absco2 + g);
+      } else {
+        const float sa = k4(K.kb, ngc, jt0, jt10, kjp0, kjp1, L, g);
+        tg = L.colco2 * sa + colh2o * ld(K.absh2o + g);
+      }
+      tr = colmol * K.rayl;
+    }
+    taug[g] = tg;
+    taur[g] = tr;
+  }
+}
+
+// cldprmc_sw for one cloudy (band, layer) (sw:1409-1626; ice >= 3, liquid 1)
+struct CloudOpt {
+  float tau, ssa, asm_, taor;
+  bool active;
+};
+
+__device__ CloudOpt sw_cloud(const Tables &T, const SLayer &L, int band, int iceflag) {
+  CloudOpt o;
+  const float cldmin = 1.0e-20f;
+  const float ciwp = L.ciwp, clwp = L.clwp, cswp = iceflag == 5 ? L.cswp : 0.0f;
+  const float cwp = (ciwp + clwp) + cswp;
+  o.active = cwp >= cldmin;
+  const float radice = L.rei, radliq = L.rel, radsno = iceflag == 5 ? L.res : 0.0f;
+  const float factor = (radice - 2.0f) / 3.0f;
+  int index = static_cast<int>(factor);
+  if (index == 46) index = 45;
+  const float fint = factor - static_cast<float>(index);
+  const int r0 = jrow(index - 1, 46), r1 = jrow(index, 46);
+  float extice = interpf(ld(T.extice3 + r0 * 14 + band), ld(T.extice3 + r1 * 14 + band), fint);
+  float ssaice = interpf(ld(T.ssaice3 + r0 * 14 + band), ld(T.ssaice3 + r1 * 14 + band), fint);
+  float gice = interpf(ld(T.asyice3 + r0 * 14 + band), ld(T.asyice3 + r1 * 14 + band), fint);
+  const float fdelta = interpf(ld(T.fdlice3 + r0 * 14 + band), ld(T.fdlice3 + r1 * 14 + band), fint);
+  const float fw = fdelta + 0.5f / ssaice;
+  float forwice = fw > gice ? gice : fw;
+  if ((ciwp + cswp) == 0.0f) { extice = 0.0f; ssaice = 0.0f; gice = 0.0f; forwice = 0.0f; }
+  float extsno = 0.0f, ssasno = 0.0f, gsno = 0.0f, forwsno = 0.0f;
+  if (iceflag == 5 && cswp > 0.0f) {
+    const float fs = (radsno - 2.0f) / 3.0f;
+    int is = static_cast<int>(fs);
+    if (is == 46) is = 45;
+    const float fints = fs - static_cast<float>(is);
+    const int s0 = jrow(is - 1, 46), s1 = jrow(is, 46);
+    extsno = interpf(ld(T.extice3 + s0 * 14 + band), ld(T.extice3 + s1 * 14 + band), fints);
+    ssasno = interpf(ld(T.ssaice3 + s0 * 14 + band), ld(T.ssaice3 + s1 * 14 + band), fints);
+    gsno = interpf(ld(T.asyice3 + s0 * 14 + band), ld(T.asyice3 + s1 * 14 + band), fints);
+    const float fds = interpf(ld(T.fdlice3 + s0 * 14 + band), ld(T.fdlice3 + s1 * 14 + band), fints);
+    const float fw2 = fds + 0.5f / ssasno;
+    forwsno = fw2 > gsno ? gsno : fw2;
+  }
+  int il = static_cast<int>(radliq - 1.5f);
+  if (il == 0) il = 1;
+  if (il == 58) il = 57;
+  const float fint_liq = (radliq - 1.5f) - static_cast<float>(il);
+  const int q0 = jrow(il - 1, 58), q1 = jrow(il, 58);
+  float extliq = interpf(ld(T.extliq1 + q0 * 14 + band), ld(T.extliq1 + q1 * 14 + band), fint_liq);
+  float ssaliq = interpf(ld(T.ssaliq1 + q0 * 14 + band), ld(T.ssaliq1 + q1 * 14 + band), fint_liq);
+  if (fint_liq < 0.0f && ssaliq > 1.0f) ssaliq = ld(T.ssaliq1 + q0 * 14 + band);
+  float gliq = interpf(ld(T.asyliq1 + q0 * 14 + band), ld(T.asyliq1 + q1 * 14 + band), fint_liq);
+  if (clwp == 0.0f) { extliq = 0.0f; ssaliq = 0.0f; gliq = 0.0f; }
+  const float forwliq = gliq * gliq;
+  const float tauliqorig = clwp * extliq;
+  const float tauiceorig = ciwp * extice;
+  const float ssaliq_d = ssaliq * (1.0f - forwliq) / (1.0f - forwliq * ssaliq);
+  const float tauliq = (1.0f - forwliq * ssaliq) * tauliqorig;
+  const float ssaice_d = ssaice * (1.0f - forwice) / (1.0f - forwice * ssaice);
+  const float tauice = (1.0f - forwice * ssaice) * tauiceorig;
+  const float scatliq = ssaliq_d * tauliq;
+  float scatice = ssaice_d * tauice;
+  float tau_new, taor_new, scatsno = 0.0f;
+  if (iceflag == 5) {
+    const float tausnoorig = cswp * extsno;
+    const float ssasno_d = ssasno * (1.0f - forwsno) / (1.0f - forwsno * ssasno);
+    const float tausno = (1.0f - forwsno * ssasno) * tausnoorig;
+    scatsno = ssasno_d * tausno;
+    tau_new = (tauliq + tauice) + tausno;
+    taor_new = (tauliqorig + tauiceorig) + tausnoorig;
+  } else {
+    tau_new = tauliq + tauice;
+    taor_new = tauliqorig + tauiceorig;
+  }
+  if (tau_new == 0.0f) tau_new = cldmin;
+  if (scatice == 0.0f) scatice = cldmin;
+  if (scatsno == 0.0f) scatsno = cldmin;
+  if (iceflag == 5) {
+    const float ssum = (scatliq + scatice) + scatsno;
+    o.ssa = ssum / tau_new;
+    const float num = (scatliq * (gliq - forwliq) / (1.0f - forwliq) + scatice * (gice - forwice) / (1.0f - forwice)) +
+                      scatsno * (gsno - forwsno) / (1.0f - forwsno);
+    o.asm_ = num / ssum;
+  } else {
+    const float ssum = scatliq + scatice;
+    o.ssa = ssum / tau_new;
+    const float num = scatliq * (gliq - forwliq) / (1.0f - forwliq) + scatice * (gice - forwice) / (1.0f - forwice);
+    o.asm_ = num / ssum;
+  }
+  o.tau = tau_new;
+  o.taor = taor_new;
+  if (!o.active) { o.tau = 0.0f; o.ssa = 1.0f; o.asm_ = 0.0f; o.taor = 0.0f; }
+  return o;
+}
+
+__device__ __forceinline__ float exp_lookup(const Tables &T, float v) {
+  if (v <= 0.06f) return (1.0f - v) + (0.5f * v) * v;
+  const float tblind = v / (T.sw_bpade + v);
+  const int it = clampi(static_cast<int>(static_cast<float>(T.sw_ntbl) * tblind + 0.5f), 0, T.sw_ntbl);
+  return ld(T.sw_pade_exp + it);
+}
+
+struct RT4 {
+  float ref, refd, tra, trad;
+};
+
+// Delta-Eddington layer reflectance/transmittance (reftra_sw_columns, sw:3490-3601)
+__device__ __forceinline__ RT4 reftra(const Tables &T, bool lrt, float zg, float mu, float zto1, float zw) {
+  RT4 r;
+  r.ref = 0.0f; r.refd = 0.0f; r.tra = 1.0f; r.trad = 1.0f;
+  if (!lrt) return r;
+  const float eps = 1.0e-8f, zwcrit = 0.9999995f;
+  const float zg3 = 3.0f * zg;
+  const float g1 = (8.0f - zw * (5.0f + zg3)) * 0.25f;
+  const float g2 = 3.0f * (zw * (1.0f - zg)) * 0.25f;
+  const float g3 = (2.0f - zg3 * mu) * 0.25f;
+  const float g4 = 1.0f - g3;
+  const float sr = zg != 1.0f ? zg / (1.0f - zg) : 0.0f;
+  const float denom = zg != 1.0f ? 1.0f - (1.0f - zw) * sr * sr : 1.0f;
+  const float zwo = (zw > 0.0f && denom != 0.0f) ? zw / denom : 0.0f;
+  if (zwo >= zwcrit) {
+    const float za = g1 * mu;
+    const float za1 = za - g3;
+    const float zgt = g1 * zto1;
+    float ze = zto1 / mu;
+    if (ze > 500.0f) ze = 500.0f;
+    const float ex = exp_lookup(T, ze);
+    r.ref = (zgt - za1 * (1.0f - ex)) / (1.0f + zgt);
+    r.tra = 1.0f - r.ref;
+    r.refd = zgt / (1.0f + zgt);
+    r.trad = 1.0f - r.refd;
+    if (ex == 1.0f) { r.ref = 0.0f; r.tra = 1.0f; r.refd = 0.0f; r.trad = 1.0f; }
+    return r;
+  }
+  const float za1 = g1 * g4 + g2 * g3;
+  const float za2 = g1 * g3 + g2 * g4;
+  const float rad = g1 * g1 - g2 * g2;
+  const float zrk = sqrtf(rad > 0.0f ? rad : 0.0f);
+  const float zrp = zrk * mu;
+  const float zrp1 = 1.0f + zrp, zrm1 = 1.0f - zrp, zrk2 = 2.0f * zrk;
+  const float zrpp = 1.0f - zrp * zrp;
+  const float zrkg = zrk + g1;
+  const float zr1 = zrm1 * (za2 + zrk * g3);
+  const float zr2 = zrp1 * (za2 - zrk * g3);
+  const float zr3 = zrk2 * (g3 - za2 * mu);
+  const float zr4 = zrpp * zrkg;
+  const float zr5 = zrpp * (zrk - g1);
+  const float zt1 = zrp1 * (za1 + zrk * g4);
+  const float zt2 = zrm1 * (za1 - zrk * g4);
+  const float zt3 = zrk2 * (g4 + za1 * mu);
+  const float zbeta = (g1 - zrk) / zrkg;
+  float ze1 = zrk * zto1;
+  if (ze1 > 500.0f) ze1 = 500.0f;
+  float ze2 = zto1 / mu;
+  if (ze2 > 500.0f) ze2 = 500.0f;
+  const float zem1 = exp_lookup(T, ze1);
+  const float zep1 = 1.0f / zem1;
+  const float zem2 = exp_lookup(T, ze2);
+  const float zep2 = 1.0f / zem2;
+  const float zdenr = zr4 * zep1 + zr5 * zem1;
+  const float zdent = zr4 * zep1 + zr5 * zem1;
+  if ((zdenr >= -eps) && (zdenr <= eps)) {
+    r.ref = eps;
+    r.tra = zem2;
+  } else {
+    r.ref = zw * (zr1 * zep1 - zr2 * zem1 - zr3 * zem2) / zdenr;
+    r.tra = zem2 - zem2 * zw * (zt1 * zep1 - zt2 * zem1 - zt3 * zep2) / zdent;
+  }
+  const float zemm = zem1 * zem1;
+  const float zdend = 1.0f / ((1.0f - zbeta * zemm) * zrkg);
+  r.refd = g2 * (1.0f - zemm) * zdend;
+  r.trad = zrk2 * zem1 * zdend;
+  return r;
+}
+
+// One adding-method path (clear or total) of one g-point: level arrays top-down.
+struct Path {
+  float ref[kMaxLev], refd[kMaxLev], tra[kMaxLev], trad[kMaxLev], dbt[kMaxLev];
+  float tdbt[kMaxLev], tdn[kMaxLev], rdnd[kMaxLev];
+};
+
+// Downward recurrence of vrtqdr (sw:3681-3702) for level r+1 once layer r is known.
+__device__ __forceinline__ void down_step(Path &P, int r) {
+  if (r == 0) {
+    P.tdn[0] = 1.0f;
+    P.rdnd[0] = 0.0f;
+    P.tdn[1] = P.tra[0];
+    P.rdnd[1] = P.refd[0];
+    return;
+  }
+  const float zreflect = 1.0f / (1.0f - P.refd[r] * P.rdnd[r]);
+  P.tdn[r + 1] = P.tdbt[r] * P.tra[r] + P.trad[r] * ((P.tdn[r] - P.tdbt[r]) + P.tdbt[r] * P.ref[r] * P.rdnd[r]) * zreflect;
+  P.rdnd[r + 1] = P.refd[r] + P.trad[r] * P.trad[r] * P.rdnd[r] * zreflect;
+}
+
+template <int B>
+__device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
+                                        int clear_only, float *accs, Path &Pc, Path &Pt) {
+  constexpr int ngc = kNgc[B];
+  constexpr int gofs = kGofs[B];
+  constexpr int bn = B + 16;
+  const int n = C.nlay;
+  const int col = C.i * C.ny + C.j;
+  const SwBand &K = T.sw[B];
+  // Per-layer band optics, thread-local: taug/taur of every g-point and the
+  // band's cloud optics for cloudy g-points.
+  float taug[kMaxLay][kMaxNgc], taur[kMaxLay][kMaxNgc];
+  float ctau[kMaxLay], cssa[kMaxLay], casm[kMaxLay], ctaor[kMaxLay];
+  float src_fs = 0.0f;
+  int src_js0 = 0;
+  // solar-source layer (sw:4430-4450 style rules per band)
+  int ls = -1;
+  const int layreffr = K.layreffr;
+  bool found = false;
+  for (int l = 0; l < n; ++l) {
+    const SLayer L = make_layer(T, a, C, l);
+    SwSpec sp8, sp4;
+    sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
+    sp4 = sp8;
+    float tg[ngc], tr[ngc];
+    sw_taumol<B>(T, L, tg, tr, sp8, sp4);
+#pragma unroll
+    for (int g = 0; g < ngc; ++g) { taug[l][g] = tg[g]; taur[l][g] = tr[g]; }
+    // cloud optics of the band at this layer (used by cloudy g-points)
+    if (!clear_only) {
+      const CloudOpt o = sw_cloud(T, L, B, C.iceflg);
+      ctau[l] = o.tau; cssa[l] = o.ssa; casm[l] = o.asm_; ctaor[l] = o.taor;
+    }
+    // solar source function layer
+    if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
+      // first troposphere crossing of layreffr, one layer up, capped at laytrop-1
+      if (!found) {
+        const int next = l + 1 < n ? make_layer(T, a, C, l + 1).jp : L.jp;
+        if (l < C.laytrop && L.jp < layreffr && next >= layreffr) {
+          found = true;
+          ls = (l + 1 < C.laytrop - 1) ? l + 1 : C.laytrop - 1;
+        }
+      }
+    }
+    if constexpr (bn == 17 || bn == 28) {
+      if (!found && l > 0 && l >= C.laytrop) {
+        const int prev = make_layer(T, a, C, l - 1).jp;
+        if (prev < layreffr && L.jp >= layreffr) { found = true; ls = l; }
+      }
+    }
+  }
+  float sflux[ngc];
+  {
+    if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
+      if (!found) ls = C.laytrop - 1;
+    }
+    if constexpr (bn == 17 || bn == 28) {
+      if (!found) ls = n - 1;
+    }
+    bool have = false;
+    if constexpr (bn == 17 || bn == 28) have = C.laytrop < n;
+    if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) have = C.laytrop > 0;
+    if (have && ls >= 0) {
+      const SLayer L = make_layer(T, a, C, ls);
+      SwSpec sp8, sp4;
+      sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
+      sp4 = sp8;
+      float tg[ngc], tr[ngc];
+      sw_taumol<B>(T, L, tg, tr, sp8, sp4);
+      if constexpr (bn == 17 || bn == 28) { src_js0 = sp4.js0; src_fs = sp4.fs; }
+      else { src_js0 = sp8.js0; src_fs = sp8.fs; }
+    }
+#pragma unroll
+    for (int g = 0; g < ngc; ++g) {
+      float sz = 0.0f;
+      if constexpr (bn == 16 || bn == 29) sz = C.laytrop < n ? ld(K.sfluxref + g) : 0.0f;
+      if constexpr (bn == 20 || bn == 23 || bn == 25 || bn == 26) sz = C.laytrop > 0 ? ld(K.sfluxref + g) : 0.0f;
+      if constexpr (bn == 27) sz = C.laytrop < n ? K.scalekur * ld(K.sfluxref + g) : 0.0f;
+      if constexpr (bn == 17 || bn == 28 || bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
+        if (have) {
+          const int c = K.sflux_cols;
+          const float s0 = ld(K.sfluxref + g * c + src_js0), s1 = ld(K.sfluxref + g * c + src_js0 + 1);
+          sz = s0 + src_fs * (s1 - s0);
+        }
+      }
+      sflux[g] = sz;
+    }
+  }
+  const float mu = C.mu;
+  const float repclc = 1.0e-12f;
+  for (int g = 0; g < ngc; ++g) {
+    const int G = gofs + g;
+    // top-down: layer optics, direct beam, downward adding
+    Pc.tdbt[0] = 1.0f;
+    Pt.tdbt[0] = 1.0f;
+    float tdbtc_nd = 1.0f, tdbt_nd = 1.0f;
+    float *accfdir = accs + 4 * kMaxLev, *acccdir = accs + 5 * kMaxLev;
+    const float zincflx = ((C.adjflux * sflux[g]) * mu) * 1.0f;
+    accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
+    acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
+    for (int r = 0; r < n; ++r) {
+      const int l = n - 1 - r;
+      const uint32_t word = maskbase[(static_cast<size_t>(l) * kSwMaskWords + (G >> 5)) * a.ncol];
+      const bool cldb = (word >> (G & 31)) & 1u;
+      const float cloud = cldb ? 1.0f : 0.0f;
+      const float clear = 1.0f - cloud;
+      const float tr = taur[l][g], tg = taug[l][g];
+      const float ztau = (tr + tg) + 0.0f;
+      float zom = tr + 0.0f * 1.0f;
+      const float zgr = 0.0f * 1.0f * 0.0f / zom;
+      zom = zom / ztau;
+      const float dbtc_nd = exp_lookup(T, ztau / mu);
+      tdbtc_nd = tdbtc_nd * dbtc_nd;
+      const float zf = zgr * zgr;
+      const float zwf = zom * zf;
+      const float ztauc = (1.0f - zwf) * ztau;
+      const float zomcc = (zom - zwf) / (1.0f - zwf);
+      const float zgcc = (zgr - zf) / (1.0f - zf);
+      const RT4 c = reftra(T, true, zgcc, mu, ztauc, zomcc);
+      Pc.ref[r] = c.ref; Pc.refd[r] = c.refd; Pc.tra[r] = c.tra; Pc.trad[r] = c.trad;
+      const float dbtc = exp_lookup(T, ztauc / mu);
+      Pc.dbt[r] = dbtc;
+      Pc.tdbt[r + 1] = Pc.tdbt[r] * dbtc;
+      down_step(Pc, r);
+      if (!clear_only) {
+        const float tcld = cldb ? ctau[l] : 0.0f;
+        const float wcld = cldb ? cssa[l] : 1.0f;
+        const float gcld = cldb ? casm[l] : 0.0f;
+        const float taor = cldb ? ctaor[l] : 0.0f;
+        const float tauorig = ztau + taor;
+        const float dbtmo_nd = exp_lookup(T, tauorig / mu);
+        const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
+        tdbt_nd = tdbt_nd * dbt_nd;
+        const float ztauo = ztauc + tcld;
+        float zomco = ztauc * zomcc + tcld * wcld;
+        const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
+        zomco = zomco / ztauo;
+        const RT4 o = reftra(T, cloud > repclc, zgco, mu, ztauo, zomco);
+        Pt.ref[r] = clear * c.ref + cloud * o.ref;
+        Pt.refd[r] = clear * c.refd + cloud * o.refd;
+        Pt.tra[r] = clear * c.tra + cloud * o.tra;
+        Pt.trad[r] = clear * c.trad + cloud * o.trad;
+        const float dbtmo = exp_lookup(T, ztauo / mu);
+        const float dbt = clear * dbtc + cloud * dbtmo;
+        Pt.dbt[r] = dbt;
+        Pt.tdbt[r + 1] = Pt.tdbt[r] * dbt;
+        down_step(Pt, r);
+      } else {
+        tdbt_nd = tdbtc_nd;
+      }
+      accfdir[r + 1] = accfdir[r + 1] + tdbt_nd * zincflx;
+      acccdir[r + 1] = acccdir[r + 1] + tdbtc_nd * zincflx;
+    }
+    // surface boundary
+    Pc.ref[n] = C.albedo; Pc.refd[n] = C.albedo; Pc.tra[n] = 0.0f; Pc.trad[n] = 0.0f; Pc.dbt[n] = 0.0f;
+    Pt.ref[n] = C.albedo; Pt.refd[n] = C.albedo; Pt.tra[n] = 0.0f; Pt.trad[n] = 0.0f; Pt.dbt[n] = 0.0f;
+    // bottom-up: upward adding and level fluxes (vrtqdr, sw:3655-3720)
+    float *accfu = accs, *accfd = accs + kMaxLev, *acccu = accs + 2 * kMaxLev, *acccd = accs + 3 * kMaxLev;
+    float rupc = Pc.ref[n], rupdc = Pc.refd[n];
+    float rupt = Pt.ref[n], rupdt = Pt.refd[n];
+    for (int k = n; k >= 0; --k) {
+      if (k < n) {
+        const float zrc = 1.0f / (1.0f - rupdc * Pc.refd[k]);
+        const float nrupc = Pc.ref[k] + Pc.trad[k] * ((Pc.tra[k] - Pc.dbt[k]) * rupdc + Pc.dbt[k] * rupc) * zrc;
+        const float nrupdc = Pc.refd[k] + Pc.trad[k] * Pc.trad[k] * rupdc * zrc;
+        rupc = nrupc;
+        rupdc = nrupdc;
+        if (!clear_only) {
+          const float zrt = 1.0f / (1.0f - rupdt * Pt.refd[k]);
+          const float nrupt = Pt.ref[k] + Pt.trad[k] * ((Pt.tra[k] - Pt.dbt[k]) * rupdt + Pt.dbt[k] * rupt) * zrt;
+          const float nrupdt = Pt.refd[k] + Pt.trad[k] * Pt.trad[k] * rupdt * zrt;
+          rupt = nrupt;
+          rupdt = nrupdt;
+        }
+      }
+      // clear-sky level fluxes
+      const float zrefc = 1.0f / (1.0f - Pc.rdnd[k] * rupdc);
+      const float fuc = (Pc.tdbt[k] * rupc + (Pc.tdn[k] - Pc.tdbt[k]) * rupdc) * zrefc;
+      const float fdc = Pc.tdbt[k] + (Pc.tdn[k] - Pc.tdbt[k] + Pc.tdbt[k] * rupc * Pc.rdnd[k]) * zrefc;
+      float fut = fuc, fdt = fdc;
+      if (!clear_only) {
+        const float zreft = 1.0f / (1.0f - Pt.rdnd[k] * rupdt);
+        fut = (Pt.tdbt[k] * rupt + (Pt.tdn[k] - Pt.tdbt[k]) * rupdt) * zreft;
+        fdt = Pt.tdbt[k] + (Pt.tdn[k] - Pt.tdbt[k] + Pt.tdbt[k] * rupt * Pt.rdnd[k]) * zreft;
+      }
+      accfu[k] = accfu[k] + fut * zincflx;
+      accfd[k] = accfd[k] + fdt * zincflx;
+      acccu[k] = acccu[k] + fuc * zincflx;
+      acccd[k] = acccd[k] + fdc * zincflx;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.ncol) return;
+  Col C;
+  C.i = col / a.ny;
+  C.j = col - C.i * a.ny;
+  C.nk = a.nk;
+  C.ny = a.ny;
+  C.nlay = a.nk + 1;
+  const int nk = C.nk, n = C.nlay;
+  const float coszen = ld(a.in.coszr + col);
+  const size_t rbase = static_cast<size_t>(C.i) * nk * C.ny + C.j;
+  a.coszr_out[col] = coszen;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
+  if (!(coszen > 0.0f)) {
+    for (int k = 0; k < nk; ++k) {
+      a.rthraten[rbase + static_cast<size_t>(k) * C.ny] = 0.0f;
+      a.rthratenc[rbase + static_cast<size_t>(k) * C.ny] = 0.0f;
+    }
+    a.upt[col] = 0.0f; a.uptc[col] = 0.0f; a.dnt[col] = 0.0f; a.dntc[col] = 0.0f;
+    a.upb[col] = 0.0f; a.upbc[col] = 0.0f; a.dnb[col] = 0.0f; a.dnbc[col] = 0.0f;
+    a.swcf[col] = 0.0f; a.gsw[col] = 0.0f; a.swddir[col] = 0.0f; a.swddni[col] = 0.0f;
+    a.swddif[col] = 0.0f; a.swdownc[col] = 0.0f; a.swddnic[col] = 0.0f; a.swddirc[col] = 0.0f;
+    return;
+  }
+  C.coszen = coszen;
+  C.mu = fmaxf(coszen, 1.0e-10f);
+  C.albedo = ld(a.in.albedo + col);
+  C.co2 = a.co2; C.n2o = a.n2o; C.ch4 = a.ch4;
+  C.inflg = a.inflg; C.iceflg = a.iceflg;
+  C.has_reqc = a.has_reqc; C.has_reqi = a.has_reqi; C.has_reqs = a.has_reqs; C.icloud = a.icloud;
+  C.adjflux = 1.0f * (a.solcon / 1.36822e3f);
+  // ozone in the extra top layer (sw:2491-2508)
+  {
+    const float amdo = 0.603461f;
+    const float pnk1 = pa_to_hpa(in3w(a.in.p8w, C, nk - 1)), pnk = pa_to_hpa(in3w(a.in.p8w, C, nk));
+    const float mmr_k = o3data_layer(T, pnk1, pnk);
+    const float mmr_t = o3data_layer(T, pnk, 1.0e-5f);
+    float top = (in3(a.in.o3, C, nk - 1) - mmr_k * amdo) + mmr_t * amdo;
+    if (top <= 0.0f) top = mmr_t * amdo;
+    C.o3top = top;
+  }
+  {
+    int laytrop = 0;
+    for (int l = 0; l < n; ++l) {
+      const float pavel = l < nk ? pa_to_hpa(in3(a.in.p3d, C, l)) : 0.5f * pa_to_hpa(in3w(a.in.p8w, C, nk));
+      laytrop += glibc_logf(T, pavel) > 4.56f;
+    }
+    C.laytrop = laytrop;
+  }
+  const int clear_only = a.icld == 0;
+  float accs[6 * kMaxLev];
+  for (int k = 0; k < 6 * kMaxLev; ++k) accs[k] = 0.0f;
+  Path Pc, Pt;
+  const uint32_t *maskbase = a.mask + col;
+  sw_band<0>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<1>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<2>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<3>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<4>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<5>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<6>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<7>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<8>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<9>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<10>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<11>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<12>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<13>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  // accumulators are top-down (index 0 = TOA); outputs are bottom-up
+  const float *fu = accs, *fd = accs + kMaxLev, *cu = accs + 2 * kMaxLev, *cd = accs + 3 * kMaxLev;
+  const float *fdir = accs + 4 * kMaxLev, *cdir = accs + 5 * kMaxLev;
+  const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
+  for (int l = 0; l < nk; ++l) {
+    // bottom-up level l is top-down index n - l
+    const float n1 = fd[n - (l + 1)] - fu[n - (l + 1)], n0 = fd[n - l] - fu[n - l];
+    const float c1 = cd[n - (l + 1)] - cu[n - (l + 1)], c0 = cd[n - l] - cu[n - l];
+    const float plev0 = pa_to_hpa(in3w(a.in.p8w, C, l));
+    const float plev1 = pa_to_hpa(in3w(a.in.p8w, C, l + 1));
+    const float zdpgcp = heatfac / (plev0 - plev1);
+    const float hr = (n1 - n0) * zdpgcp;
+    const float hrc = (c1 - c0) * zdpgcp;
+    const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * C.ny);
+    a.rthraten[rbase + static_cast<size_t>(l) * C.ny] = (hr / 86400.0f) / pi3d;
+    a.rthratenc[rbase + static_cast<size_t>(l) * C.ny] = (hrc / 86400.0f) / pi3d;
+  }
+  a.upt[col] = fu[0];
+  a.uptc[col] = cu[0];
+  a.dnt[col] = fd[0];
+  a.dntc[col] = cd[0];
+  a.upb[col] = fu[n];
+  a.upbc[col] = cu[n];
+  a.dnb[col] = fd[n];
+  a.dnbc[col] = cd[n];
+  a.swcf[col] = (fd[0] - fu[0]) - (cd[0] - cu[0]);
+  a.gsw[col] = fd[n] - fu[n];
+  a.swddir[col] = fdir[n];
+  a.swddni[col] = fdir[n] / coszen;
+  a.swddif[col] = fd[n] - fdir[n];
+  a.swdownc[col] = cd[n];
+  a.swddirc[col] = cdir[n];
+  a.swddnic[col] = cdir[n] / coszen;
+}
+
+}  // namespace
+
+cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+  const int threads = 128;
+  const int blocks = (a.ncol + threads - 1) / threads;
+  sw_kernel<<<blocks, threads, 0, stream>>>(T, a);
+  return cudaGetLastError();
+}
+
+}  // namespace rrtmg

@@ -1,0 +1,277 @@
+"""Drop-in replacements for WRF-JAX's RRTMG radiation calls, running on B200.
+
+``rrtmg_lwrad_wrf_columns`` and ``rrtmg_swrad_wrf_columns`` take the same
+keyword arguments as the reference's functions
+(src/wrf_jax/physics/module_ra_rrtmg_lw.py:6789, module_ra_rrtmg_sw.py:2386) and
+return named tuples with the same fields (RrtmgLwWrfColumnResult, lw:499;
+RrtmgSwWrfColumnResult, sw:617).
+
+Arrays may be numpy arrays (host; copied to the GPU and results copied back) or
+torch CUDA tensors (used in place; results are torch CUDA tensors), float32 in
+the WRF runtime layout (nx, nk, ny) / (nx, nk+1, ny) / (nx, ny).  The work runs
+in librrtmg_b200.so on the current torch CUDA stream.  There is no CPU path: if
+the library or a CUDA device is missing the call raises.
+
+Unsupported reference options raise NotImplementedError like the reference
+does (cldprmc liquid/ice options, lw:5750-5753, sw:1438-1441); the CAM
+greenhouse-gas table reader (ghg_input=1 with a case directory) is not part of
+this path, so such calls must pass the gas mixing ratios explicitly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+from typing import Any, NamedTuple
+
+import numpy as np
+
+from . import _capi, tables
+
+
+class RrtmgLwWrfColumnResult(NamedTuple):
+    rthratenlw: Any
+    rthratenlwc: Any
+    lwupt: Any
+    lwuptc: Any
+    lwuptcln: Any
+    lwdnt: Any
+    lwdntc: Any
+    lwdntcln: Any
+    lwupb: Any
+    lwupbc: Any
+    lwupbcln: Any
+    lwdnb: Any
+    lwdnbc: Any
+    lwdnbcln: Any
+    glw: Any
+    olr: Any
+    lwcf: Any
+
+
+class RrtmgSwWrfColumnResult(NamedTuple):
+    rthratensw: Any
+    rthratenswc: Any
+    swupt: Any
+    swuptc: Any
+    swuptcln: Any
+    swdnt: Any
+    swdntc: Any
+    swdntcln: Any
+    swupb: Any
+    swupbc: Any
+    swupbcln: Any
+    swdnb: Any
+    swdnbc: Any
+    swdnbcln: Any
+    swcf: Any
+    gsw: Any
+    swddir: Any
+    swddni: Any
+    swddif: Any
+    swdownc: Any
+    swddnic: Any
+    swddirc: Any
+    coszr: Any
+
+
+class RrtmgError(RuntimeError):
+    """A failed C-ABI call; ``status`` is the rrtmg_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_capi.STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class RrtmgContext:
+    """One library context: tables resident on one CUDA device."""
+
+    def __init__(self, blob_path: str | Path | None = None, device: int | None = None):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("rrtmg_b200 needs a CUDA device; there is no CPU fallback")
+        self.lib = _capi.load()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        path = Path(blob_path) if blob_path is not None else tables.DEFAULT_BLOB
+        if not path.exists():
+            raise FileNotFoundError(f"table blob {path} is missing (built by tables.ensure_blob)")
+        handle = ctypes.c_void_p()
+        st = self.lib.rrtmg_create(str(path).encode(), self.device, ctypes.byref(handle))
+        if st != 0:
+            raise RrtmgError(st, self.lib.rrtmg_last_error(None).decode())
+        self.handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.rrtmg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, st: int) -> None:
+        if st != 0:
+            msg = self.lib.rrtmg_last_error(self.handle).decode()
+            if st == 2:
+                raise NotImplementedError(msg)
+            raise RrtmgError(st, msg)
+
+
+_default_ctx: dict = {}
+_ctx_lock = threading.Lock()
+
+
+def default_context(device: int | None = None) -> RrtmgContext:
+    import torch
+
+    dev = torch.cuda.current_device() if device is None else int(device)
+    with _ctx_lock:
+        if dev not in _default_ctx:
+            _default_ctx[dev] = RrtmgContext(device=dev)
+        return _default_ctx[dev]
+
+
+def _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr, cfc11vmr, cfc12vmr, lw: bool):
+    """Gas scalars as the reference adapters choose them (lw:6610-6630, sw:2371-2383)."""
+    given = (co2vmr, n2ovmr, ch4vmr) + ((cfc11vmr, cfc12vmr) if lw else ())
+    if all(v is not None for v in given):
+        return given + (() if lw else (0.0, 0.0))
+    if lw and int(ghg_input) == 1 and case_dir is not None:
+        raise NotImplementedError("CAM greenhouse-gas tables are not part of this path; pass the gas scalars")
+    if int(ghg_input) == 0:
+        co2 = (280.0 + 90.0 * np.exp(0.02 * (int(yr) - 2000))) * 1.0e-6
+    else:
+        co2 = 379.0e-6
+    d = [co2, 319.0e-9, 1774.0e-9, 0.251e-9, 0.538e-9]
+    if lw:  # the LW adapter ignores partially given scalars
+        return tuple(d)
+    vals = [v if v is not None else dv for v, dv in zip(given, d)]
+    return tuple(vals) + (0.0, 0.0)
+
+
+def _as_device(arrays: dict, device: int):
+    """numpy -> torch CUDA float32 (contiguous); torch CUDA tensors pass through."""
+    import torch
+
+    out = {}
+    host = False
+    for k, v in arrays.items():
+        if isinstance(v, torch.Tensor):
+            if not v.is_cuda:
+                raise ValueError(f"{k}: torch tensors must be on a CUDA device")
+            t = v.contiguous()
+            if t.dtype != torch.float32:
+                t = t.float()
+        else:
+            host = True
+            t = torch.from_numpy(np.ascontiguousarray(np.asarray(v, dtype=np.float32))).to(
+                device=f"cuda:{device}", non_blocking=False)
+        out[k] = t
+    return out, host
+
+
+def _check_shapes(d: dict, nx: int, nk: int, ny: int, three: tuple, lev: tuple, two: tuple) -> None:
+    for k in three:
+        if tuple(d[k].shape) != (nx, nk, ny):
+            raise ValueError(f"{k} must have shape (nx, nk, ny) = {(nx, nk, ny)}, got {tuple(d[k].shape)}")
+    for k in lev:
+        if tuple(d[k].shape) != (nx, nk + 1, ny):
+            raise ValueError(f"{k} must have shape (nx, nk+1, ny) = {(nx, nk + 1, ny)}, got {tuple(d[k].shape)}")
+    for k in two:
+        if tuple(d[k].shape) != (nx, ny):
+            raise ValueError(f"{k} must have shape (nx, ny) = {(nx, ny)}, got {tuple(d[k].shape)}")
+
+
+def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, qi3d, qs3d, cldfra3d, o33d,
+                            emiss, xland, xice, snow, re_cloud, re_ice, re_snow, p_top, yr, julian,
+                            ghg_input=1, case_dir=None, cldovrlp=2, idcor=0, icloud=1, has_reqc=1,
+                            has_reqi=1, has_reqs=1, co2vmr=None, n2ovmr=None, ch4vmr=None, cfc11vmr=None,
+                            cfc12vmr=None, lookup_tables=None, spectral=None, pade_tables=None,
+                            cloud_tables=None, setcoef_tables=None, rounding_token=None,
+                            context: RrtmgContext | None = None, stream=None) -> RrtmgLwWrfColumnResult:
+    """B200 ``RRTMG_LWRAD`` (module_ra_rrtmg_lw.py:6789).  Table keywords are
+    accepted for signature parity and ignored (the context owns the tables)."""
+    import torch
+
+    del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables, setcoef_tables
+    if rounding_token is not None:
+        raise NotImplementedError("diagnostic rounding tokens are not supported")
+    ctx = context or default_context()
+    arrays = dict(p3d=p3d, p8w=p8w, pi3d=pi3d, t3d=t3d, t8w=t8w, tsk=tsk, dz8w=dz8w, qv3d=qv3d, qc3d=qc3d,
+                  qi3d=qi3d, qs3d=qs3d, cldfra3d=cldfra3d, o33d=o33d, emiss=emiss, xland=xland, xice=xice,
+                  snow=snow, re_cloud=re_cloud, re_ice=re_ice, re_snow=re_snow)
+    with torch.cuda.device(ctx.device):
+        d, host = _as_device(arrays, ctx.device)
+        nx, nk, ny = d["t3d"].shape
+        _check_shapes(d, nx, nk, ny,
+                      ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d",
+                       "re_cloud", "re_ice", "re_snow"), ("p8w", "t8w"),
+                      ("tsk", "emiss", "xland", "xice", "snow"))
+        co2, n2o, ch4, cfc11, cfc12 = _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr,
+                                                  cfc11vmr, cfc12vmr, lw=True)
+        cfg = _capi.Config(nx=nx, ny=ny, nk=nk, p_top=float(p_top), co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4,
+                           cfc11vmr=cfc11, cfc12vmr=cfc12, solcon=0.0, has_reqc=int(has_reqc),
+                           has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
+                           cldovrlp=int(cldovrlp))
+        outs = {k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny),
+                               dtype=torch.float32, device=f"cuda:{ctx.device}")
+                for k in _capi.LW_OUT_FIELDS}
+        cin = _capi.LwIn(**{k: d[k].data_ptr() for k in _capi.LW_IN_FIELDS})
+        cout = _capi.LwOut(**{k: outs[k].data_ptr() for k in _capi.LW_OUT_FIELDS})
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        ctx.check(ctx.lib.rrtmg_lwrad(ctx.handle, ctypes.byref(cfg), ctypes.byref(cin), ctypes.byref(cout),
+                                      ctypes.c_void_p(s)))
+        if host:
+            torch.cuda.current_stream().synchronize()
+            return RrtmgLwWrfColumnResult(**{k: outs[k].cpu().numpy() for k in _capi.LW_OUT_FIELDS})
+        return RrtmgLwWrfColumnResult(**outs)
+
+
+def rrtmg_swrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, qi3d, qs3d, cldfra3d, o33d,
+                            albedo, coszr, xland, xice, snow, re_cloud, re_ice, re_snow, solcon, yr, julian,
+                            ghg_input=1, cldovrlp=2, idcor=0, icloud=1, has_reqc=1, has_reqi=1, has_reqs=1,
+                            sf_surface_physics=2, alswvisdir=None, alswvisdif=None, alswnirdir=None,
+                            alswnirdif=None, co2vmr=None, n2ovmr=None, ch4vmr=None, lookup_tables=None,
+                            spectral=None, pade_tables=None, cloud_tables=None, rounding_token=None,
+                            context: RrtmgContext | None = None, stream=None) -> RrtmgSwWrfColumnResult:
+    """B200 ``rrtmg_swrad`` (module_ra_rrtmg_sw.py:2386)."""
+    import torch
+
+    del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables
+    if rounding_token is not None:
+        raise NotImplementedError("diagnostic rounding tokens are not supported")
+    if int(sf_surface_physics) == 8 and all(v is not None for v in (alswvisdir, alswvisdif, alswnirdir, alswnirdif)):
+        raise NotImplementedError("separate visible/near-IR albedos (sf_surface_physics=8) are not part of this path")
+    ctx = context or default_context()
+    arrays = dict(p3d=p3d, p8w=p8w, pi3d=pi3d, t3d=t3d, t8w=t8w, tsk=tsk, dz8w=dz8w, qv3d=qv3d, qc3d=qc3d,
+                  qi3d=qi3d, qs3d=qs3d, cldfra3d=cldfra3d, o33d=o33d, albedo=albedo, coszr=coszr,
+                  xland=xland, xice=xice, snow=snow, re_cloud=re_cloud, re_ice=re_ice, re_snow=re_snow)
+    with torch.cuda.device(ctx.device):
+        d, host = _as_device(arrays, ctx.device)
+        nx, nk, ny = d["t3d"].shape
+        _check_shapes(d, nx, nk, ny,
+                      ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d",
+                       "re_cloud", "re_ice", "re_snow"), ("p8w", "t8w"),
+                      ("tsk", "albedo", "coszr", "xland", "xice", "snow"))
+        co2, n2o, ch4, _, _ = _greenhouse(yr, ghg_input, None, co2vmr, n2ovmr, ch4vmr, None, None, lw=False)
+        cfg = _capi.Config(nx=nx, ny=ny, nk=nk, p_top=0.0, co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4, cfc11vmr=0.0,
+                           cfc12vmr=0.0, solcon=float(np.float32(solcon)), has_reqc=int(has_reqc),
+                           has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
+                           cldovrlp=int(cldovrlp))
+        outs = {k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny),
+                               dtype=torch.float32, device=f"cuda:{ctx.device}")
+                for k in _capi.SW_OUT_FIELDS}
+        cin = _capi.SwIn(**{k: d[k].data_ptr() for k in _capi.SW_IN_FIELDS})
+        cout = _capi.SwOut(**{k: outs[k].data_ptr() for k in _capi.SW_OUT_FIELDS})
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        ctx.check(ctx.lib.rrtmg_swrad(ctx.handle, ctypes.byref(cfg), ctypes.byref(cin), ctypes.byref(cout),
+                                      ctypes.c_void_p(s)))
+        if host:
+            torch.cuda.current_stream().synchronize()
+            return RrtmgSwWrfColumnResult(**{k: outs[k].cpu().numpy() for k in _capi.SW_OUT_FIELDS})
+        return RrtmgSwWrfColumnResult(**outs)

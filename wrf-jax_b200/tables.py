@@ -20,7 +20,7 @@ raw values for Planck fractions and solar source functions;
 ``module_ra_rrtmg_lw.py:829-910``, ``module_ra_rrtmg_sw.py:1068-1130``).
 
 Blob layout (little endian): ``b"RRTMGB2\\0"``, u32 version, u32 count, then
-``count`` entries of {char name[48]; u32 dtype (0=f32, 1=i32); u32 ndim;
+``count`` entries of {char name[48]; u32 dtype (0=f32, 1=i32, 2=f64, 3=u64); u32 ndim;
 u32 shape[4]; u64 offset; u64 nbytes}, then the data, each array 256-byte
 aligned.  Absorption tables ``ka``/``kb`` are stored as 2-D
 ``(rows, ngc)`` with row = ``(jp * n_t + jt) * n_species + js`` (the Fortran
@@ -58,6 +58,48 @@ def _literal_tables(path: Path, names: tuple[str, ...]) -> dict:
     if missing:
         raise ValueError(f"literal tables not found in {path}: {sorted(missing)}")
     return found
+
+
+def _hex_floats(node) -> list:
+    """All float.fromhex("...") literals under an AST node, in source order."""
+    vals = []
+    for sub in ast.walk(node):
+        if (isinstance(sub, ast.Call) and isinstance(sub.func, ast.Attribute)
+                and sub.func.attr == "fromhex" and sub.args
+                and isinstance(sub.args[0], ast.Constant)):
+            vals.append((sub.lineno, sub.col_offset, float.fromhex(sub.args[0].value)))
+    return [v for _, _, v in sorted(vals)]
+
+
+def _glibc_math_tables(path: Path) -> dict:
+    """glibc 2.39 logf/expf data as the reference reproduces it (core/wrf_math.py).
+
+    These are glibc's published constants (sysdeps/ieee754/flt-32/e_logf_data.c,
+    e_exp2f_data.c): 16 (1/c, log c) pairs and a cubic for logf; 32 table
+    entries of 2^(i/32) bit patterns, the scaled 1/ln2 and a cubic for expf.
+    """
+    tree = ast.parse(path.read_text())
+    nodes = {}
+    for node in tree.body:
+        if isinstance(node, ast.Assign) and len(node.targets) == 1 and isinstance(node.targets[0], ast.Name):
+            nodes[node.targets[0].id] = node.value
+    logf_tab = np.asarray(_hex_floats(nodes["_GLIBC_LOGF_TABLE_NP"]), np.float64).reshape(16, 2)
+    ln2 = _hex_floats(nodes["_GLIBC_LOGF_LN2"])
+    logf_poly = np.asarray(_hex_floats(nodes["_GLIBC_LOGF_POLY"]), np.float64)
+    exp_ints = [int(sub.value) for sub in ast.walk(nodes["_GLIBC_EXPF_TABLE"])
+                if isinstance(sub, ast.Constant) and isinstance(sub.value, int) and sub.value > 2**32]
+    inv_ln2 = _hex_floats(nodes["_GLIBC_EXPF_INV_LN2_SCALED"])
+    exp_poly = np.asarray(_hex_floats(nodes["_GLIBC_EXPF_POLY"]), np.float64)
+    if logf_tab.shape != (16, 2) or len(ln2) != 1 or logf_poly.size != 3:
+        raise ValueError("unexpected glibc logf data layout")
+    if len(exp_ints) != 32 or len(inv_ln2) != 1 or exp_poly.size != 3:
+        raise ValueError("unexpected glibc expf data layout")
+    return {
+        "glibc.logf_invc_logc": np.ascontiguousarray(logf_tab),
+        "glibc.logf_ln2_poly": np.asarray([ln2[0], *logf_poly], np.float64),
+        "glibc.expf_tab": np.asarray(exp_ints, np.uint64),
+        "glibc.expf_invln2n_poly": np.asarray([inv_ln2[0], *exp_poly], np.float64),
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -300,6 +342,7 @@ def build_tables(physics_dir: str | Path) -> dict:
     t["lw_buffer_pprof"] = f32(lwlit["_LW_BUFFER_PPROF"])
     t["lw_buffer_tprof"] = f32(lwlit["_LW_BUFFER_TPROF"])
     t["sw.preflog"] = f32(swlit["_PREFLOG_VALUES"])
+    t.update(_glibc_math_tables(phys.parent / "core" / "wrf_math.py"))
     t["sw.tref"] = f32(swlit["_TREF_VALUES"])
 
     for side, counts, ngs, ngm, ngn, nb, first, records, fname in (
@@ -348,6 +391,10 @@ def write_blob(tables: dict, path: str | Path) -> None:
             code = 0
         elif arr.dtype == np.int32:
             code = 1
+        elif arr.dtype == np.float64:
+            code = 2
+        elif arr.dtype == np.uint64:
+            code = 3
         else:
             raise TypeError(f"{name}: unsupported dtype {arr.dtype}")
         if arr.ndim > 4 or len(name) >= 48:
@@ -379,8 +426,9 @@ def read_blob(path: str | Path) -> dict:
         name = raw[pos:pos + 48].split(b"\0", 1)[0].decode()
         code, ndim, s0, s1, s2, s3, offset, nbytes = struct.unpack_from("<II4IQQ", raw, pos + 48)
         pos += 88
-        dt = np.float32 if code == 0 else np.int32
-        out[name] = np.frombuffer(raw, dtype=dt, count=nbytes // 4, offset=offset).reshape((s0, s1, s2, s3)[:ndim])
+        dt = {0: np.float32, 1: np.int32, 2: np.float64, 3: np.uint64}[code]
+        out[name] = np.frombuffer(raw, dtype=dt, count=nbytes // np.dtype(dt).itemsize,
+                                  offset=offset).reshape((s0, s1, s2, s3)[:ndim])
     return out
 
 
