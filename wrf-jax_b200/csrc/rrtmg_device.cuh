@@ -85,10 +85,16 @@ __device__ __forceinline__ float interpf(float lo, float hi, float f) { return l
 // (module_ra_rrtmg_common.py:70-82), identical to a binary32 division.
 __device__ __forceinline__ float pa_to_hpa(float p) { return p / 100.0f; }
 
-// glibc 2.39 logf for positive normal inputs (e_logf.c, FMA build).
+// glibc 2.39 logf (e_logf.c, FMA build), including its special inputs.
 __device__ __forceinline__ float glibc_logf(const Tables &T, float x) {
-  const uint32_t ix = __float_as_uint(x);
+  uint32_t ix = __float_as_uint(x);
   if (ix == 0x3f800000u) return 0.0f;
+  if (ix - 0x00800000u >= 0x7f800000u - 0x00800000u) {
+    if (ix * 2u == 0u) return __int_as_float(0xff800000);          // log(+-0) = -inf
+    if (ix == 0x7f800000u) return x;                                // log(inf) = inf
+    if ((ix & 0x80000000u) || ix * 2u >= 0xff000000u) return __int_as_float(0x7fc00000);  // negative or NaN
+    ix = __float_as_uint(x * 8388608.0f) - (23u << 23);             // subnormal: normalize
+  }
   const uint32_t tmp = ix - 0x3f330000u;
   const int i = (tmp >> 19) & 15;
   const int k = static_cast<int32_t>(tmp) >> 23;
@@ -105,8 +111,15 @@ __device__ __forceinline__ float glibc_logf(const Tables &T, float x) {
   return __double2float_rn(y);
 }
 
-// glibc 2.39 expf for finite inputs in range (e_expf.c, FMA build).
+// glibc 2.39 expf (e_expf.c, FMA build), including its |x| >= 88 branch.
 __device__ __forceinline__ float glibc_expf(const Tables &T, float x) {
+  const uint32_t ux = __float_as_uint(x);
+  if (((ux >> 20) & 0x7ffu) >= (0x42b00000u >> 20)) {   // |x| >= 88 or not finite
+    if (ux == 0xff800000u) return 0.0f;                   // exp(-inf) = 0
+    if (((ux >> 20) & 0x7ffu) >= (0x7f800000u >> 20)) return x + x;  // inf or NaN
+    if (x > 88.7228317f) return __int_as_float(0x7f800000);         // overflow
+    if (x < -103.972076f) return 0.0f;                               // underflow
+  }
   const double xd = static_cast<double>(x);
   const double z = __dmul_rn(T.expf_invln2n, xd);
   const double kd = rint(z);
