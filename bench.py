@@ -34,6 +34,9 @@ import numpy as np
 REPO = Path(__file__).resolve().parent
 WORKLOAD = dict(name="plain_425x425x50", nx=425, ny=425, nk=50, seed=0)
 METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0.2 K/day"
+# oracle columns timed for the CPU baseline: 100 rows of the domain, about 2-3 s
+# on 16 host threads (roughly 40 core-seconds of work)
+CPU_SAMPLE_COLUMNS = 42500
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -149,7 +152,7 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    sample = int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", "4250"))
+    sample = int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", str(CPU_SAMPLE_COLUMNS)))
     threads = os.cpu_count() or 1
     times = []
     for _ in range(args.warmup):
@@ -305,7 +308,7 @@ def main():
         "clocks": clocks.summary(),
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", "4250")))
+        v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", str(CPU_SAMPLE_COLUMNS))))
         line["cpu_baseline"] = {"value": v, "unit": "columns/s", "cores": th, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -79,3 +79,17 @@ def test_unsupported_option_raises(rrtmg, pkg):
     kw["rounding_token"] = 1
     with pytest.raises(NotImplementedError):
         rrtmg.rrtmg_lwrad_wrf_columns(**kw)
+
+
+def test_zero_rounding_token_is_a_plain_store(rrtmg, pkg):
+    """The runtime always passes its uint32 token (0 in production)."""
+    from wrf_jax_b200 import synthetic
+    st = synthetic.make_columns(5, 4, 30, seed=9)
+    plain_lw = rrtmg.rrtmg_lwrad_wrf_columns(**st.lw_kwargs())
+    plain_sw = rrtmg.rrtmg_swrad_wrf_columns(**st.sw_kwargs())
+    tok_lw = rrtmg.rrtmg_lwrad_wrf_columns(**st.lw_kwargs(), rounding_token=np.uint32(0))
+    tok_sw = rrtmg.rrtmg_swrad_wrf_columns(**st.sw_kwargs(), rounding_token=np.zeros((), np.uint32))
+    for name in plain_lw._fields:
+        np.testing.assert_array_equal(getattr(tok_lw, name), getattr(plain_lw, name))
+    for name in plain_sw._fields:
+        np.testing.assert_array_equal(getattr(tok_sw, name), getattr(plain_sw, name))

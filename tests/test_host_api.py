@@ -1,0 +1,43 @@
+"""Host-side logic of the Python drop-in that needs no GPU."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+@pytest.mark.parametrize("token", [None, 0, np.uint32(0), np.zeros((3,), np.uint32)])
+def test_zero_rounding_tokens_are_accepted(pkg, token):
+    from wrf_jax_b200 import rrtmg
+    rrtmg._check_rounding_token(token)
+
+
+@pytest.mark.parametrize("token", [1, np.uint32(0x80000000), np.array([0, 2], np.uint32)])
+def test_nonzero_rounding_tokens_are_rejected(pkg, token):
+    from wrf_jax_b200 import rrtmg
+    with pytest.raises(NotImplementedError):
+        rrtmg._check_rounding_token(token)
+
+
+def test_greenhouse_defaults_follow_the_adapters(pkg):
+    from wrf_jax_b200 import rrtmg
+    # all five given: used as is (lw:6610-6630)
+    assert rrtmg._greenhouse(2020, 1, None, 1e-4, 2e-7, 3e-6, 4e-10, 5e-10, lw=True) == (1e-4, 2e-7, 3e-6, 4e-10, 5e-10)
+    # LW with a partial set falls back to the defaults entirely
+    co2, n2o, ch4, f11, f12 = rrtmg._greenhouse(2020, 2, None, 1e-4, None, None, None, None, lw=True)
+    assert co2 == pytest.approx(379.0e-6) and n2o == pytest.approx(319.0e-9)
+    # SW keeps the given scalars and fills the rest (sw:2371-2383)
+    sw = rrtmg._greenhouse(2020, 2, None, 1e-4, None, None, None, None, lw=False)
+    assert sw[0] == 1e-4 and sw[1] == pytest.approx(319.0e-9) and sw[3:] == (0.0, 0.0)
+    # ghg_input == 0: year-dependent CO2
+    co2_0 = rrtmg._greenhouse(2000, 0, None, None, None, None, None, None, lw=True)[0]
+    assert co2_0 == pytest.approx(370.0e-6)
+
+
+def test_product_fails_loudly_without_a_gpu(pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from wrf_jax_b200 import rrtmg
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        rrtmg.RrtmgContext()

@@ -187,6 +187,19 @@ def _check_shapes(d: dict, nx: int, nk: int, ny: int, three: tuple, lev: tuple, 
             raise ValueError(f"{k} must have shape (nx, ny) = {(nx, ny)}, got {tuple(d[k].shape)}")
 
 
+def _check_rounding_token(token) -> None:
+    """The runtime passes a uint32 token that is XORed into every binary32
+    store (core/real_arithmetic.py:12-14, runtime.py:16329 sets it to 0).  A
+    zero token is a plain REAL store, which is what the kernels do; nonzero
+    tokens are diagnostic bit edits and are not supported."""
+    if token is None:
+        return
+    if hasattr(token, "detach"):  # torch tensor
+        token = token.detach().cpu().numpy()
+    if np.any(np.asarray(token).astype(np.uint64) != 0):
+        raise NotImplementedError("nonzero (diagnostic) rounding tokens are not supported")
+
+
 def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, qi3d, qs3d, cldfra3d, o33d,
                             emiss, xland, xice, snow, re_cloud, re_ice, re_snow, p_top, yr, julian,
                             ghg_input=1, case_dir=None, cldovrlp=2, idcor=0, icloud=1, has_reqc=1,
@@ -199,8 +212,7 @@ def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
     import torch
 
     del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables, setcoef_tables
-    if rounding_token is not None:
-        raise NotImplementedError("diagnostic rounding tokens are not supported")
+    _check_rounding_token(rounding_token)
     ctx = context or default_context()
     arrays = dict(p3d=p3d, p8w=p8w, pi3d=pi3d, t3d=t3d, t8w=t8w, tsk=tsk, dz8w=dz8w, qv3d=qv3d, qc3d=qc3d,
                   qi3d=qi3d, qs3d=qs3d, cldfra3d=cldfra3d, o33d=o33d, emiss=emiss, xland=xland, xice=xice,
@@ -243,8 +255,7 @@ def rrtmg_swrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
     import torch
 
     del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables
-    if rounding_token is not None:
-        raise NotImplementedError("diagnostic rounding tokens are not supported")
+    _check_rounding_token(rounding_token)
     if int(sf_surface_physics) == 8 and all(v is not None for v in (alswvisdir, alswvisdif, alswnirdir, alswnirdif)):
         raise NotImplementedError("separate visible/near-IR albedos (sf_surface_physics=8) are not part of this path")
     ctx = context or default_context()
