@@ -105,6 +105,17 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
 rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in,
                          rrtmg_sw_out *out, void *stream);
 
+/* LW with no allocation inside the call; no counterpart in the reference.
+ * Same arguments and results as rrtmg_lwrad, but the McICA scratch lives in
+ * fixed file-scope device arrays (32 MiB of mask words) instead of a per-call
+ * stream-ordered allocation.  Limit: nlay * 5 * nx * ny <= 8,388,608 mask words
+ * (nlay = rrtmg_lw_nlayers(p_top, nk)); larger domains get RRTMG_BAD_ARG.
+ * The first call on each device looks up the scratch's address; make it
+ * before any stream capture begins.  The scratch is shared by all contexts
+ * and streams of a device: calls that overlap in time on one device race. */
+rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_config *cfg,
+                                        const rrtmg_lw_in *in, rrtmg_lw_out *out, void *stream);
+
 /* Number of LW layers used for a model top and level count
  * (rrtmg_lw_nlayers, module_ra_rrtmg_common.py:1243-1247). */
 int rrtmg_lw_nlayers(double p_top, int nk);

@@ -54,7 +54,7 @@ STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "
           4: "RRTMG_TIMEOUT"}
 
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
-           "rrtmg_lw_nlayers", "rrtmg_last_error", "rrtmg_status_string")
+           "rrtmg_lwrad_static_scratch", "rrtmg_lw_nlayers", "rrtmg_last_error", "rrtmg_status_string")
 
 _lib = None
 
@@ -83,6 +83,9 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.rrtmg_swrad.restype = ctypes.c_int
     lib.rrtmg_swrad.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(SwIn),
                                 ctypes.POINTER(SwOut), ctypes.c_void_p]
+    lib.rrtmg_lwrad_static_scratch.restype = ctypes.c_int
+    lib.rrtmg_lwrad_static_scratch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(LwIn),
+                                               ctypes.POINTER(LwOut), ctypes.c_void_p]
     lib.rrtmg_lw_nlayers.restype = ctypes.c_int
     lib.rrtmg_lw_nlayers.argtypes = [ctypes.c_double, ctypes.c_int]
     lib.rrtmg_last_error.restype = ctypes.c_char_p

@@ -585,3 +585,131 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// rrtmg_lwrad_static_scratch: the LW call with its McICA scratch in fixed
+// file-scope device arrays instead of a per-call stream-ordered allocation.
+//
+// Scratch: g_static_mask holds kStaticMaskWords 32-bit words (32 MiB); a call
+// needs nlay * 5 * nx * ny of them and is rejected with RRTMG_BAD_ARG above
+// that.  g_static_jumps holds the 140 KISS jumps for the call's nlay; they are
+// uploaded (a plain copy from a static host table) only when nlay differs from
+// the last upload on that device.  Nothing has to start at zero: the McICA
+// kernel writes every mask word the LW kernel then reads.
+//
+// Set-up: the first call on each device looks up both symbols with that
+// device current (cudaGetSymbolAddress); that first call should come before
+// any stream capture begins.  The scratch is shared by every context and
+// stream on a device, so calls that overlap in time on one device race.
+namespace {
+
+constexpr size_t kStaticMaskWords = size_t(8) << 20;  // 32 MiB of mask words
+constexpr int kStaticMaxDevices = 64;
+
+__device__ __align__(256) uint32_t g_static_mask[kStaticMaskWords];
+__device__ __align__(256) KissJump g_static_jumps[kLwGpts];
+
+struct StaticScratch {
+  bool ready = false;
+  uint32_t *mask = nullptr;
+  KissJump *jumps = nullptr;
+  int loaded_nlay = -1;  // nlay of the jumps last enqueued into g_static_jumps
+};
+
+std::mutex g_static_mutex;
+StaticScratch g_static_scratch[kStaticMaxDevices];
+KissJump g_static_host_jumps[kMaxLay + 1][kLwGpts];  // host copies per nlay (static storage)
+bool g_static_host_built[kMaxLay + 1];
+
+}  // namespace
+
+extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in,
+                                                   rrtmg_lw_out *out, void *stream_ptr) {
+  rrtmg_status st = check_config(ctx, cfg);
+  if (st != RRTMG_OK) return st;
+  if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
+  if (any_null({in->p3d, in->p8w, in->pi3d, in->t3d, in->t8w, in->tsk, in->qv3d, in->qc3d, in->qi3d, in->qs3d,
+                in->cldfra3d, in->o33d, in->emiss, in->xland, in->xice, in->snow, in->re_cloud, in->re_ice,
+                in->re_snow}))
+    return fail(ctx, RRTMG_BAD_ARG, "a required LW input pointer is null");
+  if (any_null({out->rthratenlw, out->rthratenlwc, out->lwupt, out->lwuptc, out->lwuptcln, out->lwdnt, out->lwdntc,
+                out->lwdntcln, out->lwupb, out->lwupbc, out->lwupbcln, out->lwdnb, out->lwdnbc, out->lwdnbcln,
+                out->glw, out->olr, out->lwcf}))
+    return fail(ctx, RRTMG_BAD_ARG, "a required LW output pointer is null");
+  const int nlay = rrtmg_lw_nlayers(cfg->p_top, cfg->nk);
+  if (nlay > kMaxLay || nlay - cfg->nk > kMaxBuf || nlay < cfg->nk)
+    return fail(ctx, RRTMG_BAD_ARG, "too many layers (nk and p_top exceed the kernel's layer capacity)");
+  const int ncol = cfg->nx * cfg->ny;
+  const size_t words = static_cast<size_t>(nlay) * kLwMaskWords * static_cast<size_t>(ncol);
+  if (words > kStaticMaskWords)
+    return fail(ctx, RRTMG_BAD_ARG,
+                "domain too large for the static McICA scratch: needs " + std::to_string(words) +
+                    " mask words (nlay*5*nx*ny), the scratch holds " + std::to_string(kStaticMaskWords) +
+                    "; use rrtmg_lwrad");
+  int inflg, iceflg, liqflg;
+  cloud_flags(cfg, &inflg, &iceflg, &liqflg);
+  const int icld = cfg->cldovrlp;
+  if (icld >= 1 && (inflg < 2 || iceflg < 3 || liqflg != 1))
+    return fail(ctx, RRTMG_UNSUPPORTED_OPTION, "cloud optics option not supported by cldprmc_lw");
+  if (ctx->device < 0 || ctx->device >= kStaticMaxDevices)
+    return fail(ctx, RRTMG_BAD_ARG, "device ordinal beyond the static scratch's device slots");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+
+  uint32_t *mask = nullptr;
+  KissJump *jumps = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_static_mutex);
+    StaticScratch &s = g_static_scratch[ctx->device];
+    if (!s.ready) {  // once per device, with that device current
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_static_mask);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(static mcica mask)");
+      s.mask = static_cast<uint32_t *>(p);
+      e = cudaGetSymbolAddress(&p, g_static_jumps);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(static jump table)");
+      s.jumps = static_cast<KissJump *>(p);
+      s.ready = true;
+    }
+    if (!g_static_host_built[nlay]) {
+      for (int g = 0; g < kLwGpts; ++g)
+        g_static_host_jumps[nlay][g] = make_jump(150ull + static_cast<uint64_t>(g) * nlay);
+      g_static_host_built[nlay] = true;
+    }
+    if (s.loaded_nlay != nlay) {
+      s.loaded_nlay = -1;
+      e = cudaMemcpyAsync(s.jumps, g_static_host_jumps[nlay], sizeof(KissJump) * kLwGpts, cudaMemcpyHostToDevice,
+                          stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(static jump table)");
+      s.loaded_nlay = nlay;
+    }
+    mask = s.mask;
+    jumps = s.jumps;
+  }
+
+  McicaArgs m{};
+  m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kLwGpts; m.words = kLwMaskWords;
+  m.enabled = icld >= 1;
+  m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
+  e = launch_mcica(m, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "mcica kernel launch");
+  LwArgs a{};
+  a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
+  a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.cfc11 = cfg->cfc11vmr; a.cfc12 = cfg->cfc12vmr;
+  a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
+  a.icld = icld; a.inflg = inflg; a.iceflg = iceflg; a.liqflg = liqflg;
+  a.in = common_inputs(in->p3d, in->p8w, in->pi3d, in->t3d, in->t8w, in->tsk, in->qv3d, in->qc3d, in->qi3d,
+                       in->qs3d, in->cldfra3d, in->o33d, in->xland, in->xice, in->snow, in->re_cloud, in->re_ice,
+                       in->re_snow);
+  a.in.emiss = in->emiss;
+  a.mask = mask;
+  a.rthraten = out->rthratenlw; a.rthratenc = out->rthratenlwc;
+  a.upt = out->lwupt; a.uptc = out->lwuptc; a.dnt = out->lwdnt; a.dntc = out->lwdntc;
+  a.upb = out->lwupb; a.upbc = out->lwupbc; a.dnb = out->lwdnb; a.dnbc = out->lwdnbc;
+  a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
+  a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
+  e = launch_lw(ctx->tables, a, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
+  return RRTMG_OK;
+}
