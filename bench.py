@@ -303,7 +303,7 @@ def main():
                      "peak_source": peak_kind,
                      "note": "fused per-column kernel: compulsory HBM bytes / time; the kernel is "
                              "FP32-issue bound, see profiles/"},
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": 5 * args.steps,  # LW: McICA, band groups, finish; SW: McICA, columns
         "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
     }

@@ -40,6 +40,8 @@ struct rrtmg_ctx {
   std::string last_error;
   // KISS jump tables keyed by (nlay, nsub, skip); never freed before destroy
   std::map<std::tuple<int, int, int>, KissJump *> jumps;
+  // stream-ordered per-call scratch; keeps its memory between calls
+  cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -359,6 +361,21 @@ rrtmg_status finish_create(rrtmg_ctx *ctx, int device, rrtmg_ctx **out) {
     delete ctx;
     return fail(nullptr, RRTMG_BAD_ARG, err);
   }
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  e = cudaMemPoolCreate(&ctx->pool, &props);
+  if (e == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  if (e != cudaSuccess) {
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    cudaFree(ctx->dev_blob);
+    delete ctx;
+    return cuda_fail(nullptr, e, "cudaMemPoolCreate(scratch pool)");
+  }
   *out = ctx;
   return RRTMG_OK;
 }
@@ -435,6 +452,7 @@ void rrtmg_destroy(rrtmg_ctx *ctx) {
   cudaDeviceSynchronize();
   for (auto &kv : ctx->jumps) cudaFree(kv.second);
   cudaFree(ctx->dev_blob);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   cudaSetDevice(prev);
   delete ctx;
 }
@@ -484,9 +502,16 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   st = get_jumps(ctx, nlay, kLwGpts, 150, &jumps);
   if (st != RRTMG_OK) return st;
   uint32_t *mask = nullptr;
+  float *terms = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
-  e = cudaMallocAsync(reinterpret_cast<void **>(&mask), mask_bytes, stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocAsync(mcica mask)");
+  const size_t terms_bytes = lw_terms_floats(cfg->nk, ncol) * sizeof(float);
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&terms), terms_bytes, ctx->pool, stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(mask, stream);
+    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw band terms)");
+  }
 
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kLwGpts; m.words = kLwMaskWords;
@@ -494,6 +519,7 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
   if (e != cudaSuccess) {
+    cudaFreeAsync(terms, stream);
     cudaFreeAsync(mask, stream);
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
@@ -512,10 +538,13 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   a.upb = out->lwupb; a.upbc = out->lwupbc; a.dnb = out->lwdnb; a.dnbc = out->lwdnbc;
   a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
   a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
-  e = launch_lw(ctx->tables, a, stream);
-  cudaError_t ef = cudaFreeAsync(mask, stream);
+  a.terms = terms;
+  e = launch_lw_split(ctx->tables, a, stream);
+  cudaError_t ef = cudaFreeAsync(terms, stream);
+  cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
-  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(mcica mask)");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(lw band terms)");
+  if (ef2 != cudaSuccess) return cuda_fail(ctx, ef2, "cudaFreeAsync(mcica mask)");
   return RRTMG_OK;
 }
 
@@ -549,8 +578,8 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   if (st != RRTMG_OK) return st;
   uint32_t *mask = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kSwMaskWords * ncol * sizeof(uint32_t);
-  e = cudaMallocAsync(reinterpret_cast<void **>(&mask), mask_bytes, stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocAsync(mcica mask)");
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kSwGpts; m.words = kSwMaskWords;
   m.enabled = icld >= 1;

@@ -32,6 +32,7 @@ struct LwArgs {
   float *rthraten, *rthratenc;
   float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc, *glw, *olr, *lwcf;
   float *zero2[4];  // *cln fields, written as zeros
+  float *terms;     // band-group schedule scratch, lw_terms_floats(nk, ncol) floats
 };
 
 struct SwArgs {
@@ -48,7 +49,11 @@ struct SwArgs {
 };
 
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
+// fused schedule (one thread per column, no scratch)
 cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream);
+// band-group schedule (thread per column and band group) + finish kernel; needs a.terms
+size_t lw_terms_floats(int nk, int ncol);
+cudaError_t launch_lw_split(const Tables &T, const LwArgs &a, cudaStream_t stream);
 cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
 }  // namespace rrtmg

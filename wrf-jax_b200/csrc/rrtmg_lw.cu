@@ -156,7 +156,7 @@ __device__ void column_setup(const Tables &T, const LwArgs &a, Col &C) {
 }
 
 // Layer coefficients: inatm (lw:953-1035), cloud paths, setcoef (lw:1175-1441).
-__device__ Layer make_layer(const Tables &T, const LwArgs &a, const Col &C, int l) {
+__device__ __forceinline__ Layer make_layer(const Tables &T, const LwArgs &a, const Col &C, int l) {
   Layer L;
   L.pavel = play_at(a, C, l);
   L.tavel = tlay_at(a, C, l);
@@ -917,10 +917,11 @@ __device__ __forceinline__ float planck(const Tables &T, int ind, float frac, in
 
 // One band of one layer in a sweep.  kDown: downward sweep (radiances radA =
 // radld, radB = radclrd); otherwise upward (radA = radlu, radB = radclru).
+// Returns the band's g-ordered radiance sums of the new level.
 template <int B, bool kDown>
-__device__ __forceinline__ void band_step(const Tables &T, const Layer &L, const uint32_t *mask, bool cloudy_layer,
+__device__ __forceinline__ void band_sums(const Tables &T, const Layer &L, const uint32_t *mask, bool cloudy_layer,
                                           int iceflag, float secdiff, float *radA, float *radB, bool sep_clear,
-                                          float &total, float &totalc) {
+                                          float &bandsum, float &bandsumc) {
   constexpr int ngc = kNgc[B];
   constexpr int gofs = kGofs[B];
   float taug[ngc], fracs[ngc];
@@ -933,7 +934,8 @@ __device__ __forceinline__ void band_step(const Tables &T, const Layer &L, const
   if (cloudy_layer) {
     tauc = cloud_tau(T, L, B, iceflag, active);
   }
-  float bandsum = 0.0f, bandsumc = 0.0f;
+  bandsum = 0.0f;
+  bandsumc = 0.0f;
 #pragma unroll
   for (int g = 0; g < ngc; ++g) {
     const int G = gofs + g;
@@ -978,6 +980,14 @@ __device__ __forceinline__ void band_step(const Tables &T, const Layer &L, const
       bandsumc = bandsumc + rcn;
     }
   }
+}
+
+template <int B, bool kDown>
+__device__ __forceinline__ void band_step(const Tables &T, const Layer &L, const uint32_t *mask, bool cloudy_layer,
+                                          int iceflag, float secdiff, float *radA, float *radB, bool sep_clear,
+                                          float &total, float &totalc) {
+  float bandsum, bandsumc;
+  band_sums<B, kDown>(T, L, mask, cloudy_layer, iceflag, secdiff, radA, radB, sep_clear, bandsum, bandsumc);
   total = total + (bandsum * 0.5f) * kDelwave[B];
   totalc = totalc + (bandsumc * 0.5f) * kDelwave[B];
 }
@@ -1007,13 +1017,14 @@ __device__ __forceinline__ void all_bands(const Tables &T, const Layer &L, const
 // Surface: rad0 = fracs(layer 0) * plankbnd, reflected downward radiance
 // (lw:5648-5655); returns the level-0 upward flux sums.
 template <int B>
-__device__ __forceinline__ void surface_band(const Tables &T, const Layer &L0, float plankbnd, float reflect,
-                                             float *radA, float *radB, float &total, float &totalc) {
+__device__ __forceinline__ void surface_sums(const Tables &T, const Layer &L0, float plankbnd, float reflect,
+                                             float *radA, float *radB, float &bandsum, float &bandsumc) {
   constexpr int ngc = kNgc[B];
   constexpr int gofs = kGofs[B];
   float taug[ngc], fracs[ngc];
   taumol<B>(T, L0, taug, fracs);
-  float bandsum = 0.0f, bandsumc = 0.0f;
+  bandsum = 0.0f;
+  bandsumc = 0.0f;
 #pragma unroll
   for (int g = 0; g < ngc; ++g) {
     const int G = gofs + g;
@@ -1025,14 +1036,21 @@ __device__ __forceinline__ void surface_band(const Tables &T, const Layer &L0, f
     bandsum = bandsum + lu;
     bandsumc = bandsumc + lc;
   }
+}
+
+template <int B>
+__device__ __forceinline__ void surface_band(const Tables &T, const Layer &L0, float plankbnd, float reflect,
+                                             float *radA, float *radB, float &total, float &totalc) {
+  float bandsum, bandsumc;
+  surface_sums<B>(T, L0, plankbnd, reflect, radA, radB, bandsum, bandsumc);
   total = total + (bandsum * 0.5f) * kDelwave[B];
   totalc = totalc + (bandsumc * 0.5f) * kDelwave[B];
 }
 
-__global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.ncol) return;
-  Col C;
+// Column prologue of both schedules: buffer layers, laytrop, pwvcm, the band
+// diffusivities (lw:5520-5539) and whether any layer is cloudy.
+__device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a, int col, Col &C, float *secdiff,
+                                                bool &has_cloud) {
   C.i = col / a.ny;
   C.j = col - C.i * a.ny;
   C.nk = a.nk;
@@ -1070,7 +1088,6 @@ __global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
     const float wvsh = (amw * wvttl) / (amd * amttl);
     C.pwvcm = (wvsh * (1.0e3f * plev_at(a, C, 0))) / (1.0e2f * grav);
   }
-  float secdiff[kLwBands];
 #pragma unroll
   for (int b = 0; b < kLwBands; ++b) {
     const bool variable = !(b == 0 || b == 3 || b >= 9);
@@ -1084,13 +1101,23 @@ __global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
   }
 
   // cloudy layers and whether any layer is cloudy (lw:5566-5567, 5656)
-  bool has_cloud = false;
+  has_cloud = false;
   for (int l = 0; l < nlay; ++l) {
     uint32_t any = 0;
 #pragma unroll
     for (int w = 0; w < kLwMaskWords; ++w) any |= a.mask[(static_cast<size_t>(l) * kLwMaskWords + w) * a.ncol + col];
     has_cloud |= any != 0u;
   }
+}
+
+__global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.ncol) return;
+  Col C;
+  float secdiff[kLwBands];
+  bool has_cloud;
+  column_prologue(T, a, col, C, secdiff, has_cloud);
+  const int nlay = C.nlay;
 
   float radA[kLwGpts], radB[kLwGpts];
   float dfl[kMaxLay + 1], dflc[kMaxLay + 1];
@@ -1181,12 +1208,205 @@ __global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
   for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
 }
 
+// ---------------------------------------------------------------------------
+// Band-group schedule.  Thread (column, group) sweeps its column for the bands
+// of one group only, so the group's <= 16 g-point radiances stay in registers
+// and a CTA runs the gas optics of one group.  Each band's level term
+// (bandsum * 0.5) * delwave (lw:170-199) goes to a scratch array; the finish
+// kernel adds the 16 terms of a level in band order, which is the reference's
+// sum, then forms fluxes and heating rates.
+// ---------------------------------------------------------------------------
+
+// Scratch index of a band term: type 0/1 upward total/clear, 2/3 downward
+// total/clear; slot = flux level 0..nk, or nk + 1 for the top of the
+// atmosphere (level nlay) when nlay > nk.
+__device__ __forceinline__ size_t term_index(const LwArgs &a, int type, int slot, int band, int col) {
+  return ((static_cast<size_t>(type) * (a.nk + 2) + slot) * kLwBands + band) * a.ncol + col;
+}
+
+template <int B>
+__device__ __forceinline__ void zero_band(float *radA, float *radB) {
+  constexpr int ngc = kNgc[B];
+  constexpr int gofs = kGofs[B];
+#pragma unroll
+  for (int g = 0; g < ngc; ++g) {
+    radA[gofs + g] = 0.0f;
+    radB[gofs + g] = 0.0f;
+  }
+}
+
+template <int B, bool kDown>
+__device__ __forceinline__ void band_term(const Tables &T, const LwArgs &a, const Layer &L, const uint32_t *mask,
+                                          bool cloudy, int iceflag, const float *secdiff, float *radA, float *radB,
+                                          bool sep, int type, int slot, int col) {
+  float bs, bsc;
+  band_sums<B, kDown>(T, L, mask, cloudy, iceflag, secdiff[B], radA, radB, sep, bs, bsc);
+  if (slot >= 0) {
+    a.terms[term_index(a, type, slot, B, col)] = (bs * 0.5f) * kDelwave[B];
+    a.terms[term_index(a, type + 1, slot, B, col)] = (bsc * 0.5f) * kDelwave[B];
+  }
+}
+
+template <int B>
+__device__ __forceinline__ void surface_term(const Tables &T, const LwArgs &a, const Layer &L0, const Col &C,
+                                             int indbound, float tbndfrac, float reflect, float *radA, float *radB,
+                                             int col) {
+  float bs, bsc;
+  surface_sums<B>(T, L0, C.semiss * planck(T, indbound, tbndfrac, B), reflect, radA, radB, bs, bsc);
+  a.terms[term_index(a, 0, 0, B, col)] = (bs * 0.5f) * kDelwave[B];
+  a.terms[term_index(a, 1, 0, B, col)] = (bsc * 0.5f) * kDelwave[B];
+}
+
+__device__ __forceinline__ bool load_mask(const LwArgs &a, int l, int col, uint32_t *mask) {
+  uint32_t any = 0;
+#pragma unroll
+  for (int w = 0; w < kLwMaskWords; ++w) {
+    mask[w] = a.mask[(static_cast<size_t>(l) * kLwMaskWords + w) * a.ncol + col];
+    any |= mask[w];
+  }
+  return any != 0u;
+}
+
+template <int... Bs>
+__device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int col) {
+  Col C;
+  float secdiff[kLwBands];
+  bool has_cloud;
+  column_prologue(T, a, col, C, secdiff, has_cloud);
+  const int nlay = C.nlay, nk = C.nk;
+  float radA[kLwGpts], radB[kLwGpts];
+  (zero_band<Bs>(radA, radB), ...);
+
+  // downward sweep, top to bottom: level l gets the downward terms
+  bool iclddn = false;
+  for (int l = nlay - 1; l >= 0; --l) {
+    uint32_t mask[kLwMaskWords];
+    const bool cloudy = load_mask(a, l, col, mask);
+    iclddn = iclddn || cloudy;
+    const Layer L = make_layer(T, a, C, l);
+    const int slot = l <= nk ? l : -1;
+    (band_term<Bs, true>(T, a, L, mask, cloudy, C.iceflg, secdiff, radA, radB, iclddn, 2, slot, col), ...);
+  }
+  // surface emission and reflection: level 0 upward terms
+  {
+    const Layer L0 = make_layer(T, a, C, 0);
+    const float bt = C.tsfc - 159.0f;
+    const int indbound = clampi(static_cast<int>(bt), 1, 180);
+    const float tbndfrac = bt - static_cast<float>(indbound);
+    const float reflect = 1.0f - C.semiss;
+    (surface_term<Bs>(T, a, L0, C, indbound, tbndfrac, reflect, radA, radB, col), ...);
+  }
+  // upward sweep, bottom to top: level l + 1 gets the upward terms
+  for (int l = 0; l < nlay; ++l) {
+    uint32_t mask[kLwMaskWords];
+    const bool cloudy = load_mask(a, l, col, mask);
+    const Layer L = make_layer(T, a, C, l);
+    const int lev = l + 1;
+    const int slot = lev <= nk ? lev : (lev == nlay ? nk + 1 : -1);
+    (band_term<Bs, false>(T, a, L, mask, cloudy, C.iceflg, secdiff, radA, radB, has_cloud, 0, slot, col), ...);
+  }
+}
+
+// Groups of whole bands with at most 16 g-points each (140 in total).
+constexpr int kLwGroups = 9;
+
+__global__ void __launch_bounds__(128, 3) lw_group_kernel(Tables T, LwArgs a) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.ncol) return;
+  switch (blockIdx.y) {
+    case 0: lw_group<2>(T, a, col); break;
+    case 1: lw_group<4>(T, a, col); break;
+    case 2: lw_group<3, 13>(T, a, col); break;
+    case 3: lw_group<1, 12>(T, a, col); break;
+    case 4: lw_group<0, 9>(T, a, col); break;
+    case 5: lw_group<5, 7>(T, a, col); break;
+    case 6: lw_group<6, 14, 15>(T, a, col); break;
+    case 7: lw_group<8>(T, a, col); break;
+    default: lw_group<10, 11>(T, a, col); break;
+  }
+}
+
+// Ordered band sums of every level, fluxes, heating rates (lw:5702-5712,
+// 7040-7057) and the 2-D outputs (lw:7059-7077).
+__global__ void __launch_bounds__(128) lw_finish_kernel(LwArgs a) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.ncol) return;
+  const int i = col / a.ny, j = col - i * a.ny;
+  const int nk = a.nk, nlay = a.nlay;
+  const float pi = 3.1415926535897932384626433832795f;
+  const float fluxfac = pi * 2.0e4f;
+  const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
+  auto level = [&](int type, int slot) {
+    float total = 0.0f;
+#pragma unroll
+    for (int b = 0; b < kLwBands; ++b) total = total + a.terms[term_index(a, type, slot, b, col)];
+    return total * fluxfac;
+  };
+  const int top = nlay == nk ? nk : nk + 1;
+  float ufl0 = level(0, 0), uflc0 = level(1, 0), dfl0 = level(2, 0), dflc0 = level(3, 0);
+  const float upb = ufl0, upbc = uflc0, dnb = dfl0, dnbc = dflc0;
+  const size_t rbase = static_cast<size_t>(i) * nk * a.ny + j;
+  const size_t wbase = static_cast<size_t>(i) * (nk + 1) * a.ny + j;
+  for (int l = 0; l < nk; ++l) {
+    const int lev = l + 1;
+    const float ufl1 = level(0, lev), uflc1 = level(1, lev);
+    float dfl1, dflc1;
+    if (lev == nlay) {
+      dfl1 = 0.0f * fluxfac;
+      dflc1 = 0.0f * fluxfac;
+    } else {
+      dfl1 = level(2, lev);
+      dflc1 = level(3, lev);
+    }
+    const float fnet0 = ufl0 - dfl0, fnet1 = ufl1 - dfl1;
+    const float fnetc0 = uflc0 - dflc0, fnetc1 = uflc1 - dflc1;
+    const float plev0 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l) * a.ny));
+    const float plev1 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l + 1) * a.ny));
+    const float dp = plev0 - plev1;
+    const float htr = heatfac * (fnet0 - fnet1) / dp;
+    const float htrc = heatfac * (fnetc0 - fnetc1) / dp;
+    const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * a.ny);
+    a.rthraten[rbase + static_cast<size_t>(l) * a.ny] = (htr / 86400.0f) / pi3d;
+    a.rthratenc[rbase + static_cast<size_t>(l) * a.ny] = (htrc / 86400.0f) / pi3d;
+    ufl0 = ufl1; uflc0 = uflc1; dfl0 = dfl1; dflc0 = dflc1;
+  }
+  const float uflt = level(0, top), ufltc = level(1, top);
+  const float dflt = 0.0f * fluxfac;
+  a.upt[col] = uflt;
+  a.uptc[col] = ufltc;
+  a.dnt[col] = dflt;
+  a.dntc[col] = dflt;
+  a.upb[col] = upb;
+  a.upbc[col] = upbc;
+  a.dnb[col] = dnb;
+  a.dnbc[col] = dnbc;
+  a.glw[col] = dnb;
+  a.olr[col] = uflt;
+  a.lwcf[col] = ufltc - uflt;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
+}
+
 }  // namespace
 
 cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
   const int blocks = (a.ncol + threads - 1) / threads;
   lw_kernel<<<blocks, threads, 0, stream>>>(T, a);
+  return cudaGetLastError();
+}
+
+size_t lw_terms_floats(int nk, int ncol) {
+  return static_cast<size_t>(4) * (nk + 2) * kLwBands * static_cast<size_t>(ncol);
+}
+
+cudaError_t launch_lw_split(const Tables &T, const LwArgs &a, cudaStream_t stream) {
+  const int threads = 128;
+  const int blocks = (a.ncol + threads - 1) / threads;
+  lw_group_kernel<<<dim3(blocks, kLwGroups), threads, 0, stream>>>(T, a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  lw_finish_kernel<<<blocks, threads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
