@@ -577,15 +577,23 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   st = get_jumps(ctx, nlay, kSwGpts, 1, &jumps);
   if (st != RRTMG_OK) return st;
   uint32_t *mask = nullptr;
+  int *daylist = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kSwMaskWords * ncol * sizeof(uint32_t);
   e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&daylist), (static_cast<size_t>(ncol) + 1) * sizeof(int),
+                              ctx->pool, stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(mask, stream);
+    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(day list)");
+  }
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kSwGpts; m.words = kSwMaskWords;
   m.enabled = icld >= 1;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
   if (e != cudaSuccess) {
+    cudaFreeAsync(daylist, stream);
     cudaFreeAsync(mask, stream);
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
@@ -606,10 +614,14 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   a.swcf = out->swcf; a.gsw = out->gsw; a.swddir = out->swddir; a.swddni = out->swddni; a.swddif = out->swddif;
   a.swdownc = out->swdownc; a.swddnic = out->swddnic; a.swddirc = out->swddirc; a.coszr_out = out->coszr;
   a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
+  a.nday = daylist + ncol;
+  a.daylist = daylist;
   e = launch_sw(ctx->tables, a, stream);
-  cudaError_t ef = cudaFreeAsync(mask, stream);
+  cudaError_t ef = cudaFreeAsync(daylist, stream);
+  cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sw kernel launch");
-  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(mcica mask)");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(day list)");
+  if (ef2 != cudaSuccess) return cuda_fail(ctx, ef2, "cudaFreeAsync(mcica mask)");
   return RRTMG_OK;
 }
 

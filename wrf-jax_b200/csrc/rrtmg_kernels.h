@@ -46,6 +46,8 @@ struct SwArgs {
   float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc;
   float *swcf, *gsw, *swddir, *swddni, *swddif, *swdownc, *swddnic, *swddirc, *coszr_out;
   float *zero2[4];
+  int *nday;     // scratch: number of day columns (set by the compaction kernel)
+  int *daylist;  // scratch: ncol entries, day column indices
 };
 
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
@@ -54,6 +56,7 @@ cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream);
 // band-group schedule (thread per column and band group) + finish kernel; needs a.terms
 size_t lw_terms_floats(int nk, int ncol);
 cudaError_t launch_lw_split(const Tables &T, const LwArgs &a, cudaStream_t stream);
+// day-column compaction + column kernel; needs a.nday and a.daylist (1 + ncol ints)
 cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
 }  // namespace rrtmg

@@ -795,9 +795,44 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
   }
 }
 
-__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
+// Day-column compaction: a warp ballots its columns' coszr > 0 and appends the
+// day columns to a.daylist (one atomic per warp, ascending within a warp); the
+// night columns' outputs (sw:2536-2557 masks them to zero) and every column's
+// coszr / *cln outputs are written here.
+__global__ void __launch_bounds__(256) sw_daylist_kernel(SwArgs a) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.ncol) return;
+  const int lane = threadIdx.x & 31;
+  const bool inside = col < a.ncol;
+  const float coszen = inside ? ld(a.in.coszr + col) : 0.0f;
+  const bool day = coszen > 0.0f;
+  const unsigned ballot = __ballot_sync(0xffffffffu, inside && day);
+  int base = 0;
+  if (lane == 0 && ballot) base = atomicAdd(a.nday, __popc(ballot));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (!inside) return;
+  a.coszr_out[col] = coszen;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
+  if (day) {
+    a.daylist[base + __popc(ballot & ((1u << lane) - 1u))] = col;
+    return;
+  }
+  const int i = col / a.ny, j = col - i * a.ny;
+  const size_t rbase = static_cast<size_t>(i) * a.nk * a.ny + j;
+  for (int k = 0; k < a.nk; ++k) {
+    a.rthraten[rbase + static_cast<size_t>(k) * a.ny] = 0.0f;
+    a.rthratenc[rbase + static_cast<size_t>(k) * a.ny] = 0.0f;
+  }
+  a.upt[col] = 0.0f; a.uptc[col] = 0.0f; a.dnt[col] = 0.0f; a.dntc[col] = 0.0f;
+  a.upb[col] = 0.0f; a.upbc[col] = 0.0f; a.dnb[col] = 0.0f; a.dnbc[col] = 0.0f;
+  a.swcf[col] = 0.0f; a.gsw[col] = 0.0f; a.swddir[col] = 0.0f; a.swddni[col] = 0.0f;
+  a.swddif[col] = 0.0f; a.swdownc[col] = 0.0f; a.swddnic[col] = 0.0f; a.swddirc[col] = 0.0f;
+}
+
+__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *a.nday) return;
+  const int col = a.daylist[t];
   Col C;
   C.i = col / a.ny;
   C.j = col - C.i * a.ny;
@@ -807,20 +842,6 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
   const int nk = C.nk, n = C.nlay;
   const float coszen = ld(a.in.coszr + col);
   const size_t rbase = static_cast<size_t>(C.i) * nk * C.ny + C.j;
-  a.coszr_out[col] = coszen;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
-  if (!(coszen > 0.0f)) {
-    for (int k = 0; k < nk; ++k) {
-      a.rthraten[rbase + static_cast<size_t>(k) * C.ny] = 0.0f;
-      a.rthratenc[rbase + static_cast<size_t>(k) * C.ny] = 0.0f;
-    }
-    a.upt[col] = 0.0f; a.uptc[col] = 0.0f; a.dnt[col] = 0.0f; a.dntc[col] = 0.0f;
-    a.upb[col] = 0.0f; a.upbc[col] = 0.0f; a.dnb[col] = 0.0f; a.dnbc[col] = 0.0f;
-    a.swcf[col] = 0.0f; a.gsw[col] = 0.0f; a.swddir[col] = 0.0f; a.swddni[col] = 0.0f;
-    a.swddif[col] = 0.0f; a.swdownc[col] = 0.0f; a.swddnic[col] = 0.0f; a.swddirc[col] = 0.0f;
-    return;
-  }
   C.coszen = coszen;
   C.mu = fmaxf(coszen, 1.0e-10f);
   C.albedo = ld(a.in.albedo + col);
@@ -903,6 +924,11 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
 }  // namespace
 
 cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(a.nday, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  sw_daylist_kernel<<<(a.ncol + 255) / 256, 256, 0, stream>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   const int threads = 128;
   const int blocks = (a.ncol + threads - 1) / threads;
   sw_kernel<<<blocks, threads, 0, stream>>>(T, a);
