@@ -20,6 +20,7 @@ host cores, on a bounded sample of the same workload per step.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import importlib.util
 import json
 import os
@@ -37,6 +38,12 @@ METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0
 # oracle columns timed for the CPU baseline: 100 rows of the domain, about 2-3 s
 # on 16 host threads (roughly 40 core-seconds of work)
 CPU_SAMPLE_COLUMNS = 42500
+# DRAM traffic per unit of the dominant kernels, from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch on the 256x256x50 case divided by its
+# units): sw_kernel 51.76 GB over 45,794 day columns, lw_group_kernel 5.22 GB
+# over 65,536 columns
+DRAM_BYTES_PER_DAY_COLUMN_SW = 1130231
+DRAM_BYTES_PER_COLUMN_LW = 79576
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -231,6 +238,8 @@ def main():
     for _ in range(max(3, args.warmup)):
         step()
     barrier()
+    # per-launch CUDA events recorded by the library on the launching stream
+    ctx.check(ctx.lib.rrtmg_timing_enable(ctx.handle, 1))
     # per-call timing (events on the launching stream)
     with ClockSampler(local) as clocks:
         barrier()
@@ -254,6 +263,16 @@ def main():
     elapsed = t0.elapsed_time(t1) / 1e3
     lw_t = statistics.median(a.elapsed_time(b) for a, b in lw_ms) / 1e3
     sw_t = statistics.median(a.elapsed_time(b) for a, b in sw_ms) / 1e3
+    launch_ms = {}
+    for side, names in ((0, ("mcica_mask_kernel (LW)", "lw_group_kernel", "lw_finish_kernel")),
+                        (1, ("mcica_mask_kernel (SW)", "sw_daylist_kernel", "sw_kernel"))):
+        buf = (ctypes.c_float * (3 * args.steps))()
+        got = ctx.lib.rrtmg_timing_read(ctx.handle, side, buf, args.steps)
+        if got != args.steps:
+            raise RuntimeError(f"per-launch timing returned {got} calls, expected {args.steps}")
+        for k, name in enumerate(names):
+            launch_ms[name] = statistics.mean(buf[3 * q + k] for q in range(got))
+    ctx.check(ctx.lib.rrtmg_timing_enable(ctx.handle, 0))
     if dist is not None:
         tt = torch.tensor([elapsed], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -281,14 +300,29 @@ def main():
 
     hbm, bf16, peak_kind = _peaks()
     nk = WORKLOAD["nk"]
-    # compulsory HBM bytes per column: LW reads 17 (nx,nk,ny)/(nx,nk+1,ny) fields
-    # and 5 2-D fields, writes 2 3-D + 15 2-D; SW reads 18 3-D-like + 6 2-D, writes 2 3-D + 23 2-D
-    lw_bytes = 4 * (15 * nk + 2 * (nk + 1) + 5 + 2 * nk + 15)
-    sw_bytes = 4 * (15 * nk + 2 * (nk + 1) + 6 + 2 * nk + 23)
-    dom = "lw" if lw_t >= sw_t else "sw"
-    dom_t = lw_t if dom == "lw" else sw_t
-    dom_bytes = (lw_bytes if dom == "lw" else sw_bytes) * ncol
-    achieved = dom_bytes / dom_t / 1e9
+    nlay_sw = nk + 1
+    nday = int((np.asarray(sw_host["coszr"]) > 0.0).sum())
+    # Dominant kernel and its algorithmic HBM bytes per launch.  sw_kernel, per
+    # day column: reads 12 (nx,nk,ny) fields (p3d t3d qv o3 cldfra qc qi qs
+    # re_cloud re_ice re_snow pi3d), 2 level fields (p8w t8w), 5 2-D fields and
+    # the McICA mask (4 words per layer); writes 2 (nx,nk,ny) heating rates and
+    # 16 2-D fields.  lw_group_kernel, per column and band group: reads 13
+    # (nx,nk,ny) fields, 2 level fields, 5 2-D fields and the mask (5 words per
+    # layer), writes its bands' level terms (4 per level and band).
+    dom = max(launch_ms, key=launch_ms.get)
+    if dom == "sw_kernel":
+        units = nday
+        unit_bytes = 4 * (12 * nk + 2 * (nk + 1) + 5 + 4 * nlay_sw + 2 * nk + 16)
+    else:
+        nlay_lw = ctx.lib.rrtmg_lw_nlayers(float(lw_host["p_top"]), nk)
+        units = ncol
+        unit_bytes = 9 * 4 * (13 * nk + 2 * (nk + 1) + 5 + 5 * nlay_lw) + 4 * 4 * (nk + 2) * 16
+    dom_s = launch_ms[dom] / 1e3
+    achieved = units * unit_bytes / dom_s / 1e9
+    # DRAM bytes per unit measured by ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum) on the 256x256x50 case, scaled to this launch
+    traffic_per_unit = {"sw_kernel": DRAM_BYTES_PER_DAY_COLUMN_SW, "lw_group_kernel": DRAM_BYTES_PER_COLUMN_LW}
+    traffic = traffic_per_unit[dom] * units if traffic_per_unit.get(dom) else None
     line = {
         "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
@@ -299,11 +333,13 @@ def main():
                    "l2": "inputs larger than L2 (%.0f MB per step)" % (h2d / 1e6),
                    "lw_ms": lw_t * 1e3, "sw_ms": sw_t * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "kernel": f"{dom}_kernel",
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": dom,
+                     "kernel_ms": launch_ms[dom], "units_per_launch": units, "bytes_per_unit": unit_bytes,
                      "peak_source": peak_kind,
-                     "note": "fused per-column kernel: compulsory HBM bytes / time; the kernel is "
-                             "FP32-issue bound, see profiles/"},
-        "gpu_launches": 5 * args.steps,  # LW: McICA, band groups, finish; SW: McICA, columns
+                     "note": "algorithmic HBM bytes / kernel time (CUDA events around the launch); "
+                             "the column kernels are latency and FP32-issue bound, not HBM bound"},
+        "launch_ms": launch_ms,
+        "gpu_launches": 6 * args.steps,  # LW: McICA, band groups, finish; SW: McICA, day list, columns
         "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
     }

@@ -116,6 +116,16 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
 rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_config *cfg,
                                         const rrtmg_lw_in *in, rrtmg_lw_out *out, void *stream);
 
+/* Per-launch timing; no counterpart in the reference.  While enabled, every
+ * rrtmg_lwrad / rrtmg_swrad call records CUDA events on its stream around its
+ * three kernel launches (LW: McICA masks, band groups, finish; SW: McICA
+ * masks, day-column compaction, column kernel), for up to 256 calls per side.
+ * rrtmg_timing_read waits for the recorded calls and writes, oldest first,
+ * three durations in milliseconds per call to ms[3 * i + k]; side 0 = LW,
+ * 1 = SW.  It returns the number of calls written (at most max_calls), or -1. */
+rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable);
+int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_calls);
+
 /* Number of LW layers used for a model top and level count
  * (rrtmg_lw_nlayers, module_ra_rrtmg_common.py:1243-1247). */
 int rrtmg_lw_nlayers(double p_top, int nk);

@@ -54,7 +54,8 @@ STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "
           4: "RRTMG_TIMEOUT"}
 
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
-           "rrtmg_lwrad_static_scratch", "rrtmg_lw_nlayers", "rrtmg_last_error", "rrtmg_status_string")
+           "rrtmg_lwrad_static_scratch", "rrtmg_timing_enable", "rrtmg_timing_read", "rrtmg_lw_nlayers",
+           "rrtmg_last_error", "rrtmg_status_string")
 
 _lib = None
 
@@ -86,6 +87,10 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.rrtmg_lwrad_static_scratch.restype = ctypes.c_int
     lib.rrtmg_lwrad_static_scratch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(LwIn),
                                                ctypes.POINTER(LwOut), ctypes.c_void_p]
+    lib.rrtmg_timing_enable.restype = ctypes.c_int
+    lib.rrtmg_timing_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.rrtmg_timing_read.restype = ctypes.c_int
+    lib.rrtmg_timing_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
     lib.rrtmg_lw_nlayers.restype = ctypes.c_int
     lib.rrtmg_lw_nlayers.argtypes = [ctypes.c_double, ctypes.c_int]
     lib.rrtmg_last_error.restype = ctypes.c_char_p

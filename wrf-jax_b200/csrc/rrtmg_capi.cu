@@ -42,7 +42,32 @@ struct rrtmg_ctx {
   std::map<std::tuple<int, int, int>, KissJump *> jumps;
   // stream-ordered per-call scratch; keeps its memory between calls
   cudaMemPool_t pool = nullptr;
+  // optional per-launch timing: a ring of calls per side (0 LW, 1 SW), each
+  // with kTimingMarks events recorded around the call's three launches
+  bool timing = false;
+  std::vector<cudaEvent_t> events[2];
+  int timing_next[2] = {0, 0};
+  int timing_count[2] = {0, 0};
 };
+
+namespace {
+constexpr int kTimingSlots = 256;
+constexpr int kTimingMarks = 4;
+
+// Claims the next timing slot of `side`, or -1 when timing is off.
+int timing_slot(rrtmg_ctx *ctx, int side) {
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  if (!ctx->timing) return -1;
+  const int slot = ctx->timing_next[side];
+  ctx->timing_next[side] = (slot + 1) % kTimingSlots;
+  if (ctx->timing_count[side] < kTimingSlots) ++ctx->timing_count[side];
+  return slot;
+}
+
+void timing_mark(rrtmg_ctx *ctx, int side, int slot, int mark, cudaStream_t stream) {
+  if (slot >= 0) cudaEventRecord(ctx->events[side][slot * kTimingMarks + mark], stream);
+}
+}  // namespace
 
 namespace {
 
@@ -453,6 +478,8 @@ void rrtmg_destroy(rrtmg_ctx *ctx) {
   for (auto &kv : ctx->jumps) cudaFree(kv.second);
   cudaFree(ctx->dev_blob);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+  for (auto &side : ctx->events)
+    for (cudaEvent_t ev : side) cudaEventDestroy(ev);
   cudaSetDevice(prev);
   delete ctx;
 }
@@ -513,11 +540,14 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
     return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw band terms)");
   }
 
+  const int tslot = timing_slot(ctx, 0);
+  timing_mark(ctx, 0, tslot, 0, stream);
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kLwGpts; m.words = kLwMaskWords;
   m.enabled = icld >= 1;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
+  timing_mark(ctx, 0, tslot, 1, stream);
   if (e != cudaSuccess) {
     cudaFreeAsync(terms, stream);
     cudaFreeAsync(mask, stream);
@@ -539,7 +569,10 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
   a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
   a.terms = terms;
-  e = launch_lw_split(ctx->tables, a, stream);
+  e = launch_lw_groups(ctx->tables, a, stream);
+  timing_mark(ctx, 0, tslot, 2, stream);
+  if (e == cudaSuccess) e = launch_lw_finish(a, stream);
+  timing_mark(ctx, 0, tslot, 3, stream);
   cudaError_t ef = cudaFreeAsync(terms, stream);
   cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
@@ -587,11 +620,14 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
     cudaFreeAsync(mask, stream);
     return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(day list)");
   }
+  const int tslot = timing_slot(ctx, 1);
+  timing_mark(ctx, 1, tslot, 0, stream);
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kSwGpts; m.words = kSwMaskWords;
   m.enabled = icld >= 1;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
+  timing_mark(ctx, 1, tslot, 1, stream);
   if (e != cudaSuccess) {
     cudaFreeAsync(daylist, stream);
     cudaFreeAsync(mask, stream);
@@ -616,7 +652,10 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
   a.nday = daylist + ncol;
   a.daylist = daylist;
-  e = launch_sw(ctx->tables, a, stream);
+  e = launch_sw_daylist(a, stream);
+  timing_mark(ctx, 1, tslot, 2, stream);
+  if (e == cudaSuccess) e = launch_sw_columns(ctx->tables, a, stream);
+  timing_mark(ctx, 1, tslot, 3, stream);
   cudaError_t ef = cudaFreeAsync(daylist, stream);
   cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sw kernel launch");
@@ -753,4 +792,47 @@ extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_c
   e = launch_lw(ctx->tables, a, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
   return RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable) {
+  if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  if (enable && ctx->events[0].empty()) {
+    for (auto &side : ctx->events) {
+      side.resize(static_cast<size_t>(kTimingSlots) * kTimingMarks);
+      for (cudaEvent_t &ev : side) {
+        e = cudaEventCreate(&ev);
+        if (e != cudaSuccess) {
+          ctx->last_error = std::string("cudaEventCreate: ") + cudaGetErrorString(e);
+          return RRTMG_CUDA;
+        }
+      }
+    }
+  }
+  ctx->timing = enable != 0;
+  ctx->timing_next[0] = ctx->timing_next[1] = 0;
+  ctx->timing_count[0] = ctx->timing_count[1] = 0;
+  return RRTMG_OK;
+}
+
+extern "C" int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_calls) {
+  if (!ctx || side < 0 || side > 1 || !ms || max_calls <= 0) return -1;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return -1;
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  const int count = ctx->timing_count[side] < max_calls ? ctx->timing_count[side] : max_calls;
+  const int newest = (ctx->timing_next[side] + kTimingSlots - 1) % kTimingSlots;
+  for (int q = 0; q < count; ++q) {
+    // oldest of the returned calls first
+    const int slot = (newest - (count - 1 - q) + kTimingSlots) % kTimingSlots;
+    const cudaEvent_t *ev = &ctx->events[side][static_cast<size_t>(slot) * kTimingMarks];
+    if (cudaEventSynchronize(ev[kTimingMarks - 1]) != cudaSuccess) return -1;
+    for (int m = 0; m + 1 < kTimingMarks; ++m) {
+      float t = 0.0f;
+      if (cudaEventElapsedTime(&t, ev[m], ev[m + 1]) != cudaSuccess) return -1;
+      ms[q * (kTimingMarks - 1) + m] = t;
+    }
+  }
+  return count;
 }

@@ -53,10 +53,14 @@ struct SwArgs {
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
 // fused schedule (one thread per column, no scratch)
 cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream);
-// band-group schedule (thread per column and band group) + finish kernel; needs a.terms
+// band-group schedule (thread per column and band group), then the finish
+// kernel (ordered band sums, fluxes, heating); both need a.terms
 size_t lw_terms_floats(int nk, int ncol);
-cudaError_t launch_lw_split(const Tables &T, const LwArgs &a, cudaStream_t stream);
-// day-column compaction + column kernel; needs a.nday and a.daylist (1 + ncol ints)
-cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream);
+cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stream);
+cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream);
+// day-column compaction (writes the night columns), then the column kernel over
+// the day columns; both need a.nday and a.daylist (1 + ncol ints)
+cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);
+cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
 }  // namespace rrtmg

@@ -1400,12 +1400,16 @@ size_t lw_terms_floats(int nk, int ncol) {
   return static_cast<size_t>(4) * (nk + 2) * kLwBands * static_cast<size_t>(ncol);
 }
 
-cudaError_t launch_lw_split(const Tables &T, const LwArgs &a, cudaStream_t stream) {
+cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
   const int blocks = (a.ncol + threads - 1) / threads;
   lw_group_kernel<<<dim3(blocks, kLwGroups), threads, 0, stream>>>(T, a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream) {
+  const int threads = 128;
+  const int blocks = (a.ncol + threads - 1) / threads;
   lw_finish_kernel<<<blocks, threads, 0, stream>>>(a);
   return cudaGetLastError();
 }

@@ -923,12 +923,14 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
 
 }  // namespace
 
-cudaError_t launch_sw(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
   cudaError_t e = cudaMemsetAsync(a.nday, 0, sizeof(int), stream);
   if (e != cudaSuccess) return e;
   sw_daylist_kernel<<<(a.ncol + 255) / 256, 256, 0, stream>>>(a);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream) {
   const int threads = 128;
   const int blocks = (a.ncol + threads - 1) / threads;
   sw_kernel<<<blocks, threads, 0, stream>>>(T, a);
