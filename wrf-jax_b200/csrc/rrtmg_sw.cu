@@ -702,13 +702,25 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
     const float zincflx = ((C.adjflux * sflux[g]) * mu) * 1.0f;
     accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
     acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
+    // thread-local table values of the next layer are loaded one layer ahead
+    float nx_tr = taur[n - 1][g], nx_tg = taug[n - 1][g];
+    float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
+    if (!clear_only) { nx_ct = ctau[n - 1]; nx_cs = cssa[n - 1]; nx_ca = casm[n - 1]; nx_co = ctaor[n - 1]; }
+    uint32_t nx_word = maskbase[(static_cast<size_t>(n - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
     for (int r = 0; r < n; ++r) {
       const int l = n - 1 - r;
-      const uint32_t word = maskbase[(static_cast<size_t>(l) * kSwMaskWords + (G >> 5)) * a.ncol];
+      const uint32_t word = nx_word;
+      const float tr = nx_tr, tg = nx_tg;
+      const float ct = nx_ct, cs = nx_cs, ca = nx_ca, co = nx_co;
+      if (l > 0) {
+        nx_tr = taur[l - 1][g];
+        nx_tg = taug[l - 1][g];
+        if (!clear_only) { nx_ct = ctau[l - 1]; nx_cs = cssa[l - 1]; nx_ca = casm[l - 1]; nx_co = ctaor[l - 1]; }
+        nx_word = maskbase[(static_cast<size_t>(l - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
+      }
       const bool cldb = (word >> (G & 31)) & 1u;
       const float cloud = cldb ? 1.0f : 0.0f;
       const float clear = 1.0f - cloud;
-      const float tr = taur[l][g], tg = taug[l][g];
       const float ztau = (tr + tg) + 0.0f;
       float zom = tr + 0.0f * 1.0f;
       const float zgr = 0.0f * 1.0f * 0.0f / zom;
@@ -727,10 +739,10 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
       Pc.tdbt[r + 1] = Pc.tdbt[r] * dbtc;
       down_step(Pc, r);
       if (!clear_only) {
-        const float tcld = cldb ? ctau[l] : 0.0f;
-        const float wcld = cldb ? cssa[l] : 1.0f;
-        const float gcld = cldb ? casm[l] : 0.0f;
-        const float taor = cldb ? ctaor[l] : 0.0f;
+        const float tcld = cldb ? ct : 0.0f;
+        const float wcld = cldb ? cs : 1.0f;
+        const float gcld = cldb ? ca : 0.0f;
+        const float taor = cldb ? co : 0.0f;
         const float tauorig = ztau + taor;
         const float dbtmo_nd = exp_lookup(T, tauorig / mu);
         const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
@@ -762,35 +774,55 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
     float *accfu = accs, *accfd = accs + kMaxLev, *acccu = accs + 2 * kMaxLev, *acccd = accs + 3 * kMaxLev;
     float rupc = Pc.ref[n], rupdc = Pc.refd[n];
     float rupt = Pt.ref[n], rupdt = Pt.refd[n];
+    // level arrays and accumulators of the next level are loaded one level ahead
+    struct Lvl {
+      float ref, refd, tra, trad, dbt, tdbt, tdn, rdnd;
+    };
+    auto load_lvl = [&](const Path &P, int k) {
+      Lvl v;
+      v.ref = P.ref[k]; v.refd = P.refd[k]; v.tra = P.tra[k]; v.trad = P.trad[k]; v.dbt = P.dbt[k];
+      v.tdbt = P.tdbt[k]; v.tdn = P.tdn[k]; v.rdnd = P.rdnd[k];
+      return v;
+    };
+    Lvl nc = load_lvl(Pc, n), nt = nc;
+    if (!clear_only) nt = load_lvl(Pt, n);
+    float nfu = accfu[n], nfd = accfd[n], ncu = acccu[n], ncd = acccd[n];
     for (int k = n; k >= 0; --k) {
+      const Lvl c = nc, t = nt;
+      const float afu = nfu, afd = nfd, acu = ncu, acd = ncd;
+      if (k > 0) {
+        nc = load_lvl(Pc, k - 1);
+        if (!clear_only) nt = load_lvl(Pt, k - 1);
+        nfu = accfu[k - 1]; nfd = accfd[k - 1]; ncu = acccu[k - 1]; ncd = acccd[k - 1];
+      }
       if (k < n) {
-        const float zrc = 1.0f / (1.0f - rupdc * Pc.refd[k]);
-        const float nrupc = Pc.ref[k] + Pc.trad[k] * ((Pc.tra[k] - Pc.dbt[k]) * rupdc + Pc.dbt[k] * rupc) * zrc;
-        const float nrupdc = Pc.refd[k] + Pc.trad[k] * Pc.trad[k] * rupdc * zrc;
+        const float zrc = 1.0f / (1.0f - rupdc * c.refd);
+        const float nrupc = c.ref + c.trad * ((c.tra - c.dbt) * rupdc + c.dbt * rupc) * zrc;
+        const float nrupdc = c.refd + c.trad * c.trad * rupdc * zrc;
         rupc = nrupc;
         rupdc = nrupdc;
         if (!clear_only) {
-          const float zrt = 1.0f / (1.0f - rupdt * Pt.refd[k]);
-          const float nrupt = Pt.ref[k] + Pt.trad[k] * ((Pt.tra[k] - Pt.dbt[k]) * rupdt + Pt.dbt[k] * rupt) * zrt;
-          const float nrupdt = Pt.refd[k] + Pt.trad[k] * Pt.trad[k] * rupdt * zrt;
+          const float zrt = 1.0f / (1.0f - rupdt * t.refd);
+          const float nrupt = t.ref + t.trad * ((t.tra - t.dbt) * rupdt + t.dbt * rupt) * zrt;
+          const float nrupdt = t.refd + t.trad * t.trad * rupdt * zrt;
           rupt = nrupt;
           rupdt = nrupdt;
         }
       }
       // clear-sky level fluxes
-      const float zrefc = 1.0f / (1.0f - Pc.rdnd[k] * rupdc);
-      const float fuc = (Pc.tdbt[k] * rupc + (Pc.tdn[k] - Pc.tdbt[k]) * rupdc) * zrefc;
-      const float fdc = Pc.tdbt[k] + (Pc.tdn[k] - Pc.tdbt[k] + Pc.tdbt[k] * rupc * Pc.rdnd[k]) * zrefc;
+      const float zrefc = 1.0f / (1.0f - c.rdnd * rupdc);
+      const float fuc = (c.tdbt * rupc + (c.tdn - c.tdbt) * rupdc) * zrefc;
+      const float fdc = c.tdbt + (c.tdn - c.tdbt + c.tdbt * rupc * c.rdnd) * zrefc;
       float fut = fuc, fdt = fdc;
       if (!clear_only) {
-        const float zreft = 1.0f / (1.0f - Pt.rdnd[k] * rupdt);
-        fut = (Pt.tdbt[k] * rupt + (Pt.tdn[k] - Pt.tdbt[k]) * rupdt) * zreft;
-        fdt = Pt.tdbt[k] + (Pt.tdn[k] - Pt.tdbt[k] + Pt.tdbt[k] * rupt * Pt.rdnd[k]) * zreft;
+        const float zreft = 1.0f / (1.0f - t.rdnd * rupdt);
+        fut = (t.tdbt * rupt + (t.tdn - t.tdbt) * rupdt) * zreft;
+        fdt = t.tdbt + (t.tdn - t.tdbt + t.tdbt * rupt * t.rdnd) * zreft;
       }
-      accfu[k] = accfu[k] + fut * zincflx;
-      accfd[k] = accfd[k] + fdt * zincflx;
-      acccu[k] = acccu[k] + fuc * zincflx;
-      acccd[k] = acccd[k] + fdc * zincflx;
+      accfu[k] = afu + fut * zincflx;
+      accfd[k] = afd + fdt * zincflx;
+      acccu[k] = acu + fuc * zincflx;
+      acccd[k] = acd + fdc * zincflx;
     }
   }
 }
