@@ -11,8 +11,8 @@ import pytest
 from conftest import REPO
 
 
-def _declared_symbols():
-    text = (REPO / "include" / "rrtmg_b200.h").read_text()
+def _declared_symbols(header: str = "rrtmg_b200.h"):
+    text = (REPO / "include" / header).read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)  # declarations only, not comments
     return sorted(set(re.findall(r"\b(rrtmg_[a-z_0-9]+)\s*\(", text)))
 
@@ -27,9 +27,10 @@ def test_library_exports_every_declared_symbol(pkg):
     if not _capi.LIB_PATH.exists():
         build.build_library()
     lib = ctypes.CDLL(str(_capi.LIB_PATH))
-    for name in _declared_symbols():
-        assert hasattr(lib, name), name
-    assert set(_capi.EXPORTS) == set(_declared_symbols())
+    for header, exports in (("rrtmg_b200.h", _capi.EXPORTS), ("rrtmg_surrogate.h", _capi.SURROGATE_EXPORTS)):
+        for name in _declared_symbols(header):
+            assert hasattr(lib, name), name
+        assert set(exports) == set(_declared_symbols(header))
 
 
 @pytest.mark.parametrize("p_top,nk", [(5000.0, 44), (5000.0, 50), (1000.0, 30), (2000.0, 24), (0.0, 10)])

@@ -50,12 +50,24 @@ class SwOut(ctypes.Structure):
     _fields_ = [(n, _F) for n in SW_OUT_FIELDS]
 
 
+class GemmArgs(ctypes.Structure):
+    """rrtmg_gemm_args (include/rrtmg_surrogate.h)."""
+    _fields_ = [("A", _F), ("lda", ctypes.c_int), ("B", _F), ("ldb", ctypes.c_int),
+                ("M", ctypes.c_int), ("N", ctypes.c_int), ("K", ctypes.c_int), ("ksplit", ctypes.c_int),
+                ("epilogue", ctypes.c_int), ("bias", _F), ("C", _F), ("ldc", ctypes.c_int),
+                ("split_stride", ctypes.c_size_t), ("H", _F), ("ldh", ctypes.c_int), ("Ht", _F),
+                ("ldht", ctypes.c_int), ("aux", _F), ("ldaux", ctypes.c_int), ("Z", _F), ("ldz", ctypes.c_int)]
+
+
+EPI_F32, EPI_GELU, EPI_DGELU = 0, 1, 2
+
 STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
           4: "RRTMG_TIMEOUT"}
 
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
            "rrtmg_lwrad_static_scratch", "rrtmg_timing_enable", "rrtmg_timing_read", "rrtmg_lw_nlayers",
            "rrtmg_last_error", "rrtmg_status_string")
+SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error")
 
 _lib = None
 
@@ -91,6 +103,10 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.rrtmg_timing_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.rrtmg_timing_read.restype = ctypes.c_int
     lib.rrtmg_timing_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+    lib.rrtmg_gemm_bf16.restype = ctypes.c_int
+    lib.rrtmg_gemm_bf16.argtypes = [ctypes.POINTER(GemmArgs), ctypes.c_void_p]
+    lib.rrtmg_gemm_error.restype = ctypes.c_int
+    lib.rrtmg_gemm_error.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
     lib.rrtmg_lw_nlayers.restype = ctypes.c_int
     lib.rrtmg_lw_nlayers.argtypes = [ctypes.c_double, ctypes.c_int]
     lib.rrtmg_last_error.restype = ctypes.c_char_p

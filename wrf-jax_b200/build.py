@@ -18,8 +18,9 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "librrtmg_b200.so"
-SOURCES = ("rrtmg_capi.cu", "rrtmg_mcica.cu", "rrtmg_lw.cu", "rrtmg_sw.cu")
-HEADERS = ("rrtmg_device.cuh", "rrtmg_kernels.h")
+SOURCES = ("rrtmg_capi.cu", "rrtmg_mcica.cu", "rrtmg_lw.cu", "rrtmg_sw.cu", "surrogate_gemm.cu",
+           "surrogate_capi.cu")
+HEADERS = ("rrtmg_device.cuh", "rrtmg_kernels.h", "surrogate_kernels.h")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
@@ -43,7 +44,8 @@ def _stale(target: Path, deps) -> bool:
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     """Compile the CUDA sources (in parallel) and link librrtmg_b200.so."""
     BUILD.mkdir(exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [HERE.parent / "include" / "rrtmg_b200.h"]
+    headers = [CSRC / h for h in HEADERS] + [HERE.parent / "include" / "rrtmg_b200.h",
+                                             HERE.parent / "include" / "rrtmg_surrogate.h"]
     objs = []
     jobs = []
     for src in SOURCES:

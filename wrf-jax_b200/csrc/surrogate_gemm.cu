@@ -1,0 +1,244 @@
+// BF16 GEMM on the 5th-generation tensor cores (tcgen05) with fused MLP
+// epilogues, for the radiation surrogate's training and inference.
+//
+//   C[M x N] = A[M x K] * B[N x K]^T      (A, B row-major BF16, FP32 accumulate)
+//
+// One CTA of 128 threads owns a 128 x 128 output tile.  Its accumulator lives
+// in tensor memory (128 lanes x 128 FP32 columns).  K advances in blocks of
+// 64: all threads copy the A and B blocks into shared memory (cp.async, two
+// stages) in the no-swizzle K-major core-matrix layout, and one thread issues
+// four tcgen05.mma (K = 16 each) whose completion is committed to the stage's
+// mbarrier, so the copy of block k + 1 overlaps the MMAs of block k.  The
+// epilogue reads the accumulator back with tcgen05.ld (warp w owns lanes
+// 32w..32w+31, i.e. tile rows) and applies one of:
+//   kEpiF32    C (+ bias) as FP32, one slab per K split (split-K partials)
+//   kEpiGelu   Z = acc + bias (FP32), H = GELU(Z) as BF16 row-major and
+//              transposed (the transposed copy feeds the weight gradient)
+//   kEpiDgelu  dZ = acc * GELU'(aux) as BF16 row-major and transposed
+//
+// Shared-memory layout of an operand block (128 rows x 64 K, BF16): the 16-byte
+// chunk (row r, k-chunk kc) sits at kc * 2048 + r * 16, which is the canonical
+// K-major SWIZZLE_NONE layout with leading-byte offset 2048 (next k-chunk) and
+// stride-byte offset 128 (next 8-row group).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "surrogate_kernels.h"
+
+namespace rrtmg {
+namespace {
+
+constexpr int kBM = 128, kBN = 128, kBK = 64;
+constexpr int kThreads = 128;
+constexpr int kStages = 2;
+constexpr int kOperandBytes = kBM * kBK * 2;  // 16 KB
+constexpr int kSmemBytes = 2 * kStages * kOperandBytes;
+constexpr uint32_t kLbo = 2048, kSbo = 128;
+constexpr uint64_t kWaitNs = 2000000000ull;  // bounded mbarrier wait: 2 s
+
+// tcgen05 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B BF16
+// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) | (static_cast<uint32_t>(kBM >> 4) << 24);
+
+__device__ unsigned g_gemm_error;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (start, leading and stride byte offsets in
+// 16-byte units, descriptor version 1, no swizzle).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((kLbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((kSbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  return d;
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the given phase parity of an mbarrier; gives up after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > kWaitNs) return false;
+  }
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + kStages * kOperandBytes;
+  __shared__ __align__(8) uint64_t mbar[kStages];
+  __shared__ uint32_t tmem_sh;
+  __shared__ int fail_sh;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int kper = g.K / g.ksplit;
+  const int kbeg = blockIdx.z * kper;
+  const int nkb = kper / kBK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                 "r"(kBN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fail_sh = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_sh;
+
+  int issued = 0;  // K blocks whose MMAs were issued and committed
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = kb & 1;
+    if (kb >= kStages) {
+      // the MMAs of block kb - 2 read this stage; wait before overwriting it
+      if (tid == 0 && !mbar_wait(smem_u32(&mbar[s]), ((kb - kStages) >> 1) & 1)) fail_sh = 1;
+      __syncthreads();
+      if (fail_sh) break;
+    }
+    const int k0 = kbeg + kb * kBK;
+    uint8_t *a = sA + s * kOperandBytes, *b = sB + s * kOperandBytes;
+#pragma unroll
+    for (int i = 0; i < (kBM * kBK / 8) / kThreads; ++i) {
+      const int q = tid + i * kThreads;
+      const int r = q & (kBM - 1), kc = q >> 7;
+      cp_async16(a + kc * kLbo + r * 16, g.A + static_cast<size_t>(m0 + r) * g.lda + k0 + kc * 8);
+      cp_async16(b + kc * kLbo + r * 16, g.B + static_cast<size_t>(n0 + r) * g.ldb + k0 + kc * 8);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // make the generic-proxy shared-memory writes visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t abase = smem_u32(a), bbase = smem_u32(b);
+#pragma unroll
+      for (int kk = 0; kk < kBK / 16; ++kk) {
+        const uint64_t adesc = smem_desc(abase + kk * 2 * kLbo);
+        const uint64_t bdesc = smem_desc(bbase + kk * 2 * kLbo);
+        const uint32_t accumulate = (kb > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            :
+            : "r"(tmem), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[s]))
+                   : "memory");
+    }
+    issued = kb + 1;
+  }
+  // wait for the last committed group (it covers every earlier MMA)
+  if (issued > 0) {
+    const int last = issued - 1;
+    if (tid == 0 && !mbar_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1)) fail_sh = 1;
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const bool failed = fail_sh != 0 || issued != nkb;
+  if (failed) {
+    if (tid == 0) atomicOr(&g_gemm_error, 1u);
+  } else {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < kBN; c += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + c + j;
+        const float acc = __uint_as_float(v[j]);
+        if (g.epi == kEpiF32) {
+          float out = acc;
+          if (g.bias && blockIdx.z == 0) out += g.bias[n];
+          g.C[static_cast<size_t>(blockIdx.z) * g.split_stride + static_cast<size_t>(row) * g.ldc + n] = out;
+        } else if (g.epi == kEpiGelu) {
+          const float z = acc + (g.bias ? g.bias[n] : 0.0f);
+          const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
+          if (g.Z) g.Z[static_cast<size_t>(row) * g.ldz + n] = z;
+          if (g.H) g.H[static_cast<size_t>(row) * g.ldh + n] = h;
+          if (g.Ht) g.Ht[static_cast<size_t>(n) * g.ldht + row] = h;
+        } else {  // kEpiDgelu
+          const float dz = acc * gelu_grad(g.aux[static_cast<size_t>(row) * g.ldaux + n]);
+          const __nv_bfloat16 h = __float2bfloat16_rn(dz);
+          if (g.H) g.H[static_cast<size_t>(row) * g.ldh + n] = h;
+          if (g.Ht) g.Ht[static_cast<size_t>(n) * g.ldht + row] = h;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_umma_gemm(const GemmArgs &g, cudaStream_t stream) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid(g.M / kBM, g.N / kBN, g.ksplit);
+  umma_gemm_kernel<<<grid, kThreads, kSmemBytes, stream>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t gemm_error_flag(unsigned *out, bool reset) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_gemm_error, sizeof(unsigned));
+  if (e != cudaSuccess || !reset) return e;
+  const unsigned zero = 0;
+  return cudaMemcpyToSymbol(g_gemm_error, &zero, sizeof(unsigned));
+}
+
+}  // namespace rrtmg
