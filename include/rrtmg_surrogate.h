@@ -41,6 +41,103 @@ typedef struct {
 
 rrtmg_status rrtmg_gemm_bf16(const rrtmg_gemm_args *args, void *stream);
 
+/* Features of the columns of one WRF-layout domain (nx * ny = ncol columns,
+ * nk levels) into rows row_offset .. row_offset + ncol - 1.  Per level k, at
+ * f * nk + k: f = 0 t3d, 1 ln p3d, 2 qv, 3 qc, 4 qi, 5 qs, 6 cldfra, 7 o3,
+ * 8 layer thickness p8w[k] - p8w[k+1]; then tsk, albedo, coszr, emiss
+ * (9 nk + 4 features).  raw: FP32 values; X: BF16 (v - mean) * rstd, zero-
+ * padded to ldx; Xt: X transposed; flags[c] = 1 when a value lies outside
+ * [lo, hi] (the training range), else 0.  Every output is optional. */
+typedef struct {
+    int ncol, nk, ny;
+    const float *p3d, *p8w, *t3d, *qv, *qc, *qi, *qs, *cldfra, *o3, *tsk, *albedo, *coszr, *emiss;
+    int row_offset;
+    float *raw; int ldf;
+    const float *mean, *rstd;
+    void *X; int ldx;
+    void *Xt; int ldxt;
+    const float *lo, *hi;
+    unsigned *flags;
+} rrtmg_sur_features_args;
+rrtmg_status rrtmg_sur_features(const rrtmg_sur_features_args *args, void *stream);
+
+/* Training targets from plain RRTMG outputs into rows row_offset..: LW and SW
+ * heating [K/day] = rthraten * 86400 * pi3d per level, glw, lwupb, swdnb,
+ * swupb, then the LW (up - down) and SW (down - up) net fluxes at the model
+ * top implied by the heating profiles (2 nk + 6 values, zero-padded to ldt). */
+typedef struct {
+    int ncol, nk, ny;
+    const float *rthratenlw, *rthratensw, *pi3d, *p8w, *glw, *lwupb, *swdnb, *swupb;
+    int row_offset;
+    float *T; int ldt;
+} rrtmg_sur_targets_args;
+rrtmg_status rrtmg_sur_targets(const rrtmg_sur_targets_args *args, void *stream);
+
+/* Per-column statistics of F[n][ld] for columns 0..nf-1: mean, 1/std (0 for a
+ * constant column), and optionally min and max. */
+rrtmg_status rrtmg_sur_column_stats(const float *F, int n, int ld, int nf, float *mean, float *rstd, float *lo,
+                                    float *hi, void *stream);
+
+/* out[r][f] = (in[r][f] - mean[f]) * rstd[f] for f < nf, zero for nf <= f <
+ * ldo; out is BF16 when out_bf16 != 0, else FP32. */
+rrtmg_status rrtmg_sur_normalize(const float *in, int ldi, int n, int nf, const float *mean, const float *rstd,
+                                 void *out, int ldo, int out_bf16, void *stream);
+
+/* Batch gather: Xb[b] = X[idx[b]] (BF16 [B][ldx]), Xbt = Xb transposed
+ * ([ldx][ldxbt]), Tb[b] = T[idx[b]] (FP32 [B][ldt], optional). */
+rrtmg_status rrtmg_sur_gather(const void *X, int ldx, const float *T, int ldt, const int *idx, int B, void *Xb,
+                              void *Xbt, int ldxbt, float *Tb, void *stream);
+
+/* Weighted MSE gradient: dY = w[f] * 2 (Y - T) * scale as BF16 [B][ld] and
+ * transposed [ld][lddyt]; adds sum w (Y - T)^2 to loss[0] (optional). */
+rrtmg_status rrtmg_sur_loss_grad(const float *Y, const float *T, const float *w, int B, int ld, float scale,
+                                 void *dY, void *dYt, int lddyt, float *loss, void *stream);
+
+/* Bias gradient: db[r] = sum_b Gt[r][b] over a BF16 [rows][ld] matrix. */
+rrtmg_status rrtmg_sur_row_sum(const void *Gt, int ld, int rows, int B, float *db, void *stream);
+
+/* G[i] = sum_z P[z * n + i] (split-K partial sums). */
+rrtmg_status rrtmg_sur_reduce_splits(const float *P, int splits, size_t n, float *G, void *stream);
+
+/* One Adam step on an FP32 master w[rows][cols] with moments m, v:
+ * w -= lr (mhat / (sqrt(vhat) + eps) + weight_decay w), mhat = m / bc1,
+ * vhat = v / bc2; writes the BF16 copy wb [rows][ldwb] and its transpose
+ * wbt [cols][ldwbt] when given. */
+typedef struct {
+    int rows, cols;
+    float *w, *m, *v;
+    const float *grad;
+    float lr, beta1, beta2, eps, bc1, bc2, weight_decay;
+    void *wb; int ldwb;
+    void *wbt; int ldwbt;
+} rrtmg_sur_adam_args;
+rrtmg_status rrtmg_sur_adam(const rrtmg_sur_adam_args *args, void *stream);
+
+/* Network outputs Y[ncol][ldy] (normalized) to WRF fields: rthratenlw/sw
+ * (nx, nk, ny) = hr / 86400 / pi3d, glw, lwupb, swdnb, swupb (nx, ny); SW is
+ * exactly zero where coszr <= 0.  Energy gate: flags[c] |= 2 when the column-
+ * integrated LW or SW heating differs from the predicted net surface minus
+ * model-top flux by more than energy_tol W/m2. */
+typedef struct {
+    int ncol, nk, ny;
+    const float *Y; int ldy;
+    const float *out_mean, *out_std;
+    const float *coszr, *pi3d, *p8w;
+    float energy_tol;
+    float *rthratenlw, *rthratensw, *glw, *lwupb, *swdnb, *swupb;
+    unsigned *flags;
+} rrtmg_sur_decode_args;
+rrtmg_status rrtmg_sur_decode(const rrtmg_sur_decode_args *args, void *stream);
+
+/* Appends the columns with flags[c] != 0 to list; count must be zeroed first. */
+rrtmg_status rrtmg_sur_compact(const unsigned *flags, int ncol, int *list, int *count, void *stream);
+
+/* Gathers (to_compact = 1) or scatters (0) a field of nz levels between a
+ * domain with south_north size ny and the compact (1, nz, count) domain of the
+ * listed columns; max_n bounds the device-side count. */
+rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
+                                    float *dst, int to_compact, void *stream);
+
 /* Synchronous: reads the sticky flag that a GEMM CTA sets when it gives up
  * waiting (2 s) for its tensor-core work; clears it when reset != 0. */
 rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag);

@@ -61,13 +61,44 @@ class GemmArgs(ctypes.Structure):
 
 EPI_F32, EPI_GELU, EPI_DGELU = 0, 1, 2
 
+_I, _FL = ctypes.c_int, ctypes.c_float
+
+
+class SurFeaturesArgs(ctypes.Structure):
+    _fields_ = [("ncol", _I), ("nk", _I), ("ny", _I)] + \
+        [(n, _F) for n in ("p3d", "p8w", "t3d", "qv", "qc", "qi", "qs", "cldfra", "o3", "tsk", "albedo", "coszr",
+                           "emiss")] + \
+        [("row_offset", _I), ("raw", _F), ("ldf", _I), ("mean", _F), ("rstd", _F), ("X", _F), ("ldx", _I),
+         ("Xt", _F), ("ldxt", _I), ("lo", _F), ("hi", _F), ("flags", _F)]
+
+
+class SurTargetsArgs(ctypes.Structure):
+    _fields_ = [("ncol", _I), ("nk", _I), ("ny", _I)] + \
+        [(n, _F) for n in ("rthratenlw", "rthratensw", "pi3d", "p8w", "glw", "lwupb", "swdnb", "swupb")] + \
+        [("row_offset", _I), ("T", _F), ("ldt", _I)]
+
+
+class SurAdamArgs(ctypes.Structure):
+    _fields_ = [("rows", _I), ("cols", _I), ("w", _F), ("m", _F), ("v", _F), ("grad", _F), ("lr", _FL),
+                ("beta1", _FL), ("beta2", _FL), ("eps", _FL), ("bc1", _FL), ("bc2", _FL), ("weight_decay", _FL),
+                ("wb", _F), ("ldwb", _I), ("wbt", _F), ("ldwbt", _I)]
+
+
+class SurDecodeArgs(ctypes.Structure):
+    _fields_ = [("ncol", _I), ("nk", _I), ("ny", _I), ("Y", _F), ("ldy", _I), ("out_mean", _F), ("out_std", _F),
+                ("coszr", _F), ("pi3d", _F), ("p8w", _F), ("energy_tol", _FL)] + \
+        [(n, _F) for n in ("rthratenlw", "rthratensw", "glw", "lwupb", "swdnb", "swupb", "flags")]
+
 STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
           4: "RRTMG_TIMEOUT"}
 
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
            "rrtmg_lwrad_static_scratch", "rrtmg_timing_enable", "rrtmg_timing_read", "rrtmg_lw_nlayers",
            "rrtmg_last_error", "rrtmg_status_string")
-SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error")
+SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_sur_features", "rrtmg_sur_targets",
+                     "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
+                     "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
+                     "rrtmg_sur_compact", "rrtmg_sur_move_columns")
 
 _lib = None
 
@@ -107,6 +138,25 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.rrtmg_gemm_bf16.argtypes = [ctypes.POINTER(GemmArgs), ctypes.c_void_p]
     lib.rrtmg_gemm_error.restype = ctypes.c_int
     lib.rrtmg_gemm_error.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
+    V, I, P, FL, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_float, ctypes.c_size_t
+    sigs = {
+        "rrtmg_sur_features": [ctypes.POINTER(SurFeaturesArgs), V],
+        "rrtmg_sur_targets": [ctypes.POINTER(SurTargetsArgs), V],
+        "rrtmg_sur_column_stats": [P, I, I, I, P, P, P, P, V],
+        "rrtmg_sur_normalize": [P, I, I, I, P, P, P, I, I, V],
+        "rrtmg_sur_gather": [P, I, P, I, P, I, P, P, I, P, V],
+        "rrtmg_sur_loss_grad": [P, P, P, I, I, FL, P, P, I, P, V],
+        "rrtmg_sur_row_sum": [P, I, I, I, P, V],
+        "rrtmg_sur_reduce_splits": [P, I, SZ, P, V],
+        "rrtmg_sur_adam": [ctypes.POINTER(SurAdamArgs), V],
+        "rrtmg_sur_decode": [ctypes.POINTER(SurDecodeArgs), V],
+        "rrtmg_sur_compact": [P, I, P, P, V],
+        "rrtmg_sur_move_columns": [P, P, I, I, I, P, P, I, V],
+    }
+    for name, argtypes in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = ctypes.c_int
+        fn.argtypes = argtypes
     lib.rrtmg_lw_nlayers.restype = ctypes.c_int
     lib.rrtmg_lw_nlayers.argtypes = [ctypes.c_double, ctypes.c_int]
     lib.rrtmg_last_error.restype = ctypes.c_char_p

@@ -53,3 +53,95 @@ extern "C" rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag) {
   if (!flag) return RRTMG_BAD_ARG;
   return gemm_error_flag(flag, reset != 0) == cudaSuccess ? RRTMG_OK : RRTMG_CUDA;
 }
+
+namespace {
+rrtmg_status cuda_status(cudaError_t e) { return e == cudaSuccess ? RRTMG_OK : RRTMG_CUDA; }
+cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" rrtmg_status rrtmg_sur_features(const rrtmg_sur_features_args *a, void *stream) {
+  if (!a || a->ncol < 0 || a->nk <= 0 || a->ny <= 0 || a->row_offset < 0) return RRTMG_BAD_ARG;
+  if (!a->p3d || !a->p8w || !a->t3d || !a->qv || !a->qc || !a->qi || !a->qs || !a->cldfra || !a->o3 || !a->tsk ||
+      !a->albedo || !a->coszr || !a->emiss)
+    return RRTMG_BAD_ARG;
+  const int nf = 9 * a->nk + 4;
+  if (a->raw && a->ldf < nf) return RRTMG_BAD_ARG;
+  if (a->X && (a->ldx < nf || !a->mean || !a->rstd)) return RRTMG_BAD_ARG;
+  if (a->Xt && (!a->X || a->ldxt < a->row_offset + a->ncol)) return RRTMG_BAD_ARG;
+  if ((a->lo == nullptr) != (a->hi == nullptr)) return RRTMG_BAD_ARG;
+  if (a->ncol == 0) return RRTMG_OK;
+  return cuda_status(launch_sur_features(*a, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_targets(const rrtmg_sur_targets_args *a, void *stream) {
+  if (!a || a->ncol < 0 || a->nk <= 0 || a->ny <= 0 || a->row_offset < 0 || !a->T || a->ldt < 2 * a->nk + 6)
+    return RRTMG_BAD_ARG;
+  if (!a->rthratenlw || !a->rthratensw || !a->pi3d || !a->p8w || !a->glw || !a->lwupb || !a->swdnb || !a->swupb)
+    return RRTMG_BAD_ARG;
+  if (a->ncol == 0) return RRTMG_OK;
+  return cuda_status(launch_sur_targets(*a, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_column_stats(const float *F, int n, int ld, int nf, float *mean, float *rstd,
+                                               float *lo, float *hi, void *stream) {
+  if (!F || n <= 0 || nf <= 0 || ld < nf || !mean || !rstd) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_column_stats(F, n, ld, nf, mean, rstd, lo, hi, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_gather(const void *X, int ldx, const float *T, int ldt, const int *idx, int B,
+                                         void *Xb, void *Xbt, int ldxbt, float *Tb, void *stream) {
+  if (!X || !idx || B <= 0 || ldx <= 0 || !Xb || !Xbt || ldxbt < B || (Tb && (!T || ldt <= 0))) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_gather(static_cast<const __nv_bfloat16 *>(X), ldx, T, ldt, idx, B,
+                                       static_cast<__nv_bfloat16 *>(Xb), static_cast<__nv_bfloat16 *>(Xbt), ldxbt,
+                                       Tb, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_loss_grad(const float *Y, const float *T, const float *w, int B, int ld,
+                                            float scale, void *dY, void *dYt, int lddyt, float *loss, void *stream) {
+  if (!Y || !T || !w || B <= 0 || ld <= 0 || !dY || !dYt || lddyt < B) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_loss_grad(Y, T, w, B, ld, scale, static_cast<__nv_bfloat16 *>(dY),
+                                          static_cast<__nv_bfloat16 *>(dYt), lddyt, loss, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_row_sum(const void *Gt, int ld, int rows, int B, float *db, void *stream) {
+  if (!Gt || !db || rows <= 0 || B <= 0 || ld < B) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_row_sum(static_cast<const __nv_bfloat16 *>(Gt), ld, rows, B, db, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_reduce_splits(const float *P, int splits, size_t n, float *G, void *stream) {
+  if (!P || !G || splits <= 0 || n == 0) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_reduce_splits(P, splits, n, G, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_adam(const rrtmg_sur_adam_args *a, void *stream) {
+  if (!a || a->rows <= 0 || a->cols <= 0 || !a->w || !a->m || !a->v || !a->grad) return RRTMG_BAD_ARG;
+  if ((a->wb && a->ldwb < a->cols) || (a->wbt && a->ldwbt < a->rows)) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_adam(*a, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_decode(const rrtmg_sur_decode_args *a, void *stream) {
+  if (!a || a->ncol < 0 || a->nk <= 0 || a->ny <= 0 || !a->Y || a->ldy < 2 * a->nk + 6 || !a->out_mean ||
+      !a->out_std || !a->coszr || !a->pi3d || !a->p8w || !a->rthratenlw || !a->rthratensw || !a->glw || !a->lwupb ||
+      !a->swdnb || !a->swupb || !a->flags)
+    return RRTMG_BAD_ARG;
+  if (a->ncol == 0) return RRTMG_OK;
+  return cuda_status(launch_sur_decode(*a, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_compact(const unsigned *flags, int ncol, int *list, int *count, void *stream) {
+  if (!flags || ncol < 0 || !list || !count) return RRTMG_BAD_ARG;
+  if (ncol == 0) return RRTMG_OK;
+  return cuda_status(launch_sur_compact(flags, ncol, list, count, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny,
+                                               const float *src, float *dst, int to_compact, void *stream) {
+  if (!list || !count || max_n < 0 || nz <= 0 || ny <= 0 || !src || !dst) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_move_columns(list, count, max_n, nz, ny, src, dst, to_compact, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_normalize(const float *in, int ldi, int n, int nf, const float *mean,
+                                            const float *rstd, void *out, int ldo, int out_bf16, void *stream) {
+  if (!in || !mean || !rstd || !out || n <= 0 || nf <= 0 || ldi < nf || ldo < nf) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_normalize(in, ldi, n, nf, mean, rstd, out, ldo, out_bf16, as_stream(stream)));
+}

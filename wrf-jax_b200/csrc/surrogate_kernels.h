@@ -7,6 +7,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "../../include/rrtmg_surrogate.h"
+
 namespace rrtmg {
 
 enum GemmEpilogue { kEpiF32 = 0, kEpiGelu = 1, kEpiDgelu = 2 };
@@ -35,6 +37,28 @@ struct GemmArgs {
 };
 
 cudaError_t launch_umma_gemm(const GemmArgs &g, cudaStream_t stream);
+
+using SurFeatureArgs = rrtmg_sur_features_args;
+using SurTargetArgs = rrtmg_sur_targets_args;
+using SurAdamArgs = rrtmg_sur_adam_args;
+using SurDecodeArgs = rrtmg_sur_decode_args;
+cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s);
+cudaError_t launch_sur_targets(const SurTargetArgs &a, cudaStream_t s);
+cudaError_t launch_sur_column_stats(const float *F, int n, int ld, int nf, float *mean, float *rstd, float *lo,
+                                    float *hi, cudaStream_t s);
+cudaError_t launch_sur_normalize(const float *in, int ldi, int n, int nf, const float *mean, const float *rstd,
+                                 void *out, int ldo, int out_bf16, cudaStream_t s);
+cudaError_t launch_sur_gather(const __nv_bfloat16 *X, int ldx, const float *T, int ldt, const int *idx, int B,
+                              __nv_bfloat16 *Xb, __nv_bfloat16 *Xbt, int ldxbt, float *Tb, cudaStream_t s);
+cudaError_t launch_sur_loss_grad(const float *Y, const float *T, const float *w, int B, int ld, float scale,
+                                 __nv_bfloat16 *dY, __nv_bfloat16 *dYt, int lddyt, float *loss, cudaStream_t s);
+cudaError_t launch_sur_row_sum(const __nv_bfloat16 *Gt, int ld, int rows, int B, float *db, cudaStream_t s);
+cudaError_t launch_sur_reduce_splits(const float *P, int splits, size_t n, float *G, cudaStream_t s);
+cudaError_t launch_sur_adam(const SurAdamArgs &a, cudaStream_t s);
+cudaError_t launch_sur_decode(const SurDecodeArgs &a, cudaStream_t s);
+cudaError_t launch_sur_compact(const unsigned *flags, int ncol, int *list, int *count, cudaStream_t s);
+cudaError_t launch_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
+                                    float *dst, int to_compact, cudaStream_t s);
 // Reads (and optionally clears) the sticky flag set when a GEMM CTA gave up
 // waiting for its tensor-core work.
 cudaError_t gemm_error_flag(unsigned *out, bool reset);

@@ -1,0 +1,389 @@
+// Radiation surrogate: feature/target construction, training kernels (batch
+// gather, loss gradient, bias gradients, split-K reduction, Adam), inference
+// decode with the per-column gate, and the fallback gather/scatter that hands
+// rejected columns to the plain RRTMG kernels.
+//
+// Column c = i * ny + j of a WRF-layout domain; 3-D fields (nx, nk, ny) at
+// (i * nk + k) * ny + j, level fields (nx, nk + 1, ny), 2-D fields (nx, ny).
+//
+// Feature vector of a column (kSurFeatures = 9 * nk + 4, padded with zeros to
+// the row length): per level k, at f * nk + k,
+//   f = 0 t3d [K], 1 ln p3d [Pa], 2 qv, 3 qc, 4 qi, 5 qs [kg/kg], 6 cldfra,
+//       7 o3, 8 layer thickness p8w[k] - p8w[k+1] [Pa];
+// then tsk, albedo, coszr, emiss.  Target vector (kSurTargets = 2 * nk + 6):
+// LW heating [K/day] per level, SW heating per level, glw (LW down at the
+// surface), lwupb, swdnb, swupb [W/m2], then the LW and SW net fluxes at the
+// model top implied by the heating profile (the energy-gate quantities).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "surrogate_kernels.h"
+
+namespace rrtmg {
+namespace {
+
+// heatfac = g * 86400 / (cp * 100): K/day per (W/m2 per hPa)  (lw:5706, sw:2289)
+constexpr float kHeatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
+
+__device__ __forceinline__ size_t idx3(int c, int k, int nk, int ny) {
+  const int i = c / ny, j = c - i * ny;
+  return (static_cast<size_t>(i) * nk + k) * ny + j;
+}
+
+__global__ void features_kernel(SurFeatureArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncol) return;
+  const int nk = a.nk, ny = a.ny;
+  const size_t row = static_cast<size_t>(a.row_offset + c);
+  __nv_bfloat16 *X = static_cast<__nv_bfloat16 *>(a.X), *Xt = static_cast<__nv_bfloat16 *>(a.Xt);
+  bool in_range = true;
+  auto put = [&](int f, float v) {
+    if (a.raw) a.raw[row * a.ldf + f] = v;
+    if (X) {
+      const float z = (v - a.mean[f]) * a.rstd[f];
+      X[row * a.ldx + f] = __float2bfloat16_rn(z);
+      if (Xt) Xt[static_cast<size_t>(f) * a.ldxt + row] = __float2bfloat16_rn(z);
+    }
+    if (a.lo && (v < a.lo[f] || v > a.hi[f])) in_range = false;
+  };
+  for (int k = 0; k < nk; ++k) {
+    const size_t q = idx3(c, k, nk, ny);
+    const float plo = a.p8w[idx3(c, k, nk + 1, ny)], phi = a.p8w[idx3(c, k + 1, nk + 1, ny)];
+    put(0 * nk + k, a.t3d[q]);
+    put(1 * nk + k, logf(a.p3d[q]));
+    put(2 * nk + k, a.qv[q]);
+    put(3 * nk + k, a.qc[q]);
+    put(4 * nk + k, a.qi[q]);
+    put(5 * nk + k, a.qs[q]);
+    put(6 * nk + k, a.cldfra[q]);
+    put(7 * nk + k, a.o3[q]);
+    put(8 * nk + k, plo - phi);
+  }
+  put(9 * nk + 0, a.tsk[c]);
+  put(9 * nk + 1, a.albedo[c]);
+  put(9 * nk + 2, a.coszr[c]);
+  put(9 * nk + 3, a.emiss[c]);
+  if (X) {
+    for (int f = 9 * nk + 4; f < a.ldx; ++f) {
+      X[row * a.ldx + f] = __float2bfloat16_rn(0.0f);
+      if (Xt) Xt[static_cast<size_t>(f) * a.ldxt + row] = __float2bfloat16_rn(0.0f);
+    }
+  }
+  if (a.flags) a.flags[c] = in_range ? 0u : 1u;
+}
+
+__global__ void targets_kernel(SurTargetArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncol) return;
+  const int nk = a.nk, ny = a.ny;
+  float *t = a.T + static_cast<size_t>(a.row_offset + c) * a.ldt;
+  float slw = 0.0f, ssw = 0.0f;
+  for (int k = 0; k < nk; ++k) {
+    const size_t q = idx3(c, k, nk, ny);
+    const float pi = a.pi3d[q];
+    const float hlw = a.rthratenlw[q] * 86400.0f * pi;
+    const float hsw = a.rthratensw[q] * 86400.0f * pi;
+    t[k] = hlw;
+    t[nk + k] = hsw;
+    const float dp = (a.p8w[idx3(c, k, nk + 1, ny)] - a.p8w[idx3(c, k + 1, nk + 1, ny)]) * 0.01f;
+    slw += hlw * dp / kHeatfac;
+    ssw += hsw * dp / kHeatfac;
+  }
+  const float glw = a.glw[c], lwupb = a.lwupb[c], swdnb = a.swdnb[c], swupb = a.swupb[c];
+  t[2 * nk + 0] = glw;
+  t[2 * nk + 1] = lwupb;
+  t[2 * nk + 2] = swdnb;
+  t[2 * nk + 3] = swupb;
+  // LW: hr = heatfac (Fn_k - Fn_k+1) / dp with Fn = up - down; SW: Fn = down - up
+  t[2 * nk + 4] = (lwupb - glw) - slw;
+  t[2 * nk + 5] = (swdnb - swupb) + ssw;
+  for (int f = 2 * nk + 6; f < a.ldt; ++f) t[f] = 0.0f;
+}
+
+// Per-feature mean and 1/std (and min/max) over rows [0, n): one block per
+// feature, fixed reduction order.
+__global__ void column_stats_kernel(const float *F, int n, int ld, int nf, float *mean, float *rstd, float *lo,
+                                    float *hi) {
+  const int f = blockIdx.x;
+  if (f >= nf) return;
+  __shared__ double s1[256], s2[256];
+  __shared__ float smin[256], smax[256];
+  double a1 = 0.0, a2 = 0.0;
+  float mn = 3.0e38f, mx = -3.0e38f;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const float v = F[static_cast<size_t>(r) * ld + f];
+    a1 += v;
+    a2 += static_cast<double>(v) * v;
+    mn = fminf(mn, v);
+    mx = fmaxf(mx, v);
+  }
+  s1[threadIdx.x] = a1; s2[threadIdx.x] = a2; smin[threadIdx.x] = mn; smax[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+      smin[threadIdx.x] = fminf(smin[threadIdx.x], smin[threadIdx.x + w]);
+      smax[threadIdx.x] = fmaxf(smax[threadIdx.x], smax[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double m = s1[0] / n;
+    const double var = s2[0] / n - m * m;
+    mean[f] = static_cast<float>(m);
+    rstd[f] = var > 1.0e-20 ? static_cast<float>(1.0 / sqrt(var)) : 0.0f;
+    if (lo) lo[f] = smin[0];
+    if (hi) hi[f] = smax[0];
+  }
+}
+
+__global__ void normalize_kernel(const float *in, int ldi, int n, int nf, const float *mean, const float *rstd,
+                                 void *out, int ldo, int out_bf16) {
+  const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<size_t>(n) * ldo) return;
+  const int r = static_cast<int>(i / ldo), f = static_cast<int>(i - static_cast<size_t>(r) * ldo);
+  const float v = f < nf ? (in[static_cast<size_t>(r) * ldi + f] - mean[f]) * rstd[f] : 0.0f;
+  if (out_bf16) static_cast<__nv_bfloat16 *>(out)[i] = __float2bfloat16_rn(v);
+  else static_cast<float *>(out)[i] = v;
+}
+
+// Batch gather: Xb[b] = X[idx[b]] (BF16), Xbt = Xb^T, Tb[b] = T[idx[b]] (FP32).
+__global__ void gather_kernel(const __nv_bfloat16 *X, int ldx, const float *T, int ldt, const int *idx, int B,
+                              __nv_bfloat16 *Xb, __nv_bfloat16 *Xbt, int ldxbt, float *Tb) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  const int b0 = blockIdx.x * 32, f0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const int b = b0 + r, f = f0 + tx;
+    if (b < B && f < ldx) {
+      const __nv_bfloat16 v = X[static_cast<size_t>(idx[b]) * ldx + f];
+      Xb[static_cast<size_t>(b) * ldx + f] = v;
+      tile[r][tx] = v;
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int f = f0 + r, b = b0 + tx;
+    if (b < B && f < ldx) Xbt[static_cast<size_t>(f) * ldxbt + b] = tile[tx][r];
+  }
+  if (blockIdx.y == 0 && Tb) {
+    for (int r = ty; r < 32; r += 8) {
+      const int b = b0 + r;
+      if (b >= B) continue;
+      for (int f = tx; f < ldt; f += 32) Tb[static_cast<size_t>(b) * ldt + f] = T[static_cast<size_t>(idx[b]) * ldt + f];
+    }
+  }
+}
+
+// dY = weight * 2 (Y - T) / count as BF16 (row-major and transposed), and the
+// weighted squared error summed into loss[0].
+__global__ void loss_grad_kernel(const float *Y, const float *T, const float *w, int B, int ld, float scale,
+                                 __nv_bfloat16 *dY, __nv_bfloat16 *dYt, int lddyt, float *loss) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  __shared__ float part[256];
+  const int b0 = blockIdx.x * 32, f0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  float acc = 0.0f;
+  for (int r = ty; r < 32; r += 8) {
+    const int b = b0 + r, f = f0 + tx;
+    float g = 0.0f;
+    if (b < B && f < ld) {
+      const float d = Y[static_cast<size_t>(b) * ld + f] - T[static_cast<size_t>(b) * ld + f];
+      acc += w[f] * d * d;
+      g = w[f] * 2.0f * d * scale;
+      dY[static_cast<size_t>(b) * ld + f] = __float2bfloat16_rn(g);
+    }
+    tile[r][tx] = __float2bfloat16_rn(g);
+  }
+  part[ty * 32 + tx] = acc;
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int f = f0 + r, b = b0 + tx;
+    if (b < B && f < ld) dYt[static_cast<size_t>(f) * lddyt + b] = tile[tx][r];
+  }
+  for (int s = 128; s > 0; s >>= 1) {
+    if (ty * 32 + tx < s) part[ty * 32 + tx] += part[ty * 32 + tx + s];
+    __syncthreads();
+  }
+  if (tx == 0 && ty == 0 && loss) atomicAdd(loss, part[0]);
+}
+
+// db[n] = sum_b Gt[n][b] (BF16 rows), one block per row, fixed order.
+__global__ void row_sum_kernel(const __nv_bfloat16 *Gt, int ld, int B, float *db) {
+  __shared__ float part[256];
+  float acc = 0.0f;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) acc += __bfloat162float(Gt[static_cast<size_t>(blockIdx.x) * ld + b]);
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) db[blockIdx.x] = part[0];
+}
+
+__global__ void reduce_splits_kernel(const float *P, int splits, size_t n, float *G) {
+  const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s = P[i];
+  for (int z = 1; z < splits; ++z) s += P[static_cast<size_t>(z) * n + i];
+  G[i] = s;
+}
+
+// Adam on an FP32 master [rows][cols]; writes the BF16 copy and its transpose.
+__global__ void adam_kernel(SurAdamArgs a) {
+  const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t n = static_cast<size_t>(a.rows) * a.cols;
+  if (i >= n) return;
+  const float g = a.grad[i];
+  const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+  const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+  a.m[i] = m;
+  a.v[i] = v;
+  const float mhat = m / a.bc1, vhat = v / a.bc2;
+  const float w = a.w[i] - a.lr * (mhat / (sqrtf(vhat) + a.eps) + a.weight_decay * a.w[i]);
+  a.w[i] = w;
+  const int r = static_cast<int>(i / a.cols), c = static_cast<int>(i - static_cast<size_t>(r) * a.cols);
+  if (a.wb) static_cast<__nv_bfloat16 *>(a.wb)[static_cast<size_t>(r) * a.ldwb + c] = __float2bfloat16_rn(w);
+  if (a.wbt) static_cast<__nv_bfloat16 *>(a.wbt)[static_cast<size_t>(c) * a.ldwbt + r] = __float2bfloat16_rn(w);
+}
+
+// Decode normalized network outputs into WRF fields and apply the energy gate.
+__global__ void decode_kernel(SurDecodeArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncol) return;
+  const int nk = a.nk, ny = a.ny;
+  const float *y = a.Y + static_cast<size_t>(c) * a.ldy;
+  auto out = [&](int f) { return y[f] * a.out_std[f] + a.out_mean[f]; };
+  const bool day = a.coszr[c] > 0.0f;
+  float slw = 0.0f, ssw = 0.0f;
+  for (int k = 0; k < nk; ++k) {
+    const size_t q = idx3(c, k, nk, ny);
+    const float pi = a.pi3d[q];
+    const float hlw = out(k);
+    const float hsw = day ? out(nk + k) : 0.0f;
+    a.rthratenlw[q] = (hlw / 86400.0f) / pi;
+    a.rthratensw[q] = (hsw / 86400.0f) / pi;
+    const float dp = (a.p8w[idx3(c, k, nk + 1, ny)] - a.p8w[idx3(c, k + 1, nk + 1, ny)]) * 0.01f;
+    slw += hlw * dp / kHeatfac;
+    ssw += hsw * dp / kHeatfac;
+  }
+  const float glw = out(2 * nk), lwupb = out(2 * nk + 1);
+  const float swdnb = day ? out(2 * nk + 2) : 0.0f, swupb = day ? out(2 * nk + 3) : 0.0f;
+  a.glw[c] = glw;
+  a.lwupb[c] = lwupb;
+  a.swdnb[c] = swdnb;
+  a.swupb[c] = swupb;
+  // energy gate: column-integrated heating against net surface minus model-top flux
+  const float lw_res = fabsf(((lwupb - glw) - out(2 * nk + 4)) - slw);
+  const float sw_res = day ? fabsf((out(2 * nk + 5) - (swdnb - swupb)) - ssw) : 0.0f;
+  unsigned f = a.flags[c];
+  if (!(lw_res <= a.energy_tol) || !(sw_res <= a.energy_tol)) f |= 2u;
+  a.flags[c] = f;
+}
+
+// Append flagged columns to a list (one atomic per warp).
+__global__ void compact_kernel(const unsigned *flags, int ncol, int *list, int *count) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool sel = c < ncol && flags[c] != 0u;
+  const unsigned ballot = __ballot_sync(0xffffffffu, sel);
+  int base = 0;
+  if (lane == 0 && ballot) base = atomicAdd(count, __popc(ballot));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (sel) list[base + __popc(ballot & ((1u << lane) - 1u))] = c;
+}
+
+// Gather (to_compact = 1) or scatter (0) a field between a domain and the
+// compact (1, nz, n) domain of listed columns.
+__global__ void move_columns_kernel(const int *list, const int *count, int nz, int ny, const float *src, float *dst,
+                                    int to_compact) {
+  const int n = *count;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nz) return;
+  const int k = t / n, j = t - k * n;
+  const int c = list[j];
+  const size_t full = idx3(c, k, nz, ny);
+  const size_t comp = static_cast<size_t>(k) * n + j;
+  if (to_compact) dst[comp] = src[full];
+  else dst[full] = src[comp];
+}
+
+}  // namespace
+
+cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s) {
+  features_kernel<<<(a.ncol + 127) / 128, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_targets(const SurTargetArgs &a, cudaStream_t s) {
+  targets_kernel<<<(a.ncol + 127) / 128, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_column_stats(const float *F, int n, int ld, int nf, float *mean, float *rstd, float *lo,
+                                    float *hi, cudaStream_t s) {
+  column_stats_kernel<<<nf, 256, 0, s>>>(F, n, ld, nf, mean, rstd, lo, hi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_normalize(const float *in, int ldi, int n, int nf, const float *mean, const float *rstd,
+                                 void *out, int ldo, int out_bf16, cudaStream_t s) {
+  const size_t total = static_cast<size_t>(n) * ldo;
+  normalize_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(in, ldi, n, nf, mean, rstd, out, ldo,
+                                                                              out_bf16);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_gather(const __nv_bfloat16 *X, int ldx, const float *T, int ldt, const int *idx, int B,
+                              __nv_bfloat16 *Xb, __nv_bfloat16 *Xbt, int ldxbt, float *Tb, cudaStream_t s) {
+  dim3 grid((B + 31) / 32, (ldx + 31) / 32);
+  gather_kernel<<<grid, dim3(32, 8), 0, s>>>(X, ldx, T, ldt, idx, B, Xb, Xbt, ldxbt, Tb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_loss_grad(const float *Y, const float *T, const float *w, int B, int ld, float scale,
+                                 __nv_bfloat16 *dY, __nv_bfloat16 *dYt, int lddyt, float *loss, cudaStream_t s) {
+  dim3 grid((B + 31) / 32, (ld + 31) / 32);
+  loss_grad_kernel<<<grid, dim3(32, 8), 0, s>>>(Y, T, w, B, ld, scale, dY, dYt, lddyt, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_row_sum(const __nv_bfloat16 *Gt, int ld, int rows, int B, float *db, cudaStream_t s) {
+  row_sum_kernel<<<rows, 256, 0, s>>>(Gt, ld, B, db);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_reduce_splits(const float *P, int splits, size_t n, float *G, cudaStream_t s) {
+  reduce_splits_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(P, splits, n, G);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_adam(const SurAdamArgs &a, cudaStream_t s) {
+  const size_t n = static_cast<size_t>(a.rows) * a.cols;
+  adam_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_decode(const SurDecodeArgs &a, cudaStream_t s) {
+  decode_kernel<<<(a.ncol + 127) / 128, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_compact(const unsigned *flags, int ncol, int *list, int *count, cudaStream_t s) {
+  compact_kernel<<<(ncol + 255) / 256, 256, 0, s>>>(flags, ncol, list, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
+                                    float *dst, int to_compact, cudaStream_t s) {
+  const long long total = static_cast<long long>(max_n) * nz;
+  if (total == 0) return cudaSuccess;
+  move_columns_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(list, count, nz, ny, src, dst,
+                                                                                 to_compact);
+  return cudaGetLastError();
+}
+
+}  // namespace rrtmg

@@ -1,21 +1,57 @@
 """Learned radiation surrogate: an MLP from a column profile to LW/SW heating
 profiles and surface fluxes, trained and run on B200 tensor cores.
 
-Every arithmetic step of training and inference runs in librrtmg_b200.so:
-tcgen05 BF16 GEMMs with fused bias/GELU epilogues (include/rrtmg_surrogate.h)
-and small CUDA kernels for features, loss, bias gradients and Adam.  torch is
-used only to hold device buffers and streams.
+Network: 454 inputs (9 per-level fields x 50 levels + 4 surface scalars,
+zero-padded to 512) -> 3 hidden layers of 512 with GELU -> 106 outputs (50 LW
+and 50 SW heating rates [K/day], 4 surface fluxes, and 2 gate-only outputs: the
+LW and SW net fluxes at the model top), padded to 128.  Weights are BF16 for
+the tensor cores with an FP32 Adam master copy; all GEMMs are the hand-written
+tcgen05 kernel of librrtmg_b200.so (FP32 accumulation in tensor memory), and
+every other arithmetic step (features, targets, normalization, batch gather,
+loss gradient, bias gradients, split-K sums, Adam, decode, gate, fallback
+gather/scatter) is a CUDA kernel of the same library.  torch only holds device
+buffers and the stream.
+
+Inference with fallback: every column is predicted; a column is rejected when
+an input lies outside the training range or when its predicted heating does
+not integrate to its predicted net-flux divergence (energy gate).  Rejected
+columns are gathered into a compact domain, solved by the plain RRTMG kernels,
+and scattered back, so their outputs are the plain kernel's bits.
 """
 
 from __future__ import annotations
 
 import ctypes
+import math
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
 
 from . import _capi
+
+NK = 50                    # model levels the network is built for
+N_FEATURES = 9 * NK + 4    # 454
+N_TARGETS = 2 * NK + 6     # 106
+K_IN = 512                 # padded input width
+N_OUT = 128                # padded output width
+HIDDEN = 512
+LAYER_SHAPES = ((HIDDEN, K_IN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (N_OUT, HIDDEN))  # (out, in)
+HEATFAC = (9.8066 * 8.6400e4) / (1004.5 * 1.0e2)
 
 
 def _ptr(t) -> int | None:
     return None if t is None else t.data_ptr()
+
+
+def _stream(stream=None) -> ctypes.c_void_p:
+    import torch
+    return ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+
+
+def _check(st: int, what: str) -> None:
+    if st != 0:
+        raise RuntimeError(f"{what} failed with status {st}")
 
 
 def gemm_bf16(A, B, *, epilogue: int = _capi.EPI_F32, bias=None, C=None, ksplit: int = 1, H=None, Ht=None,
@@ -24,8 +60,6 @@ def gemm_bf16(A, B, *, epilogue: int = _capi.EPI_F32, bias=None, C=None, ksplit:
     of include/rrtmg_surrogate.h.  A and B are contiguous bf16 CUDA tensors;
     outputs are preallocated tensors (C: float32 [ksplit, M, N] or [M, N];
     H: bf16 [M, N]; Ht: bf16 [N, M]; Z, aux: float32 [M, N])."""
-    import torch
-
     M, K = A.shape
     N, K2 = B.shape
     if K2 != K:
@@ -46,8 +80,7 @@ def gemm_bf16(A, B, *, epilogue: int = _capi.EPI_F32, bias=None, C=None, ksplit:
         g.aux, g.ldaux = aux.data_ptr(), aux.stride(0)
     if Z is not None:
         g.Z, g.ldz = Z.data_ptr(), Z.stride(0)
-    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
-    st = lib.rrtmg_gemm_bf16(ctypes.byref(g), ctypes.c_void_p(s))
+    st = lib.rrtmg_gemm_bf16(ctypes.byref(g), _stream(stream))
     if st != 0:
         raise ValueError(f"rrtmg_gemm_bf16 rejected the arguments (status {st}): M={M} N={N} K={K} ksplit={ksplit}")
 
@@ -55,7 +88,386 @@ def gemm_bf16(A, B, *, epilogue: int = _capi.EPI_F32, bias=None, C=None, ksplit:
 def gemm_error(reset: bool = True) -> int:
     """Synchronous read of the GEMM timeout flag (0 = no CTA gave up)."""
     flag = ctypes.c_uint(0)
-    st = _capi.load().rrtmg_gemm_error(int(reset), ctypes.byref(flag))
-    if st != 0:
-        raise RuntimeError(f"rrtmg_gemm_error failed with status {st}")
+    _check(_capi.load().rrtmg_gemm_error(int(reset), ctypes.byref(flag)), "rrtmg_gemm_error")
     return flag.value
+
+
+# ---------------------------------------------------------------------------
+# features and targets
+# ---------------------------------------------------------------------------
+def _feature_args(d: dict, nk: int, ny: int, ncol: int, row_offset: int = 0) -> _capi.SurFeaturesArgs:
+    a = _capi.SurFeaturesArgs()
+    a.ncol, a.nk, a.ny, a.row_offset = ncol, nk, ny, row_offset
+    a.p3d, a.p8w, a.t3d = _ptr(d["p3d"]), _ptr(d["p8w"]), _ptr(d["t3d"])
+    a.qv, a.qc, a.qi, a.qs = _ptr(d["qv3d"]), _ptr(d["qc3d"]), _ptr(d["qi3d"]), _ptr(d["qs3d"])
+    a.cldfra, a.o3, a.tsk = _ptr(d["cldfra3d"]), _ptr(d["o33d"]), _ptr(d["tsk"])
+    a.albedo, a.coszr, a.emiss = _ptr(d["albedo"]), _ptr(d["coszr"]), _ptr(d["emiss"])
+    return a
+
+
+def _device_fields(st, device: str) -> dict:
+    import torch
+    return {k: torch.from_numpy(v).to(device) for k, v in st.fields.items()}
+
+
+def _plain(st, d: dict):
+    from . import rrtmg
+    lw_kw = {k: (d[k] if k in d else v) for k, v in st.lw_kwargs().items()}
+    sw_kw = {k: (d[k] if k in d else v) for k, v in st.sw_kwargs().items()}
+    return rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw), rrtmg.rrtmg_swrad_wrf_columns(**sw_kw)
+
+
+def generate_dataset(n_columns: int, *, seed: int = 1, chunk: tuple[int, int] = (512, 256), t_noise: float = 4.0,
+                     rh_lo: float = 0.05, cloud_p=(0.0, 0.6), log=print):
+    """Columns from the seeded generator (widened perturbations), solved by the
+    plain B200 kernels.  Returns raw FP32 features [n, N_FEATURES] and targets
+    [n, N_OUT] on the GPU."""
+    import torch
+    from . import synthetic
+
+    lib = _capi.load()
+    cx, cy = chunk
+    per = cx * cy
+    nchunks = math.ceil(n_columns / per)
+    n = nchunks * per
+    raw = torch.empty(n, N_FEATURES, device="cuda")
+    T = torch.empty(n, N_OUT, device="cuda")
+    for q in range(nchunks):
+        st = synthetic.make_columns(cx, cy, NK, seed=seed * 1000 + q, t_noise=t_noise, rh_lo=rh_lo, cloud_p=cloud_p)
+        d = _device_fields(st, "cuda")
+        lw, sw = _plain(st, d)
+        fa = _feature_args(d, NK, cy, per, q * per)
+        fa.raw, fa.ldf = raw.data_ptr(), raw.stride(0)
+        _check(lib.rrtmg_sur_features(ctypes.byref(fa), _stream()), "rrtmg_sur_features")
+        ta = _capi.SurTargetsArgs()
+        ta.ncol, ta.nk, ta.ny, ta.row_offset = per, NK, cy, q * per
+        ta.rthratenlw, ta.rthratensw = lw.rthratenlw.data_ptr(), sw.rthratensw.data_ptr()
+        ta.pi3d, ta.p8w = d["pi3d"].data_ptr(), d["p8w"].data_ptr()
+        ta.glw, ta.lwupb = lw.glw.data_ptr(), lw.lwupb.data_ptr()
+        ta.swdnb, ta.swupb = sw.swdnb.data_ptr(), sw.swupb.data_ptr()
+        ta.T, ta.ldt = T.data_ptr(), T.stride(0)
+        _check(lib.rrtmg_sur_targets(ctypes.byref(ta), _stream()), "rrtmg_sur_targets")
+        if log and (q % 4 == 0 or q == nchunks - 1):
+            torch.cuda.synchronize()
+            log(f"dataset chunk {q + 1}/{nchunks}")
+    torch.cuda.synchronize()
+    return raw[:n_columns], T[:n_columns]
+
+
+# ---------------------------------------------------------------------------
+# model
+# ---------------------------------------------------------------------------
+@dataclass
+class Normalization:
+    in_mean: object
+    in_rstd: object
+    in_lo: object
+    in_hi: object
+    out_mean: object
+    out_std: object
+
+
+class SurrogateModel:
+    """Weights (FP32 master + BF16 copies), Adam moments and normalization, on one GPU."""
+
+    def __init__(self, seed: int = 0):
+        import torch
+
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.w, self.b = [], []
+        for out_f, in_f in LAYER_SHAPES:
+            w = rng.normal(0.0, 1.0 / math.sqrt(in_f), size=(out_f, in_f)).astype(np.float32)
+            self.w.append(torch.from_numpy(w).cuda())
+            self.b.append(torch.zeros(out_f, device="cuda"))
+        if LAYER_SHAPES[0][1] > N_FEATURES:  # padded inputs carry no weight
+            self.w[0][:, N_FEATURES:] = 0.0
+        self.wb = [w.to(torch.bfloat16).contiguous() for w in self.w]
+        self.wbt = [w.t().contiguous().to(torch.bfloat16) for w in self.w]
+        self.mw = [torch.zeros_like(w) for w in self.w]
+        self.vw = [torch.zeros_like(w) for w in self.w]
+        self.mb = [torch.zeros_like(b) for b in self.b]
+        self.vb = [torch.zeros_like(b) for b in self.b]
+        self.step = 0
+        self.norm: Normalization | None = None
+
+    # -- normalization ------------------------------------------------------
+    def fit_normalization(self, raw, T) -> None:
+        import torch
+        lib = _capi.load()
+        f = lambda n: torch.zeros(n, device="cuda")
+        in_mean, in_rstd, in_lo, in_hi = f(K_IN), f(K_IN), f(K_IN), f(K_IN)
+        _check(lib.rrtmg_sur_column_stats(raw.data_ptr(), raw.shape[0], raw.stride(0), N_FEATURES,
+                                          in_mean.data_ptr(), in_rstd.data_ptr(), in_lo.data_ptr(),
+                                          in_hi.data_ptr(), _stream()), "column stats (inputs)")
+        out_mean, out_rstd = f(N_OUT), f(N_OUT)
+        _check(lib.rrtmg_sur_column_stats(T.data_ptr(), T.shape[0], T.stride(0), N_TARGETS, out_mean.data_ptr(),
+                                          out_rstd.data_ptr(), None, None, _stream()), "column stats (targets)")
+        torch.cuda.synchronize()
+        # outputs: a constant target (rstd 0) keeps std 1; widened input range for the gate
+        out_std = torch.where(out_rstd > 0, 1.0 / torch.where(out_rstd > 0, out_rstd, torch.ones_like(out_rstd)),
+                              torch.ones_like(out_rstd))
+        span = (in_hi - in_lo) * 0.05
+        self.norm = Normalization(in_mean, in_rstd, in_lo - span, in_hi + span, out_mean, out_std)
+
+    def normalized(self, raw, T):
+        """BF16 normalized inputs [n, K_IN] and FP32 normalized targets [n, N_OUT]."""
+        import torch
+        lib = _capi.load()
+        n = raw.shape[0]
+        X = torch.empty(n, K_IN, device="cuda", dtype=torch.bfloat16)
+        _check(lib.rrtmg_sur_normalize(raw.data_ptr(), raw.stride(0), n, N_FEATURES, self.norm.in_mean.data_ptr(),
+                                       self.norm.in_rstd.data_ptr(), X.data_ptr(), K_IN, 1, _stream()),
+               "normalize inputs")
+        Tn = torch.empty(n, N_OUT, device="cuda")
+        out_rstd = torch.where(self.norm.out_std > 0, 1.0 / self.norm.out_std, torch.zeros_like(self.norm.out_std))
+        _check(lib.rrtmg_sur_normalize(T.data_ptr(), T.stride(0), n, N_TARGETS, self.norm.out_mean.data_ptr(),
+                                       out_rstd.data_ptr(), Tn.data_ptr(), N_OUT, 0, _stream()), "normalize targets")
+        return X, Tn
+
+    # -- forward / backward --------------------------------------------------
+    def _buffers(self, B: int):
+        import torch
+        if getattr(self, "_buf_batch", None) == B:
+            return self._buf
+        bf, f32 = torch.bfloat16, torch.float32
+        e = lambda *s, dt=f32: torch.empty(*s, device="cuda", dtype=dt)
+        buf = dict(
+            Xb=e(B, K_IN, dt=bf), Xbt=e(K_IN, B, dt=bf), Tb=e(B, N_OUT),
+            Z=[e(B, HIDDEN) for _ in range(3)], H=[e(B, HIDDEN, dt=bf) for _ in range(3)],
+            Ht=[e(HIDDEN, B, dt=bf) for _ in range(3)], Y=e(B, N_OUT),
+            dY=e(B, N_OUT, dt=bf), dYt=e(N_OUT, B, dt=bf),
+            dZ=[e(B, HIDDEN, dt=bf) for _ in range(3)], dZt=[e(HIDDEN, B, dt=bf) for _ in range(3)],
+            gw=[torch.empty_like(w) for w in self.w], gb=[torch.empty_like(b) for b in self.b],
+            loss=e(1),
+        )
+        self._ksplit = max(1, min(16, B // 1024))
+        while B % (64 * self._ksplit):
+            self._ksplit //= 2
+        buf["part"] = e(self._ksplit * HIDDEN * max(K_IN, HIDDEN))
+        self._buf, self._buf_batch = buf, B
+        return buf
+
+    def forward(self, X, *, Z=None, H=None, Ht=None, Y=None):
+        """Y = MLP(X) for BF16 X [M, K_IN] (M a multiple of 128)."""
+        import torch
+        M = X.shape[0]
+        inp = X
+        for i in range(3):
+            gemm_bf16(inp, self.wb[i], epilogue=_capi.EPI_GELU, bias=self.b[i], Z=None if Z is None else Z[i],
+                      H=H[i], Ht=None if Ht is None else Ht[i])
+            inp = H[i]
+        if Y is None:
+            Y = torch.empty(M, N_OUT, device="cuda")
+        gemm_bf16(inp, self.wb[3], epilogue=_capi.EPI_F32, bias=self.b[3], C=Y)
+        return Y
+
+    def train_step(self, X, Tn, idx, weights, *, lr: float, beta1=0.9, beta2=0.999, eps=1e-8,
+                   weight_decay: float = 0.0) -> None:
+        """One Adam step on the batch idx of (X, Tn); the batch loss is added to
+        self._buf['loss'] (sum of weighted squared errors)."""
+        lib = _capi.load()
+        B = idx.shape[0]
+        b = self._buffers(B)
+        s = _stream()
+        _check(lib.rrtmg_sur_gather(X.data_ptr(), K_IN, Tn.data_ptr(), N_OUT, idx.data_ptr(), B, b["Xb"].data_ptr(),
+                                    b["Xbt"].data_ptr(), B, b["Tb"].data_ptr(), s), "gather")
+        self.forward(b["Xb"], Z=b["Z"], H=b["H"], Ht=b["Ht"], Y=b["Y"])
+        _check(lib.rrtmg_sur_loss_grad(b["Y"].data_ptr(), b["Tb"].data_ptr(), weights.data_ptr(), B, N_OUT,
+                                       1.0 / (B * N_TARGETS), b["dY"].data_ptr(), b["dYt"].data_ptr(), B,
+                                       b["loss"].data_ptr(), s), "loss gradient")
+        ks = self._ksplit
+        # layer 4 (linear), then the three GELU layers, last to first
+        grads_in = (b["dYt"], b["dZt"][2], b["dZt"][1], b["dZt"][0])   # d(pre-activation)^T per layer 3..0
+        acts_t = (b["Ht"][2], b["Ht"][1], b["Ht"][0], b["Xbt"])          # layer inputs^T
+        for layer, gt, at in zip((3, 2, 1, 0), grads_in, acts_t):
+            out_f, in_f = LAYER_SHAPES[layer]
+            part = b["part"][:ks * out_f * in_f].view(ks, out_f, in_f)
+            gemm_bf16(gt, at, epilogue=_capi.EPI_F32, C=part, ksplit=ks)
+            _check(lib.rrtmg_sur_reduce_splits(part.data_ptr(), ks, out_f * in_f, b["gw"][layer].data_ptr(), s),
+                   "reduce splits")
+            _check(lib.rrtmg_sur_row_sum(gt.data_ptr(), B, out_f, B, b["gb"][layer].data_ptr(), s), "bias gradient")
+            if layer > 0:
+                g_rows = b["dY"] if layer == 3 else b["dZ"][layer]
+                gemm_bf16(g_rows, self.wbt[layer], epilogue=_capi.EPI_DGELU, aux=b["Z"][layer - 1],
+                          H=b["dZ"][layer - 1], Ht=b["dZt"][layer - 1])
+        self.step += 1
+        bc1, bc2 = 1.0 - beta1 ** self.step, 1.0 - beta2 ** self.step
+        for i, (out_f, in_f) in enumerate(LAYER_SHAPES):
+            a = _capi.SurAdamArgs(rows=out_f, cols=in_f, w=self.w[i].data_ptr(), m=self.mw[i].data_ptr(),
+                                  v=self.vw[i].data_ptr(), grad=b["gw"][i].data_ptr(), lr=lr, beta1=beta1,
+                                  beta2=beta2, eps=eps, bc1=bc1, bc2=bc2, weight_decay=weight_decay,
+                                  wb=self.wb[i].data_ptr(), ldwb=in_f, wbt=self.wbt[i].data_ptr(), ldwbt=out_f)
+            _check(lib.rrtmg_sur_adam(ctypes.byref(a), s), "adam (weights)")
+            a = _capi.SurAdamArgs(rows=1, cols=out_f, w=self.b[i].data_ptr(), m=self.mb[i].data_ptr(),
+                                  v=self.vb[i].data_ptr(), grad=b["gb"][i].data_ptr(), lr=lr, beta1=beta1,
+                                  beta2=beta2, eps=eps, bc1=bc1, bc2=bc2, weight_decay=0.0)
+            _check(lib.rrtmg_sur_adam(ctypes.byref(a), s), "adam (biases)")
+
+    # -- persistence ----------------------------------------------------------
+    def state(self) -> dict:
+        out = {f"w{i}": w.cpu().numpy() for i, w in enumerate(self.w)}
+        out.update({f"b{i}": b.cpu().numpy() for i, b in enumerate(self.b)})
+        for k in ("in_mean", "in_rstd", "in_lo", "in_hi", "out_mean", "out_std"):
+            out[k] = getattr(self.norm, k).cpu().numpy()
+        out["step"] = np.array(self.step)
+        return out
+
+    def save(self, path) -> None:
+        np.savez_compressed(path, **self.state())
+
+    @classmethod
+    def load(cls, path) -> "SurrogateModel":
+        import torch
+        z = np.load(path)
+        m = cls.__new__(cls)
+        m.w = [torch.from_numpy(z[f"w{i}"]).cuda() for i in range(len(LAYER_SHAPES))]
+        m.b = [torch.from_numpy(z[f"b{i}"]).cuda() for i in range(len(LAYER_SHAPES))]
+        m.wb = [w.to(torch.bfloat16).contiguous() for w in m.w]
+        m.wbt = [w.t().contiguous().to(torch.bfloat16) for w in m.w]
+        m.mw = [torch.zeros_like(w) for w in m.w]
+        m.vw = [torch.zeros_like(w) for w in m.w]
+        m.mb = [torch.zeros_like(b) for b in m.b]
+        m.vb = [torch.zeros_like(b) for b in m.b]
+        m.step = int(z["step"])
+        m.norm = Normalization(*(torch.from_numpy(z[k]).cuda() for k in
+                                 ("in_mean", "in_rstd", "in_lo", "in_hi", "out_mean", "out_std")))
+        return m
+
+
+def target_weights():
+    """Loss weight per output: 1 for the 106 targets, 0 for the padding."""
+    import torch
+    w = torch.zeros(N_OUT, device="cuda")
+    w[:N_TARGETS] = 1.0
+    return w
+
+
+def train(model: SurrogateModel, X, Tn, *, epochs: int, batch: int = 16384, lr: float = 1e-3, seed: int = 0,
+          log=print) -> list[float]:
+    """Adam with cosine learning-rate decay over `epochs` passes of (X, Tn);
+    returns the mean normalized squared error of each epoch."""
+    import torch
+    n = X.shape[0]
+    steps_per_epoch = n // batch
+    total = epochs * steps_per_epoch
+    w = target_weights()
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    history = []
+    step = 0
+    for ep in range(epochs):
+        perm = torch.randperm(n, device="cuda", generator=g).to(torch.int32)
+        model._buffers(batch)["loss"].zero_()
+        for q in range(steps_per_epoch):
+            rate = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(1, total)))
+            model.train_step(X, Tn, perm[q * batch:(q + 1) * batch], w, lr=rate)
+            step += 1
+        loss = float(model._buf["loss"].item()) / (steps_per_epoch * batch * N_TARGETS)
+        history.append(loss)
+        if log:
+            log(f"epoch {ep + 1}/{epochs}: normalized MSE {loss:.5f}")
+    return history
+
+
+# ---------------------------------------------------------------------------
+# inference with gate and plain-kernel fallback
+# ---------------------------------------------------------------------------
+@dataclass
+class SurrogateResult:
+    rthratenlw: object
+    rthratensw: object
+    glw: object
+    lwupb: object
+    swdnb: object
+    swupb: object
+    flags: object          # per column: 0 surrogate, 1 input range, 2 energy gate (bits)
+    n_fallback: int
+
+
+def infer(model: SurrogateModel, st, d: dict | None = None, *, energy_tol: float = 5.0,
+          fallback: bool = True) -> SurrogateResult:
+    """Surrogate radiation for a domain (synthetic.ColumnState; device fields d
+    as torch CUDA tensors, built from st when None) with per-column gate and
+    plain-kernel fallback."""
+    import torch
+    lib = _capi.load()
+    if st.nk != NK:
+        raise ValueError(f"the surrogate is built for {NK} levels, got {st.nk}")
+    d = d if d is not None else _device_fields(st, "cuda")
+    nx, ny, nk = st.nx, st.ny, st.nk
+    ncol = nx * ny
+    mpad = (ncol + 127) // 128 * 128
+    s = _stream()
+    X = torch.zeros(mpad, K_IN, device="cuda", dtype=torch.bfloat16)
+    flags = torch.empty(ncol, device="cuda", dtype=torch.int32)
+    fa = _feature_args(d, nk, ny, ncol)
+    fa.mean, fa.rstd = model.norm.in_mean.data_ptr(), model.norm.in_rstd.data_ptr()
+    fa.X, fa.ldx = X.data_ptr(), K_IN
+    fa.lo, fa.hi, fa.flags = model.norm.in_lo.data_ptr(), model.norm.in_hi.data_ptr(), flags.data_ptr()
+    _check(lib.rrtmg_sur_features(ctypes.byref(fa), s), "features")
+    bf = torch.bfloat16
+    H = [torch.empty(mpad, HIDDEN, device="cuda", dtype=bf) for _ in range(3)]
+    Y = model.forward(X, H=H)
+    out = dict(rthratenlw=torch.empty(nx, nk, ny, device="cuda"), rthratensw=torch.empty(nx, nk, ny, device="cuda"))
+    for k in ("glw", "lwupb", "swdnb", "swupb"):
+        out[k] = torch.empty(nx, ny, device="cuda")
+    da = _capi.SurDecodeArgs(ncol=ncol, nk=nk, ny=ny, Y=Y.data_ptr(), ldy=N_OUT,
+                             out_mean=model.norm.out_mean.data_ptr(), out_std=model.norm.out_std.data_ptr(),
+                             coszr=d["coszr"].data_ptr(), pi3d=d["pi3d"].data_ptr(), p8w=d["p8w"].data_ptr(),
+                             energy_tol=energy_tol, **{k: v.data_ptr() for k, v in out.items()},
+                             flags=flags.data_ptr())
+    _check(lib.rrtmg_sur_decode(ctypes.byref(da), s), "decode")
+    n_fb = 0
+    if fallback:
+        n_fb = _fallback(st, d, flags, out)
+    return SurrogateResult(flags=flags, n_fallback=n_fb, **out)
+
+
+_FIELDS_3D = ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d", "re_cloud",
+              "re_ice", "re_snow")
+_FIELDS_LEV = ("p8w", "t8w")
+_FIELDS_2D = ("tsk", "emiss", "albedo", "coszr", "xland", "xice", "snow")
+
+
+def _fallback(st, d: dict, flags, out: dict) -> int:
+    """Re-solve the flagged columns with the plain kernels, writing their
+    surrogate outputs over; returns how many columns were re-solved."""
+    import torch
+    from . import rrtmg
+    lib = _capi.load()
+    s = _stream()
+    nx, ny, nk = st.nx, st.ny, st.nk
+    ncol = nx * ny
+    lst = torch.empty(ncol, device="cuda", dtype=torch.int32)
+    cnt = torch.zeros(1, device="cuda", dtype=torch.int32)
+    _check(lib.rrtmg_sur_compact(flags.data_ptr(), ncol, lst.data_ptr(), cnt.data_ptr(), s), "compact")
+    n = int(cnt.item())
+    if n == 0:
+        return 0
+    mv = lambda src, dst, nz, to: _check(lib.rrtmg_sur_move_columns(lst.data_ptr(), cnt.data_ptr(), n, nz, ny,
+                                                                     src.data_ptr(), dst.data_ptr(), to, s), "move")
+    sub = {}
+    for k in _FIELDS_3D:
+        sub[k] = torch.empty(1, nk, n, device="cuda")
+        mv(d[k], sub[k], nk, 1)
+    for k in _FIELDS_LEV:
+        sub[k] = torch.empty(1, nk + 1, n, device="cuda")
+        mv(d[k], sub[k], nk + 1, 1)
+    for k in _FIELDS_2D:
+        sub[k] = torch.empty(1, n, device="cuda")
+        mv(d[k], sub[k], 1, 1)
+    lw_kw = {k: (sub[k] if k in sub else v) for k, v in st.lw_kwargs().items()}
+    sw_kw = {k: (sub[k] if k in sub else v) for k, v in st.sw_kwargs().items()}
+    lw = rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw)
+    sw = rrtmg.rrtmg_swrad_wrf_columns(**sw_kw)
+    mv(lw.rthratenlw, out["rthratenlw"], nk, 0)
+    mv(sw.rthratensw, out["rthratensw"], nk, 0)
+    mv(lw.glw, out["glw"], 1, 0)
+    mv(lw.lwupb, out["lwupb"], 1, 0)
+    mv(sw.swdnb, out["swdnb"], 1, 0)
+    mv(sw.swupb, out["swupb"], 1, 0)
+    return n
+
+
+def heating_kday(rthraten, pi3d):
+    """Heating rate in K/day from a theta tendency (rthraten * 86400 * pi3d)."""
+    return rthraten * 86400.0 * pi3d
