@@ -1,20 +1,29 @@
-"""Benchmark: LW+SW RRTMG radiation columns per second on B200.
+"""Benchmark: LW+SW radiation columns per second on B200.
 
-One step = one rrtmg_lwrad + one rrtmg_swrad call over the whole 425 x 425 x 50
-domain (180,625 columns, the plain-kernel workload) with inputs resident in
-HBM.  `e2e` repeats the step through the public Python API with host (numpy)
-buffers, so the host->device copies of the inputs and the device->host copies
-of every output are inside the timed region.
+Default workload (the metric's own configuration): the learned surrogate with
+its per-column gate and plain-kernel fallback on a 1000 x 1000 x 50 domain
+(1,000,000 columns, inference generator), against the plain B200 RRTMG
+kernels on the same columns.  One step = one full-domain LW+SW radiation
+call; `value` is the surrogate+fallback columns/s, `plain_value` the plain
+kernels' columns/s, and the line carries the heating and surface-flux RMSE of
+the surrogate path against the plain kernels and the fallback fraction.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+`--workload plain` measures the plain kernels alone on the 425 x 425 x 50
+domain (180,625 columns) with per-launch kernel times and their roofline.
 
-With N > 1 (torchrun, one rank per GPU) every rank runs its own 425x425x50
-domain (weak scaling; columns are independent, so there is no collective on the
-data path) and the time is the maximum over ranks.
+`e2e` repeats the step with host (numpy) inputs: the host->device copies of
+the inputs and the device->host copies of the outputs are inside the timed
+region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload surrogate|plain] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs its own domain (weak
+scaling; columns are independent, so there is no collective on the data path)
+and the time is the maximum over ranks.
 
 `--impl reference` times the CPU restatement of the reference's algorithm
-(oracle/, the reference itself needs jax/jaxlib which are not installed) on the
-host cores, on a bounded sample of the same workload per step.
+(oracle/; the reference itself needs jax/jaxlib, which are not installed) on
+the host cores, on a bounded sample of the same workload per step.
 """
 
 from __future__ import annotations
@@ -34,6 +43,9 @@ import numpy as np
 
 REPO = Path(__file__).resolve().parent
 WORKLOAD = dict(name="plain_425x425x50", nx=425, ny=425, nk=50, seed=0)
+SURROGATE_WORKLOAD = dict(name="surrogate_fallback_1000x1000x50", nx=1000, ny=1000, nk=50, seed=2)
+WEIGHTS = REPO / "wrf-jax_b200" / "weights" / "surrogate_nk50.npz"
+GATE = REPO / "wrf-jax_b200" / "weights" / "surrogate_nk50_gate.json"
 METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0.2 K/day"
 # oracle columns timed for the CPU baseline: 100 rows of the domain, about 2-3 s
 # on 16 host threads (roughly 40 core-seconds of work)
@@ -128,22 +140,21 @@ def _dist():
     return ws, rank, local
 
 
-def cpu_baseline(ncols_sample: int, threads: int | None = None, reps: int = 1):
-    """Time the oracle (CPU restatement, 'port') on a bounded sample of the workload."""
+def cpu_baseline(ncols_sample: int, threads: int | None = None, reps: int = 1, workload: dict | None = None):
+    """Time the oracle (CPU restatement, 'port') on a bounded sample of the
+    workload: a domain of the workload's row length and generator seed with
+    ncols_sample // ny rows."""
     _package()
     from wrf_jax_b200 import synthetic, tables
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle
 
+    wl = workload or WORKLOAD
     threads = threads or os.cpu_count() or 1
-    ny = WORKLOAD["ny"]
+    ny = wl["ny"]
     nx = max(1, ncols_sample // ny)
-    st = synthetic.make_columns(WORKLOAD["nx"], ny, WORKLOAD["nk"], seed=WORKLOAD["seed"])
+    st = synthetic.make_columns(nx, ny, wl["nk"], seed=wl["seed"])
     kw_lw, kw_sw = st.lw_kwargs(), st.sw_kwargs()
-    for kw in (kw_lw, kw_sw):
-        for k, v in list(kw.items()):
-            if isinstance(v, np.ndarray):
-                kw[k] = np.ascontiguousarray(v[:nx])
     ora = oracle.Oracle(tables.DEFAULT_BLOB, nthreads=threads)
     times = []
     for _ in range(reps):
@@ -152,10 +163,11 @@ def cpu_baseline(ncols_sample: int, threads: int | None = None, reps: int = 1):
         ora.swrad(**kw_sw)
         times.append(time.perf_counter() - t0)
     cols = nx * ny
-    return cols / min(times), threads, f"{nx}x{ny}x{WORKLOAD['nk']} rows of the 425x425x50 domain ({cols} columns)", min(times)
+    desc = f"{nx}x{ny}x{wl['nk']} columns ({cols}) from the {wl['name']} generator"
+    return cols / min(times), threads, desc, min(times)
 
 
-def run_reference(args):
+def run_reference(args, wl: dict):
     ws, rank, _ = _dist()
     if rank != 0:
         return
@@ -163,48 +175,34 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     times = []
     for _ in range(args.warmup):
-        cpu_baseline(sample, threads)
+        cpu_baseline(sample, threads, workload=wl)
+    desc = ""
     for _ in range(args.steps):
-        v, th, desc, dt = cpu_baseline(sample, threads)
+        v, th, desc, dt = cpu_baseline(sample, threads, workload=wl)
         times.append(dt)
     dt = statistics.median(times)
-    ncols = (sample // WORKLOAD["ny"]) * WORKLOAD["ny"]
+    ncols = (sample // wl["ny"]) * wl["ny"]
     value = ncols / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOAD["name"], "columns_per_step": ncols, "nk": WORKLOAD["nk"]},
+        "config": {"workload": wl["name"], "columns_per_step": ncols, "nk": wl["nk"]},
         "cpu_baseline": {"value": value, "unit": "columns/s", "cores": threads, "kind": "port",
-                         "sample": f"{ncols} columns of the 425x425x50 domain per step; C restatement "
-                                   "of the reference path (jax/jaxlib are not installed, so the "
-                                   "reference's own JAX code cannot run on this host)"},
+                         "sample": desc + " per step; C restatement of the reference's plain RRTMG path "
+                                   "(jax/jaxlib are not installed, so the reference's own JAX code cannot run "
+                                   "on this host)"},
         "e2e": {"value": value, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--nx", type=int, default=None, help="override the domain (profiling cases)")
-    ap.add_argument("--ny", type=int, default=None)
-    ap.add_argument("--nk", type=int, default=None)
-    ap.add_argument("--e2e-steps", type=int, default=None)
-    args = ap.parse_args()
+def run_plain(args):
     for key in ("nx", "ny", "nk"):
         if getattr(args, key) is not None:
             WORKLOAD[key] = getattr(args, key)
     if any(getattr(args, k) is not None for k in ("nx", "ny", "nk")):
         WORKLOAD["name"] = "plain_%dx%dx%d" % (WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nk"])
-    if args.impl == "reference":
-        run_reference(args)
-        return
-
     import torch
 
     ws, rank, local = _dist()
@@ -344,12 +342,163 @@ def main():
         "clocks": clocks.summary(),
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", str(CPU_SAMPLE_COLUMNS))))
+        v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", str(CPU_SAMPLE_COLUMNS))),
+                                       workload=WORKLOAD)
         line["cpu_baseline"] = {"value": v, "unit": "columns/s", "cores": th, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def _surrogate_launches(n_fallback: int) -> int:
+    """Kernel launches of one surrogate step: features, 4 GEMMs, decode,
+    compact; with fallback columns also 22 gathers, 6 scatters and the plain
+    LW (3) and SW (3) launches."""
+    return 7 + (34 if n_fallback > 0 else 0)
+
+
+def run_surrogate(args):
+    import torch
+
+    wl = dict(SURROGATE_WORKLOAD)
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    _package()
+    from wrf_jax_b200 import surrogate as S, synthetic
+
+    if not WEIGHTS.exists():
+        raise FileNotFoundError(f"{WEIGHTS} is missing: train it with wrf-jax_b200/train_surrogate.py")
+    model = S.SurrogateModel.load(WEIGHTS)
+    tol = json.loads(GATE.read_text())["energy_tol"] if GATE.exists() else 5.0
+    st = synthetic.make_columns(wl["nx"], wl["ny"], wl["nk"], seed=wl["seed"] + rank)
+    ncol = st.nx * st.ny
+    d = S._device_fields(st, "cuda")
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, steps):
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        out = None
+        for _ in range(steps):
+            out = fn()
+        t1.record(stream)
+        barrier()
+        el = t0.elapsed_time(t1) / 1e3
+        if dist is not None:
+            tt = torch.tensor([el], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = float(tt.item())
+        return el, out
+
+    sur = lambda: S.infer(model, st, d, energy_tol=tol, fallback=True)
+    plain = lambda: S._plain(st, d)
+    for _ in range(max(3, args.warmup)):
+        sur()
+    plain()
+    with ClockSampler(local) as clocks:
+        el_sur, res = timed(sur, args.steps)
+        el_plain, (lw, sw) = timed(plain, max(1, min(args.steps, 3)))
+    n_plain_steps = max(1, min(args.steps, 3))
+    value = ws * ncol * args.steps / el_sur
+    plain_value = ws * ncol * n_plain_steps / el_plain
+
+    # accuracy of the surrogate path against the plain kernels on the same columns
+    pi = d["pi3d"]
+    hl, hs = S.heating_kday(res.rthratenlw, pi), S.heating_kday(res.rthratensw, pi)
+    rl, rs = S.heating_kday(lw.rthratenlw, pi), S.heating_kday(sw.rthratensw, pi)
+    heat_rmse = float(torch.sqrt(torch.cat([(hl - rl).flatten(), (hs - rs).flatten()]).pow(2).mean()))
+    flux = torch.stack([res.glw - lw.glw, res.lwupb - lw.lwupb, res.swdnb - sw.swdnb, res.swupb - sw.swupb])
+    flux_rmse = float(torch.sqrt((flux ** 2).mean()))
+
+    # forward GEMMs alone (the tensor-core part) for the roofline
+    mpad = (ncol + 127) // 128 * 128
+    X = torch.zeros(mpad, S.K_IN, device="cuda", dtype=torch.bfloat16)
+    H = [torch.empty(mpad, S.HIDDEN, device="cuda", dtype=torch.bfloat16) for _ in range(3)]
+    Y = torch.empty(mpad, S.N_OUT, device="cuda")
+    for _ in range(3):
+        model.forward(X, H=H, Y=Y)
+    el_gemm, _ = timed(lambda: model.forward(X, H=H, Y=Y), args.steps)
+    gemm_ms = el_gemm / args.steps * 1e3
+    flops = 2.0 * mpad * sum(o * i for o, i in S.LAYER_SHAPES)
+    hbm, bf16, peak_kind = _peaks()
+    achieved = flops / (gemm_ms / 1e3) / 1e12
+
+    # end to end with host inputs and host outputs
+    e2e_steps = max(0, args.e2e_steps) if args.e2e_steps is not None else 2
+    h2d = sum(v.nbytes for v in st.fields.values())
+    d2h = 0
+    barrier()
+    t_e2e = time.perf_counter()
+    for _ in range(e2e_steps):
+        dh = {k: torch.from_numpy(v).to("cuda", non_blocking=False) for k, v in st.fields.items()}
+        r = S.infer(model, st, dh, energy_tol=tol, fallback=True)
+        outs = [x.cpu().numpy() for x in (r.rthratenlw, r.rthratensw, r.glw, r.lwupb, r.swdnb, r.swupb)]
+        d2h = sum(o.nbytes for o in outs)
+    barrier()
+    t_e2e = max(time.perf_counter() - t_e2e, 1e-9)
+    e2e = ws * ncol * e2e_steps / t_e2e if e2e_steps else None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el_sur / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (surrogate GEMMs, FP32 accumulate) + f32 (fallback)",
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": wl["name"], "nx": wl["nx"], "ny": wl["ny"], "nk": wl["nk"], "columns_per_gpu": ncol,
+                   "l2": "inputs larger than L2 (%.0f MB per step)" % (h2d / 1e6),
+                   "energy_gate_tol_wm2": tol, "weights": WEIGHTS.name},
+        "plain_value": plain_value, "plain_ms_per_step": el_plain / n_plain_steps * 1e3,
+        "speedup_vs_plain": value / plain_value,
+        "heating_rmse_kday": heat_rmse, "surface_flux_rmse_wm2": flux_rmse,
+        "fallback_fraction": res.n_fallback / ncol,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                     "frac": achieved / bf16, "traffic": None, "kernel": "umma_gemm_kernel (4 forward GEMMs)",
+                     "kernel_ms": gemm_ms, "flops_per_launch_set": flops, "peak_source": peak_kind},
+        "gpu_launches": _surrogate_launches(res.n_fallback) * args.steps,
+        "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", str(CPU_SAMPLE_COLUMNS))),
+                                       workload=wl)
+        line["cpu_baseline"] = {"value": v, "unit": "columns/s", "cores": th, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--workload", choices=("surrogate", "plain"), default="surrogate")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=None, help="override the plain domain (profiling cases)")
+    ap.add_argument("--ny", type=int, default=None)
+    ap.add_argument("--nk", type=int, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args, SURROGATE_WORKLOAD if args.workload == "surrogate" else WORKLOAD)
+    elif args.workload == "plain":
+        run_plain(args)
+    else:
+        run_surrogate(args)
 
 
 if __name__ == "__main__":

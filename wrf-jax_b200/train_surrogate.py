@@ -70,6 +70,34 @@ def evaluate(model, nx: int, ny: int, seed: int, energy_tol: float) -> dict:
     return out
 
 
+def calibrate_gate(model, nx: int, ny: int, seed: int, heating_target: float = 0.2, flux_target: float = 2.0,
+                   tolerances=(1e30, 20.0, 10.0, 5.0, 3.0, 2.0, 1.5, 1.0, 0.75, 0.5, 0.3, 0.2, 0.1, 0.05)) -> dict:
+    """Energy-gate tolerance sweep on a calibration domain: the largest
+    tolerance whose surrogate+fallback heating and surface-flux RMSE against
+    the plain kernels meet the targets (0: every column falls back)."""
+    import torch
+    from wrf_jax_b200 import surrogate as S, synthetic
+
+    st = synthetic.make_columns(nx, ny, S.NK, seed=seed)
+    d = S._device_fields(st, "cuda")
+    lw, sw = S._plain(st, d)
+    pi = d["pi3d"]
+    rl, rs = S.heating_kday(lw.rthratenlw, pi), S.heating_kday(sw.rthratensw, pi)
+    sweep, chosen = [], 0.0
+    for tol in tolerances:
+        res = S.infer(model, st, d, energy_tol=tol, fallback=True)
+        hl, hs = S.heating_kday(res.rthratenlw, pi), S.heating_kday(res.rthratensw, pi)
+        heat = float(torch.sqrt(torch.cat([(hl - rl).flatten(), (hs - rs).flatten()]).pow(2).mean()))
+        flux = torch.stack([res.glw - lw.glw, res.lwupb - lw.lwupb, res.swdnb - sw.swdnb, res.swupb - sw.swupb])
+        fl = float(torch.sqrt((flux ** 2).mean()))
+        frac = res.n_fallback / (nx * ny)
+        sweep.append(dict(energy_tol=tol, heating_rmse_kday=heat, surface_flux_rmse_wm2=fl, fallback_fraction=frac))
+        if heat <= heating_target and fl <= flux_target and chosen == 0.0:
+            chosen = tol
+    return dict(energy_tol=chosen, heating_target_kday=heating_target, flux_target_wm2=flux_target,
+                calibration_domain=[nx, ny, seed], sweep=sweep)
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--columns", type=int, default=2_000_000)
@@ -81,6 +109,7 @@ def main(argv=None) -> int:
     ap.add_argument("--eval", type=int, nargs=2, default=(256, 256), metavar=("NX", "NY"))
     ap.add_argument("--out", type=Path, required=True)
     ap.add_argument("--metrics", type=Path, default=None)
+    ap.add_argument("--gate", type=Path, default=None, help="write the calibrated energy-gate tolerance here")
     args = ap.parse_args(argv)
     _package()
     import torch
@@ -106,6 +135,11 @@ def main(argv=None) -> int:
                    data_seconds=t_data, train_seconds=t_train, steps=model.step, loss_history=hist,
                    gemm_timeout_flag=flag,
                    eval=evaluate(model, args.eval[0], args.eval[1], seed=2, energy_tol=args.energy_tol))
+    gate = calibrate_gate(model, 256, 256, seed=3)
+    metrics["gate"] = gate
+    metrics["eval_calibrated"] = evaluate(model, args.eval[0], args.eval[1], seed=2, energy_tol=gate["energy_tol"])
+    if args.gate:
+        args.gate.write_text(json.dumps(gate, indent=1))
     text = json.dumps(metrics, indent=1)
     print(text)
     if args.metrics:
