@@ -26,7 +26,8 @@ def _operands(torch, M, N, K, seed):
     return A, B, bias
 
 
-@pytest.mark.parametrize("M,N,K,ksplit", [(128, 128, 64, 1), (256, 384, 512, 1), (512, 128, 1024, 4)])
+@pytest.mark.parametrize("M,N,K,ksplit", [(128, 128, 64, 1), (256, 384, 512, 1), (512, 128, 1024, 4),
+                                         (384, 512, 192, 1), (256, 256, 2048, 8)])
 def test_gemm_f32_matches_torch(torch_cuda, M, N, K, ksplit):
     torch = torch_cuda
     from wrf_jax_b200 import surrogate, _capi

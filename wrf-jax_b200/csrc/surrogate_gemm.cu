@@ -3,22 +3,22 @@
 //
 //   C[M x N] = A[M x K] * B[N x K]^T      (A, B row-major BF16, FP32 accumulate)
 //
-// One CTA of 128 threads owns a 128 x 128 output tile.  Its accumulator lives
-// in tensor memory (128 lanes x 128 FP32 columns).  K advances in blocks of
-// 64: all threads copy the A and B blocks into shared memory (cp.async, two
-// stages) in the no-swizzle K-major core-matrix layout, and one thread issues
-// four tcgen05.mma (K = 16 each) whose completion is committed to the stage's
-// mbarrier, so the copy of block k + 1 overlaps the MMAs of block k.  The
-// epilogue reads the accumulator back with tcgen05.ld (warp w owns lanes
-// 32w..32w+31, i.e. tile rows) and applies one of:
+// One CTA of 128 threads owns a 128 x BN output tile (BN = 256 when N allows,
+// else 128).  Its accumulator lives in tensor memory (128 lanes x BN FP32
+// columns).  K advances in blocks of 64: all threads copy the A and B blocks
+// into shared memory (cp.async, 3-4 stages in flight) in the no-swizzle K-major
+// core-matrix layout, and one thread issues four tcgen05.mma (K = 16 each)
+// whose completion is committed to the stage's mbarrier before the stage is
+// refilled.  The epilogue reads the accumulator back with tcgen05.ld (warp w
+// owns lanes 32w..32w+31, i.e. tile rows) and applies one of:
 //   kEpiF32    C (+ bias) as FP32, one slab per K split (split-K partials)
 //   kEpiGelu   Z = acc + bias (FP32), H = GELU(Z) as BF16 row-major and
 //              transposed (the transposed copy feeds the weight gradient)
 //   kEpiDgelu  dZ = acc * GELU'(aux) as BF16 row-major and transposed
 //
-// Shared-memory layout of an operand block (128 rows x 64 K, BF16): the 16-byte
-// chunk (row r, k-chunk kc) sits at kc * 2048 + r * 16, which is the canonical
-// K-major SWIZZLE_NONE layout with leading-byte offset 2048 (next k-chunk) and
+// Shared-memory layout of an operand block (R rows x 64 K, BF16): the 16-byte
+// chunk (row r, k-chunk kc) sits at kc * 16 R + r * 16, which is the canonical
+// K-major SWIZZLE_NONE layout with leading-byte offset 16 R (next k-chunk) and
 // stride-byte offset 128 (next 8-row group).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -29,18 +29,25 @@
 namespace rrtmg {
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64;
+constexpr int kBM = 128, kBK = 64;
 constexpr int kThreads = 128;
-constexpr int kStages = 2;
-constexpr int kOperandBytes = kBM * kBK * 2;  // 16 KB
-constexpr int kSmemBytes = 2 * kStages * kOperandBytes;
-constexpr uint32_t kLbo = 2048, kSbo = 128;
+constexpr uint32_t kSbo = 128;               // next 8-row group of a k-chunk
+constexpr uint32_t kLboA = kBM * 16;         // next k-chunk of an A block
 constexpr uint64_t kWaitNs = 2000000000ull;  // bounded mbarrier wait: 2 s
 
-// tcgen05 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B BF16
-// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
-constexpr uint32_t kIdesc =
-    (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) | (static_cast<uint32_t>(kBM >> 4) << 24);
+template <int BN>
+struct Tile {
+  static constexpr int kStages = BN == 256 ? 3 : 4;
+  static constexpr int kBytesA = kBM * kBK * 2;
+  static constexpr int kBytesB = BN * kBK * 2;
+  static constexpr int kStageBytes = kBytesA + kBytesB;
+  static constexpr int kSmemBytes = kStages * kStageBytes;
+  static constexpr uint32_t kLboB = BN * 16;
+  // tcgen05 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B
+  // BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+  static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
+                                     (static_cast<uint32_t>(kBM >> 4) << 24);
+};
 
 __device__ unsigned g_gemm_error;
 
@@ -50,9 +57,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 // Shared-memory matrix descriptor (start, leading and stride byte offsets in
 // 16-byte units, descriptor version 1, no swizzle).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo) {
   uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>((kLbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
   d |= static_cast<uint64_t>((kSbo >> 4) & 0x3FFFu) << 32;
   d |= static_cast<uint64_t>(1) << 46;
   return d;
@@ -91,27 +98,32 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
+// Tile (m-tile = blockIdx.y, n-tile = blockIdx.x, K split = blockIdx.z): the
+// n-tiles of one m-tile are neighbouring CTAs, so they share the A rows in L2.
+// K blocks stream through kStages shared-memory stages: the copies of block
+// kb + kStages - 1 are in flight while the tensor cores work on block kb.
+template <int BN>
 __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
+  using TL = Tile<BN>;
+  constexpr int S = TL::kStages;
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t *sA = smem;
-  uint8_t *sB = smem + kStages * kOperandBytes;
-  __shared__ __align__(8) uint64_t mbar[kStages];
+  __shared__ __align__(8) uint64_t mbar[S];
   __shared__ uint32_t tmem_sh;
   __shared__ int fail_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * kBM;
   const int kper = g.K / g.ksplit;
   const int kbeg = blockIdx.z * kper;
   const int nkb = kper / kBK;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
-                 "r"(kBN));
+                 "r"(BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s)
+    for (int s = 0; s < S; ++s)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[s])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fail_sh = 0;
@@ -121,44 +133,54 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_sh;
 
-  int issued = 0;  // K blocks whose MMAs were issued and committed
-  for (int kb = 0; kb < nkb; ++kb) {
-    const int s = kb & 1;
-    if (kb >= kStages) {
-      // the MMAs of block kb - 2 read this stage; wait before overwriting it
-      if (tid == 0 && !mbar_wait(smem_u32(&mbar[s]), ((kb - kStages) >> 1) & 1)) fail_sh = 1;
-      __syncthreads();
-      if (fail_sh) break;
-    }
+  auto stage_a = [&](int s) { return smem + s * TL::kStageBytes; };
+  auto stage_b = [&](int s) { return smem + s * TL::kStageBytes + TL::kBytesA; };
+  auto load = [&](int kb, int s) {
     const int k0 = kbeg + kb * kBK;
-    uint8_t *a = sA + s * kOperandBytes, *b = sB + s * kOperandBytes;
+    uint8_t *a = stage_a(s), *b = stage_b(s);
 #pragma unroll
     for (int i = 0; i < (kBM * kBK / 8) / kThreads; ++i) {
       const int q = tid + i * kThreads;
-      const int r = q & (kBM - 1), kc = q >> 7;
-      cp_async16(a + kc * kLbo + r * 16, g.A + static_cast<size_t>(m0 + r) * g.lda + k0 + kc * 8);
-      cp_async16(b + kc * kLbo + r * 16, g.B + static_cast<size_t>(n0 + r) * g.ldb + k0 + kc * 8);
+      const int r = q & (kBM - 1), kc = q / kBM;
+      cp_async16(a + kc * kLboA + r * 16, g.A + static_cast<size_t>(m0 + r) * g.lda + k0 + kc * 8);
     }
+#pragma unroll
+    for (int i = 0; i < (BN * kBK / 8) / kThreads; ++i) {
+      const int q = tid + i * kThreads;
+      const int r = q & (BN - 1), kc = q / BN;
+      cp_async16(b + kc * TL::kLboB + r * 16, g.B + static_cast<size_t>(n0 + r) * g.ldb + k0 + kc * 8);
+    }
+  };
+
+  // prologue: blocks 0 .. S-2, one commit group each (empty groups keep the count)
+#pragma unroll
+  for (int s = 0; s < S - 1; ++s) {
+    if (s < nkb) load(s, s);
     asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
+  }
+  bool ok = true;
+  int issued = 0;
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = kb % S;
+    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
     // make the generic-proxy shared-memory writes visible to the tensor cores
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t abase = smem_u32(a), bbase = smem_u32(b);
+      const uint32_t abase = smem_u32(stage_a(s)), bbase = smem_u32(stage_b(s));
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; ++kk) {
-        const uint64_t adesc = smem_desc(abase + kk * 2 * kLbo);
-        const uint64_t bdesc = smem_desc(bbase + kk * 2 * kLbo);
+        const uint64_t adesc = smem_desc(abase + kk * 2 * kLboA, kLboA);
+        const uint64_t bdesc = smem_desc(bbase + kk * 2 * TL::kLboB, TL::kLboB);
         const uint32_t accumulate = (kb > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
             :
-            : "r"(tmem), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+            : "r"(tmem), "l"(adesc), "l"(bdesc), "r"(TL::kIdesc), "r"(accumulate)
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -166,11 +188,23 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
                    : "memory");
     }
     issued = kb + 1;
+    const int next = kb + S - 1;
+    if (next < nkb) {
+      // stage next % S was last read by the MMAs of block kb - 1
+      if (kb >= 1 && !mbar_wait(smem_u32(&mbar[(kb - 1) % S]), static_cast<uint32_t>((kb - 1) / S) & 1u)) ok = false;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) fail_sh = 1;
+        break;
+      }
+      load(next, next % S);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   // wait for the last committed group (it covers every earlier MMA)
   if (issued > 0) {
     const int last = issued - 1;
-    if (tid == 0 && !mbar_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1)) fail_sh = 1;
+    if (tid == 0 && !mbar_wait(smem_u32(&mbar[last % S]), static_cast<uint32_t>(last / S) & 1u)) fail_sh = 1;
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -180,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
   } else {
     const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
-    for (int c = 0; c < kBN; c += 16) {
+    for (int c = 0; c < BN; c += 16) {
       uint32_t v[16];
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
@@ -216,22 +250,28 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
   }
+}
+
+template <int BN>
+cudaError_t launch_tile(const GemmArgs &g, cudaStream_t stream) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Tile<BN>::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid(g.N / BN, g.M / kBM, g.ksplit);
+  umma_gemm_kernel<BN><<<grid, kThreads, Tile<BN>::kSmemBytes, stream>>>(g);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_umma_gemm(const GemmArgs &g, cudaStream_t stream) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  dim3 grid(g.M / kBM, g.N / kBN, g.ksplit);
-  umma_gemm_kernel<<<grid, kThreads, kSmemBytes, stream>>>(g);
-  return cudaGetLastError();
+  return g.N % 256 == 0 ? launch_tile<256>(g, stream) : launch_tile<128>(g, stream);
 }
 
 cudaError_t gemm_error_flag(unsigned *out, bool reset) {
