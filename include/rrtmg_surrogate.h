@@ -21,7 +21,8 @@ enum { RRTMG_EPI_F32 = 0, RRTMG_EPI_GELU = 1, RRTMG_EPI_DGELU = 2 };
 
 /* C[M x N] = A[M x K] * B[N x K]^T with A, B row-major BF16 and FP32
  * accumulation in tensor memory.  M and N multiples of 128; K a multiple of
- * 64 * ksplit; lda, ldb multiples of 8; 16-byte aligned A and B.
+ * 64 * ksplit; lda, ldb, ldh multiples of 8 and ldc, ldz, ldaux, split_stride
+ * multiples of 4; every pointer 16-byte aligned.
  *   RRTMG_EPI_F32:   C + z * split_stride [M][ldc] = partial sum of K split z
  *                    (+ bias[N] on split 0).
  *   RRTMG_EPI_GELU:  Z[M][ldz] = acc + bias (FP32, optional), H[M][ldh] and

@@ -18,6 +18,10 @@ extern "C" rrtmg_status rrtmg_gemm_bf16(const rrtmg_gemm_args *a, void *stream) 
   if (a->M % 128 || a->N % 128 || a->K % (64 * a->ksplit)) return RRTMG_BAD_ARG;
   if (a->lda % 8 || a->ldb % 8 || a->lda < a->K || a->ldb < a->K) return RRTMG_BAD_ARG;
   if (!aligned16(a->A) || !aligned16(a->B)) return RRTMG_BAD_ARG;
+  // the epilogue stores 16-byte vectors along rows
+  if ((a->C && (!aligned16(a->C) || a->ldc % 4 || a->split_stride % 4)) || (a->Z && (!aligned16(a->Z) || a->ldz % 4)) ||
+      (a->aux && (!aligned16(a->aux) || a->ldaux % 4)) || (a->H && (!aligned16(a->H) || a->ldh % 8)))
+    return RRTMG_BAD_ARG;
   switch (a->epilogue) {
     case RRTMG_EPI_F32:
       if (!a->C || a->ldc < a->N) return RRTMG_BAD_ARG;

@@ -223,25 +223,53 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
             "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
           : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c)));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      // each thread holds 16 consecutive columns of its row: row-major outputs
+      // are written as 16-byte vectors, transposed ones as 2-byte elements
+      // that are contiguous across the warp's 32 rows
+      float acc[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c + j;
-        const float acc = __uint_as_float(v[j]);
-        if (g.epi == kEpiF32) {
-          float out = acc;
-          if (g.bias && blockIdx.z == 0) out += g.bias[n];
-          g.C[static_cast<size_t>(blockIdx.z) * g.split_stride + static_cast<size_t>(row) * g.ldc + n] = out;
-        } else if (g.epi == kEpiGelu) {
-          const float z = acc + (g.bias ? g.bias[n] : 0.0f);
-          const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
-          if (g.Z) g.Z[static_cast<size_t>(row) * g.ldz + n] = z;
-          if (g.H) g.H[static_cast<size_t>(row) * g.ldh + n] = h;
-          if (g.Ht) g.Ht[static_cast<size_t>(n) * g.ldht + row] = h;
+      for (int j = 0; j < 16; ++j) acc[j] = __uint_as_float(v[j]);
+      const int nc = n0 + c;
+      if (g.epi == kEpiF32) {
+        if (g.bias && blockIdx.z == 0) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[j] += g.bias[nc + j];
+        }
+        float4 *dst = reinterpret_cast<float4 *>(g.C + static_cast<size_t>(blockIdx.z) * g.split_stride +
+                                                 static_cast<size_t>(row) * g.ldc + nc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dst[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+      } else {
+        __align__(16) __nv_bfloat16 h[16];
+        if (g.epi == kEpiGelu) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[j] += g.bias ? g.bias[nc + j] : 0.0f;
+          if (g.Z) {
+            float4 *dz = reinterpret_cast<float4 *>(g.Z + static_cast<size_t>(row) * g.ldz + nc);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dz[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) h[j] = __float2bfloat16_rn(gelu(acc[j]));
         } else {  // kEpiDgelu
-          const float dz = acc * gelu_grad(g.aux[static_cast<size_t>(row) * g.ldaux + n]);
-          const __nv_bfloat16 h = __float2bfloat16_rn(dz);
-          if (g.H) g.H[static_cast<size_t>(row) * g.ldh + n] = h;
-          if (g.Ht) g.Ht[static_cast<size_t>(n) * g.ldht + row] = h;
+          const float4 *za = reinterpret_cast<const float4 *>(g.aux + static_cast<size_t>(row) * g.ldaux + nc);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 z = za[q];
+            h[4 * q + 0] = __float2bfloat16_rn(acc[4 * q + 0] * gelu_grad(z.x));
+            h[4 * q + 1] = __float2bfloat16_rn(acc[4 * q + 1] * gelu_grad(z.y));
+            h[4 * q + 2] = __float2bfloat16_rn(acc[4 * q + 2] * gelu_grad(z.z));
+            h[4 * q + 3] = __float2bfloat16_rn(acc[4 * q + 3] * gelu_grad(z.w));
+          }
+        }
+        if (g.H) {
+          uint4 *dh = reinterpret_cast<uint4 *>(g.H + static_cast<size_t>(row) * g.ldh + nc);
+          dh[0] = *reinterpret_cast<const uint4 *>(&h[0]);
+          dh[1] = *reinterpret_cast<const uint4 *>(&h[8]);
+        }
+        if (g.Ht) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) g.Ht[static_cast<size_t>(nc + j) * g.ldht + row] = h[j];
         }
       }
     }
