@@ -120,6 +120,8 @@ rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_config *cfg,
  * rrtmg_lwrad / rrtmg_swrad call records CUDA events on its stream around its
  * three kernel launches (LW: McICA masks, band groups, finish; SW: McICA
  * masks, day-column compaction, column kernel), for up to 256 calls per side.
+ * Domains of more than 131,072 columns run LW in column chunks; the band-
+ * group duration then includes the finish kernels of all but the last chunk.
  * rrtmg_timing_read waits for the recorded calls and writes, oldest first,
  * three durations in milliseconds per call to ms[3 * i + k]; side 0 = LW,
  * 1 = SW.  It returns the number of calls written (at most max_calls), or -1. */

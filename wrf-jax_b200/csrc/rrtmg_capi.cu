@@ -531,7 +531,8 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   uint32_t *mask = nullptr;
   float *terms = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
-  const size_t terms_bytes = lw_terms_floats(cfg->nk, ncol) * sizeof(float);
+  const int chunk = ncol < kLwChunkColumns ? ncol : kLwChunkColumns;
+  const size_t terms_bytes = lw_terms_floats(cfg->nk, chunk) * sizeof(float);
   e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
   e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&terms), terms_bytes, ctx->pool, stream);
@@ -569,9 +570,16 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
   a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
   a.terms = terms;
-  e = launch_lw_groups(ctx->tables, a, stream);
-  timing_mark(ctx, 0, tslot, 2, stream);
-  if (e == cudaSuccess) e = launch_lw_finish(a, stream);
+  // chunks of columns: band groups then finish per chunk, reusing the term
+  // scratch; timing mark 2 follows the last chunk's band groups, so the
+  // finish launches of the earlier chunks count with the band groups
+  for (int first = 0; first < ncol && e == cudaSuccess; first += chunk) {
+    a.chunk_first = first;
+    a.chunk_count = ncol - first < chunk ? ncol - first : chunk;
+    e = launch_lw_groups(ctx->tables, a, stream);
+    if (first + chunk >= ncol) timing_mark(ctx, 0, tslot, 2, stream);
+    if (e == cudaSuccess) e = launch_lw_finish(a, stream);
+  }
   timing_mark(ctx, 0, tslot, 3, stream);
   cudaError_t ef = cudaFreeAsync(terms, stream);
   cudaError_t ef2 = cudaFreeAsync(mask, stream);

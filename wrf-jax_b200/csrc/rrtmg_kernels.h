@@ -32,8 +32,12 @@ struct LwArgs {
   float *rthraten, *rthratenc;
   float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc, *glw, *olr, *lwcf;
   float *zero2[4];  // *cln fields, written as zeros
-  float *terms;     // band-group schedule scratch, lw_terms_floats(nk, ncol) floats
+  float *terms;     // band-group schedule scratch, lw_terms_floats(nk, chunk_count) floats
+  int chunk_first, chunk_count;  // columns of one band-group/finish launch pair
 };
+
+// columns per band-group/finish launch pair (the term scratch holds one chunk)
+constexpr int kLwChunkColumns = 131072;
 
 struct SwArgs {
   int nx, ny, nk, nlay, ncol;

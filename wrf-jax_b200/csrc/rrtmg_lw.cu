@@ -1221,7 +1221,7 @@ __global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
 // total/clear; slot = flux level 0..nk, or nk + 1 for the top of the
 // atmosphere (level nlay) when nlay > nk.
 __device__ __forceinline__ size_t term_index(const LwArgs &a, int type, int slot, int band, int col) {
-  return ((static_cast<size_t>(type) * (a.nk + 2) + slot) * kLwBands + band) * a.ncol + col;
+  return ((static_cast<size_t>(type) * (a.nk + 2) + slot) * kLwBands + band) * a.chunk_count + (col - a.chunk_first);
 }
 
 template <int B>
@@ -1311,8 +1311,8 @@ __device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int c
 constexpr int kLwGroups = 9;
 
 __global__ void __launch_bounds__(128, 3) lw_group_kernel(Tables T, LwArgs a) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.ncol) return;
+  const int col = a.chunk_first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.chunk_first + a.chunk_count) return;
   switch (blockIdx.y) {
     case 0: lw_group<2>(T, a, col); break;
     case 1: lw_group<4>(T, a, col); break;
@@ -1329,8 +1329,8 @@ __global__ void __launch_bounds__(128, 3) lw_group_kernel(Tables T, LwArgs a) {
 // Ordered band sums of every level, fluxes, heating rates (lw:5702-5712,
 // 7040-7057) and the 2-D outputs (lw:7059-7077).
 __global__ void __launch_bounds__(128) lw_finish_kernel(LwArgs a) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.ncol) return;
+  const int col = a.chunk_first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.chunk_first + a.chunk_count) return;
   const int i = col / a.ny, j = col - i * a.ny;
   const int nk = a.nk, nlay = a.nlay;
   const float pi = 3.1415926535897932384626433832795f;
@@ -1402,14 +1402,14 @@ size_t lw_terms_floats(int nk, int ncol) {
 
 cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
-  const int blocks = (a.ncol + threads - 1) / threads;
+  const int blocks = (a.chunk_count + threads - 1) / threads;
   lw_group_kernel<<<dim3(blocks, kLwGroups), threads, 0, stream>>>(T, a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
-  const int blocks = (a.ncol + threads - 1) / threads;
+  const int blocks = (a.chunk_count + threads - 1) / threads;
   lw_finish_kernel<<<blocks, threads, 0, stream>>>(a);
   return cudaGetLastError();
 }

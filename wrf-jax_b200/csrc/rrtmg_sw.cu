@@ -25,6 +25,8 @@ namespace {
 constexpr int kNgc[kSwBands] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};
 constexpr int kGofs[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
 constexpr int kMaxNgc = 12;
+// day columns per launch of the column kernel
+constexpr int kSwChunkColumns = 131072;
 constexpr int kMaxLev = kMaxLay + 1;
 constexpr float kOneMinus = 1.0f - 1.0e-6f;
 
@@ -861,9 +863,9 @@ __global__ void __launch_bounds__(256) sw_daylist_kernel(SwArgs a) {
   a.swddif[col] = 0.0f; a.swdownc[col] = 0.0f; a.swddnic[col] = 0.0f; a.swddirc[col] = 0.0f;
 }
 
-__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= *a.nday) return;
+__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, int count) {
+  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= first + count || t >= *a.nday) return;
   const int col = a.daylist[t];
   Col C;
   C.i = col / a.ny;
@@ -963,10 +965,16 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
 }
 
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+  // The day count is known only on the device: launch over ncol list slots in
+  // chunks; slots at or beyond the day count exit at once.
   const int threads = 128;
-  const int blocks = (a.ncol + threads - 1) / threads;
-  sw_kernel<<<blocks, threads, 0, stream>>>(T, a);
-  return cudaGetLastError();
+  for (int first = 0; first < a.ncol; first += kSwChunkColumns) {
+    const int count = a.ncol - first < kSwChunkColumns ? a.ncol - first : kSwChunkColumns;
+    sw_kernel<<<(count + threads - 1) / threads, threads, 0, stream>>>(T, a, first, count);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace rrtmg
