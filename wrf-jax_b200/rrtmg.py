@@ -155,15 +155,18 @@ def _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr, cfc11vmr, cfc12
 
 
 def _as_device(arrays: dict, device: int):
-    """numpy -> torch CUDA float32 (contiguous); torch CUDA tensors pass through."""
+    """numpy or host torch tensors -> torch CUDA float32 (contiguous); torch CUDA
+    tensors pass through.  Returns the tensors and whether any input was on the host."""
     import torch
 
     out = {}
     host = False
     for k, v in arrays.items():
-        if isinstance(v, torch.Tensor):
-            if not v.is_cuda:
-                raise ValueError(f"{k}: torch tensors must be on a CUDA device")
+        if isinstance(v, torch.Tensor) and not v.is_cuda:
+            # host tensor (pinned memory copies asynchronously); results come back to the host
+            host = True
+            t = v.contiguous().float().to(device=f"cuda:{device}", non_blocking=v.is_pinned())
+        elif isinstance(v, torch.Tensor):
             t = v.contiguous()
             if t.dtype != torch.float32:
                 t = t.float()
