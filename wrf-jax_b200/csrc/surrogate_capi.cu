@@ -124,7 +124,8 @@ extern "C" rrtmg_status rrtmg_sur_adam(const rrtmg_sur_adam_args *a, void *strea
 }
 
 extern "C" rrtmg_status rrtmg_sur_decode(const rrtmg_sur_decode_args *a, void *stream) {
-  if (!a || a->ncol < 0 || a->nk <= 0 || a->ny <= 0 || !a->Y || a->ldy < 2 * a->nk + 6 || !a->out_mean ||
+  if (!a || a->ncol < 0 || a->nk <= 0 || a->ny <= 0 || !a->Y || a->ldy < 2 * a->nk + 6 || 2 * a->nk + 6 > 128 ||
+      !a->out_mean ||
       !a->out_std || !a->coszr || !a->pi3d || !a->p8w || !a->rthratenlw || !a->rthratensw || !a->glw || !a->lwupb ||
       !a->swdnb || !a->swupb || !a->flags)
     return RRTMG_BAD_ARG;

@@ -31,46 +31,89 @@ __device__ __forceinline__ size_t idx3(int c, int k, int nk, int ny) {
   return (static_cast<size_t>(i) * nk + k) * ny + j;
 }
 
-__global__ void features_kernel(SurFeatureArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncol) return;
+// Value of feature f (f < 9 nk + 4) of column c.
+__device__ __forceinline__ float feature_value(const SurFeatureArgs &a, int c, int f) {
   const int nk = a.nk, ny = a.ny;
-  const size_t row = static_cast<size_t>(a.row_offset + c);
+  if (f >= 9 * nk) {
+    switch (f - 9 * nk) {
+      case 0: return a.tsk[c];
+      case 1: return a.albedo[c];
+      case 2: return a.coszr[c];
+      default: return a.emiss[c];
+    }
+  }
+  const int field = f / nk, k = f - field * nk;
+  const size_t q = idx3(c, k, nk, ny);
+  switch (field) {
+    case 0: return a.t3d[q];
+    case 1: return logf(a.p3d[q]);
+    case 2: return a.qv[q];
+    case 3: return a.qc[q];
+    case 4: return a.qi[q];
+    case 5: return a.qs[q];
+    case 6: return a.cldfra[q];
+    case 7: return a.o3[q];
+    default: return a.p8w[idx3(c, k, nk + 1, ny)] - a.p8w[idx3(c, k + 1, nk + 1, ny)];
+  }
+}
+
+// A block owns kFeatCols consecutive columns and walks the features in chunks
+// of kFeatChunk: each thread evaluates one (column, feature) at a time with
+// the columns fastest (coalesced field reads), the chunk is staged in shared
+// memory, and the rows of the row-major outputs are written contiguously.
+constexpr int kFeatCols = 64, kFeatChunk = 64;
+
+__global__ void __launch_bounds__(256) features_kernel(SurFeatureArgs a) {
+  __shared__ float tile[kFeatChunk][kFeatCols + 1];
+  __shared__ int oob[kFeatCols];
+  const int c0 = blockIdx.x * kFeatCols;
+  const int nf = 9 * a.nk + 4;
+  const int width = a.X ? a.ldx : nf;
   __nv_bfloat16 *X = static_cast<__nv_bfloat16 *>(a.X), *Xt = static_cast<__nv_bfloat16 *>(a.Xt);
-  bool in_range = true;
-  auto put = [&](int f, float v) {
-    if (a.raw) a.raw[row * a.ldf + f] = v;
-    if (X) {
-      const float z = (v - a.mean[f]) * a.rstd[f];
-      X[row * a.ldx + f] = __float2bfloat16_rn(z);
-      if (Xt) Xt[static_cast<size_t>(f) * a.ldxt + row] = __float2bfloat16_rn(z);
+  for (int i = threadIdx.x; i < kFeatCols; i += blockDim.x) oob[i] = 0;
+  __syncthreads();
+  for (int f0 = 0; f0 < width; f0 += kFeatChunk) {
+    // evaluate: thread -> (feature, column) with the column fastest
+    for (int e = threadIdx.x; e < kFeatChunk * kFeatCols; e += blockDim.x) {
+      const int lf = e / kFeatCols, lc = e - lf * kFeatCols;
+      const int f = f0 + lf, c = c0 + lc;
+      float v = 0.0f;
+      if (c < a.ncol && f < nf) {
+        v = feature_value(a, c, f);
+        if (a.lo && (v < a.lo[f] || v > a.hi[f])) oob[lc] = 1;
+      }
+      tile[lf][lc] = v;
     }
-    if (a.lo && (v < a.lo[f] || v > a.hi[f])) in_range = false;
-  };
-  for (int k = 0; k < nk; ++k) {
-    const size_t q = idx3(c, k, nk, ny);
-    const float plo = a.p8w[idx3(c, k, nk + 1, ny)], phi = a.p8w[idx3(c, k + 1, nk + 1, ny)];
-    put(0 * nk + k, a.t3d[q]);
-    put(1 * nk + k, logf(a.p3d[q]));
-    put(2 * nk + k, a.qv[q]);
-    put(3 * nk + k, a.qc[q]);
-    put(4 * nk + k, a.qi[q]);
-    put(5 * nk + k, a.qs[q]);
-    put(6 * nk + k, a.cldfra[q]);
-    put(7 * nk + k, a.o3[q]);
-    put(8 * nk + k, plo - phi);
+    __syncthreads();
+    // store: thread -> (column, feature) with the feature fastest (row-major rows)
+    for (int e = threadIdx.x; e < kFeatChunk * kFeatCols; e += blockDim.x) {
+      const int lc = e / kFeatChunk, lf = e - lc * kFeatChunk;
+      const int f = f0 + lf, c = c0 + lc;
+      if (c >= a.ncol || f >= width) continue;
+      const size_t row = static_cast<size_t>(a.row_offset + c);
+      const float v = tile[lf][lc];
+      if (a.raw && f < nf) a.raw[row * a.ldf + f] = v;
+      if (X) X[row * a.ldx + f] = __float2bfloat16_rn(f < nf ? (v - a.mean[f]) * a.rstd[f] : 0.0f);
+    }
+    if (Xt) {
+      // transposed copy: thread -> (feature, column) with the column fastest
+      for (int e = threadIdx.x; e < kFeatChunk * kFeatCols; e += blockDim.x) {
+        const int lf = e / kFeatCols, lc = e - lf * kFeatCols;
+        const int f = f0 + lf, c = c0 + lc;
+        if (c >= a.ncol || f >= a.ldx) continue;
+        const float v = tile[lf][lc];
+        Xt[static_cast<size_t>(f) * a.ldxt + a.row_offset + c] =
+            __float2bfloat16_rn(f < nf ? (v - a.mean[f]) * a.rstd[f] : 0.0f);
+      }
+    }
+    __syncthreads();
   }
-  put(9 * nk + 0, a.tsk[c]);
-  put(9 * nk + 1, a.albedo[c]);
-  put(9 * nk + 2, a.coszr[c]);
-  put(9 * nk + 3, a.emiss[c]);
-  if (X) {
-    for (int f = 9 * nk + 4; f < a.ldx; ++f) {
-      X[row * a.ldx + f] = __float2bfloat16_rn(0.0f);
-      if (Xt) Xt[static_cast<size_t>(f) * a.ldxt + row] = __float2bfloat16_rn(0.0f);
+  if (a.flags) {
+    for (int lc = threadIdx.x; lc < kFeatCols; lc += blockDim.x) {
+      const int c = c0 + lc;
+      if (c < a.ncol) a.flags[c] = oob[lc] ? 1u : 0u;
     }
   }
-  if (a.flags) a.flags[c] = in_range ? 0u : 1u;
 }
 
 __global__ void targets_kernel(SurTargetArgs a) {
@@ -251,34 +294,46 @@ __global__ void adam_kernel(SurAdamArgs a) {
 }
 
 // Decode normalized network outputs into WRF fields and apply the energy gate.
-__global__ void decode_kernel(SurDecodeArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncol) return;
+// A block of kDecCols columns first copies their output rows (contiguous) into
+// shared memory, then each thread decodes one column.
+constexpr int kDecCols = 64, kDecWidth = 128;
+
+__global__ void __launch_bounds__(kDecCols) decode_kernel(SurDecodeArgs a) {
+  __shared__ float ys[kDecCols][kDecWidth + 1];
+  const int c0 = blockIdx.x * kDecCols;
   const int nk = a.nk, ny = a.ny;
-  const float *y = a.Y + static_cast<size_t>(c) * a.ldy;
-  auto out = [&](int f) { return y[f] * a.out_std[f] + a.out_mean[f]; };
+  const int width = 2 * nk + 6;
+  for (int e = threadIdx.x; e < kDecCols * width; e += blockDim.x) {
+    const int lc = e / width, f = e - lc * width;
+    const int c = c0 + lc;
+    ys[lc][f] = c < a.ncol ? a.Y[static_cast<size_t>(c) * a.ldy + f] * a.out_std[f] + a.out_mean[f] : 0.0f;
+  }
+  __syncthreads();
+  const int c = c0 + threadIdx.x;
+  if (c >= a.ncol) return;
+  const float *y = ys[threadIdx.x];
   const bool day = a.coszr[c] > 0.0f;
   float slw = 0.0f, ssw = 0.0f;
   for (int k = 0; k < nk; ++k) {
     const size_t q = idx3(c, k, nk, ny);
     const float pi = a.pi3d[q];
-    const float hlw = out(k);
-    const float hsw = day ? out(nk + k) : 0.0f;
+    const float hlw = y[k];
+    const float hsw = day ? y[nk + k] : 0.0f;
     a.rthratenlw[q] = (hlw / 86400.0f) / pi;
     a.rthratensw[q] = (hsw / 86400.0f) / pi;
     const float dp = (a.p8w[idx3(c, k, nk + 1, ny)] - a.p8w[idx3(c, k + 1, nk + 1, ny)]) * 0.01f;
     slw += hlw * dp / kHeatfac;
     ssw += hsw * dp / kHeatfac;
   }
-  const float glw = out(2 * nk), lwupb = out(2 * nk + 1);
-  const float swdnb = day ? out(2 * nk + 2) : 0.0f, swupb = day ? out(2 * nk + 3) : 0.0f;
+  const float glw = y[2 * nk], lwupb = y[2 * nk + 1];
+  const float swdnb = day ? y[2 * nk + 2] : 0.0f, swupb = day ? y[2 * nk + 3] : 0.0f;
   a.glw[c] = glw;
   a.lwupb[c] = lwupb;
   a.swdnb[c] = swdnb;
   a.swupb[c] = swupb;
   // energy gate: column-integrated heating against net surface minus model-top flux
-  const float lw_res = fabsf(((lwupb - glw) - out(2 * nk + 4)) - slw);
-  const float sw_res = day ? fabsf((out(2 * nk + 5) - (swdnb - swupb)) - ssw) : 0.0f;
+  const float lw_res = fabsf(((lwupb - glw) - y[2 * nk + 4]) - slw);
+  const float sw_res = day ? fabsf((y[2 * nk + 5] - (swdnb - swupb)) - ssw) : 0.0f;
   unsigned f = a.flags[c];
   if (!(lw_res <= a.energy_tol) || !(sw_res <= a.energy_tol)) f |= 2u;
   a.flags[c] = f;
@@ -314,7 +369,7 @@ __global__ void move_columns_kernel(const int *list, const int *count, int nz, i
 }  // namespace
 
 cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s) {
-  features_kernel<<<(a.ncol + 127) / 128, 128, 0, s>>>(a);
+  features_kernel<<<(a.ncol + kFeatCols - 1) / kFeatCols, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -368,7 +423,7 @@ cudaError_t launch_sur_adam(const SurAdamArgs &a, cudaStream_t s) {
 }
 
 cudaError_t launch_sur_decode(const SurDecodeArgs &a, cudaStream_t s) {
-  decode_kernel<<<(a.ncol + 127) / 128, 128, 0, s>>>(a);
+  decode_kernel<<<(a.ncol + kDecCols - 1) / kDecCols, kDecCols, 0, s>>>(a);
   return cudaGetLastError();
 }
 
