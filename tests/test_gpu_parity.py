@@ -48,6 +48,9 @@ def test_sw_matches_reference_golden(rrtmg, golden, case):
     (17, 23, 50, 1, dict(fractional_clouds=True)),
     (9, 40, 60, 2, dict(has_req=True, cloud_p=0.6)),
     (33, 7, 24, 3, dict(p_top=2000.0, night_fraction=0.0)),
+    # more than 4,096 columns: the one-thread-per-column SW schedule (smaller
+    # domains above run the band-split schedule)
+    (96, 64, 44, 4, dict(fractional_clouds=True)),
 ])
 def test_random_domains_match_oracle(rrtmg, oracle, pkg, nx, ny, nk, seed, extra):
     from wrf_jax_b200 import synthetic

@@ -660,10 +660,25 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
   a.nday = daylist + ncol;
   a.daylist = daylist;
+  float *split_terms = nullptr;
+  if (ncol <= kSwSplitMaxColumns) {
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&split_terms),
+                                sw_split_terms_floats(cfg->nk, ncol) * sizeof(float), ctx->pool, stream);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(daylist, stream);
+      cudaFreeAsync(mask, stream);
+      return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(sw band terms)");
+    }
+  }
+  a.split_terms = split_terms;
   e = launch_sw_daylist(a, stream);
   timing_mark(ctx, 1, tslot, 2, stream);
   if (e == cudaSuccess) e = launch_sw_columns(ctx->tables, a, stream);
   timing_mark(ctx, 1, tslot, 3, stream);
+  if (split_terms) {
+    cudaError_t es = cudaFreeAsync(split_terms, stream);
+    if (e == cudaSuccess) e = es;
+  }
   cudaError_t ef = cudaFreeAsync(daylist, stream);
   cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sw kernel launch");

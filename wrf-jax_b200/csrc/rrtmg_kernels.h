@@ -52,7 +52,11 @@ struct SwArgs {
   float *zero2[4];
   int *nday;     // scratch: number of day columns (set by the compaction kernel)
   int *daylist;  // scratch: ncol entries, day column indices
+  float *split_terms;  // small domains: sw_split_terms_floats(nk, ncol) floats, else null
 };
+
+// domains up to this many columns use the band-split SW schedule
+constexpr int kSwSplitMaxColumns = 4096;
 
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
 // fused schedule (one thread per column, no scratch)
@@ -65,6 +69,7 @@ cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream);
 // day-column compaction (writes the night columns), then the column kernel over
 // the day columns; both need a.nday and a.daylist (1 + ncol ints)
 cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);
+size_t sw_split_terms_floats(int nk, int ncol);
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
 }  // namespace rrtmg

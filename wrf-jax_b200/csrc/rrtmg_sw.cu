@@ -604,9 +604,14 @@ __device__ __forceinline__ void down_step(Path &P, int r) {
   P.rdnd[r + 1] = P.refd[r] + P.trad[r] * P.trad[r] * P.rdnd[r] * zreflect;
 }
 
-template <int B>
+// kTerms = false: add each level term into the thread's accumulators (accs).
+// kTerms = true: store each level term (type, level, g-point) to `terms` with
+// stride tstride between (type, level, g-point) planes, for the ordered sums
+// of the finish kernel.
+template <int B, bool kTerms = false>
 __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
-                                        int clear_only, float *accs, Path &Pc, Path &Pt) {
+                                        int clear_only, float *accs, Path &Pc, Path &Pt, float *terms = nullptr,
+                                        size_t tstride = 0) {
   constexpr int ngc = kNgc[B];
   constexpr int gofs = kGofs[B];
   constexpr int bn = B + 16;
@@ -700,10 +705,18 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
     Pc.tdbt[0] = 1.0f;
     Pt.tdbt[0] = 1.0f;
     float tdbtc_nd = 1.0f, tdbt_nd = 1.0f;
-    float *accfdir = accs + 4 * kMaxLev, *acccdir = accs + 5 * kMaxLev;
     const float zincflx = ((C.adjflux * sflux[g]) * mu) * 1.0f;
-    accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
-    acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
+    auto term = [&](int type, int level) -> float & {
+      return terms[((static_cast<size_t>(type) * (n + 1) + level) * kSwGpts + G) * tstride];
+    };
+    float *accfdir = kTerms ? nullptr : accs + 4 * kMaxLev, *acccdir = kTerms ? nullptr : accs + 5 * kMaxLev;
+    if constexpr (kTerms) {
+      term(4, 0) = tdbt_nd * zincflx;
+      term(5, 0) = tdbtc_nd * zincflx;
+    } else {
+      accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
+      acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
+    }
     // thread-local table values of the next layer are loaded one layer ahead
     float nx_tr = taur[n - 1][g], nx_tg = taug[n - 1][g];
     float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
@@ -766,14 +779,20 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
       } else {
         tdbt_nd = tdbtc_nd;
       }
-      accfdir[r + 1] = accfdir[r + 1] + tdbt_nd * zincflx;
-      acccdir[r + 1] = acccdir[r + 1] + tdbtc_nd * zincflx;
+      if constexpr (kTerms) {
+        term(4, r + 1) = tdbt_nd * zincflx;
+        term(5, r + 1) = tdbtc_nd * zincflx;
+      } else {
+        accfdir[r + 1] = accfdir[r + 1] + tdbt_nd * zincflx;
+        acccdir[r + 1] = acccdir[r + 1] + tdbtc_nd * zincflx;
+      }
     }
     // surface boundary
     Pc.ref[n] = C.albedo; Pc.refd[n] = C.albedo; Pc.tra[n] = 0.0f; Pc.trad[n] = 0.0f; Pc.dbt[n] = 0.0f;
     Pt.ref[n] = C.albedo; Pt.refd[n] = C.albedo; Pt.tra[n] = 0.0f; Pt.trad[n] = 0.0f; Pt.dbt[n] = 0.0f;
     // bottom-up: upward adding and level fluxes (vrtqdr, sw:3655-3720)
-    float *accfu = accs, *accfd = accs + kMaxLev, *acccu = accs + 2 * kMaxLev, *acccd = accs + 3 * kMaxLev;
+    float *accfu = accs, *accfd = kTerms ? nullptr : accs + kMaxLev;
+    float *acccu = kTerms ? nullptr : accs + 2 * kMaxLev, *acccd = kTerms ? nullptr : accs + 3 * kMaxLev;
     float rupc = Pc.ref[n], rupdc = Pc.refd[n];
     float rupt = Pt.ref[n], rupdt = Pt.refd[n];
     // level arrays and accumulators of the next level are loaded one level ahead
@@ -788,14 +807,15 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
     };
     Lvl nc = load_lvl(Pc, n), nt = nc;
     if (!clear_only) nt = load_lvl(Pt, n);
-    float nfu = accfu[n], nfd = accfd[n], ncu = acccu[n], ncd = acccd[n];
+    float nfu = 0.0f, nfd = 0.0f, ncu = 0.0f, ncd = 0.0f;
+    if constexpr (!kTerms) { nfu = accfu[n]; nfd = accfd[n]; ncu = acccu[n]; ncd = acccd[n]; }
     for (int k = n; k >= 0; --k) {
       const Lvl c = nc, t = nt;
       const float afu = nfu, afd = nfd, acu = ncu, acd = ncd;
       if (k > 0) {
         nc = load_lvl(Pc, k - 1);
         if (!clear_only) nt = load_lvl(Pt, k - 1);
-        nfu = accfu[k - 1]; nfd = accfd[k - 1]; ncu = acccu[k - 1]; ncd = acccd[k - 1];
+        if constexpr (!kTerms) { nfu = accfu[k - 1]; nfd = accfd[k - 1]; ncu = acccu[k - 1]; ncd = acccd[k - 1]; }
       }
       if (k < n) {
         const float zrc = 1.0f / (1.0f - rupdc * c.refd);
@@ -821,10 +841,17 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
         fut = (t.tdbt * rupt + (t.tdn - t.tdbt) * rupdt) * zreft;
         fdt = t.tdbt + (t.tdn - t.tdbt + t.tdbt * rupt * t.rdnd) * zreft;
       }
-      accfu[k] = afu + fut * zincflx;
-      accfd[k] = afd + fdt * zincflx;
-      acccu[k] = acu + fuc * zincflx;
-      acccd[k] = acd + fdc * zincflx;
+      if constexpr (kTerms) {
+        term(0, k) = fut * zincflx;
+        term(1, k) = fdt * zincflx;
+        term(2, k) = fuc * zincflx;
+        term(3, k) = fdc * zincflx;
+      } else {
+        accfu[k] = afu + fut * zincflx;
+        accfd[k] = afd + fdt * zincflx;
+        acccu[k] = acu + fuc * zincflx;
+        acccd[k] = acd + fdc * zincflx;
+      }
     }
   }
 }
@@ -863,11 +890,8 @@ __global__ void __launch_bounds__(256) sw_daylist_kernel(SwArgs a) {
   a.swddif[col] = 0.0f; a.swdownc[col] = 0.0f; a.swddnic[col] = 0.0f; a.swddirc[col] = 0.0f;
 }
 
-__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, int count) {
-  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= first + count || t >= *a.nday) return;
-  const int col = a.daylist[t];
-  Col C;
+// Column set-up of a day column (buffer ozone, laytrop; sw:2491-2508, 7101-7306).
+__device__ __forceinline__ void sw_setup(const Tables &T, const SwArgs &a, int col, Col &C) {
   C.i = col / a.ny;
   C.j = col - C.i * a.ny;
   C.nk = a.nk;
@@ -875,7 +899,6 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, 
   C.nlay = a.nk + 1;
   const int nk = C.nk, n = C.nlay;
   const float coszen = ld(a.in.coszr + col);
-  const size_t rbase = static_cast<size_t>(C.i) * nk * C.ny + C.j;
   C.coszen = coszen;
   C.mu = fmaxf(coszen, 1.0e-10f);
   C.albedo = ld(a.in.albedo + col);
@@ -901,26 +924,14 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, 
     }
     C.laytrop = laytrop;
   }
-  const int clear_only = a.icld == 0;
-  float accs[6 * kMaxLev];
-  for (int k = 0; k < 6 * kMaxLev; ++k) accs[k] = 0.0f;
-  Path Pc, Pt;
-  const uint32_t *maskbase = a.mask + col;
-  sw_band<0>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<1>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<2>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<3>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<4>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<5>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<6>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<7>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<8>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<9>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<10>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<11>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<12>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<13>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  // accumulators are top-down (index 0 = TOA); outputs are bottom-up
+}
+
+// Heating rates, theta tendencies and 2-D outputs of a day column from its
+// level sums accs (six arrays of kMaxLev, top-down; sw:2285-2301, 2536-2719).
+__device__ __forceinline__ void sw_outputs(const SwArgs &a, const Col &C, int col, const float *accs) {
+  const int nk = C.nk, n = C.nlay;
+  const float coszen = C.coszen;
+  const size_t rbase = static_cast<size_t>(C.i) * nk * C.ny + C.j;
   const float *fu = accs, *fd = accs + kMaxLev, *cu = accs + 2 * kMaxLev, *cd = accs + 3 * kMaxLev;
   const float *fdir = accs + 4 * kMaxLev, *cdir = accs + 5 * kMaxLev;
   const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
@@ -955,6 +966,96 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, 
   a.swddnic[col] = cdir[n] / coszen;
 }
 
+
+__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, int count) {
+  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= first + count || t >= *a.nday) return;
+  const int col = a.daylist[t];
+  Col C;
+  sw_setup(T, a, col, C);
+  const int clear_only = a.icld == 0;
+  float accs[6 * kMaxLev];
+  for (int k = 0; k < 6 * kMaxLev; ++k) accs[k] = 0.0f;
+  Path Pc, Pt;
+  const uint32_t *maskbase = a.mask + col;
+  sw_band<0>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<1>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<2>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<3>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<4>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<5>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<6>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<7>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<8>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<9>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<10>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<11>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<12>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_band<13>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
+  sw_outputs(a, C, col, accs);
+}
+
+// Band-split schedule for small domains: thread (day column, band) runs one
+// band and stores its level terms; the finish kernel adds each level's terms
+// in g-point order (band order, then g within the band), which is the order
+// the accumulators of sw_kernel see.  A column's latency drops to its longest
+// band.
+__global__ void __launch_bounds__(128) sw_split_kernel(Tables T, SwArgs a, int first, int count) {
+  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= first + count || t >= *a.nday) return;
+  const int col = a.daylist[t];
+  Col C;
+  sw_setup(T, a, col, C);
+  const int clear_only = a.icld == 0;
+  Path Pc, Pt;
+  const uint32_t *maskbase = a.mask + col;
+  float *terms = a.split_terms + (t - first);
+  const size_t ts = static_cast<size_t>(count);
+  switch (blockIdx.y) {
+    case 0: sw_band<0, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 1: sw_band<1, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 2: sw_band<2, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 3: sw_band<3, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 4: sw_band<4, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 5: sw_band<5, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 6: sw_band<6, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 7: sw_band<7, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 8: sw_band<8, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 9: sw_band<9, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 10: sw_band<10, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 11: sw_band<11, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    case 12: sw_band<12, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+    default: sw_band<13, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+  }
+}
+
+__global__ void __launch_bounds__(128) sw_split_finish_kernel(Tables T, SwArgs a, int first, int count) {
+  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= first + count || t >= *a.nday) return;
+  const int col = a.daylist[t];
+  Col C;
+  C.i = col / a.ny;
+  C.j = col - C.i * a.ny;
+  C.nk = a.nk;
+  C.ny = a.ny;
+  C.nlay = a.nk + 1;
+  C.coszen = ld(a.in.coszr + col);
+  const int n = C.nlay;
+  const float *terms = a.split_terms + (t - first);
+  const size_t ts = static_cast<size_t>(count);
+  float accs[6 * kMaxLev];
+  for (int type = 0; type < 6; ++type) {
+    for (int level = 0; level <= n; ++level) {
+      float acc = 0.0f;
+      const float *p = terms + (static_cast<size_t>(type) * (n + 1) + level) * kSwGpts * ts;
+      for (int G = 0; G < kSwGpts; ++G) acc = acc + p[static_cast<size_t>(G) * ts];
+      accs[type * kMaxLev + level] = acc;
+    }
+  }
+  (void)T;
+  sw_outputs(a, C, col, accs);
+}
+
 }  // namespace
 
 cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
@@ -964,10 +1065,23 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+size_t sw_split_terms_floats(int nk, int ncol) {
+  return static_cast<size_t>(6) * (nk + 2) * kSwGpts * static_cast<size_t>(ncol);
+}
+
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+  const int threads = 128;
+  if (a.split_terms) {
+    // small domain: band-split schedule over all ncol list slots in one launch pair
+    const int blocks = (a.ncol + threads - 1) / threads;
+    sw_split_kernel<<<dim3(blocks, kSwBands), threads, 0, stream>>>(T, a, 0, a.ncol);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sw_split_finish_kernel<<<blocks, threads, 0, stream>>>(T, a, 0, a.ncol);
+    return cudaGetLastError();
+  }
   // The day count is known only on the device: launch over ncol list slots in
   // chunks; slots at or beyond the day count exit at once.
-  const int threads = 128;
   for (int first = 0; first < a.ncol; first += kSwChunkColumns) {
     const int count = a.ncol - first < kSwChunkColumns ? a.ncol - first : kSwChunkColumns;
     sw_kernel<<<(count + threads - 1) / threads, threads, 0, stream>>>(T, a, first, count);
