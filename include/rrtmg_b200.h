@@ -128,6 +128,18 @@ rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_config *cfg,
 rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable);
 int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_calls);
 
+/* Launch schedule of a context; no counterpart in the reference.  Columns per
+ * launch of the LW band-group/finish pair and of the SW column kernel, and the
+ * largest domain (columns) that runs the band-split SW schedule.  Defaults:
+ * 131072, 131072, 4096.  The autotuner of the ensemble runner sets them. */
+typedef struct {
+    int lw_chunk_columns;
+    int sw_chunk_columns;
+    int sw_split_max_columns;
+} rrtmg_schedule;
+rrtmg_status rrtmg_set_schedule(rrtmg_ctx *ctx, const rrtmg_schedule *schedule);
+rrtmg_status rrtmg_get_schedule(const rrtmg_ctx *ctx, rrtmg_schedule *schedule);
+
 /* Number of LW layers used for a model top and level count
  * (rrtmg_lw_nlayers, module_ra_rrtmg_common.py:1243-1247). */
 int rrtmg_lw_nlayers(double p_top, int nk);

@@ -130,14 +130,24 @@ typedef struct {
 } rrtmg_sur_decode_args;
 rrtmg_status rrtmg_sur_decode(const rrtmg_sur_decode_args *args, void *stream);
 
+/* Writes the GPU global timer (ns) to *slot when the stream reaches this point
+ * (stream-ordered, capturable in CUDA graphs; used for per-domain latencies). */
+rrtmg_status rrtmg_sur_timestamp(unsigned long long *slot, void *stream);
+
 /* Appends the columns with flags[c] != 0 to list; count must be zeroed first. */
 rrtmg_status rrtmg_sur_compact(const unsigned *flags, int ncol, int *list, int *count, void *stream);
 
 /* Gathers (to_compact = 1) or scatters (0) a field of nz levels between a
- * domain with south_north size ny and the compact (1, nz, count) domain of the
- * listed columns; max_n bounds the device-side count. */
+ * domain with south_north size ny and columns offset .. offset + count - 1 of
+ * a compact (1, nz, stride) domain holding the listed columns; max_n bounds
+ * the device-side count. */
 rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
-                                    float *dst, int to_compact, void *stream);
+                                    float *dst, int to_compact, int stride, int offset, void *stream);
+
+/* GEMM tile width: 0 = automatic (256 columns when N allows, else 128), or
+ * 128 / 256 (256 needs N % 256 == 0; narrower N falls back to 128).  Process-
+ * wide; set by the ensemble autotuner. */
+rrtmg_status rrtmg_gemm_set_tile(int bn);
 
 /* Synchronous: reads the sticky flag that a GEMM CTA sets when it gives up
  * waiting (2 s) for its tensor-core work; clears it when reset != 0. */

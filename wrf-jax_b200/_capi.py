@@ -50,6 +50,12 @@ class SwOut(ctypes.Structure):
     _fields_ = [(n, _F) for n in SW_OUT_FIELDS]
 
 
+class Schedule(ctypes.Structure):
+    """rrtmg_schedule (include/rrtmg_b200.h)."""
+    _fields_ = [("lw_chunk_columns", ctypes.c_int), ("sw_chunk_columns", ctypes.c_int),
+                ("sw_split_max_columns", ctypes.c_int)]
+
+
 class GemmArgs(ctypes.Structure):
     """rrtmg_gemm_args (include/rrtmg_surrogate.h)."""
     _fields_ = [("A", _F), ("lda", ctypes.c_int), ("B", _F), ("ldb", ctypes.c_int),
@@ -93,12 +99,12 @@ STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "
           4: "RRTMG_TIMEOUT"}
 
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
-           "rrtmg_lwrad_static_scratch", "rrtmg_timing_enable", "rrtmg_timing_read", "rrtmg_lw_nlayers",
-           "rrtmg_last_error", "rrtmg_status_string")
-SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_sur_features", "rrtmg_sur_targets",
+           "rrtmg_lwrad_static_scratch", "rrtmg_timing_enable", "rrtmg_timing_read", "rrtmg_set_schedule",
+           "rrtmg_get_schedule", "rrtmg_lw_nlayers", "rrtmg_last_error", "rrtmg_status_string")
+SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile", "rrtmg_sur_features", "rrtmg_sur_targets",
                      "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
                      "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
-                     "rrtmg_sur_compact", "rrtmg_sur_move_columns")
+                     "rrtmg_sur_compact", "rrtmg_sur_move_columns", "rrtmg_sur_timestamp")
 
 _lib = None
 
@@ -151,7 +157,11 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_sur_adam": [ctypes.POINTER(SurAdamArgs), V],
         "rrtmg_sur_decode": [ctypes.POINTER(SurDecodeArgs), V],
         "rrtmg_sur_compact": [P, I, P, P, V],
-        "rrtmg_sur_move_columns": [P, P, I, I, I, P, P, I, V],
+        "rrtmg_sur_move_columns": [P, P, I, I, I, P, P, I, I, I, V],
+        "rrtmg_gemm_set_tile": [I],
+        "rrtmg_sur_timestamp": [P, V],
+        "rrtmg_set_schedule": [V, ctypes.POINTER(Schedule)],
+        "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
     }
     for name, argtypes in sigs.items():
         fn = getattr(lib, name)

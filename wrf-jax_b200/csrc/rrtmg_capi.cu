@@ -42,6 +42,8 @@ struct rrtmg_ctx {
   std::map<std::tuple<int, int, int>, KissJump *> jumps;
   // stream-ordered per-call scratch; keeps its memory between calls
   cudaMemPool_t pool = nullptr;
+  // launch schedule (rrtmg_set_schedule)
+  int lw_chunk = kLwChunkColumns, sw_chunk = kSwChunkColumns, sw_split_max = kSwSplitMaxColumns;
   // optional per-launch timing: a ring of calls per side (0 LW, 1 SW), each
   // with kTimingMarks events recorded around the call's three launches
   bool timing = false;
@@ -531,7 +533,12 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   uint32_t *mask = nullptr;
   float *terms = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
-  const int chunk = ncol < kLwChunkColumns ? ncol : kLwChunkColumns;
+  int lw_chunk_setting;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mutex);
+    lw_chunk_setting = ctx->lw_chunk;
+  }
+  const int chunk = ncol < lw_chunk_setting ? ncol : lw_chunk_setting;
   const size_t terms_bytes = lw_terms_floats(cfg->nk, chunk) * sizeof(float);
   e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
@@ -660,8 +667,15 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
   a.nday = daylist + ncol;
   a.daylist = daylist;
+  int sw_split_max, sw_chunk;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mutex);
+    sw_split_max = ctx->sw_split_max;
+    sw_chunk = ctx->sw_chunk;
+  }
+  a.chunk_columns = sw_chunk;
   float *split_terms = nullptr;
-  if (ncol <= kSwSplitMaxColumns) {
+  if (ncol <= sw_split_max) {
     e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&split_terms),
                                 sw_split_terms_floats(cfg->nk, ncol) * sizeof(float), ctx->pool, stream);
     if (e != cudaSuccess) {
@@ -858,4 +872,27 @@ extern "C" int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_ca
     }
   }
   return count;
+}
+
+extern "C" rrtmg_status rrtmg_set_schedule(rrtmg_ctx *ctx, const rrtmg_schedule *sch) {
+  if (!ctx || !sch) return fail(ctx, RRTMG_BAD_ARG, "null context or schedule");
+  const int lo = 1024, hi = 1 << 24;
+  if (sch->lw_chunk_columns < lo || sch->lw_chunk_columns > hi || sch->sw_chunk_columns < lo ||
+      sch->sw_chunk_columns > hi || sch->sw_split_max_columns < 0 || sch->sw_split_max_columns > 16384)
+    return fail(ctx, RRTMG_BAD_ARG,
+                "schedule out of range: chunks 1024..16777216 columns, band-split limit 0..16384 columns");
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  ctx->lw_chunk = sch->lw_chunk_columns;
+  ctx->sw_chunk = sch->sw_chunk_columns;
+  ctx->sw_split_max = sch->sw_split_max_columns;
+  return RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_get_schedule(const rrtmg_ctx *ctx, rrtmg_schedule *sch) {
+  if (!ctx || !sch) return RRTMG_BAD_ARG;
+  std::lock_guard<std::mutex> lk(const_cast<rrtmg_ctx *>(ctx)->mutex);
+  sch->lw_chunk_columns = ctx->lw_chunk;
+  sch->sw_chunk_columns = ctx->sw_chunk;
+  sch->sw_split_max_columns = ctx->sw_split_max;
+  return RRTMG_OK;
 }

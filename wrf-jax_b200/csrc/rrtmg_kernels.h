@@ -36,7 +36,7 @@ struct LwArgs {
   int chunk_first, chunk_count;  // columns of one band-group/finish launch pair
 };
 
-// columns per band-group/finish launch pair (the term scratch holds one chunk)
+// default columns per band-group/finish launch pair (the term scratch holds one chunk)
 constexpr int kLwChunkColumns = 131072;
 
 struct SwArgs {
@@ -53,9 +53,12 @@ struct SwArgs {
   int *nday;     // scratch: number of day columns (set by the compaction kernel)
   int *daylist;  // scratch: ncol entries, day column indices
   float *split_terms;  // small domains: sw_split_terms_floats(nk, ncol) floats, else null
+  int chunk_columns;   // day-list slots per launch of the column kernel
 };
 
-// domains up to this many columns use the band-split SW schedule
+// defaults: columns per SW column-kernel launch, and the largest domain that
+// uses the band-split SW schedule
+constexpr int kSwChunkColumns = 131072;
 constexpr int kSwSplitMaxColumns = 4096;
 
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);

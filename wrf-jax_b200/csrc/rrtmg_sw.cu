@@ -25,8 +25,6 @@ namespace {
 constexpr int kNgc[kSwBands] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};
 constexpr int kGofs[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
 constexpr int kMaxNgc = 12;
-// day columns per launch of the column kernel
-constexpr int kSwChunkColumns = 131072;
 constexpr int kMaxLev = kMaxLay + 1;
 constexpr float kOneMinus = 1.0f - 1.0e-6f;
 
@@ -1082,8 +1080,9 @@ cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t str
   }
   // The day count is known only on the device: launch over ncol list slots in
   // chunks; slots at or beyond the day count exit at once.
-  for (int first = 0; first < a.ncol; first += kSwChunkColumns) {
-    const int count = a.ncol - first < kSwChunkColumns ? a.ncol - first : kSwChunkColumns;
+  const int chunk = a.chunk_columns > 0 ? a.chunk_columns : kSwChunkColumns;
+  for (int first = 0; first < a.ncol; first += chunk) {
+    const int count = a.ncol - first < chunk ? a.ncol - first : chunk;
     sw_kernel<<<(count + threads - 1) / threads, threads, 0, stream>>>(T, a, first, count);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

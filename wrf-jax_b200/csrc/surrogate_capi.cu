@@ -140,13 +140,27 @@ extern "C" rrtmg_status rrtmg_sur_compact(const unsigned *flags, int ncol, int *
 }
 
 extern "C" rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny,
-                                               const float *src, float *dst, int to_compact, void *stream) {
-  if (!list || !count || max_n < 0 || nz <= 0 || ny <= 0 || !src || !dst) return RRTMG_BAD_ARG;
-  return cuda_status(launch_sur_move_columns(list, count, max_n, nz, ny, src, dst, to_compact, as_stream(stream)));
+                                               const float *src, float *dst, int to_compact, int stride, int offset,
+                                               void *stream) {
+  if (!list || !count || max_n < 0 || nz <= 0 || ny <= 0 || !src || !dst || offset < 0 || stride < offset + max_n)
+    return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_move_columns(list, count, max_n, nz, ny, src, dst, to_compact, stride, offset,
+                                             as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_gemm_set_tile(int bn) {
+  if (bn != 0 && bn != 128 && bn != 256) return RRTMG_BAD_ARG;
+  set_gemm_tile(bn);
+  return RRTMG_OK;
 }
 
 extern "C" rrtmg_status rrtmg_sur_normalize(const float *in, int ldi, int n, int nf, const float *mean,
                                             const float *rstd, void *out, int ldo, int out_bf16, void *stream) {
   if (!in || !mean || !rstd || !out || n <= 0 || nf <= 0 || ldi < nf || ldo < nf) return RRTMG_BAD_ARG;
   return cuda_status(launch_sur_normalize(in, ldi, n, nf, mean, rstd, out, ldo, out_bf16, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_timestamp(unsigned long long *slot, void *stream) {
+  if (!slot) return RRTMG_BAD_ARG;
+  return cuda_status(launch_timestamp(slot, as_stream(stream)));
 }

@@ -298,8 +298,15 @@ cudaError_t launch_tile(const GemmArgs &g, cudaStream_t stream) {
 
 }  // namespace
 
+namespace {
+int g_tile_choice = 0;  // 0 automatic, else 128 or 256
+}  // namespace
+
+void set_gemm_tile(int bn) { g_tile_choice = bn; }
+
 cudaError_t launch_umma_gemm(const GemmArgs &g, cudaStream_t stream) {
-  return g.N % 256 == 0 ? launch_tile<256>(g, stream) : launch_tile<128>(g, stream);
+  const bool wide = g.N % 256 == 0 && g_tile_choice != 128;
+  return wide ? launch_tile<256>(g, stream) : launch_tile<128>(g, stream);
 }
 
 cudaError_t gemm_error_flag(unsigned *out, bool reset) {

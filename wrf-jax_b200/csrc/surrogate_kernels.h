@@ -58,7 +58,9 @@ cudaError_t launch_sur_adam(const SurAdamArgs &a, cudaStream_t s);
 cudaError_t launch_sur_decode(const SurDecodeArgs &a, cudaStream_t s);
 cudaError_t launch_sur_compact(const unsigned *flags, int ncol, int *list, int *count, cudaStream_t s);
 cudaError_t launch_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
-                                    float *dst, int to_compact, cudaStream_t s);
+                                    float *dst, int to_compact, int stride, int offset, cudaStream_t s);
+void set_gemm_tile(int bn);
+cudaError_t launch_timestamp(unsigned long long *slot, cudaStream_t s);
 // Reads (and optionally clears) the sticky flag set when a GEMM CTA gave up
 // waiting for its tensor-core work.
 cudaError_t gemm_error_flag(unsigned *out, bool reset);

@@ -339,6 +339,12 @@ __global__ void __launch_bounds__(kDecCols) decode_kernel(SurDecodeArgs a) {
   a.flags[c] = f;
 }
 
+__global__ void timestamp_kernel(unsigned long long *slot) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  *slot = t;
+}
+
 // Append flagged columns to a list (one atomic per warp).
 __global__ void compact_kernel(const unsigned *flags, int ncol, int *list, int *count) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -354,14 +360,14 @@ __global__ void compact_kernel(const unsigned *flags, int ncol, int *list, int *
 // Gather (to_compact = 1) or scatter (0) a field between a domain and the
 // compact (1, nz, n) domain of listed columns.
 __global__ void move_columns_kernel(const int *list, const int *count, int nz, int ny, const float *src, float *dst,
-                                    int to_compact) {
+                                    int to_compact, int stride, int offset) {
   const int n = *count;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * nz) return;
   const int k = t / n, j = t - k * n;
   const int c = list[j];
   const size_t full = idx3(c, k, nz, ny);
-  const size_t comp = static_cast<size_t>(k) * n + j;
+  const size_t comp = static_cast<size_t>(k) * stride + offset + j;
   if (to_compact) dst[comp] = src[full];
   else dst[full] = src[comp];
 }
@@ -433,11 +439,16 @@ cudaError_t launch_sur_compact(const unsigned *flags, int ncol, int *list, int *
 }
 
 cudaError_t launch_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
-                                    float *dst, int to_compact, cudaStream_t s) {
+                                    float *dst, int to_compact, int stride, int offset, cudaStream_t s) {
   const long long total = static_cast<long long>(max_n) * nz;
   if (total == 0) return cudaSuccess;
   move_columns_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(list, count, nz, ny, src, dst,
-                                                                                 to_compact);
+                                                                                 to_compact, stride, offset);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_timestamp(unsigned long long *slot, cudaStream_t s) {
+  timestamp_kernel<<<1, 1, 0, s>>>(slot);
   return cudaGetLastError();
 }
 

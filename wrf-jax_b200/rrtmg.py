@@ -203,15 +203,27 @@ def _check_rounding_token(token) -> None:
         raise NotImplementedError("nonzero (diagnostic) rounding tokens are not supported")
 
 
+def _check_outputs(out: dict, names, nx: int, nk: int, ny: int) -> None:
+    import torch
+    for k in names:
+        t = out[k]
+        shape = (nx, nk, ny) if k.startswith("rthraten") else (nx, ny)
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()
+                and tuple(t.shape) == shape):
+            raise ValueError(f"out[{k!r}] must be a contiguous float32 CUDA tensor of shape {shape}")
+
+
 def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, qi3d, qs3d, cldfra3d, o33d,
                             emiss, xland, xice, snow, re_cloud, re_ice, re_snow, p_top, yr, julian,
                             ghg_input=1, case_dir=None, cldovrlp=2, idcor=0, icloud=1, has_reqc=1,
                             has_reqi=1, has_reqs=1, co2vmr=None, n2ovmr=None, ch4vmr=None, cfc11vmr=None,
                             cfc12vmr=None, lookup_tables=None, spectral=None, pade_tables=None,
                             cloud_tables=None, setcoef_tables=None, rounding_token=None,
-                            context: RrtmgContext | None = None, stream=None) -> RrtmgLwWrfColumnResult:
+                            context: RrtmgContext | None = None, stream=None, out=None) -> RrtmgLwWrfColumnResult:
     """B200 ``RRTMG_LWRAD`` (module_ra_rrtmg_lw.py:6789).  Table keywords are
-    accepted for signature parity and ignored (the context owns the tables)."""
+    accepted for signature parity and ignored (the context owns the tables).
+    ``out``: optional dict of preallocated float32 CUDA tensors, one per result
+    field, written in place (used for CUDA-graph capture)."""
     import torch
 
     del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables, setcoef_tables
@@ -233,9 +245,11 @@ def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                            cfc11vmr=cfc11, cfc12vmr=cfc12, solcon=0.0, has_reqc=int(has_reqc),
                            has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
                            cldovrlp=int(cldovrlp))
-        outs = {k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny),
-                               dtype=torch.float32, device=f"cuda:{ctx.device}")
-                for k in _capi.LW_OUT_FIELDS}
+        outs = out if out is not None else {
+            k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), dtype=torch.float32,
+                           device=f"cuda:{ctx.device}") for k in _capi.LW_OUT_FIELDS}
+        if out is not None:
+            _check_outputs(out, _capi.LW_OUT_FIELDS, nx, nk, ny)
         cin = _capi.LwIn(**{k: d[k].data_ptr() for k in _capi.LW_IN_FIELDS})
         cout = _capi.LwOut(**{k: outs[k].data_ptr() for k in _capi.LW_OUT_FIELDS})
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
@@ -253,8 +267,8 @@ def rrtmg_swrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                             sf_surface_physics=2, alswvisdir=None, alswvisdif=None, alswnirdir=None,
                             alswnirdif=None, co2vmr=None, n2ovmr=None, ch4vmr=None, lookup_tables=None,
                             spectral=None, pade_tables=None, cloud_tables=None, rounding_token=None,
-                            context: RrtmgContext | None = None, stream=None) -> RrtmgSwWrfColumnResult:
-    """B200 ``rrtmg_swrad`` (module_ra_rrtmg_sw.py:2386)."""
+                            context: RrtmgContext | None = None, stream=None, out=None) -> RrtmgSwWrfColumnResult:
+    """B200 ``rrtmg_swrad`` (module_ra_rrtmg_sw.py:2386); ``out`` as for the LW call."""
     import torch
 
     del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables
@@ -277,9 +291,11 @@ def rrtmg_swrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                            cfc12vmr=0.0, solcon=float(np.float32(solcon)), has_reqc=int(has_reqc),
                            has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
                            cldovrlp=int(cldovrlp))
-        outs = {k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny),
-                               dtype=torch.float32, device=f"cuda:{ctx.device}")
-                for k in _capi.SW_OUT_FIELDS}
+        outs = out if out is not None else {
+            k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), dtype=torch.float32,
+                           device=f"cuda:{ctx.device}") for k in _capi.SW_OUT_FIELDS}
+        if out is not None:
+            _check_outputs(out, _capi.SW_OUT_FIELDS, nx, nk, ny)
         cin = _capi.SwIn(**{k: d[k].data_ptr() for k in _capi.SW_IN_FIELDS})
         cout = _capi.SwOut(**{k: outs[k].data_ptr() for k in _capi.SW_OUT_FIELDS})
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream

@@ -444,7 +444,8 @@ def _fallback(st, d: dict, flags, out: dict) -> int:
     if n == 0:
         return 0
     mv = lambda src, dst, nz, to: _check(lib.rrtmg_sur_move_columns(lst.data_ptr(), cnt.data_ptr(), n, nz, ny,
-                                                                     src.data_ptr(), dst.data_ptr(), to, s), "move")
+                                                                     src.data_ptr(), dst.data_ptr(), to, n, 0, s),
+                                         "move")
     sub = {}
     for k in _FIELDS_3D:
         sub[k] = torch.empty(1, nk, n, device="cuda")
