@@ -6,8 +6,8 @@
 // One CTA of 128 threads owns a 128 x BN output tile (BN = 256 when N allows,
 // else 128).  Its accumulator lives in tensor memory (128 lanes x BN FP32
 // columns).  K advances in blocks of 64: all threads copy the A and B blocks
-// into shared memory (cp.async, 3-4 stages in flight) in the no-swizzle K-major
-// core-matrix layout, and one thread issues four tcgen05.mma (K = 16 each)
+// into shared memory (cp.async, 3-4 stages in flight) in the 128-byte swizzled
+// K-major layout, and one thread issues four tcgen05.mma (K = 16 each)
 // whose completion is committed to the stage's mbarrier before the stage is
 // refilled.  The epilogue reads the accumulator back with tcgen05.ld (warp w
 // owns lanes 32w..32w+31, i.e. tile rows) and applies one of:
@@ -16,10 +16,10 @@
 //              transposed (the transposed copy feeds the weight gradient)
 //   kEpiDgelu  dZ = acc * GELU'(aux) as BF16 row-major and transposed
 //
-// Shared-memory layout of an operand block (R rows x 64 K, BF16): the 16-byte
-// chunk (row r, k-chunk kc) sits at kc * 16 R + r * 16, which is the canonical
-// K-major SWIZZLE_NONE layout with leading-byte offset 16 R (next k-chunk) and
-// stride-byte offset 128 (next 8-row group).
+// Shared-memory layout of an operand block (R rows x 64 K, BF16): the
+// canonical K-major SWIZZLE_128B layout, row r at r * 128 bytes with its eight
+// 16-byte chunks permuted by XOR with r mod 8, 8-row groups 1024 bytes apart;
+// each block stage starts on a 1024-byte boundary.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -31,8 +31,7 @@ namespace {
 
 constexpr int kBM = 128, kBK = 64;
 constexpr int kThreads = 128;
-constexpr uint32_t kSbo = 128;               // next 8-row group of a k-chunk
-constexpr uint32_t kLboA = kBM * 16;         // next k-chunk of an A block
+constexpr uint32_t kSbo = 1024;              // next 8-row group (8 rows x 128 B)
 constexpr uint64_t kWaitNs = 2000000000ull;  // bounded mbarrier wait: 2 s
 
 template <int BN>
@@ -41,8 +40,8 @@ struct Tile {
   static constexpr int kBytesA = kBM * kBK * 2;
   static constexpr int kBytesB = BN * kBK * 2;
   static constexpr int kStageBytes = kBytesA + kBytesB;
-  static constexpr int kSmemBytes = kStages * kStageBytes;
-  static constexpr uint32_t kLboB = BN * 16;
+  // one extra KB so the stages can start on a 1024-byte boundary
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024;
   // tcgen05 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B
   // BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
   static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
@@ -55,14 +54,24 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor (start, leading and stride byte offsets in
-// 16-byte units, descriptor version 1, no swizzle).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo) {
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte
+// swizzled layout: start address, leading-byte offset 16 (unused by this
+// layout), stride-byte offset 1024 between 8-row groups (all in 16-byte
+// units), descriptor version 1, layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
   uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>(1) << 16;
   d |= static_cast<uint64_t>((kSbo >> 4) & 0x3FFFu) << 32;
   d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(2) << 61;
   return d;
+}
+
+// Byte offset of the 16-byte chunk kc (0..7) of row r in a 128-byte swizzled
+// tile: rows are 128 B apart and the chunk index is XORed with r mod 8 (the
+// hardware applies the same XOR to the addresses the descriptors produce).
+__device__ __forceinline__ uint32_t swz(int r, int kc) {
+  return static_cast<uint32_t>(r) * 128u + (static_cast<uint32_t>(kc ^ (r & 7)) << 4);
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -133,22 +142,25 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_sh;
 
-  auto stage_a = [&](int s) { return smem + s * TL::kStageBytes; };
-  auto stage_b = [&](int s) { return smem + s * TL::kStageBytes + TL::kBytesA; };
+  uint8_t *tiles = smem + ((1024u - (smem_u32(smem) & 1023u)) & 1023u);
+  auto stage_a = [&](int s) { return tiles + s * TL::kStageBytes; };
+  auto stage_b = [&](int s) { return tiles + s * TL::kStageBytes + TL::kBytesA; };
   auto load = [&](int kb, int s) {
     const int k0 = kbeg + kb * kBK;
     uint8_t *a = stage_a(s), *b = stage_b(s);
+    // 8 consecutive threads copy one 128-byte row: coalesced global reads and
+    // conflict-free swizzled shared-memory writes
 #pragma unroll
     for (int i = 0; i < (kBM * kBK / 8) / kThreads; ++i) {
       const int q = tid + i * kThreads;
-      const int r = q & (kBM - 1), kc = q / kBM;
-      cp_async16(a + kc * kLboA + r * 16, g.A + static_cast<size_t>(m0 + r) * g.lda + k0 + kc * 8);
+      const int r = q >> 3, kc = q & 7;
+      cp_async16(a + swz(r, kc), g.A + static_cast<size_t>(m0 + r) * g.lda + k0 + kc * 8);
     }
 #pragma unroll
     for (int i = 0; i < (BN * kBK / 8) / kThreads; ++i) {
       const int q = tid + i * kThreads;
-      const int r = q & (BN - 1), kc = q / BN;
-      cp_async16(b + kc * TL::kLboB + r * 16, g.B + static_cast<size_t>(n0 + r) * g.ldb + k0 + kc * 8);
+      const int r = q >> 3, kc = q & 7;
+      cp_async16(b + swz(r, kc), g.B + static_cast<size_t>(n0 + r) * g.ldb + k0 + kc * 8);
     }
   };
 
@@ -172,8 +184,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
       const uint32_t abase = smem_u32(stage_a(s)), bbase = smem_u32(stage_b(s));
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; ++kk) {
-        const uint64_t adesc = smem_desc(abase + kk * 2 * kLboA, kLboA);
-        const uint64_t bdesc = smem_desc(bbase + kk * 2 * TL::kLboB, TL::kLboB);
+        const uint64_t adesc = smem_desc(abase + kk * 32);
+        const uint64_t bdesc = smem_desc(bbase + kk * 32);
         const uint32_t accumulate = (kb > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

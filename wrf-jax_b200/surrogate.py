@@ -428,6 +428,17 @@ _FIELDS_LEV = ("p8w", "t8w")
 _FIELDS_2D = ("tsk", "emiss", "albedo", "coszr", "xland", "xice", "snow")
 
 
+_SIDE = {}
+
+
+def _side_stream():
+    import torch
+    dev = torch.cuda.current_device()
+    if dev not in _SIDE:
+        _SIDE[dev] = torch.cuda.Stream(device=dev)
+    return _SIDE[dev]
+
+
 def _fallback(st, d: dict, flags, out: dict) -> int:
     """Re-solve the flagged columns with the plain kernels, writing their
     surrogate outputs over; returns how many columns were re-solved."""
@@ -458,8 +469,21 @@ def _fallback(st, d: dict, flags, out: dict) -> int:
         mv(d[k], sub[k], 1, 1)
     lw_kw = {k: (sub[k] if k in sub else v) for k, v in st.lw_kwargs().items()}
     sw_kw = {k: (sub[k] if k in sub else v) for k, v in st.sw_kwargs().items()}
-    lw = rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw)
+    # LW on a side stream overlaps SW on the current stream.  Every buffer the
+    # side stream touches is allocated on the current stream beforehand, and the
+    # current stream waits for the side stream before it reads or frees them.
+    main, side = torch.cuda.current_stream(), _side_stream()
+    lw_out = {k: torch.empty((1, nk, n) if k.startswith("rthraten") else (1, n), device="cuda")
+              for k in _capi.LW_OUT_FIELDS}
+    ready = torch.cuda.Event()
+    ready.record(main)
+    side.wait_event(ready)
+    with torch.cuda.stream(side):
+        lw = rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw, stream=side.cuda_stream, out=lw_out)
     sw = rrtmg.rrtmg_swrad_wrf_columns(**sw_kw)
+    done = torch.cuda.Event()
+    done.record(side)
+    main.wait_event(done)
     mv(lw.rthratenlw, out["rthratenlw"], nk, 0)
     mv(sw.rthratensw, out["rthratensw"], nk, 0)
     mv(lw.glw, out["glw"], 1, 0)
