@@ -365,6 +365,9 @@ def run_surrogate(args):
     import torch
 
     wl = dict(SURROGATE_WORKLOAD)
+    if args.nx or args.ny:
+        wl["nx"], wl["ny"] = args.nx or wl["nx"], args.ny or wl["ny"]
+        wl["name"] = "surrogate_fallback_%dx%dx%d" % (wl["nx"], wl["ny"], wl["nk"])
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     dist = None
@@ -408,9 +411,9 @@ def run_surrogate(args):
 
     sur = lambda: S.infer(model, st, d, energy_tol=tol, fallback=True)
     plain = lambda: S._plain(st, d)
+    plain()
     for _ in range(max(3, args.warmup)):
         sur()
-    plain()
     with ClockSampler(local) as clocks:
         el_sur, res = timed(sur, args.steps)
         el_plain, (lw, sw) = timed(plain, max(1, min(args.steps, 3)))

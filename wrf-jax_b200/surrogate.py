@@ -397,16 +397,15 @@ def infer(model: SurrogateModel, st, d: dict | None = None, *, energy_tol: float
     ncol = nx * ny
     mpad = (ncol + 127) // 128 * 128
     s = _stream()
-    X = torch.zeros(mpad, K_IN, device="cuda", dtype=torch.bfloat16)
+    ws = _workspace(mpad)
+    X, H, Y = ws["X"], ws["H"], ws["Y"]
     flags = torch.empty(ncol, device="cuda", dtype=torch.int32)
     fa = _feature_args(d, nk, ny, ncol)
     fa.mean, fa.rstd = model.norm.in_mean.data_ptr(), model.norm.in_rstd.data_ptr()
     fa.X, fa.ldx = X.data_ptr(), K_IN
     fa.lo, fa.hi, fa.flags = model.norm.in_lo.data_ptr(), model.norm.in_hi.data_ptr(), flags.data_ptr()
     _check(lib.rrtmg_sur_features(ctypes.byref(fa), s), "features")
-    bf = torch.bfloat16
-    H = [torch.empty(mpad, HIDDEN, device="cuda", dtype=bf) for _ in range(3)]
-    Y = model.forward(X, H=H)
+    Y = model.forward(X, H=H, Y=Y)
     out = dict(rthratenlw=torch.empty(nx, nk, ny, device="cuda"), rthratensw=torch.empty(nx, nk, ny, device="cuda"))
     for k in ("glw", "lwupb", "swdnb", "swupb"):
         out[k] = torch.empty(nx, ny, device="cuda")
@@ -420,6 +419,26 @@ def infer(model: SurrogateModel, st, d: dict | None = None, *, energy_tol: float
     if fallback:
         n_fb = _fallback(st, d, flags, out)
     return SurrogateResult(flags=flags, n_fallback=n_fb, **out)
+
+
+_WORKSPACES: dict = {}
+
+
+def _workspace(mpad: int) -> dict:
+    """Network buffers for mpad rows, kept per device and reused by every call
+    with the same padded column count (the calls on one device are ordered on
+    its stream).  Rows of X past the real columns stay zero."""
+    import torch
+    key = (torch.cuda.current_device(), mpad)
+    ws = _WORKSPACES.get(key)
+    if ws is None:
+        bf = torch.bfloat16
+        ws = dict(X=torch.zeros(mpad, K_IN, device="cuda", dtype=bf),
+                  H=[torch.empty(mpad, HIDDEN, device="cuda", dtype=bf) for _ in range(3)],
+                  Y=torch.empty(mpad, N_OUT, device="cuda"))
+        _WORKSPACES.clear()  # keep one domain size resident
+        _WORKSPACES[key] = ws
+    return ws
 
 
 _FIELDS_3D = ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d", "re_cloud",
