@@ -354,11 +354,11 @@ def run_plain(args):
         dist.destroy_process_group()
 
 
-def _surrogate_launches(n_fallback: int) -> int:
-    """Kernel launches of one surrogate step: features, 4 GEMMs, decode,
-    compact; with fallback columns also 22 gathers, 6 scatters and the plain
-    LW (3) and SW (3) launches."""
-    return 7 + (34 if n_fallback > 0 else 0)
+def _surrogate_launches(n_fallback: int, fused: bool) -> int:
+    """Kernel launches of one surrogate step: features, the fused network
+    kernel (or 4 GEMMs and a decode), compact; with fallback columns also 22
+    gathers, 6 scatters and the plain LW (3) and SW (3) launches."""
+    return (3 if fused else 7) + (34 if n_fallback > 0 else 0)
 
 
 def run_surrogate(args):
@@ -409,7 +409,8 @@ def run_surrogate(args):
             el = float(tt.item())
         return el, out
 
-    sur = lambda: S.infer(model, st, d, energy_tol=tol, fallback=True)
+    fused = not args.unfused
+    sur = lambda: S.infer(model, st, d, energy_tol=tol, fallback=True, fused=fused)
     plain = lambda: S._plain(st, d)
     plain()
     for _ in range(max(3, args.warmup)):
@@ -429,8 +430,16 @@ def run_surrogate(args):
     flux = torch.stack([res.glw - lw.glw, res.lwupb - lw.lwupb, res.swdnb - sw.swdnb, res.swupb - sw.swupb])
     flux_rmse = float(torch.sqrt((flux ** 2).mean()))
 
-    # forward GEMMs alone (the tensor-core part) for the roofline
+    # the network alone (the tensor-core part) for the roofline: the fused
+    # kernel (four layers + decode), and for comparison the four unfused GEMMs
     mpad = (ncol + 127) // 128 * 128
+    flops = 2.0 * mpad * sum(o * i for o, i in S.LAYER_SHAPES)
+    call = S.fused_kernel_call(model, st, d, energy_tol=tol)
+    for _ in range(3):
+        call()
+    el_fused, _ = timed(call, args.steps)
+    fused_ms = el_fused / args.steps * 1e3
+    del call
     X = torch.zeros(mpad, S.K_IN, device="cuda", dtype=torch.bfloat16)
     H = [torch.empty(mpad, S.HIDDEN, device="cuda", dtype=torch.bfloat16) for _ in range(3)]
     Y = torch.empty(mpad, S.N_OUT, device="cuda")
@@ -438,9 +447,10 @@ def run_surrogate(args):
         model.forward(X, H=H, Y=Y)
     el_gemm, _ = timed(lambda: model.forward(X, H=H, Y=Y), args.steps)
     gemm_ms = el_gemm / args.steps * 1e3
-    flops = 2.0 * mpad * sum(o * i for o, i in S.LAYER_SHAPES)
+    del X, H, Y
+    kernel_ms = fused_ms if fused else gemm_ms
     hbm, bf16, peak_kind = _peaks()
-    achieved = flops / (gemm_ms / 1e3) / 1e12
+    achieved = flops / (kernel_ms / 1e3) / 1e12
 
     # end to end with host inputs and host outputs
     # (inputs and outputs in pinned host memory, allocated before the timed region)
@@ -477,9 +487,11 @@ def run_surrogate(args):
         "heating_rmse_kday": heat_rmse, "surface_flux_rmse_wm2": flux_rmse,
         "fallback_fraction": res.n_fallback / ncol,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                     "frac": achieved / bf16, "traffic": None, "kernel": "umma_gemm_kernel (4 forward GEMMs)",
-                     "kernel_ms": gemm_ms, "flops_per_launch_set": flops, "peak_source": peak_kind},
-        "gpu_launches": _surrogate_launches(res.n_fallback) * args.steps,
+                     "frac": achieved / bf16, "traffic": None,
+                     "kernel": "mlp_kernel (4 layers + decode, fused)" if fused else "umma_gemm_kernel (4 GEMMs)",
+                     "kernel_ms": kernel_ms, "flops_per_launch": flops, "peak_source": peak_kind,
+                     "unfused_gemms_ms": gemm_ms, "fused_ms": fused_ms},
+        "gpu_launches": _surrogate_launches(res.n_fallback, fused) * args.steps,
         "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
     }
@@ -549,6 +561,7 @@ def main():
     ap.add_argument("--ny", type=int, default=None)
     ap.add_argument("--nk", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--unfused", action="store_true", help="surrogate network as 4 GEMMs + decode kernel")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args, SURROGATE_WORKLOAD if args.workload == "surrogate" else WORKLOAD)

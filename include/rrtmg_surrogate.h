@@ -48,7 +48,13 @@ rrtmg_status rrtmg_gemm_bf16(const rrtmg_gemm_args *args, void *stream);
  * 8 layer thickness p8w[k] - p8w[k+1]; then tsk, albedo, coszr, emiss
  * (9 nk + 4 features).  raw: FP32 values; X: BF16 (v - mean) * rstd, zero-
  * padded to ldx; Xt: X transposed; flags[c] = 1 when a value lies outside
- * [lo, hi] (the training range), else 0.  Every output is optional. */
+ * [lo, hi] (the training range), else 0.  Every output is optional.
+ * x_layout 0: X row-major [rows][ldx].  x_layout 1 (ldx = 512, X 16-byte
+ * aligned, no raw or Xt): X as the feature tiles of rrtmg_sur_mlp: row
+ * r = row_offset + c lies in tile r / 128 (128 KB per tile), whose eight
+ * 16 KB blocks hold K = 64 b .. 64 b + 63 of its 128 rows, row r mod 128 at
+ * (r mod 128) * 128 bytes with 16-byte chunk q (8 features) stored at chunk
+ * position q XOR (r mod 8). */
 typedef struct {
     int ncol, nk, ny;
     const float *p3d, *p8w, *t3d, *qv, *qc, *qi, *qs, *cldfra, *o3, *tsk, *albedo, *coszr, *emiss;
@@ -59,6 +65,7 @@ typedef struct {
     void *Xt; int ldxt;
     const float *lo, *hi;
     unsigned *flags;
+    int x_layout;
 } rrtmg_sur_features_args;
 rrtmg_status rrtmg_sur_features(const rrtmg_sur_features_args *args, void *stream);
 
@@ -130,6 +137,40 @@ typedef struct {
 } rrtmg_sur_decode_args;
 rrtmg_status rrtmg_sur_decode(const rrtmg_sur_decode_args *args, void *stream);
 
+/* Bytes of the packed weight image read by rrtmg_sur_mlp. */
+#define RRTMG_SUR_WEIGHT_IMAGE_BYTES 1703936
+
+/* Packs the network's BF16 weights (W[0..2]: 512 x 512, W[3]: 128 x 512,
+ * row-major [out][in], 16-byte aligned) into the image rrtmg_sur_mlp streams
+ * through shared memory: 48 blocks of 32 KB (layer L < 3, rows 256 h ..
+ * 256 h + 255, K = 64 b .. 64 b + 63 for block 16 L + 8 h + b) then 8 blocks
+ * of 16 KB (layer 3, all 128 rows, K block b), each in the 128-byte swizzled
+ * K-major layout of the feature tiles.  Repack after the weights change. */
+rrtmg_status rrtmg_sur_pack_weights(const void *const W[4], void *image, void *stream);
+
+/* Fused inference for 50-level columns: the four layers and the decode with
+ * the energy gate of rrtmg_sur_decode in one kernel, giving the same bits as
+ * rrtmg_gemm_bf16 (GELU, GELU, GELU, F32 epilogues) followed by
+ * rrtmg_sur_decode.  X: the features of the ncol columns in x_layout 1
+ * (ceil(ncol / 128) tiles, 16-byte aligned; rows past ncol are computed and
+ * discarded); W: the packed weight image; bias[l]: FP32 biases (512, 512,
+ * 512, 128).  flags: the range bits of rrtmg_sur_features on entry, | 2 for
+ * the energy gate on exit.  Outputs as rrtmg_sur_decode.  One CTA per SM;
+ * a CTA that gives up waiting for its copies or tensor-core work sets the
+ * flag rrtmg_gemm_error reports. */
+typedef struct {
+    int ncol, nk, ny;
+    const void *X;
+    const void *W;
+    const float *bias[4];
+    const float *out_mean, *out_std;
+    const float *coszr, *pi3d, *p8w;
+    float energy_tol;
+    float *rthratenlw, *rthratensw, *glw, *lwupb, *swdnb, *swupb;
+    unsigned *flags;
+} rrtmg_sur_mlp_args;
+rrtmg_status rrtmg_sur_mlp(const rrtmg_sur_mlp_args *args, void *stream);
+
 /* Writes the GPU global timer (ns) to *slot when the stream reaches this point
  * (stream-ordered, capturable in CUDA graphs; used for per-domain latencies). */
 rrtmg_status rrtmg_sur_timestamp(unsigned long long *slot, void *stream);
@@ -149,8 +190,9 @@ rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n
  * wide; set by the ensemble autotuner. */
 rrtmg_status rrtmg_gemm_set_tile(int bn);
 
-/* Synchronous: reads the sticky flag that a GEMM CTA sets when it gives up
- * waiting (2 s) for its tensor-core work; clears it when reset != 0. */
+/* Synchronous: reads the sticky flag that a CTA of rrtmg_gemm_bf16 or
+ * rrtmg_sur_mlp sets when it gives up waiting (2 s) for its copies or
+ * tensor-core work; clears it when reset != 0. */
 rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag);
 
 #ifdef __cplusplus

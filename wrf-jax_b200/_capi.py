@@ -75,7 +75,7 @@ class SurFeaturesArgs(ctypes.Structure):
         [(n, _F) for n in ("p3d", "p8w", "t3d", "qv", "qc", "qi", "qs", "cldfra", "o3", "tsk", "albedo", "coszr",
                            "emiss")] + \
         [("row_offset", _I), ("raw", _F), ("ldf", _I), ("mean", _F), ("rstd", _F), ("X", _F), ("ldx", _I),
-         ("Xt", _F), ("ldxt", _I), ("lo", _F), ("hi", _F), ("flags", _F)]
+         ("Xt", _F), ("ldxt", _I), ("lo", _F), ("hi", _F), ("flags", _F), ("x_layout", _I)]
 
 
 class SurTargetsArgs(ctypes.Structure):
@@ -95,6 +95,17 @@ class SurDecodeArgs(ctypes.Structure):
                 ("coszr", _F), ("pi3d", _F), ("p8w", _F), ("energy_tol", _FL)] + \
         [(n, _F) for n in ("rthratenlw", "rthratensw", "glw", "lwupb", "swdnb", "swupb", "flags")]
 
+
+class SurMlpArgs(ctypes.Structure):
+    """rrtmg_sur_mlp_args (include/rrtmg_surrogate.h)."""
+    _fields_ = [("ncol", _I), ("nk", _I), ("ny", _I), ("X", _F), ("W", _F), ("bias", _F * 4),
+                ("out_mean", _F), ("out_std", _F), ("coszr", _F), ("pi3d", _F), ("p8w", _F),
+                ("energy_tol", _FL)] + \
+        [(n, _F) for n in ("rthratenlw", "rthratensw", "glw", "lwupb", "swdnb", "swupb", "flags")]
+
+
+WEIGHT_IMAGE_BYTES = 1703936  # RRTMG_SUR_WEIGHT_IMAGE_BYTES
+
 STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
           4: "RRTMG_TIMEOUT"}
 
@@ -104,7 +115,8 @@ EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_l
 SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile", "rrtmg_sur_features", "rrtmg_sur_targets",
                      "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
                      "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
-                     "rrtmg_sur_compact", "rrtmg_sur_move_columns", "rrtmg_sur_timestamp")
+                     "rrtmg_sur_compact", "rrtmg_sur_move_columns", "rrtmg_sur_timestamp",
+                     "rrtmg_sur_pack_weights", "rrtmg_sur_mlp")
 
 _lib = None
 
@@ -160,6 +172,8 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_sur_move_columns": [P, P, I, I, I, P, P, I, I, I, V],
         "rrtmg_gemm_set_tile": [I],
         "rrtmg_sur_timestamp": [P, V],
+        "rrtmg_sur_pack_weights": [ctypes.POINTER(ctypes.c_void_p * 4), V, V],
+        "rrtmg_sur_mlp": [ctypes.POINTER(SurMlpArgs), V],
         "rrtmg_set_schedule": [V, ctypes.POINTER(Schedule)],
         "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
     }

@@ -55,7 +55,11 @@ extern "C" rrtmg_status rrtmg_gemm_bf16(const rrtmg_gemm_args *a, void *stream) 
 
 extern "C" rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag) {
   if (!flag) return RRTMG_BAD_ARG;
-  return gemm_error_flag(flag, reset != 0) == cudaSuccess ? RRTMG_OK : RRTMG_CUDA;
+  unsigned g = 0, m = 0;
+  if (gemm_error_flag(&g, reset != 0) != cudaSuccess || mlp_error_flag(&m, reset != 0) != cudaSuccess)
+    return RRTMG_CUDA;
+  *flag = g | m;
+  return RRTMG_OK;
 }
 
 namespace {
@@ -72,6 +76,9 @@ extern "C" rrtmg_status rrtmg_sur_features(const rrtmg_sur_features_args *a, voi
   if (a->raw && a->ldf < nf) return RRTMG_BAD_ARG;
   if (a->X && (a->ldx < nf || !a->mean || !a->rstd)) return RRTMG_BAD_ARG;
   if (a->Xt && (!a->X || a->ldxt < a->row_offset + a->ncol)) return RRTMG_BAD_ARG;
+  if (a->x_layout != 0 && (a->x_layout != 1 || !a->X || a->ldx != 512 || !aligned16(a->X) || a->raw || a->Xt ||
+                           9 * a->nk + 4 > 512))
+    return RRTMG_BAD_ARG;
   if ((a->lo == nullptr) != (a->hi == nullptr)) return RRTMG_BAD_ARG;
   if (a->ncol == 0) return RRTMG_OK;
   return cuda_status(launch_sur_features(*a, as_stream(stream)));
@@ -163,4 +170,23 @@ extern "C" rrtmg_status rrtmg_sur_normalize(const float *in, int ldi, int n, int
 extern "C" rrtmg_status rrtmg_sur_timestamp(unsigned long long *slot, void *stream) {
   if (!slot) return RRTMG_BAD_ARG;
   return cuda_status(launch_timestamp(slot, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_pack_weights(const void *const W[4], void *image, void *stream) {
+  if (!W || !image || !aligned16(image)) return RRTMG_BAD_ARG;
+  for (int l = 0; l < 4; ++l)
+    if (!W[l] || !aligned16(W[l])) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_pack_weights(W, image, as_stream(stream)));
+}
+
+extern "C" rrtmg_status rrtmg_sur_mlp(const rrtmg_sur_mlp_args *a, void *stream) {
+  if (!a || a->ncol < 0 || a->nk != 50 || a->ny <= 0 || !a->X || !a->W || !aligned16(a->X) || !aligned16(a->W))
+    return RRTMG_BAD_ARG;
+  for (int l = 0; l < 4; ++l)
+    if (!a->bias[l]) return RRTMG_BAD_ARG;
+  if (!a->out_mean || !a->out_std || !a->coszr || !a->pi3d || !a->p8w || !a->rthratenlw || !a->rthratensw ||
+      !a->glw || !a->lwupb || !a->swdnb || !a->swupb || !a->flags)
+    return RRTMG_BAD_ARG;
+  if (a->ncol == 0) return RRTMG_OK;
+  return cuda_status(launch_sur_mlp(*a, as_stream(stream)));
 }

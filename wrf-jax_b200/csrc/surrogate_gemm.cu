@@ -25,14 +25,20 @@
 #include <stdint.h>
 
 #include "surrogate_kernels.h"
+#include "umma_common.cuh"
 
 namespace rrtmg {
 namespace {
 
+using umma::gelu;
+using umma::gelu_grad;
+using umma::mbar_wait;
+using umma::smem_desc;
+using umma::smem_u32;
+using umma::swz;
+
 constexpr int kBM = 128, kBK = 64;
 constexpr int kThreads = 128;
-constexpr uint32_t kSbo = 1024;              // next 8-row group (8 rows x 128 B)
-constexpr uint64_t kWaitNs = 2000000000ull;  // bounded mbarrier wait: 2 s
 
 template <int BN>
 struct Tile {
@@ -42,69 +48,13 @@ struct Tile {
   static constexpr int kStageBytes = kBytesA + kBytesB;
   // one extra KB so the stages can start on a 1024-byte boundary
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024;
-  // tcgen05 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B
-  // BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
-  static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
-                                     (static_cast<uint32_t>(kBM >> 4) << 24);
+  static constexpr uint32_t kIdesc = umma::idesc_bf16(kBM, BN);
 };
 
 __device__ unsigned g_gemm_error;
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor of a K-major operand in the 128-byte
-// swizzled layout: start address, leading-byte offset 16 (unused by this
-// layout), stride-byte offset 1024 between 8-row groups (all in 16-byte
-// units), descriptor version 1, layout type 2 (SWIZZLE_128B).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
-  uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>(1) << 16;
-  d |= static_cast<uint64_t>((kSbo >> 4) & 0x3FFFu) << 32;
-  d |= static_cast<uint64_t>(1) << 46;
-  d |= static_cast<uint64_t>(2) << 61;
-  return d;
-}
-
-// Byte offset of the 16-byte chunk kc (0..7) of row r in a 128-byte swizzled
-// tile: rows are 128 B apart and the chunk index is XORed with r mod 8 (the
-// hardware applies the same XOR to the addresses the descriptors produce).
-__device__ __forceinline__ uint32_t swz(int r, int kc) {
-  return static_cast<uint32_t>(r) * 128u + (static_cast<uint32_t>(kc ^ (r & 7)) << 4);
-}
-
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Waits for the given phase parity of an mbarrier; gives up after kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
-  const uint64_t t0 = global_ns();
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (global_ns() - t0 > kWaitNs) return false;
-  }
-}
-
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
-
-__device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
 // Tile (m-tile = blockIdx.y, n-tile = blockIdx.x, K split = blockIdx.z): the

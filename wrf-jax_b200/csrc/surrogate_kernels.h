@@ -42,6 +42,7 @@ using SurFeatureArgs = rrtmg_sur_features_args;
 using SurTargetArgs = rrtmg_sur_targets_args;
 using SurAdamArgs = rrtmg_sur_adam_args;
 using SurDecodeArgs = rrtmg_sur_decode_args;
+using SurMlpArgs = rrtmg_sur_mlp_args;
 cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s);
 cudaError_t launch_sur_targets(const SurTargetArgs &a, cudaStream_t s);
 cudaError_t launch_sur_column_stats(const float *F, int n, int ld, int nf, float *mean, float *rstd, float *lo,
@@ -64,5 +65,10 @@ cudaError_t launch_timestamp(unsigned long long *slot, cudaStream_t s);
 // Reads (and optionally clears) the sticky flag set when a GEMM CTA gave up
 // waiting for its tensor-core work.
 cudaError_t gemm_error_flag(unsigned *out, bool reset);
+// Fused inference (surrogate_mlp.cu) and its weight packing and error flag.
+size_t sur_weight_image_bytes();
+cudaError_t launch_sur_pack_weights(const void *const W[4], void *image, cudaStream_t s);
+cudaError_t launch_sur_mlp(const SurMlpArgs &a, cudaStream_t s);
+cudaError_t mlp_error_flag(unsigned *out, bool reset);
 
 }  // namespace rrtmg

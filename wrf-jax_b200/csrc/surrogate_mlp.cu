@@ -1,0 +1,471 @@
+// Fused surrogate inference: the four layers of the radiation MLP
+// (512 -> 512 -> 512 -> 512 -> 128, GELU between) and the decode with the
+// energy gate in one persistent kernel, so hidden activations never leave
+// the SM.
+//
+// One CTA per SM walks 128-row tiles (a row is one model column).  Per tile:
+//   * the BF16 feature tile (128 x 512, 128 KB) arrives by one bulk copy into
+//     the activation buffer, already in the 128-byte swizzled K-major layout
+//     (rrtmg_sur_features with x_layout = 1 writes it that way);
+//   * each layer's weights stream through three 32 KB shared-memory stages
+//     (bulk copies of a pre-packed weight image, rrtmg_sur_pack_weights);
+//     one thread issues tcgen05.mma (M = 128, N = 256 per half, K = 16) into
+//     tensor memory: layers 0-2 fill columns 0-511, layer 3 columns 384-511;
+//   * eight epilogue warps read the accumulator back (tcgen05.ld, warp w owns
+//     lanes 32 (w mod 4) ..), add the bias, apply GELU and write the BF16
+//     result over the activation buffer as the next layer's A operand;
+//   * after layer 3 the same warps denormalize the outputs and write the WRF
+//     fields directly (LW half: LW heating, glw, lwupb; SW half: SW heating,
+//     swdnb, swupb), with the energy gate of rrtmg_sur_decode.
+// The next tile's features load while the decode runs, and its layer-0 MMAs
+// into columns 0-255 overlap the decode's reads of columns 384-511.
+//
+// Arithmetic is the unfused path's, operation for operation (same MMA
+// shapes and K order, same epilogue and decode expressions), so both paths
+// give the same bits.
+//
+// Warp roles (384 threads): warp 0 lane 0 issues the MMAs, warp 1 lane 0 the
+// bulk copies, warps 4-11 run the epilogues; warp 0 also owns the tensor
+// memory.  Every wait is an mbarrier wait bounded by the global timer; a role
+// that gives up raises a shared abort flag the others poll, the copies and
+// MMAs in flight are drained (again bounded), and the kernel sets a sticky
+// error flag the host reads with rrtmg_gemm_error.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "surrogate_kernels.h"
+#include "umma_common.cuh"
+
+namespace rrtmg {
+namespace {
+
+using namespace umma;
+
+constexpr int kRows = 128;                       // rows per tile
+constexpr int kWidth = 512;                      // K of every layer, N of layers 0-2
+constexpr int kOutCols = 128;                    // N of layer 3
+constexpr int kKb = 64;                          // K per block (one 128-byte swizzle row)
+constexpr int kNkb = kWidth / kKb;               // 8
+constexpr uint32_t kActBlock = kRows * kKb * 2;  // 16 KB: one K block of the activation tile
+constexpr uint32_t kActBytes = kActBlock * kNkb; // 128 KB
+constexpr uint32_t kStageBytes = 256 * kKb * 2;  // 32 KB: 256 weight rows x 64 K
+constexpr int kStages = 3;
+constexpr int kSmemBytes = static_cast<int>(kActBytes + kStages * kStageBytes) + 1024;
+constexpr int kThreads = 384;
+constexpr int kEpiWarp0 = 4;                     // warps 4-11: epilogue
+constexpr int kEpiWarps = 8;
+constexpr int kLoadsHidden = 3 * 2 * kNkb;       // 48 stage loads of 32 KB (layers 0-2, two halves)
+constexpr int kLoadsPerTile = kLoadsHidden + kNkb;  // + 8 stage loads of 16 KB (layer 3)
+constexpr uint32_t kOutCol0 = 384;               // tensor-memory column of layer 3's output 0
+constexpr int kNk = 50;                          // levels of the network's columns
+
+// heatfac = g * 86400 / (cp * 100): K/day per (W/m2 per hPa)  (lw:5706, sw:2289)
+constexpr float kHeatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
+
+__device__ unsigned g_mlp_error;
+
+// Weight stage load j (0..55) of a tile: offset into the packed image and size.
+__device__ __forceinline__ uint32_t load_offset(int j) {
+  return j < kLoadsHidden ? static_cast<uint32_t>(j) * kStageBytes
+                          : static_cast<uint32_t>(kLoadsHidden) * kStageBytes +
+                                static_cast<uint32_t>(j - kLoadsHidden) * (kStageBytes / 2);
+}
+__device__ __forceinline__ uint32_t load_bytes(int j) { return j < kLoadsHidden ? kStageBytes : kStageBytes / 2; }
+
+struct Bars {
+  uint64_t full[kStages], empty[kStages];
+  uint64_t act_full;   // feature tile landed (tx)
+  uint64_t act_free;   // layer-3 MMAs done reading the activation buffer (commit)
+  uint64_t acc_full;   // a layer's MMAs complete (commit)
+  uint64_t act_ready;  // epilogue wrote the next layer's A operand (8 warps)
+  uint64_t tmem_free;  // decode read layer 3's accumulator (8 warps)
+  uint64_t sw_done;    // SW half of the decode published its gate result (4 warps)
+  uint64_t mma_done;   // drain at exit (commit)
+};
+
+// All lanes wait; the warp agrees on the outcome.
+__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, const volatile int *abort) {
+  const bool ok = mbar_wait_or_abort(bar, parity, abort);
+  return __all_sync(0xffffffffu, ok);
+}
+
+__device__ __forceinline__ void fail(volatile int *abort) {
+  *abort = 1;
+  atomicOr(&g_mlp_error, 1u);
+}
+
+__device__ __forceinline__ float dec(uint32_t acc, const float *bias, const float *mean, const float *stdv, int f) {
+  // the unfused path: Y = acc + bias (F32 epilogue), then Y * out_std + out_mean
+  const float y = __uint_as_float(acc) + bias[f];
+  return y * stdv[f] + mean[f];
+}
+
+// Decode of one column by one half of the epilogue: HALF 0 writes the LW
+// heating, glw and lwupb, HALF 1 the SW heating (zero at night), swdnb and
+// swupb; returns whether that side fails the energy gate.  The registers
+// hold output columns f0 .. f0 + 63 (f0 = 0 for LW, 48 for SW) and 96 .. 111.
+// Expressions follow rrtmg_sur_decode operation for operation.
+template <int HALF>
+__device__ __forceinline__ bool decode_half(const SurMlpArgs &a, int col, const uint32_t (&h0)[16],
+                                            const uint32_t (&h1)[16], const uint32_t (&h2)[16],
+                                            const uint32_t (&h3)[16], const uint32_t (&t)[16]) {
+  constexpr int f0 = HALF == 0 ? 0 : 48;
+  const float *b3 = a.bias[3], *om = a.out_mean, *os = a.out_std;
+  const int ny = a.ny;
+  const int i = col / ny, jj = col - i * ny;
+  const size_t q0 = static_cast<size_t>(i) * kNk * ny + jj;
+  const size_t l0 = static_cast<size_t>(i) * (kNk + 1) * ny + jj;
+  const bool day = a.coszr[col] > 0.0f;
+  float *out = HALF == 0 ? a.rthratenlw : a.rthratensw;
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kNk; ++k) {
+    const int f = HALF == 0 ? k : kNk + k;
+    const int rel = f - f0;
+    const uint32_t raw = (rel >> 4) == 0 ? h0[rel & 15] : (rel >> 4) == 1 ? h1[rel & 15]
+                                                      : (rel >> 4) == 2 ? h2[rel & 15] : h3[rel & 15];
+    const size_t q = q0 + static_cast<size_t>(k) * ny;
+    const float pi = a.pi3d[q];
+    float hr = dec(raw, b3, om, os, f);
+    if (HALF == 1 && !day) hr = 0.0f;
+    out[q] = (hr / 86400.0f) / pi;
+    const float dp = (a.p8w[l0 + static_cast<size_t>(k) * ny] - a.p8w[l0 + static_cast<size_t>(k + 1) * ny]) * 0.01f;
+    s += hr * dp / kHeatfac;
+  }
+  // outputs 2 nk .. 2 nk + 5 (f = 100 .. 105) sit at t[4] .. t[9]
+  if (HALF == 0) {
+    const float glw = dec(t[4], b3, om, os, 2 * kNk), lwupb = dec(t[5], b3, om, os, 2 * kNk + 1);
+    a.glw[col] = glw;
+    a.lwupb[col] = lwupb;
+    const float lw_res = fabsf(((lwupb - glw) - dec(t[8], b3, om, os, 2 * kNk + 4)) - s);
+    return !(lw_res <= a.energy_tol);
+  } else {
+    const float swdnb = day ? dec(t[6], b3, om, os, 2 * kNk + 2) : 0.0f;
+    const float swupb = day ? dec(t[7], b3, om, os, 2 * kNk + 3) : 0.0f;
+    a.swdnb[col] = swdnb;
+    a.swupb[col] = swupb;
+    const float sw_res = day ? fabsf((dec(t[9], b3, om, os, 2 * kNk + 5) - (swdnb - swupb)) - s) : 0.0f;
+    return !(sw_res <= a.energy_tol);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntiles) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) Bars bars;
+  __shared__ uint32_t tmem_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ int sw_fail[kRows];
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint8_t *base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint8_t *act = base;
+  uint8_t *stage0 = base + kActBytes;
+  const uint32_t act_s = smem_u32(act), stage_s = smem_u32(stage0);
+  auto bar = [](uint64_t &b) { return smem_u32(&b); };
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 32) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(bar(bars.full[s]), 1);
+      mbar_init(bar(bars.empty[s]), 1);
+    }
+    mbar_init(bar(bars.act_full), 1);
+    mbar_init(bar(bars.act_free), 1);
+    mbar_init(bar(bars.acc_full), 1);
+    mbar_init(bar(bars.act_ready), kEpiWarps);
+    mbar_init(bar(bars.tmem_free), kEpiWarps);
+    mbar_init(bar(bars.sw_done), kEpiWarps / 2);
+    mbar_init(bar(bars.mma_done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_sh = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_sh;
+  const uint8_t *X = static_cast<const uint8_t *>(a.X);
+  const uint8_t *W = static_cast<const uint8_t *>(a.W);
+
+  if (warp == 1) {
+    // ---------------- producer: bulk copies ----------------
+    if (lane == 0) {
+      uint32_t li = 0;
+      int it = 0, last_tile_it = -1;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        if (it > 0 && !mbar_wait_or_abort(bar(bars.act_free), (it - 1) & 1, &abort_sh)) {
+          fail(&abort_sh);
+          break;
+        }
+        mbar_expect_tx(bar(bars.act_full), kActBytes);
+        bulk_g2s(act_s, X + static_cast<size_t>(tile) * kActBytes, kActBytes, bar(bars.act_full));
+        last_tile_it = it;
+        bool ok = true;
+        for (int j = 0; j < kLoadsPerTile; ++j, ++li) {
+          const int s = static_cast<int>(li % kStages);
+          if (li >= kStages && !mbar_wait_or_abort(bar(bars.empty[s]), ((li / kStages) - 1) & 1, &abort_sh)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(bar(bars.full[s]), load_bytes(j));
+          bulk_g2s(stage_s + s * kStageBytes, W + load_offset(j), load_bytes(j), bar(bars.full[s]));
+        }
+        if (!ok) {
+          fail(&abort_sh);
+          break;
+        }
+      }
+      // drain: every copy this thread issued has landed before the CTA exits
+      if (last_tile_it >= 0) mbar_wait(bar(bars.act_full), last_tile_it & 1);
+      for (uint32_t q = li > kStages ? li - kStages : 0; q < li; ++q)
+        mbar_wait(bar(bars.full[q % kStages]), (q / kStages) & 1);
+    }
+  } else if (warp == 0) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      constexpr uint32_t kIdescHidden = idesc_bf16(kRows, 256);
+      constexpr uint32_t kIdescOut = idesc_bf16(kRows, kOutCols);
+      uint32_t li = 0, ready = 0;
+      int it = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+        if (!mbar_wait_or_abort(bar(bars.act_full), it & 1, &abort_sh)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int layer = 0; layer < 4 && ok; ++layer) {
+          if (layer > 0) {
+            if (!mbar_wait_or_abort(bar(bars.act_ready), ready & 1, &abort_sh)) {
+              ok = false;
+              break;
+            }
+            ++ready;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          }
+          const int halves = layer < 3 ? 2 : 1;
+          for (int h = 0; h < halves && ok; ++h) {
+            if (layer == 0 && h == 1 && it > 0) {
+              if (!mbar_wait_or_abort(bar(bars.tmem_free), (it - 1) & 1, &abort_sh)) {
+                ok = false;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            }
+            const uint32_t d = tmem + (layer < 3 ? static_cast<uint32_t>(h) * 256u : kOutCol0);
+            const uint32_t idesc = layer < 3 ? kIdescHidden : kIdescOut;
+            for (int kb = 0; kb < kNkb; ++kb, ++li) {
+              const int s = static_cast<int>(li % kStages);
+              if (!mbar_wait_or_abort(bar(bars.full[s]), (li / kStages) & 1, &abort_sh)) {
+                ok = false;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+              const uint32_t ab = act_s + kb * kActBlock, bb = stage_s + s * kStageBytes;
+#pragma unroll
+              for (int kk = 0; kk < kKb / 16; ++kk)
+                umma_bf16(d, smem_desc(ab + kk * 32), smem_desc(bb + kk * 32), idesc, (kb | kk) != 0 ? 1u : 0u);
+              umma_commit(bar(bars.empty[s]));
+            }
+          }
+          if (!ok) break;
+          umma_commit(bar(bars.acc_full));
+          if (layer == 3) umma_commit(bar(bars.act_free));
+        }
+      }
+      if (!ok) fail(&abort_sh);
+      // drain: every MMA this thread issued has completed before the CTA exits
+      umma_commit(bar(bars.mma_done));
+      mbar_wait(bar(bars.mma_done), 0);
+    }
+  } else if (warp >= kEpiWarp0) {
+    // ---------------- epilogue / decode ----------------
+    const int e = warp - kEpiWarp0;
+    const int quarter = warp & 3;         // tensor-memory lanes 32 * quarter ..
+    const int half = e >> 2;              // 0: columns 0-255 / LW decode, 1: 256-511 / SW decode
+    const int r = quarter * 32 + lane;    // tile row of this thread
+    const uint32_t trow = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
+    uint32_t acc_uses = 0;
+    int it = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+      for (int layer = 0; layer < 3 && ok; ++layer) {
+        if (!warp_wait(bar(bars.acc_full), acc_uses & 1, &abort_sh)) {
+          ok = false;
+          break;
+        }
+        ++acc_uses;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const float *bias = a.bias[layer];
+#pragma unroll 1
+        for (int c = half * 256; c < half * 256 + 256; c += 32) {
+          uint32_t v0[16], v1[16];
+          tmem_ld16(trow + static_cast<uint32_t>(c), v0);
+          tmem_ld16(trow + static_cast<uint32_t>(c + 16), v1);
+          tmem_ld_wait();
+          uint32_t p[16];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float x0 = __uint_as_float(v0[2 * j]) + bias[c + 2 * j];
+            const float x1 = __uint_as_float(v0[2 * j + 1]) + bias[c + 2 * j + 1];
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(x0), gelu(x1));
+            p[j] = *reinterpret_cast<const uint32_t *>(&h2);
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float x0 = __uint_as_float(v1[2 * j]) + bias[c + 16 + 2 * j];
+            const float x1 = __uint_as_float(v1[2 * j + 1]) + bias[c + 16 + 2 * j + 1];
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(x0), gelu(x1));
+            p[8 + j] = *reinterpret_cast<const uint32_t *>(&h2);
+          }
+          // columns c .. c+31 of this layer are K = c .. c+31 of the next:
+          // block c / 64, 16-byte chunks (c mod 64) / 8 .. + 3
+          uint8_t *blk = act + (c / kKb) * kActBlock;
+          const int kc0 = (c % kKb) / 8;
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4 *>(blk + swz(r, kc0 + q)) = make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2],
+                                                                           p[4 * q + 3]);
+        }
+        // generic-proxy writes -> visible to the tensor cores; accumulator reads done
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar(bars.act_ready));
+      }
+      if (!ok) break;
+      // ---- layer 3: decode ----
+      if (!warp_wait(bar(bars.acc_full), acc_uses & 1, &abort_sh)) {
+        ok = false;
+        break;
+      }
+      ++acc_uses;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int col = tile * kRows + r;
+      const bool live = col < a.ncol;
+      // heating columns of this half: LW f = 0..49 in chunks 0,16,32,48;
+      // SW f = 50..99 in chunks 48,64,80,96; both need the chunk 96..111
+      uint32_t h0[16], h1[16], h2[16], h3[16], t[16];
+      const uint32_t cb = trow + kOutCol0;
+      const int f0 = half == 0 ? 0 : 48;
+      tmem_ld16(cb + f0, h0);
+      tmem_ld16(cb + f0 + 16, h1);
+      tmem_ld16(cb + f0 + 32, h2);
+      tmem_ld16(cb + f0 + 48, h3);
+      tmem_ld16(cb + 96, t);
+      tmem_ld_wait();
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar(bars.tmem_free));
+
+      const bool gate_fail = live && (half == 0 ? decode_half<0>(a, col, h0, h1, h2, h3, t)
+                                                : decode_half<1>(a, col, h0, h1, h2, h3, t));
+      if (half == 1) {
+        sw_fail[r] = gate_fail ? 1 : 0;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar(bars.sw_done));
+      } else {
+        if (!warp_wait(bar(bars.sw_done), it & 1, &abort_sh)) {
+          ok = false;
+          break;
+        }
+        if (live) {
+          unsigned f = a.flags[col];
+          if (gate_fail || sw_fail[r]) f |= 2u;
+          a.flags[col] = f;
+        }
+      }
+    }
+    if (!ok) fail(&abort_sh);
+  }
+
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    __syncwarp();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+  }
+}
+
+// Packed weight image: stage load j of a tile (the order the kernel consumes
+// them) holds, in the 128-byte swizzled K-major layout, rows h*256 .. +255 of
+// layer L (j = 16 L + 8 h + kb, L < 3) or all 128 rows of layer 3
+// (j = 48 + kb), K = 64 kb .. 64 kb + 63.  One thread per 16-byte chunk.
+__global__ void pack_weights_kernel(const __nv_bfloat16 *W0, const __nv_bfloat16 *W1, const __nv_bfloat16 *W2,
+                                    const __nv_bfloat16 *W3, uint8_t *img) {
+  const uint32_t chunk = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t byte = chunk * 16u;
+  const uint32_t hidden_bytes = kLoadsHidden * kStageBytes;
+  if (byte >= hidden_bytes + kNkb * (kStageBytes / 2)) return;
+  int layer, kb, row;
+  uint32_t within;
+  if (byte < hidden_bytes) {
+    const uint32_t j = byte / kStageBytes;
+    within = byte % kStageBytes;
+    layer = static_cast<int>(j / 16);
+    const int h = static_cast<int>((j % 16) / 8);
+    kb = static_cast<int>(j % 8);
+    row = h * 256 + static_cast<int>(within / 128);
+  } else {
+    const uint32_t rem = byte - hidden_bytes;
+    layer = 3;
+    kb = static_cast<int>(rem / (kStageBytes / 2));
+    within = rem % (kStageBytes / 2);
+    row = static_cast<int>(within / 128);
+  }
+  const int r = static_cast<int>(within / 128) & 255;
+  const int pos = static_cast<int>((within % 128) / 16);
+  const int kc = pos ^ (r & 7);
+  const __nv_bfloat16 *Wl = layer == 0 ? W0 : layer == 1 ? W1 : layer == 2 ? W2 : W3;
+  const uint4 v = *reinterpret_cast<const uint4 *>(Wl + static_cast<size_t>(row) * kWidth + kb * kKb + kc * 8);
+  *reinterpret_cast<uint4 *>(img + byte) = v;
+}
+
+constexpr int kMaxDevices = 64;
+int g_sm_count[kMaxDevices];  // 0 until the device is configured
+
+}  // namespace
+
+size_t sur_weight_image_bytes() { return static_cast<size_t>(kLoadsHidden) * kStageBytes + kNkb * (kStageBytes / 2); }
+
+cudaError_t launch_sur_pack_weights(const void *const W[4], void *image, cudaStream_t s) {
+  const size_t chunks = sur_weight_image_bytes() / 16;
+  pack_weights_kernel<<<static_cast<unsigned>((chunks + 255) / 256), 256, 0, s>>>(
+      static_cast<const __nv_bfloat16 *>(W[0]), static_cast<const __nv_bfloat16 *>(W[1]),
+      static_cast<const __nv_bfloat16 *>(W[2]), static_cast<const __nv_bfloat16 *>(W[3]),
+      static_cast<uint8_t *>(image));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sur_mlp(const SurMlpArgs &a, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (g_sm_count[dev] == 0) {
+    e = cudaFuncSetAttribute(mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    g_sm_count[dev] = sms;
+  }
+  const int ntiles = (a.ncol + kRows - 1) / kRows;
+  const int grid = ntiles < g_sm_count[dev] ? ntiles : g_sm_count[dev];
+  mlp_kernel<<<grid, kThreads, kSmemBytes, s>>>(a, ntiles);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_error_flag(unsigned *out, bool reset) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_mlp_error, sizeof(unsigned));
+  if (e != cudaSuccess || !reset) return e;
+  const unsigned zero = 0;
+  return cudaMemcpyToSymbol(g_mlp_error, &zero, sizeof(unsigned));
+}
+
+}  // namespace rrtmg

@@ -116,6 +116,109 @@ __global__ void __launch_bounds__(256) features_kernel(SurFeatureArgs a) {
   }
 }
 
+// Inference features, one thread per column: the thread walks its column's
+// features 16 at a time (field reads coalesced across the warp's consecutive
+// columns), normalizes them, and writes 32 contiguous bytes of its output row:
+// row-major X, or (kTiled) the swizzled 128-row tiles of the fused inference
+// kernel, where chunks 2p and 2p + 1 of a row stay one 32-byte pair.  Values,
+// rounding and range flags are those of features_kernel.
+constexpr int kRowThreads = 128, kMaxFeatures = 512;
+
+template <bool kTiled>
+__global__ void __launch_bounds__(kRowThreads) features_rows_kernel(SurFeatureArgs a) {
+  __shared__ float4 st[kMaxFeatures];  // mean, rstd, lo, hi
+  __shared__ const float *src[13];
+  const int nk = a.nk, ny = a.ny, nf = 9 * nk + 4;
+  for (int f = threadIdx.x; f < nf; f += blockDim.x)
+    st[f] = make_float4(a.mean[f], a.rstd[f], a.lo ? a.lo[f] : -__int_as_float(0x7f800000),
+                        a.hi ? a.hi[f] : __int_as_float(0x7f800000));
+  if (threadIdx.x == 0) {
+    src[0] = a.t3d; src[1] = a.p3d; src[2] = a.qv; src[3] = a.qc; src[4] = a.qi; src[5] = a.qs;
+    src[6] = a.cldfra; src[7] = a.o3; src[8] = a.p8w;
+    src[9] = a.tsk; src[10] = a.albedo; src[11] = a.coszr; src[12] = a.emiss;
+  }
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncol) return;
+  const int i = c / ny, j = c - i * ny;
+  const size_t b3 = static_cast<size_t>(i) * nk * ny + j, bl = static_cast<size_t>(i) * (nk + 1) * ny + j;
+  const size_t row = static_cast<size_t>(a.row_offset) + c;
+  uint8_t *xrow;
+  if (kTiled) {
+    xrow = static_cast<uint8_t *>(a.X) + (row >> 7) * 131072u;
+  } else {
+    xrow = static_cast<uint8_t *>(a.X) + row * a.ldx * 2;
+  }
+  const int rr = static_cast<int>(row & 127);
+  unsigned oob = 0;
+  int fld = 0, k = 0;  // field and level of the next feature
+  for (int f0 = 0; f0 < a.ldx; f0 += 16) {
+    float v[16], w[16];
+    {
+      int fl = fld, kk = k;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        v[e] = 0.0f;
+        w[e] = 0.0f;
+        if (f0 + e < nf) {
+          if (fl < 9) {
+            const float *p = src[fl] + (fl == 8 ? bl : b3) + static_cast<size_t>(kk) * ny;
+            v[e] = __ldg(p);
+            if (fl == 8) w[e] = __ldg(p + ny);
+            if (++kk == nk) {
+              kk = 0;
+              ++fl;
+            }
+          } else {
+            v[e] = __ldg(src[9 + kk] + c);
+            ++kk;
+          }
+        }
+      }
+    }
+    uint32_t pk[8];
+#pragma unroll
+    for (int e = 0; e < 16; e += 2) {
+      float x[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int f = f0 + e + u;
+        float val = 0.0f;
+        if (f < nf) {
+          float r = v[e + u];
+          if (fld == 1) r = logf(r);
+          else if (fld == 8) r = r - w[e + u];
+          const float4 sf = st[f];
+          if (r < sf.z || r > sf.w) oob = 1u;
+          val = (r - sf.x) * sf.y;
+          if (fld < 9) {
+            if (++k == nk) {
+              k = 0;
+              ++fld;
+            }
+          } else {
+            ++k;
+          }
+        }
+        x[u] = val;
+      }
+      const __nv_bfloat162 h = __floats2bfloat162_rn(x[0], x[1]);
+      pk[e / 2] = *reinterpret_cast<const uint32_t *>(&h);
+    }
+    const int q = f0 / 8;
+    const uint4 lo4 = make_uint4(pk[0], pk[1], pk[2], pk[3]), hi4 = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    if (kTiled) {
+      uint8_t *blk = xrow + (q >> 3) * 16384;
+      *reinterpret_cast<uint4 *>(blk + rr * 128 + (((q & 7) ^ (rr & 7)) << 4)) = lo4;
+      *reinterpret_cast<uint4 *>(blk + rr * 128 + ((((q + 1) & 7) ^ (rr & 7)) << 4)) = hi4;
+    } else {
+      *reinterpret_cast<uint4 *>(xrow + f0 * 2) = lo4;
+      if (f0 + 8 < a.ldx) *reinterpret_cast<uint4 *>(xrow + f0 * 2 + 16) = hi4;
+    }
+  }
+  if (a.flags) a.flags[c] = oob;
+}
+
 __global__ void targets_kernel(SurTargetArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncol) return;
@@ -375,7 +478,16 @@ __global__ void move_columns_kernel(const int *list, const int *count, int nz, i
 }  // namespace
 
 cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s) {
-  features_kernel<<<(a.ncol + kFeatCols - 1) / kFeatCols, 256, 0, s>>>(a);
+  const unsigned row_blocks = static_cast<unsigned>((a.ncol + kRowThreads - 1) / kRowThreads);
+  const bool rows_ok = a.X && !a.raw && !a.Xt && a.ldx % 8 == 0 && 9 * a.nk + 4 <= kMaxFeatures &&
+                       (reinterpret_cast<uintptr_t>(a.X) & 15u) == 0;
+  if (a.x_layout == 1 && !rows_ok) return cudaErrorInvalidValue;
+  if (a.x_layout == 1)
+    features_rows_kernel<true><<<row_blocks, kRowThreads, 0, s>>>(a);
+  else if (a.x_layout == 0 && rows_ok)
+    features_rows_kernel<false><<<row_blocks, kRowThreads, 0, s>>>(a);
+  else
+    features_kernel<<<(a.ncol + kFeatCols - 1) / kFeatCols, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

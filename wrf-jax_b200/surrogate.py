@@ -261,6 +261,19 @@ class SurrogateModel:
         gemm_bf16(inp, self.wb[3], epilogue=_capi.EPI_F32, bias=self.b[3], C=Y)
         return Y
 
+    def weight_image(self):
+        """The BF16 weights packed for the fused inference kernel
+        (rrtmg_sur_pack_weights), rebuilt after the weights change."""
+        import torch
+        img = getattr(self, "_wimg", None)
+        if img is None or self._wimg_step != self.step:
+            lib = _capi.load()
+            img = torch.empty(_capi.WEIGHT_IMAGE_BYTES, device="cuda", dtype=torch.uint8)
+            ptrs = (ctypes.c_void_p * 4)(*[w.data_ptr() for w in self.wb])
+            _check(lib.rrtmg_sur_pack_weights(ctypes.byref(ptrs), img.data_ptr(), _stream()), "pack weights")
+            self._wimg, self._wimg_step = img, self.step
+        return img
+
     def train_step(self, X, Tn, idx, weights, *, lr: float, beta1=0.9, beta2=0.999, eps=1e-8,
                    weight_decay: float = 0.0) -> None:
         """One Adam step on the batch idx of (X, Tn); the batch loss is added to
@@ -384,10 +397,12 @@ class SurrogateResult:
 
 
 def infer(model: SurrogateModel, st, d: dict | None = None, *, energy_tol: float = 5.0,
-          fallback: bool = True) -> SurrogateResult:
+          fallback: bool = True, fused: bool = True) -> SurrogateResult:
     """Surrogate radiation for a domain (synthetic.ColumnState; device fields d
     as torch CUDA tensors, built from st when None) with per-column gate and
-    plain-kernel fallback."""
+    plain-kernel fallback.  fused: one kernel for the four layers and the
+    decode (rrtmg_sur_mlp); otherwise one GEMM per layer and a decode kernel.
+    Both give the same bits."""
     import torch
     lib = _capi.load()
     if st.nk != NK:
@@ -397,45 +412,87 @@ def infer(model: SurrogateModel, st, d: dict | None = None, *, energy_tol: float
     ncol = nx * ny
     mpad = (ncol + 127) // 128 * 128
     s = _stream()
-    ws = _workspace(mpad)
-    X, H, Y = ws["X"], ws["H"], ws["Y"]
+    ws = _workspace(mpad, fused)
     flags = torch.empty(ncol, device="cuda", dtype=torch.int32)
     fa = _feature_args(d, nk, ny, ncol)
     fa.mean, fa.rstd = model.norm.in_mean.data_ptr(), model.norm.in_rstd.data_ptr()
-    fa.X, fa.ldx = X.data_ptr(), K_IN
+    fa.X, fa.ldx, fa.x_layout = ws["X"].data_ptr(), K_IN, 1 if fused else 0
     fa.lo, fa.hi, fa.flags = model.norm.in_lo.data_ptr(), model.norm.in_hi.data_ptr(), flags.data_ptr()
     _check(lib.rrtmg_sur_features(ctypes.byref(fa), s), "features")
-    Y = model.forward(X, H=H, Y=Y)
     out = dict(rthratenlw=torch.empty(nx, nk, ny, device="cuda"), rthratensw=torch.empty(nx, nk, ny, device="cuda"))
     for k in ("glw", "lwupb", "swdnb", "swupb"):
         out[k] = torch.empty(nx, ny, device="cuda")
-    da = _capi.SurDecodeArgs(ncol=ncol, nk=nk, ny=ny, Y=Y.data_ptr(), ldy=N_OUT,
-                             out_mean=model.norm.out_mean.data_ptr(), out_std=model.norm.out_std.data_ptr(),
-                             coszr=d["coszr"].data_ptr(), pi3d=d["pi3d"].data_ptr(), p8w=d["p8w"].data_ptr(),
-                             energy_tol=energy_tol, **{k: v.data_ptr() for k, v in out.items()},
-                             flags=flags.data_ptr())
-    _check(lib.rrtmg_sur_decode(ctypes.byref(da), s), "decode")
+    common = dict(ncol=ncol, nk=nk, ny=ny, out_mean=model.norm.out_mean.data_ptr(),
+                  out_std=model.norm.out_std.data_ptr(), coszr=d["coszr"].data_ptr(), pi3d=d["pi3d"].data_ptr(),
+                  p8w=d["p8w"].data_ptr(), energy_tol=energy_tol, flags=flags.data_ptr(),
+                  **{k: v.data_ptr() for k, v in out.items()})
+    if fused:
+        ma = _capi.SurMlpArgs(X=ws["X"].data_ptr(), W=model.weight_image().data_ptr(), **common)
+        for i in range(4):
+            ma.bias[i] = model.b[i].data_ptr()
+        _check(lib.rrtmg_sur_mlp(ctypes.byref(ma), s), "fused inference")
+    else:
+        Y = model.forward(ws["X"], H=ws["H"], Y=ws["Y"])
+        da = _capi.SurDecodeArgs(Y=Y.data_ptr(), ldy=N_OUT, **common)
+        _check(lib.rrtmg_sur_decode(ctypes.byref(da), s), "decode")
     n_fb = 0
     if fallback:
         n_fb = _fallback(st, d, flags, out)
     return SurrogateResult(flags=flags, n_fallback=n_fb, **out)
 
 
+def fused_kernel_call(model: SurrogateModel, st, d: dict, *, energy_tol: float = 5.0):
+    """Runs the features of a 50-level domain once and returns a callable that
+    launches only the fused inference kernel on them (for timing and
+    profiling the dominant kernel); outputs land in fresh device buffers."""
+    import torch
+    lib = _capi.load()
+    nx, ny, nk = st.nx, st.ny, st.nk
+    ncol = nx * ny
+    mpad = (ncol + 127) // 128 * 128
+    s = _stream()
+    X = torch.zeros(mpad, K_IN, device="cuda", dtype=torch.bfloat16)
+    flags = torch.empty(ncol, device="cuda", dtype=torch.int32)
+    fa = _feature_args(d, nk, ny, ncol)
+    fa.mean, fa.rstd = model.norm.in_mean.data_ptr(), model.norm.in_rstd.data_ptr()
+    fa.X, fa.ldx, fa.x_layout = X.data_ptr(), K_IN, 1
+    fa.lo, fa.hi, fa.flags = model.norm.in_lo.data_ptr(), model.norm.in_hi.data_ptr(), flags.data_ptr()
+    _check(lib.rrtmg_sur_features(ctypes.byref(fa), s), "features")
+    out = dict(rthratenlw=torch.empty(nx, nk, ny, device="cuda"), rthratensw=torch.empty(nx, nk, ny, device="cuda"))
+    for k in ("glw", "lwupb", "swdnb", "swupb"):
+        out[k] = torch.empty(nx, ny, device="cuda")
+    ma = _capi.SurMlpArgs(ncol=ncol, nk=nk, ny=ny, X=X.data_ptr(), W=model.weight_image().data_ptr(),
+                          out_mean=model.norm.out_mean.data_ptr(), out_std=model.norm.out_std.data_ptr(),
+                          coszr=d["coszr"].data_ptr(), pi3d=d["pi3d"].data_ptr(), p8w=d["p8w"].data_ptr(),
+                          energy_tol=energy_tol, flags=flags.data_ptr(), **{k: v.data_ptr() for k, v in out.items()})
+    for i in range(4):
+        ma.bias[i] = model.b[i].data_ptr()
+    keep = (X, flags, out, ma)
+
+    def call():
+        _check(lib.rrtmg_sur_mlp(ctypes.byref(keep[3]), _stream()), "fused inference")
+    call.buffers = keep
+    return call
+
+
 _WORKSPACES: dict = {}
 
 
-def _workspace(mpad: int) -> dict:
+def _workspace(mpad: int, fused: bool) -> dict:
     """Network buffers for mpad rows, kept per device and reused by every call
-    with the same padded column count (the calls on one device are ordered on
-    its stream).  Rows of X past the real columns stay zero."""
+    with the same padded column count and path (the calls on one device are
+    ordered on its stream).  X starts zero; the fused path needs only X (in
+    the 128-row tile layout), the unfused one also the hidden activations and
+    the outputs."""
     import torch
-    key = (torch.cuda.current_device(), mpad)
+    key = (torch.cuda.current_device(), mpad, fused)
     ws = _WORKSPACES.get(key)
     if ws is None:
         bf = torch.bfloat16
-        ws = dict(X=torch.zeros(mpad, K_IN, device="cuda", dtype=bf),
-                  H=[torch.empty(mpad, HIDDEN, device="cuda", dtype=bf) for _ in range(3)],
-                  Y=torch.empty(mpad, N_OUT, device="cuda"))
+        ws = dict(X=torch.zeros(mpad, K_IN, device="cuda", dtype=bf))
+        if not fused:
+            ws["H"] = [torch.empty(mpad, HIDDEN, device="cuda", dtype=bf) for _ in range(3)]
+            ws["Y"] = torch.empty(mpad, N_OUT, device="cuda")
         _WORKSPACES.clear()  # keep one domain size resident
         _WORKSPACES[key] = ws
     return ws
