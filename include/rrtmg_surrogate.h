@@ -122,7 +122,8 @@ typedef struct {
 rrtmg_status rrtmg_sur_adam(const rrtmg_sur_adam_args *args, void *stream);
 
 /* Network outputs Y[ncol][ldy] (normalized) to WRF fields: rthratenlw/sw
- * (nx, nk, ny) = hr / 86400 / pi3d, glw, lwupb, swdnb, swupb (nx, ny); SW is
+ * (nx, nk, ny) = hr / 86400 / pi3d (a multiplication by 1/86400 and a fast
+ * division), glw, lwupb, swdnb, swupb (nx, ny); SW is
  * exactly zero where coszr <= 0.  Energy gate: flags[c] |= 2 when the column-
  * integrated LW or SW heating differs from the predicted net surface minus
  * model-top flux by more than energy_tol W/m2. */

@@ -11,6 +11,22 @@
 
 namespace rrtmg {
 
+#ifdef __CUDACC__
+// Decode arithmetic shared by rrtmg_sur_decode and the fused inference
+// kernel, so both give the same bits.  The surrogate's outputs are
+// approximations, so these use multiplications by constant reciprocals and
+// one fast division instead of correctly rounded divisions (whose slow path
+// every zero night-time SW rate takes).
+// heatfac = g * 86400 / (cp * 100): K/day per (W/m2 per hPa)  (lw:5706, sw:2289)
+constexpr float kSurHeatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
+constexpr float kSurInvHeatfac = 1.0f / kSurHeatfac;
+constexpr float kSurInvDay = 1.0f / 86400.0f;
+// theta tendency [K/s] of a heating rate hr [K/day] at Exner function pi
+__device__ __forceinline__ float sur_tendency(float hr, float pi) { return __fdividef(hr * kSurInvDay, pi); }
+// flux divergence [W/m2] of heating rate hr over a layer of dp [hPa]
+__device__ __forceinline__ float sur_flux_term(float hr, float dp) { return hr * dp * kSurInvHeatfac; }
+#endif
+
 enum GemmEpilogue { kEpiF32 = 0, kEpiGelu = 1, kEpiDgelu = 2 };
 
 // C[M x N] = A[M x K] * B[N x K]^T; M, N multiples of 128, K a multiple of

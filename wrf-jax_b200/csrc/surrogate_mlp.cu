@@ -11,12 +11,15 @@
 //     (bulk copies of a pre-packed weight image, rrtmg_sur_pack_weights);
 //     one thread issues tcgen05.mma (M = 128, N = 256 per half, K = 16) into
 //     tensor memory: layers 0-2 fill columns 0-511, layer 3 columns 384-511;
-//   * eight epilogue warps read the accumulator back (tcgen05.ld, warp w owns
-//     lanes 32 (w mod 4) ..), add the bias, apply GELU and write the BF16
-//     result over the activation buffer as the next layer's A operand;
-//   * after layer 3 the same warps denormalize the outputs and write the WRF
-//     fields directly (LW half: LW heating, glw, lwupb; SW half: SW heating,
-//     swdnb, swupb), with the energy gate of rrtmg_sur_decode.
+//   * twelve epilogue warps read the accumulator back (tcgen05.ld, warp w
+//     owns lanes 32 (w mod 4) .. and one of three column groups), add the bias,
+//     apply GELU and write the BF16 result over the activation buffer as the
+//     next layer's A operand, each chunk's accumulator read in flight while
+//     the previous chunk is processed;
+//   * after layer 3 two groups denormalize the outputs and write the WRF
+//     fields directly (LW group: LW heating, glw, lwupb; SW group: SW
+//     heating, swdnb, swupb), with the energy gate of rrtmg_sur_decode; their
+//     level fields were prefetched into L2 when the tile started.
 // The next tile's features load while the decode runs, and its layer-0 MMAs
 // into columns 0-255 overlap the decode's reads of columns 384-511.
 //
@@ -24,9 +27,10 @@
 // shapes and K order, same epilogue and decode expressions), so both paths
 // give the same bits.
 //
-// Warp roles (384 threads): warp 0 lane 0 issues the MMAs, warp 1 lane 0 the
-// bulk copies, warps 4-11 run the epilogues; warp 0 also owns the tensor
-// memory.  Every wait is an mbarrier wait bounded by the global timer; a role
+// Warp roles (512 threads): warp 0 lane 0 issues the MMAs, warp 1 lane 0 the
+// bulk copies, warps 4-15 run the epilogues (warps 2-3 idle: each epilogue
+// warp must sit on the lane quarter its warp index selects); warp 0 also owns
+// the tensor memory.  Every wait is an mbarrier wait bounded by the global timer; a role
 // that gives up raises a shared abort flag the others poll, the copies and
 // MMAs in flight are drained (again bounded), and the kernel sets a sticky
 // error flag the host reads with rrtmg_gemm_error.
@@ -52,16 +56,15 @@ constexpr uint32_t kActBytes = kActBlock * kNkb; // 128 KB
 constexpr uint32_t kStageBytes = 256 * kKb * 2;  // 32 KB: 256 weight rows x 64 K
 constexpr int kStages = 3;
 constexpr int kSmemBytes = static_cast<int>(kActBytes + kStages * kStageBytes) + 1024;
-constexpr int kThreads = 384;
-constexpr int kEpiWarp0 = 4;                     // warps 4-11: epilogue
-constexpr int kEpiWarps = 8;
+constexpr int kThreads = 512;                    // 16 warps: 4 per scheduler, 128 registers each
+constexpr int kEpiWarp0 = 4;                     // warps 4-15: epilogue
+constexpr int kEpiWarps = 12;
+constexpr int kDecodeWarps = 8;                  // epilogue groups 0 (LW) and 1 (SW) decode
+constexpr int kDecBatch = 10;                    // levels per batch of decode loads
 constexpr int kLoadsHidden = 3 * 2 * kNkb;       // 48 stage loads of 32 KB (layers 0-2, two halves)
 constexpr int kLoadsPerTile = kLoadsHidden + kNkb;  // + 8 stage loads of 16 KB (layer 3)
 constexpr uint32_t kOutCol0 = 384;               // tensor-memory column of layer 3's output 0
 constexpr int kNk = 50;                          // levels of the network's columns
-
-// heatfac = g * 86400 / (cp * 100): K/day per (W/m2 per hPa)  (lw:5706, sw:2289)
-constexpr float kHeatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
 
 __device__ unsigned g_mlp_error;
 
@@ -78,8 +81,8 @@ struct Bars {
   uint64_t act_full;   // feature tile landed (tx)
   uint64_t act_free;   // layer-3 MMAs done reading the activation buffer (commit)
   uint64_t acc_full;   // a layer's MMAs complete (commit)
-  uint64_t act_ready;  // epilogue wrote the next layer's A operand (8 warps)
-  uint64_t tmem_free;  // decode read layer 3's accumulator (8 warps)
+  uint64_t act_ready;  // epilogue wrote the next layer's A operand (12 warps)
+  uint64_t tmem_free;  // decode read layer 3's accumulator (8 decode warps)
   uint64_t sw_done;    // SW half of the decode published its gate result (4 warps)
   uint64_t mma_done;   // drain at exit (commit)
 };
@@ -101,53 +104,110 @@ __device__ __forceinline__ float dec(uint32_t acc, const float *bias, const floa
   return y * stdv[f] + mean[f];
 }
 
-// Decode of one column by one half of the epilogue: HALF 0 writes the LW
-// heating, glw and lwupb, HALF 1 the SW heating (zero at night), swdnb and
-// swupb; returns whether that side fails the energy gate.  The registers
-// hold output columns f0 .. f0 + 63 (f0 = 0 for LW, 48 for SW) and 96 .. 111.
-// Expressions follow rrtmg_sur_decode operation for operation.
+// Decode of one column by one side: HALF 0 writes the LW heating, glw and
+// lwupb, HALF 1 the SW heating (zero at night), swdnb and swupb; returns
+// whether that side fails the energy gate.  y: the side's 50 denormalized
+// heating rates; y2a, y2b: its two surface fluxes; ytop: its model-top net
+// flux.  Expressions follow rrtmg_sur_decode operation for operation
+// (sur_tendency, sur_flux_term); the level fields are read in batches so
+// their loads overlap.
 template <int HALF>
-__device__ __forceinline__ bool decode_half(const SurMlpArgs &a, int col, const uint32_t (&h0)[16],
-                                            const uint32_t (&h1)[16], const uint32_t (&h2)[16],
-                                            const uint32_t (&h3)[16], const uint32_t (&t)[16]) {
-  constexpr int f0 = HALF == 0 ? 0 : 48;
-  const float *b3 = a.bias[3], *om = a.out_mean, *os = a.out_std;
+__device__ __forceinline__ bool decode_side(const SurMlpArgs &a, int col, const float (&y)[kNk], float y2a,
+                                            float y2b, float ytop) {
   const int ny = a.ny;
   const int i = col / ny, jj = col - i * ny;
   const size_t q0 = static_cast<size_t>(i) * kNk * ny + jj;
   const size_t l0 = static_cast<size_t>(i) * (kNk + 1) * ny + jj;
-  const bool day = a.coszr[col] > 0.0f;
-  float *out = HALF == 0 ? a.rthratenlw : a.rthratensw;
+  const bool day = __ldg(a.coszr + col) > 0.0f;
+  float *__restrict__ out = HALF == 0 ? a.rthratenlw : a.rthratensw;
   float s = 0.0f;
 #pragma unroll
-  for (int k = 0; k < kNk; ++k) {
-    const int f = HALF == 0 ? k : kNk + k;
-    const int rel = f - f0;
-    const uint32_t raw = (rel >> 4) == 0 ? h0[rel & 15] : (rel >> 4) == 1 ? h1[rel & 15]
-                                                      : (rel >> 4) == 2 ? h2[rel & 15] : h3[rel & 15];
-    const size_t q = q0 + static_cast<size_t>(k) * ny;
-    const float pi = a.pi3d[q];
-    float hr = dec(raw, b3, om, os, f);
-    if (HALF == 1 && !day) hr = 0.0f;
-    out[q] = (hr / 86400.0f) / pi;
-    const float dp = (a.p8w[l0 + static_cast<size_t>(k) * ny] - a.p8w[l0 + static_cast<size_t>(k + 1) * ny]) * 0.01f;
-    s += hr * dp / kHeatfac;
+  for (int k0 = 0; k0 < kNk; k0 += kDecBatch) {
+    float pi[kDecBatch], pw[kDecBatch + 1];
+#pragma unroll
+    for (int b = 0; b < kDecBatch; ++b) pi[b] = __ldg(a.pi3d + q0 + static_cast<size_t>(k0 + b) * ny);
+#pragma unroll
+    for (int b = 0; b <= kDecBatch; ++b) pw[b] = __ldg(a.p8w + l0 + static_cast<size_t>(k0 + b) * ny);
+#pragma unroll
+    for (int b = 0; b < kDecBatch; ++b) {
+      float hr = y[k0 + b];
+      if (HALF == 1 && !day) hr = 0.0f;
+      out[q0 + static_cast<size_t>(k0 + b) * ny] = sur_tendency(hr, pi[b]);
+      const float dp = (pw[b] - pw[b + 1]) * 0.01f;
+      s += sur_flux_term(hr, dp);
+    }
   }
-  // outputs 2 nk .. 2 nk + 5 (f = 100 .. 105) sit at t[4] .. t[9]
   if (HALF == 0) {
-    const float glw = dec(t[4], b3, om, os, 2 * kNk), lwupb = dec(t[5], b3, om, os, 2 * kNk + 1);
-    a.glw[col] = glw;
-    a.lwupb[col] = lwupb;
-    const float lw_res = fabsf(((lwupb - glw) - dec(t[8], b3, om, os, 2 * kNk + 4)) - s);
+    a.glw[col] = y2a;
+    a.lwupb[col] = y2b;
+    const float lw_res = fabsf(((y2b - y2a) - ytop) - s);
     return !(lw_res <= a.energy_tol);
   } else {
-    const float swdnb = day ? dec(t[6], b3, om, os, 2 * kNk + 2) : 0.0f;
-    const float swupb = day ? dec(t[7], b3, om, os, 2 * kNk + 3) : 0.0f;
+    const float swdnb = day ? y2a : 0.0f, swupb = day ? y2b : 0.0f;
     a.swdnb[col] = swdnb;
     a.swupb[col] = swupb;
-    const float sw_res = day ? fabsf((dec(t[9], b3, om, os, 2 * kNk + 5) - (swdnb - swupb)) - s) : 0.0f;
+    const float sw_res = day ? fabsf((ytop - (swdnb - swupb)) - s) : 0.0f;
     return !(sw_res <= a.energy_tol);
   }
+}
+
+// Layer 3's outputs for one side of one row, read from tensor memory and
+// denormalized, then the decode; arrives on tmem_free once the accumulator
+// has been read.  Output columns: LW heating f = 0..49, SW heating 50..99,
+// glw 100, lwupb 101, swdnb 102, swupb 103, LW and SW model-top net 104, 105.
+template <int HALF>
+__device__ __forceinline__ bool decode_row(const SurMlpArgs &a, uint32_t cb, int col, bool live, int lane,
+                                           uint32_t tmem_free_bar) {
+  constexpr int f0 = HALF == 0 ? 0 : 48;
+  const float *b3 = a.bias[3], *om = a.out_mean, *os = a.out_std;
+  // one 16-column read at a time keeps the register footprint small
+  uint32_t v[16];
+  tmem_ld16(cb + 96, v);  // f = 96 .. 111: f = 100 + d sits at v[4 + d]
+  tmem_ld_wait();
+  const float y2a = dec(v[HALF == 0 ? 4 : 6], b3, om, os, 2 * kNk + (HALF == 0 ? 0 : 2));
+  const float y2b = dec(v[HALF == 0 ? 5 : 7], b3, om, os, 2 * kNk + (HALF == 0 ? 1 : 3));
+  const float ytop = dec(v[HALF == 0 ? 8 : 9], b3, om, os, 2 * kNk + (HALF == 0 ? 4 : 5));
+  float y[kNk];
+#pragma unroll
+  for (int ch = 0; ch < 4; ++ch) {
+    tmem_ld16(cb + f0 + ch * 16, v);
+    tmem_ld_wait();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const int f = f0 + ch * 16 + e;
+      const int k = HALF == 0 ? f : f - kNk;
+      if (k >= 0 && k < kNk) y[k] = dec(v[e], b3, om, os, f);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncwarp();
+  if (lane == 0) mbar_arrive(tmem_free_bar);
+  if (!live) return false;
+  return decode_side<HALF>(a, col, y, y2a, y2b, ytop);
+}
+
+// 16 accumulator columns of this thread's row: + bias, GELU, BF16, written as
+// K = c .. c + 15 of the next layer's A operand (two 16-byte chunks).
+__device__ __forceinline__ void gelu_store(const uint32_t (&v)[16], const float *bias, int c, uint8_t *act, int r) {
+  const float4 *b4 = reinterpret_cast<const float4 *>(bias + c);
+  float b[16];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float4 t = __ldg(b4 + q);
+    b[4 * q] = t.x; b[4 * q + 1] = t.y; b[4 * q + 2] = t.z; b[4 * q + 3] = t.w;
+  }
+  uint32_t p[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float x0 = __uint_as_float(v[2 * j]) + b[2 * j];
+    const float x1 = __uint_as_float(v[2 * j + 1]) + b[2 * j + 1];
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(x0), gelu(x1));
+    p[j] = *reinterpret_cast<const uint32_t *>(&h2);
+  }
+  uint8_t *blk = act + (c / kKb) * kActBlock;
+  const int kc = (c % kKb) / 8;
+  *reinterpret_cast<uint4 *>(blk + swz(r, kc)) = make_uint4(p[0], p[1], p[2], p[3]);
+  *reinterpret_cast<uint4 *>(blk + swz(r, kc + 1)) = make_uint4(p[4], p[5], p[6], p[7]);
 }
 
 __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntiles) {
@@ -178,8 +238,8 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
     mbar_init(bar(bars.act_free), 1);
     mbar_init(bar(bars.acc_full), 1);
     mbar_init(bar(bars.act_ready), kEpiWarps);
-    mbar_init(bar(bars.tmem_free), kEpiWarps);
-    mbar_init(bar(bars.sw_done), kEpiWarps / 2);
+    mbar_init(bar(bars.tmem_free), kDecodeWarps);
+    mbar_init(bar(bars.sw_done), kDecodeWarps / 2);
     mbar_init(bar(bars.mma_done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_sh = 0;
@@ -284,15 +344,26 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
     }
   } else if (warp >= kEpiWarp0) {
     // ---------------- epilogue / decode ----------------
-    const int e = warp - kEpiWarp0;
-    const int quarter = warp & 3;         // tensor-memory lanes 32 * quarter ..
-    const int half = e >> 2;              // 0: columns 0-255 / LW decode, 1: 256-511 / SW decode
-    const int r = quarter * 32 + lane;    // tile row of this thread
+    const int quarter = warp & 3;                  // tensor-memory lanes 32 * quarter ..
+    const int group = (warp - kEpiWarp0) >> 2;     // column group 0-2; decode side 0 / 1
+    const int r = quarter * 32 + lane;             // tile row of this thread
     const uint32_t trow = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
     uint32_t acc_uses = 0;
     int it = 0;
     bool ok = true;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+      const int col = tile * kRows + r;
+      const bool live = col < a.ncol;
+      if (group < 2 && live) {
+        // the decode's level fields: into L2 now, read after layer 3
+        const int i = col / a.ny, jj = col - i * a.ny;
+        const float *pp = (group == 0 ? a.p8w : a.pi3d);
+        const size_t base = group == 0 ? static_cast<size_t>(i) * (kNk + 1) * a.ny + jj
+                                       : static_cast<size_t>(i) * kNk * a.ny + jj;
+        const int levels = group == 0 ? kNk + 1 : kNk;
+        for (int k = 0; k < levels; ++k)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(pp + base + static_cast<size_t>(k) * a.ny));
+      }
       for (int layer = 0; layer < 3 && ok; ++layer) {
         if (!warp_wait(bar(bars.acc_full), acc_uses & 1, &abort_sh)) {
           ok = false;
@@ -301,35 +372,23 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
         ++acc_uses;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const float *bias = a.bias[layer];
+        // columns of this group: 176, 176 and 160 (11, 11 and 10 chunks of 16)
+        const int c0 = group * 176;
+        const int nch = group == 2 ? 10 : 11;
+        const uint32_t tl = trow + static_cast<uint32_t>(c0);
+        // the next chunk's accumulator read is in flight while this one is processed
+        uint32_t va[16], vb[16];
+        tmem_ld16(tl, va);
 #pragma unroll 1
-        for (int c = half * 256; c < half * 256 + 256; c += 32) {
-          uint32_t v0[16], v1[16];
-          tmem_ld16(trow + static_cast<uint32_t>(c), v0);
-          tmem_ld16(trow + static_cast<uint32_t>(c + 16), v1);
+        for (int ch = 0; ch < nch; ch += 2) {
           tmem_ld_wait();
-          uint32_t p[16];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const float x0 = __uint_as_float(v0[2 * j]) + bias[c + 2 * j];
-            const float x1 = __uint_as_float(v0[2 * j + 1]) + bias[c + 2 * j + 1];
-            const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(x0), gelu(x1));
-            p[j] = *reinterpret_cast<const uint32_t *>(&h2);
+          if (ch + 1 < nch) tmem_ld16(tl + (ch + 1) * 16, vb);
+          gelu_store(va, bias, c0 + ch * 16, act, r);
+          if (ch + 1 < nch) {
+            tmem_ld_wait();
+            if (ch + 2 < nch) tmem_ld16(tl + (ch + 2) * 16, va);
+            gelu_store(vb, bias, c0 + (ch + 1) * 16, act, r);
           }
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const float x0 = __uint_as_float(v1[2 * j]) + bias[c + 16 + 2 * j];
-            const float x1 = __uint_as_float(v1[2 * j + 1]) + bias[c + 16 + 2 * j + 1];
-            const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(x0), gelu(x1));
-            p[8 + j] = *reinterpret_cast<const uint32_t *>(&h2);
-          }
-          // columns c .. c+31 of this layer are K = c .. c+31 of the next:
-          // block c / 64, 16-byte chunks (c mod 64) / 8 .. + 3
-          uint8_t *blk = act + (c / kKb) * kActBlock;
-          const int kc0 = (c % kKb) / 8;
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            *reinterpret_cast<uint4 *>(blk + swz(r, kc0 + q)) = make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2],
-                                                                           p[4 * q + 3]);
         }
         // generic-proxy writes -> visible to the tensor cores; accumulator reads done
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -338,37 +397,22 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
         if (lane == 0) mbar_arrive(bar(bars.act_ready));
       }
       if (!ok) break;
-      // ---- layer 3: decode ----
+      // ---- layer 3: decode (groups 0 and 1; group 2 only keeps the phase) ----
       if (!warp_wait(bar(bars.acc_full), acc_uses & 1, &abort_sh)) {
         ok = false;
         break;
       }
       ++acc_uses;
+      if (group >= 2) continue;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int col = tile * kRows + r;
-      const bool live = col < a.ncol;
-      // heating columns of this half: LW f = 0..49 in chunks 0,16,32,48;
-      // SW f = 50..99 in chunks 48,64,80,96; both need the chunk 96..111
-      uint32_t h0[16], h1[16], h2[16], h3[16], t[16];
       const uint32_t cb = trow + kOutCol0;
-      const int f0 = half == 0 ? 0 : 48;
-      tmem_ld16(cb + f0, h0);
-      tmem_ld16(cb + f0 + 16, h1);
-      tmem_ld16(cb + f0 + 32, h2);
-      tmem_ld16(cb + f0 + 48, h3);
-      tmem_ld16(cb + 96, t);
-      tmem_ld_wait();
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(bar(bars.tmem_free));
-
-      const bool gate_fail = live && (half == 0 ? decode_half<0>(a, col, h0, h1, h2, h3, t)
-                                                : decode_half<1>(a, col, h0, h1, h2, h3, t));
-      if (half == 1) {
+      if (group == 1) {
+        const bool gate_fail = decode_row<1>(a, cb, col, live, lane, bar(bars.tmem_free));
         sw_fail[r] = gate_fail ? 1 : 0;
         __syncwarp();
         if (lane == 0) mbar_arrive(bar(bars.sw_done));
       } else {
+        const bool gate_fail = decode_row<0>(a, cb, col, live, lane, bar(bars.tmem_free));
         if (!warp_wait(bar(bars.sw_done), it & 1, &abort_sh)) {
           ok = false;
           break;

@@ -422,11 +422,11 @@ __global__ void __launch_bounds__(kDecCols) decode_kernel(SurDecodeArgs a) {
     const float pi = a.pi3d[q];
     const float hlw = y[k];
     const float hsw = day ? y[nk + k] : 0.0f;
-    a.rthratenlw[q] = (hlw / 86400.0f) / pi;
-    a.rthratensw[q] = (hsw / 86400.0f) / pi;
+    a.rthratenlw[q] = sur_tendency(hlw, pi);
+    a.rthratensw[q] = sur_tendency(hsw, pi);
     const float dp = (a.p8w[idx3(c, k, nk + 1, ny)] - a.p8w[idx3(c, k + 1, nk + 1, ny)]) * 0.01f;
-    slw += hlw * dp / kHeatfac;
-    ssw += hsw * dp / kHeatfac;
+    slw += sur_flux_term(hlw, dp);
+    ssw += sur_flux_term(hsw, dp);
   }
   const float glw = y[2 * nk], lwupb = y[2 * nk + 1];
   const float swdnb = day ? y[2 * nk + 2] : 0.0f, swupb = day ? y[2 * nk + 3] : 0.0f;
