@@ -2,7 +2,7 @@
 // shared-memory matrix descriptors of the 128-byte swizzled K-major layout,
 // bounded mbarrier waits, bulk copies, and the activation functions (one
 // definition, so the unfused GEMM epilogues and the fused inference kernel
-// round alike).
+// round alike, in training and inference).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -134,10 +134,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// Standard normal distribution function Phi(x) = erfc(-x / sqrt 2) / 2,
+// branch-free: erfc(z) for z = |x| / sqrt 2 by Abramowitz & Stegun, Handbook
+// of Mathematical Functions, formula 7.1.26 (Hastings' rational form,
+// |error| <= 1.5e-7), with the hardware reciprocal and base-2 exponential.
+__device__ __forceinline__ float normal_cdf(float x) {
+  const float z = fabsf(x) * 0.70710678118654752f;
+  const float t = __fdividef(1.0f, fmaf(0.3275911f, z, 1.0f));
+  float p = fmaf(t, 1.061405429f, -1.453152027f);
+  p = fmaf(t, p, 1.421413741f);
+  p = fmaf(t, p, -0.284496736f);
+  p = fmaf(t, p, 0.254829592f);
+  const float half_erfc = 0.5f * (t * p) * __expf(-(z * z));
+  return x >= 0.0f ? 1.0f - half_erfc : half_erfc;
+}
+
+// GELU(x) = x Phi(x) (the erf form) and its derivative Phi(x) + x phi(x).
+__device__ __forceinline__ float gelu(float z) { return z * normal_cdf(z); }
 
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  return normal_cdf(z) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
 }
 
 }  // namespace umma
