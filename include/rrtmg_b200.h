@@ -129,13 +129,17 @@ rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable);
 int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_calls);
 
 /* Launch schedule of a context; no counterpart in the reference.  Columns per
- * launch of the LW band-group/finish pair and of the SW column kernel, and the
- * largest domain (columns) that runs the band-split SW schedule.  Defaults:
- * 131072, 131072, 4096.  The autotuner of the ensemble runner sets them. */
+ * launch of the LW band-group/finish pair and of the SW column kernel, the
+ * largest domains (columns) that run the g-point split SW and LW schedules
+ * (one thread per column and g-point; the LW one keeps 1,376 bytes of layer
+ * optics per column and layer).  Defaults: 131072, 131072, 4096, 2048;
+ * limits 1024..16777216, 1024..16777216, 0..16384, 0..8192.  Results do not
+ * depend on the schedule.  The autotuner of the ensemble runner sets it. */
 typedef struct {
     int lw_chunk_columns;
     int sw_chunk_columns;
     int sw_split_max_columns;
+    int lw_split_max_columns;
 } rrtmg_schedule;
 rrtmg_status rrtmg_set_schedule(rrtmg_ctx *ctx, const rrtmg_schedule *schedule);
 rrtmg_status rrtmg_get_schedule(const rrtmg_ctx *ctx, rrtmg_schedule *schedule);

@@ -53,7 +53,7 @@ class SwOut(ctypes.Structure):
 class Schedule(ctypes.Structure):
     """rrtmg_schedule (include/rrtmg_b200.h)."""
     _fields_ = [("lw_chunk_columns", ctypes.c_int), ("sw_chunk_columns", ctypes.c_int),
-                ("sw_split_max_columns", ctypes.c_int)]
+                ("sw_split_max_columns", ctypes.c_int), ("lw_split_max_columns", ctypes.c_int)]
 
 
 class GemmArgs(ctypes.Structure):

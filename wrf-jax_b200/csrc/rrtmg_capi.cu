@@ -44,6 +44,7 @@ struct rrtmg_ctx {
   cudaMemPool_t pool = nullptr;
   // launch schedule (rrtmg_set_schedule)
   int lw_chunk = kLwChunkColumns, sw_chunk = kSwChunkColumns, sw_split_max = kSwSplitMaxColumns;
+  int lw_split_max = kLwSplitMaxColumns;
   // optional per-launch timing: a ring of calls per side (0 LW, 1 SW), each
   // with kTimingMarks events recorded around the call's three launches
   bool timing = false;
@@ -533,12 +534,14 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   uint32_t *mask = nullptr;
   float *terms = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
-  int lw_chunk_setting;
+  int lw_chunk_setting, lw_split_max;
   {
     std::lock_guard<std::mutex> lk(ctx->mutex);
     lw_chunk_setting = ctx->lw_chunk;
+    lw_split_max = ctx->lw_split_max;
   }
-  const int chunk = ncol < lw_chunk_setting ? ncol : lw_chunk_setting;
+  const bool gsplit = ncol <= lw_split_max;
+  const int chunk = gsplit || ncol < lw_chunk_setting ? ncol : lw_chunk_setting;
   const size_t terms_bytes = lw_terms_floats(cfg->nk, chunk) * sizeof(float);
   e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
@@ -546,6 +549,16 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   if (e != cudaSuccess) {
     cudaFreeAsync(mask, stream);
     return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw band terms)");
+  }
+  float *optics = nullptr;
+  if (gsplit) {
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&optics), lw_optics_floats(nlay, ncol) * sizeof(float),
+                                ctx->pool, stream);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(terms, stream);
+      cudaFreeAsync(mask, stream);
+      return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw layer optics)");
+    }
   }
 
   const int tslot = timing_slot(ctx, 0);
@@ -557,6 +570,7 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   e = launch_mcica(m, stream);
   timing_mark(ctx, 0, tslot, 1, stream);
   if (e != cudaSuccess) {
+    if (optics) cudaFreeAsync(optics, stream);
     cudaFreeAsync(terms, stream);
     cudaFreeAsync(mask, stream);
     return cuda_fail(ctx, e, "mcica kernel launch");
@@ -577,17 +591,22 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
   a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
   a.terms = terms;
+  a.optics = optics;
   // chunks of columns: band groups then finish per chunk, reusing the term
   // scratch; timing mark 2 follows the last chunk's band groups, so the
   // finish launches of the earlier chunks count with the band groups
   for (int first = 0; first < ncol && e == cudaSuccess; first += chunk) {
     a.chunk_first = first;
     a.chunk_count = ncol - first < chunk ? ncol - first : chunk;
-    e = launch_lw_groups(ctx->tables, a, stream);
+    e = gsplit ? launch_lw_gsplit(ctx->tables, a, stream) : launch_lw_groups(ctx->tables, a, stream);
     if (first + chunk >= ncol) timing_mark(ctx, 0, tslot, 2, stream);
     if (e == cudaSuccess) e = launch_lw_finish(a, stream);
   }
   timing_mark(ctx, 0, tslot, 3, stream);
+  if (optics) {
+    cudaError_t eo = cudaFreeAsync(optics, stream);
+    if (e == cudaSuccess && eo != cudaSuccess) e = eo;
+  }
   cudaError_t ef = cudaFreeAsync(terms, stream);
   cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
@@ -878,13 +897,16 @@ extern "C" rrtmg_status rrtmg_set_schedule(rrtmg_ctx *ctx, const rrtmg_schedule 
   if (!ctx || !sch) return fail(ctx, RRTMG_BAD_ARG, "null context or schedule");
   const int lo = 1024, hi = 1 << 24;
   if (sch->lw_chunk_columns < lo || sch->lw_chunk_columns > hi || sch->sw_chunk_columns < lo ||
-      sch->sw_chunk_columns > hi || sch->sw_split_max_columns < 0 || sch->sw_split_max_columns > 16384)
+      sch->sw_chunk_columns > hi || sch->sw_split_max_columns < 0 || sch->sw_split_max_columns > 16384 ||
+      sch->lw_split_max_columns < 0 || sch->lw_split_max_columns > 8192)
     return fail(ctx, RRTMG_BAD_ARG,
-                "schedule out of range: chunks 1024..16777216 columns, band-split limit 0..16384 columns");
+                "schedule out of range: chunks 1024..16777216 columns, split limits 0..16384 (SW) and "
+                "0..8192 (LW) columns");
   std::lock_guard<std::mutex> lk(ctx->mutex);
   ctx->lw_chunk = sch->lw_chunk_columns;
   ctx->sw_chunk = sch->sw_chunk_columns;
   ctx->sw_split_max = sch->sw_split_max_columns;
+  ctx->lw_split_max = sch->lw_split_max_columns;
   return RRTMG_OK;
 }
 
@@ -894,5 +916,6 @@ extern "C" rrtmg_status rrtmg_get_schedule(const rrtmg_ctx *ctx, rrtmg_schedule 
   sch->lw_chunk_columns = ctx->lw_chunk;
   sch->sw_chunk_columns = ctx->sw_chunk;
   sch->sw_split_max_columns = ctx->sw_split_max;
+  sch->lw_split_max_columns = ctx->lw_split_max;
   return RRTMG_OK;
 }

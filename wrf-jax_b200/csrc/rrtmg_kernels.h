@@ -33,11 +33,15 @@ struct LwArgs {
   float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc, *glw, *olr, *lwcf;
   float *zero2[4];  // *cln fields, written as zeros
   float *terms;     // band-group schedule scratch, lw_terms_floats(nk, chunk_count) floats
+  float *optics;    // g-point split schedule: lw_optics_floats(nlay, chunk_count) floats, else null
   int chunk_first, chunk_count;  // columns of one band-group/finish launch pair
 };
 
 // default columns per band-group/finish launch pair (the term scratch holds one chunk)
 constexpr int kLwChunkColumns = 131072;
+// Domains of at most this many columns run the LW g-point split schedule
+// (its optics scratch: 1,376 bytes per column and layer).
+constexpr int kLwSplitMaxColumns = 2048;
 
 struct SwArgs {
   int nx, ny, nk, nlay, ncol;
@@ -57,7 +61,7 @@ struct SwArgs {
 };
 
 // defaults: columns per SW column-kernel launch, and the largest domain that
-// uses the band-split SW schedule
+// uses the g-point split SW schedule
 constexpr int kSwChunkColumns = 131072;
 constexpr int kSwSplitMaxColumns = 4096;
 
@@ -69,6 +73,10 @@ cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream);
 size_t lw_terms_floats(int nk, int ncol);
 cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stream);
 cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream);
+// g-point split schedule for small domains (columns chunk_first ..): fills the
+// same band terms as launch_lw_groups.
+cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream);
+size_t lw_optics_floats(int nlay, int ncol);
 // day-column compaction (writes the night columns), then the column kernel over
 // the day columns; both need a.nday and a.daylist (1 + ncol ints)
 cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);

@@ -1049,8 +1049,8 @@ __device__ __forceinline__ void surface_band(const Tables &T, const Layer &L0, f
 
 // Column prologue of both schedules: buffer layers, laytrop, pwvcm, the band
 // diffusivities (lw:5520-5539) and whether any layer is cloudy.
-__device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a, int col, Col &C, float *secdiff,
-                                                bool &has_cloud) {
+// Column set-up shared by both prologues: buffer layers, laytrop and pwvcm.
+__device__ __forceinline__ void column_core(const Tables &T, const LwArgs &a, int col, Col &C) {
   C.i = col / a.ny;
   C.j = col - C.i * a.ny;
   C.nk = a.nk;
@@ -1088,6 +1088,12 @@ __device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a
     const float wvsh = (amw * wvttl) / (amd * amttl);
     C.pwvcm = (wvsh * (1.0e3f * plev_at(a, C, 0))) / (1.0e2f * grav);
   }
+}
+
+__device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a, int col, Col &C, float *secdiff,
+                                                bool &has_cloud) {
+  column_core(T, a, col, C);
+  const int nlay = C.nlay;
 #pragma unroll
   for (int b = 0; b < kLwBands; ++b) {
     const bool variable = !(b == 0 || b == 3 || b >= 9);
@@ -1307,6 +1313,198 @@ __device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int c
   }
 }
 
+// ---------------------------------------------------------------------------
+// g-point split schedule for small domains, in two launches.
+// lw_optics_kernel: thread (column, layer, band) computes the layer's gas
+//   optics of the band (taumol), its Planck terms and the band cloud optical
+//   depth into a per-column record (kLwOpticsFloats per layer).
+// lw_gsplit_kernel: thread (column, band, g-point) runs the two sweeps of one
+//   g-point from those records.  A half-warp owns one (column, band), lane g
+//   its g-point; the band's radiance sum of a level is taken in g order
+//   through shuffles and stored as the band term the finish kernel adds in
+//   band order: the operations and order of band_sums, so the results are
+//   bit-identical to the band-group schedule's while a column's latency drops
+//   from its largest band group to one g-point.
+// Record of a layer: taug[140], fracs[140], then per band blay, dplankup,
+// dplankdn and the cloud optical depth the band's cloudy g-points use.
+// ---------------------------------------------------------------------------
+constexpr int kLwOpticsFloats = 2 * kLwGpts + 4 * kLwBands;
+
+template <int B>
+__device__ __forceinline__ void band_optics(const Tables &T, const Layer &L, bool cloudy_layer, int iceflag,
+                                            float *rec) {
+  constexpr int ngc = kNgc[B];
+  constexpr int gofs = kGofs[B];
+  float taug[ngc], fracs[ngc];
+  taumol<B>(T, L, taug, fracs);
+#pragma unroll
+  for (int g = 0; g < ngc; ++g) {
+    rec[gofs + g] = taug[g];
+    rec[kLwGpts + gofs + g] = fracs[g];
+  }
+  const float blay = planck(T, L.indlay, L.tlayfrac, B);
+  float *bq = rec + 2 * kLwGpts + 4 * B;
+  bq[0] = blay;
+  bq[1] = planck(T, L.indlev1, L.tlev1frac, B) - blay;
+  bq[2] = planck(T, L.indlev0, L.tlev0frac, B) - blay;
+  float teff = 0.0f;
+  if (cloudy_layer) {
+    bool active = false;
+    const float tauc = cloud_tau(T, L, B, iceflag, active);
+    teff = active ? tauc : 0.0f;
+  }
+  bq[3] = teff;
+}
+
+__global__ void __launch_bounds__(128) lw_optics_kernel(Tables T, LwArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int band = blockIdx.y;
+  if (t >= a.chunk_count * a.nlay) return;
+  const int lc = t / a.nlay, l = t - lc * a.nlay;
+  const int col = a.chunk_first + lc;
+  Col C;
+  column_core(T, a, col, C);
+  uint32_t mask[kLwMaskWords];
+  const bool cloudy = load_mask(a, l, col, mask);
+  const Layer L = make_layer(T, a, C, l);
+  float *rec = a.optics + static_cast<size_t>(t) * kLwOpticsFloats;
+  switch (band) {
+    case 0: band_optics<0>(T, L, cloudy, C.iceflg, rec); break;
+    case 1: band_optics<1>(T, L, cloudy, C.iceflg, rec); break;
+    case 2: band_optics<2>(T, L, cloudy, C.iceflg, rec); break;
+    case 3: band_optics<3>(T, L, cloudy, C.iceflg, rec); break;
+    case 4: band_optics<4>(T, L, cloudy, C.iceflg, rec); break;
+    case 5: band_optics<5>(T, L, cloudy, C.iceflg, rec); break;
+    case 6: band_optics<6>(T, L, cloudy, C.iceflg, rec); break;
+    case 7: band_optics<7>(T, L, cloudy, C.iceflg, rec); break;
+    case 8: band_optics<8>(T, L, cloudy, C.iceflg, rec); break;
+    case 9: band_optics<9>(T, L, cloudy, C.iceflg, rec); break;
+    case 10: band_optics<10>(T, L, cloudy, C.iceflg, rec); break;
+    case 11: band_optics<11>(T, L, cloudy, C.iceflg, rec); break;
+    case 12: band_optics<12>(T, L, cloudy, C.iceflg, rec); break;
+    case 13: band_optics<13>(T, L, cloudy, C.iceflg, rec); break;
+    case 14: band_optics<14>(T, L, cloudy, C.iceflg, rec); break;
+    default: band_optics<15>(T, L, cloudy, C.iceflg, rec); break;
+  }
+}
+
+// One g-point of band_sums from a layer record: the new radiances (rA, rB).
+template <bool kDown>
+__device__ __forceinline__ void gpoint_step(const Tables &T, const float *rec, int G, int band, const uint32_t *mask,
+                                            bool cloudy_layer, float secdiff, float &rA, float &rB, bool sep_clear) {
+  const float tg = rec[G], fr = rec[kLwGpts + G];
+  const float *bq = rec + 2 * kLwGpts + 4 * band;
+  const float blay = bq[0], dplankup = bq[1], dplankdn = bq[2], teff = bq[3];
+  const bool cld = (mask[G >> 5] >> (G & 31)) & 1u;
+  float odepth = secdiff * tg;
+  if (odepth < 0.0f) odepth = 0.0f;
+  float odcld = 0.0f, efcl = 0.0f;
+  if (cld) {
+    const float odcld_raw = secdiff * teff;
+    const float abscld = 1.0f - glibc_expf(T, -odcld_raw);
+    odcld = odcld_raw;
+    efcl = abscld * 1.0f;
+  }
+  const Terms tm = layer_terms(T, cloudy_layer, odepth, odcld, fr, blay, dplankdn, dplankup);
+  const float cf = cld ? 1.0f : 0.0f;
+  const float r = rA, rc = rB;
+  float rn;
+  if constexpr (kDown) {
+    if (cloudy_layer) {
+      rn = r - r * (tm.a + efcl * (1.0f - tm.a)) + tm.gassrc + cf * (tm.bbdtot * tm.atot - tm.gassrc);
+    } else {
+      rn = r + (tm.bbdgas - r) * tm.a;
+    }
+    rB = sep_clear ? rc + (tm.bbdgas - rc) * tm.a : rn;
+  } else {
+    if (cloudy_layer) {
+      const float gas = tm.bbugas * tm.a;
+      rn = r - r * (tm.a + efcl * (1.0f - tm.a)) + gas + cf * (tm.bbutot * tm.atot - gas);
+    } else {
+      rn = r + (tm.bbugas - r) * tm.a;
+    }
+    rB = sep_clear ? rc + (tm.bbugas - rc) * tm.a : rn;
+  }
+  rA = rn;
+}
+
+// Band term of a level from the half-warp's g-point radiances (g order), by
+// the lane of g-point 0 (g < 0: store nothing).
+__device__ __forceinline__ void store_band_term(const LwArgs &a, float rn, float rcn, int ngc, int g, int band,
+                                                int type, int slot, int col) {
+  const int base = threadIdx.x & 16;
+  float s = 0.0f, sc = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const float v = __shfl_sync(0xffffffffu, rn, base + q);
+    const float vc = __shfl_sync(0xffffffffu, rcn, base + q);
+    if (q < ngc) {
+      s = s + v;
+      sc = sc + vc;
+    }
+  }
+  if (g == 0 && slot >= 0) {
+    a.terms[term_index(a, type, slot, band, col)] = (s * 0.5f) * kDelwave[band];
+    a.terms[term_index(a, type + 1, slot, band, col)] = (sc * 0.5f) * kDelwave[band];
+  }
+}
+
+__constant__ int kNgcDev[kLwBands] = {10, 12, 16, 14, 16, 8, 12, 8, 12, 6, 8, 8, 4, 2, 2, 2};
+__constant__ int kGofsDev[kLwBands] = {0, 10, 22, 38, 52, 68, 76, 88, 96, 108, 114, 122, 130, 134, 136, 138};
+
+// Band-major grid (blockIdx.y = band), two columns per warp (one per half-warp).
+__global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int band = blockIdx.y;
+  const int lane16 = t & 15;
+  if ((t & ~31) >> 4 >= a.chunk_count) return;  // the whole warp is past the end
+  // a half-warp past the last column repeats it and stores nothing
+  const int lraw = t >> 4;
+  const bool valid = lraw < a.chunk_count;
+  const int lc = valid ? lraw : a.chunk_count - 1;
+  const int col = a.chunk_first + lc;
+  const int ngc = kNgcDev[band];
+  // lanes past the band's g-points repeat its last one and are not summed
+  const int G = kGofsDev[band] + (lane16 < ngc ? lane16 : ngc - 1);
+  const int store_g = valid ? lane16 : -1;
+  Col C;
+  float secdiff[kLwBands];
+  bool has_cloud;
+  column_prologue(T, a, col, C, secdiff, has_cloud);
+  const float sd = secdiff[band];
+  const int nlay = C.nlay, nk = C.nk;
+  const float *recs = a.optics + static_cast<size_t>(lc) * nlay * kLwOpticsFloats;
+  float rA = 0.0f, rB = 0.0f;
+  bool iclddn = false;
+  for (int l = nlay - 1; l >= 0; --l) {
+    uint32_t mask[kLwMaskWords];
+    const bool cloudy = load_mask(a, l, col, mask);
+    iclddn = iclddn || cloudy;
+    gpoint_step<true>(T, recs + static_cast<size_t>(l) * kLwOpticsFloats, G, band, mask, cloudy, sd, rA, rB, iclddn);
+    store_band_term(a, rA, rB, ngc, store_g, band, 2, l <= nk ? l : -1, col);
+  }
+  {
+    // surface emission and reflection (surface_sums)
+    const float bt = C.tsfc - 159.0f;
+    const int indbound = clampi(static_cast<int>(bt), 1, 180);
+    const float tbndfrac = bt - static_cast<float>(indbound);
+    const float reflect = 1.0f - C.semiss;
+    const float plankbnd = C.semiss * planck(T, indbound, tbndfrac, band);
+    const float rad0 = recs[kLwGpts + G] * plankbnd;
+    rA = rad0 + reflect * rA;
+    rB = rad0 + reflect * rB;
+    store_band_term(a, rA, rB, ngc, store_g, band, 0, 0, col);
+  }
+  for (int l = 0; l < nlay; ++l) {
+    uint32_t mask[kLwMaskWords];
+    const bool cloudy = load_mask(a, l, col, mask);
+    gpoint_step<false>(T, recs + static_cast<size_t>(l) * kLwOpticsFloats, G, band, mask, cloudy, sd, rA, rB,
+                       has_cloud);
+    const int lev = l + 1;
+    store_band_term(a, rA, rB, ngc, store_g, band, 0, lev <= nk ? lev : (lev == nlay ? nk + 1 : -1), col);
+  }
+}
+
 // Groups of whole bands with at most 16 g-points each (140 in total).
 constexpr int kLwGroups = 9;
 
@@ -1404,6 +1602,23 @@ cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stre
   const int threads = 128;
   const int blocks = (a.chunk_count + threads - 1) / threads;
   lw_group_kernel<<<dim3(blocks, kLwGroups), threads, 0, stream>>>(T, a);
+  return cudaGetLastError();
+}
+
+size_t lw_optics_floats(int nlay, int ncol) {
+  return static_cast<size_t>(kLwOpticsFloats) * nlay * static_cast<size_t>(ncol);
+}
+
+cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream) {
+  const int threads = 128;
+  const long long layers = static_cast<long long>(a.chunk_count) * a.nlay;
+  lw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kLwBands), threads, 0, stream>>>(
+      T, a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long total = static_cast<long long>(a.chunk_count) * 16;
+  const dim3 grid(static_cast<unsigned>((total + threads - 1) / threads), kLwBands);
+  lw_gsplit_kernel<<<grid, threads, 0, stream>>>(T, a);
   return cudaGetLastError();
 }
 

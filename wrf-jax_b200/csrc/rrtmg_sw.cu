@@ -606,10 +606,11 @@ __device__ __forceinline__ void down_step(Path &P, int r) {
 // kTerms = true: store each level term (type, level, g-point) to `terms` with
 // stride tstride between (type, level, g-point) planes, for the ordered sums
 // of the finish kernel.
+// g_only >= 0: only that g-point of the band (the g-point split schedule).
 template <int B, bool kTerms = false>
 __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
                                         int clear_only, float *accs, Path &Pc, Path &Pt, float *terms = nullptr,
-                                        size_t tstride = 0) {
+                                        size_t tstride = 0, int g_only = -1) {
   constexpr int ngc = kNgc[B];
   constexpr int gofs = kGofs[B];
   constexpr int bn = B + 16;
@@ -698,6 +699,7 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
   const float mu = C.mu;
   const float repclc = 1.0e-12f;
   for (int g = 0; g < ngc; ++g) {
+    if (g_only >= 0 && g != g_only) continue;
     const int G = gofs + g;
     // top-down: layer optics, direct beam, downward adding
     Pc.tdbt[0] = 1.0f;
@@ -993,12 +995,11 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, 
   sw_outputs(a, C, col, accs);
 }
 
-// Band-split schedule for small domains: thread (day column, band) runs one
-// band and stores its level terms; the finish kernel adds each level's terms
-// in g-point order (band order, then g within the band), which is the order
-// the accumulators of sw_kernel see.  A column's latency drops to its longest
-// band.
-__global__ void __launch_bounds__(128) sw_split_kernel(Tables T, SwArgs a, int first, int count) {
+// g-point split schedule for small domains: thread (day column, g-point G =
+// blockIdx.y) runs one g-point of its band and stores its level terms, so a
+// column's latency drops to one g-point.  The terms (type, level, g-point) are
+// summed by sw_gsum_kernel and finished by sw_split_finish_kernel.
+__global__ void __launch_bounds__(128) sw_gsplit_kernel(Tables T, SwArgs a, int first, int count) {
   const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= first + count || t >= *a.nday) return;
   const int col = a.daylist[t];
@@ -1009,22 +1010,35 @@ __global__ void __launch_bounds__(128) sw_split_kernel(Tables T, SwArgs a, int f
   const uint32_t *maskbase = a.mask + col;
   float *terms = a.split_terms + (t - first);
   const size_t ts = static_cast<size_t>(count);
-  switch (blockIdx.y) {
-    case 0: sw_band<0, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 1: sw_band<1, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 2: sw_band<2, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 3: sw_band<3, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 4: sw_band<4, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 5: sw_band<5, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 6: sw_band<6, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 7: sw_band<7, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 8: sw_band<8, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 9: sw_band<9, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 10: sw_band<10, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 11: sw_band<11, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    case 12: sw_band<12, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
-    default: sw_band<13, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts); break;
+  const int G = blockIdx.y;
+#define RRTMG_SW_G(B)                                                                                       \
+  {                                                                                                         \
+    constexpr int lo_ = kGofs[B], n_ = kNgc[B];                                                             \
+    if (G >= lo_ && G < lo_ + n_) sw_band<B, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts, G - lo_); \
   }
+  RRTMG_SW_G(0) RRTMG_SW_G(1) RRTMG_SW_G(2) RRTMG_SW_G(3) RRTMG_SW_G(4) RRTMG_SW_G(5) RRTMG_SW_G(6)
+  RRTMG_SW_G(7) RRTMG_SW_G(8) RRTMG_SW_G(9) RRTMG_SW_G(10) RRTMG_SW_G(11) RRTMG_SW_G(12) RRTMG_SW_G(13)
+#undef RRTMG_SW_G
+}
+
+// Ordered g-point sums of the split schedules: thread (day-list slot t, plane
+// (type, level) = blockIdx.y) adds the plane's 112 terms in g-point order,
+// starting from zero as the accumulators of sw_kernel do, and stores the sum
+// over the plane's g-point-0 term.
+__global__ void __launch_bounds__(128) sw_gsum_kernel(SwArgs a, int first, int count) {
+  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= first + count || t >= *a.nday) return;
+  const size_t ts = static_cast<size_t>(count);
+  float *p = a.split_terms + (t - first) + static_cast<size_t>(blockIdx.y) * kSwGpts * ts;
+  float acc = 0.0f;
+  for (int G0 = 0; G0 < kSwGpts; G0 += 16) {
+    float v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = p[static_cast<size_t>(G0 + q) * ts];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc = acc + v[q];
+  }
+  p[0] = acc;
 }
 
 __global__ void __launch_bounds__(128) sw_split_finish_kernel(Tables T, SwArgs a, int first, int count) {
@@ -1043,12 +1057,8 @@ __global__ void __launch_bounds__(128) sw_split_finish_kernel(Tables T, SwArgs a
   const size_t ts = static_cast<size_t>(count);
   float accs[6 * kMaxLev];
   for (int type = 0; type < 6; ++type) {
-    for (int level = 0; level <= n; ++level) {
-      float acc = 0.0f;
-      const float *p = terms + (static_cast<size_t>(type) * (n + 1) + level) * kSwGpts * ts;
-      for (int G = 0; G < kSwGpts; ++G) acc = acc + p[static_cast<size_t>(G) * ts];
-      accs[type * kMaxLev + level] = acc;
-    }
+    for (int level = 0; level <= n; ++level)
+      accs[type * kMaxLev + level] = terms[(static_cast<size_t>(type) * (n + 1) + level) * kSwGpts * ts];
   }
   (void)T;
   sw_outputs(a, C, col, accs);
@@ -1070,10 +1080,14 @@ size_t sw_split_terms_floats(int nk, int ncol) {
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream) {
   const int threads = 128;
   if (a.split_terms) {
-    // small domain: band-split schedule over all ncol list slots in one launch pair
+    // small domain: g-point split schedule over all ncol list slots, ordered
+    // g-point sums, then the column outputs
     const int blocks = (a.ncol + threads - 1) / threads;
-    sw_split_kernel<<<dim3(blocks, kSwBands), threads, 0, stream>>>(T, a, 0, a.ncol);
+    sw_gsplit_kernel<<<dim3(blocks, kSwGpts), threads, 0, stream>>>(T, a, 0, a.ncol);
     cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sw_gsum_kernel<<<dim3(blocks, 6 * (a.nk + 2)), threads, 0, stream>>>(a, 0, a.ncol);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     sw_split_finish_kernel<<<blocks, threads, 0, stream>>>(T, a, 0, a.ncol);
     return cudaGetLastError();

@@ -298,7 +298,7 @@ def autotune(runner: EnsembleRunner, *, log=None) -> dict:
 
     def apply(cfg):
         sch = _capi.Schedule(lw_chunk_columns=cfg["lw_chunk"], sw_chunk_columns=cfg["sw_chunk"],
-                             sw_split_max_columns=cfg["sw_split_max"])
+                             sw_split_max_columns=cfg["sw_split_max"], lw_split_max_columns=cfg["lw_split_max"])
         ctx.check(lib.rrtmg_set_schedule(ctx.handle, ctypes.byref(sch)))
         S._check(lib.rrtmg_gemm_set_tile(cfg["gemm_tile"]), "gemm tile")
         runner.set_streams(cfg["streams"])
@@ -318,8 +318,9 @@ def autotune(runner: EnsembleRunner, *, log=None) -> dict:
         return ev0.elapsed_time(ev1) / 2
 
     space = dict(lw_chunk=[65536, 131072, 262144], sw_chunk=[65536, 131072, 262144],
-                 sw_split_max=[2048, 4096, 8192], gemm_tile=[128, 256], streams=[1, 2, 4])
-    best = dict(lw_chunk=131072, sw_chunk=131072, sw_split_max=4096, gemm_tile=256, streams=4)
+                 sw_split_max=[2048, 4096, 8192], lw_split_max=[1024, 2048, 4096], gemm_tile=[128, 256],
+                 streams=[1, 2, 4])
+    best = dict(lw_chunk=131072, sw_chunk=131072, sw_split_max=4096, lw_split_max=2048, gemm_tile=256, streams=4)
     best_ms = measure(best)
     trials = [dict(best, ms=best_ms)]
     for key, values in space.items():
