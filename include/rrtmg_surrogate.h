@@ -186,6 +186,20 @@ rrtmg_status rrtmg_sur_compact(const unsigned *flags, int ncol, int *list, int *
 rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
                                     float *dst, int to_compact, int stride, int offset, void *stream);
 
+/* Gathers (to_compact = 1) or scatters (0) up to RRTMG_SUR_MAX_FIELDS fields
+ * in one launch, each as rrtmg_sur_move_columns does with src[i], dst[i] and
+ * nz[i] levels; every compact field has level stride `stride` and column
+ * offset `offset`. */
+#define RRTMG_SUR_MAX_FIELDS 32
+typedef struct {
+    int nfields;
+    const float *src[RRTMG_SUR_MAX_FIELDS];
+    float *dst[RRTMG_SUR_MAX_FIELDS];
+    int nz[RRTMG_SUR_MAX_FIELDS];
+} rrtmg_sur_fields;
+rrtmg_status rrtmg_sur_move_fields(const int *list, const int *count, int max_n, int ny, const rrtmg_sur_fields *f,
+                                   int to_compact, int stride, int offset, void *stream);
+
 /* GEMM tile width: 0 = automatic (256 columns when N allows, else 128), or
  * 128 / 256 (256 needs N % 256 == 0; narrower N falls back to 128).  Process-
  * wide; set by the ensemble autotuner. */

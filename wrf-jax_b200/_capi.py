@@ -105,6 +105,12 @@ class SurMlpArgs(ctypes.Structure):
 
 
 WEIGHT_IMAGE_BYTES = 1703936  # RRTMG_SUR_WEIGHT_IMAGE_BYTES
+MAX_FIELDS = 32  # RRTMG_SUR_MAX_FIELDS
+
+
+class SurFields(ctypes.Structure):
+    """rrtmg_sur_fields (include/rrtmg_surrogate.h)."""
+    _fields_ = [("nfields", _I), ("src", _F * MAX_FIELDS), ("dst", _F * MAX_FIELDS), ("nz", _I * MAX_FIELDS)]
 
 STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
           4: "RRTMG_TIMEOUT"}
@@ -116,7 +122,7 @@ SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile
                      "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
                      "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
                      "rrtmg_sur_compact", "rrtmg_sur_move_columns", "rrtmg_sur_timestamp",
-                     "rrtmg_sur_pack_weights", "rrtmg_sur_mlp")
+                     "rrtmg_sur_pack_weights", "rrtmg_sur_mlp", "rrtmg_sur_move_fields")
 
 _lib = None
 
@@ -174,6 +180,7 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_sur_timestamp": [P, V],
         "rrtmg_sur_pack_weights": [ctypes.POINTER(ctypes.c_void_p * 4), V, V],
         "rrtmg_sur_mlp": [ctypes.POINTER(SurMlpArgs), V],
+        "rrtmg_sur_move_fields": [P, P, I, I, ctypes.POINTER(SurFields), I, I, I, V],
         "rrtmg_set_schedule": [V, ctypes.POINTER(Schedule)],
         "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
     }

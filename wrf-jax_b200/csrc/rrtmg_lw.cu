@@ -1315,6 +1315,7 @@ __device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int c
 
 // ---------------------------------------------------------------------------
 // g-point split schedule for small domains, in two launches.
+// lw_colprep_kernel: thread (column) computes the column set-up once.
 // lw_optics_kernel: thread (column, layer, band) computes the layer's gas
 //   optics of the band (taumol), its Planck terms and the band cloud optical
 //   depth into a per-column record (kLwOpticsFloats per layer).
@@ -1329,6 +1330,32 @@ __device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int c
 // dplankdn and the cloud optical depth the band's cloudy g-points use.
 // ---------------------------------------------------------------------------
 constexpr int kLwOpticsFloats = 2 * kLwGpts + 4 * kLwBands;
+
+// Per-column record of the split schedule, computed once per column.
+struct ColRec {
+  Col C;
+  float secdiff[kLwBands];
+  int has_cloud;
+};
+// column records first, 16-byte aligned, then the layer records
+constexpr size_t kColRecFloats = (sizeof(ColRec) + 15) / 16 * 4;
+
+__device__ __forceinline__ const ColRec *col_records(const LwArgs &a) {
+  return reinterpret_cast<const ColRec *>(a.optics);
+}
+__device__ __forceinline__ float *layer_records(const LwArgs &a) {
+  return a.optics + kColRecFloats * static_cast<size_t>(a.chunk_count);
+}
+
+__global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
+  const int lc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lc >= a.chunk_count) return;
+  ColRec r;
+  bool has_cloud;
+  column_prologue(T, a, a.chunk_first + lc, r.C, r.secdiff, has_cloud);
+  r.has_cloud = has_cloud ? 1 : 0;
+  reinterpret_cast<ColRec *>(a.optics)[lc] = r;
+}
 
 template <int B>
 __device__ __forceinline__ void band_optics(const Tables &T, const Layer &L, bool cloudy_layer, int iceflag,
@@ -1362,12 +1389,11 @@ __global__ void __launch_bounds__(128) lw_optics_kernel(Tables T, LwArgs a) {
   if (t >= a.chunk_count * a.nlay) return;
   const int lc = t / a.nlay, l = t - lc * a.nlay;
   const int col = a.chunk_first + lc;
-  Col C;
-  column_core(T, a, col, C);
+  const Col &C = col_records(a)[lc].C;
   uint32_t mask[kLwMaskWords];
   const bool cloudy = load_mask(a, l, col, mask);
   const Layer L = make_layer(T, a, C, l);
-  float *rec = a.optics + static_cast<size_t>(t) * kLwOpticsFloats;
+  float *rec = layer_records(a) + static_cast<size_t>(t) * kLwOpticsFloats;
   switch (band) {
     case 0: band_optics<0>(T, L, cloudy, C.iceflg, rec); break;
     case 1: band_optics<1>(T, L, cloudy, C.iceflg, rec); break;
@@ -1467,13 +1493,12 @@ __global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
   // lanes past the band's g-points repeat its last one and are not summed
   const int G = kGofsDev[band] + (lane16 < ngc ? lane16 : ngc - 1);
   const int store_g = valid ? lane16 : -1;
-  Col C;
-  float secdiff[kLwBands];
-  bool has_cloud;
-  column_prologue(T, a, col, C, secdiff, has_cloud);
-  const float sd = secdiff[band];
-  const int nlay = C.nlay, nk = C.nk;
-  const float *recs = a.optics + static_cast<size_t>(lc) * nlay * kLwOpticsFloats;
+  const ColRec &R = col_records(a)[lc];
+  const float sd = R.secdiff[band];
+  const bool has_cloud = R.has_cloud != 0;
+  const float tsfc = R.C.tsfc, semiss = R.C.semiss;
+  const int nlay = R.C.nlay, nk = R.C.nk;
+  const float *recs = layer_records(a) + static_cast<size_t>(lc) * nlay * kLwOpticsFloats;
   float rA = 0.0f, rB = 0.0f;
   bool iclddn = false;
   for (int l = nlay - 1; l >= 0; --l) {
@@ -1485,11 +1510,11 @@ __global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
   }
   {
     // surface emission and reflection (surface_sums)
-    const float bt = C.tsfc - 159.0f;
+    const float bt = tsfc - 159.0f;
     const int indbound = clampi(static_cast<int>(bt), 1, 180);
     const float tbndfrac = bt - static_cast<float>(indbound);
-    const float reflect = 1.0f - C.semiss;
-    const float plankbnd = C.semiss * planck(T, indbound, tbndfrac, band);
+    const float reflect = 1.0f - semiss;
+    const float plankbnd = semiss * planck(T, indbound, tbndfrac, band);
     const float rad0 = recs[kLwGpts + G] * plankbnd;
     rA = rad0 + reflect * rA;
     rB = rad0 + reflect * rB;
@@ -1606,11 +1631,14 @@ cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stre
 }
 
 size_t lw_optics_floats(int nlay, int ncol) {
-  return static_cast<size_t>(kLwOpticsFloats) * nlay * static_cast<size_t>(ncol);
+  return (static_cast<size_t>(kLwOpticsFloats) * nlay + kColRecFloats) * static_cast<size_t>(ncol);
 }
 
 cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
+  lw_colprep_kernel<<<(a.chunk_count + threads - 1) / threads, threads, 0, stream>>>(T, a);
+  cudaError_t e0 = cudaGetLastError();
+  if (e0 != cudaSuccess) return e0;
   const long long layers = static_cast<long long>(a.chunk_count) * a.nlay;
   lw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kLwBands), threads, 0, stream>>>(
       T, a);

@@ -190,3 +190,15 @@ extern "C" rrtmg_status rrtmg_sur_mlp(const rrtmg_sur_mlp_args *a, void *stream)
   if (a->ncol == 0) return RRTMG_OK;
   return cuda_status(launch_sur_mlp(*a, as_stream(stream)));
 }
+
+extern "C" rrtmg_status rrtmg_sur_move_fields(const int *list, const int *count, int max_n, int ny,
+                                              const rrtmg_sur_fields *f, int to_compact, int stride, int offset,
+                                              void *stream) {
+  if (!list || !count || !f || max_n < 0 || ny <= 0 || offset < 0 || stride < offset + max_n || f->nfields < 0 ||
+      f->nfields > RRTMG_SUR_MAX_FIELDS)
+    return RRTMG_BAD_ARG;
+  for (int i = 0; i < f->nfields; ++i)
+    if (!f->src[i] || !f->dst[i] || f->nz[i] <= 0) return RRTMG_BAD_ARG;
+  return cuda_status(launch_sur_move_fields(list, count, max_n, ny, *f, to_compact, stride, offset,
+                                            as_stream(stream)));
+}

@@ -76,6 +76,8 @@ cudaError_t launch_sur_decode(const SurDecodeArgs &a, cudaStream_t s);
 cudaError_t launch_sur_compact(const unsigned *flags, int ncol, int *list, int *count, cudaStream_t s);
 cudaError_t launch_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
                                     float *dst, int to_compact, int stride, int offset, cudaStream_t s);
+cudaError_t launch_sur_move_fields(const int *list, const int *count, int max_n, int ny, const rrtmg_sur_fields &f,
+                                   int to_compact, int stride, int offset, cudaStream_t s);
 void set_gemm_tile(int bn);
 cudaError_t launch_timestamp(unsigned long long *slot, cudaStream_t s);
 // Reads (and optionally clears) the sticky flag set when a GEMM CTA gave up

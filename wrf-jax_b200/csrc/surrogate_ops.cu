@@ -475,7 +475,40 @@ __global__ void move_columns_kernel(const int *list, const int *count, int nz, i
   else dst[full] = src[comp];
 }
 
+// Several fields in one launch: blockIdx.y = field, grid-stride over its
+// (level, listed column) pairs.
+__global__ void move_fields_kernel(const int *list, const int *count, int ny, rrtmg_sur_fields f, int to_compact,
+                                   int stride, int offset) {
+  const int field = blockIdx.y;
+  const int n = *count, nz = f.nz[field];
+  const float *src = f.src[field];
+  float *dst = f.dst[field];
+  const long long total = static_cast<long long>(n) * nz;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(t / n), j = static_cast<int>(t - static_cast<long long>(k) * n);
+    const int c = list[j];
+    const size_t full = idx3(c, k, nz, ny);
+    const size_t comp = static_cast<size_t>(k) * stride + offset + j;
+    if (to_compact) dst[comp] = src[full];
+    else dst[full] = src[comp];
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_sur_move_fields(const int *list, const int *count, int max_n, int ny, const rrtmg_sur_fields &f,
+                                   int to_compact, int stride, int offset, cudaStream_t s) {
+  int max_nz = 0;
+  for (int i = 0; i < f.nfields; ++i) max_nz = f.nz[i] > max_nz ? f.nz[i] : max_nz;
+  const long long total = static_cast<long long>(max_n) * max_nz;
+  if (total == 0 || f.nfields == 0) return cudaSuccess;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  move_fields_kernel<<<dim3(static_cast<unsigned>(blocks), f.nfields), 256, 0, s>>>(list, count, ny, f, to_compact,
+                                                                                     stride, offset);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s) {
   const unsigned row_blocks = static_cast<unsigned>((a.ncol + kRowThreads - 1) / kRowThreads);

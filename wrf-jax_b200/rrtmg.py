@@ -154,6 +154,28 @@ def _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr, cfc11vmr, cfc12
     return tuple(vals) + (0.0, 0.0)
 
 
+def lw_config(nx: int, ny: int, nk: int, *, p_top, yr, ghg_input=1, case_dir=None, co2vmr=None, n2ovmr=None,
+              ch4vmr=None, cfc11vmr=None, cfc12vmr=None, icloud=1, has_reqc=1, has_reqi=1, has_reqs=1,
+              cldovrlp=2) -> "_capi.Config":
+    """rrtmg_config of an LW call: the scalar keywords of rrtmg_lwrad_wrf_columns."""
+    co2, n2o, ch4, cfc11, cfc12 = _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr,
+                                              cfc11vmr, cfc12vmr, lw=True)
+    return _capi.Config(nx=nx, ny=ny, nk=nk, p_top=float(p_top), co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4,
+                        cfc11vmr=cfc11, cfc12vmr=cfc12, solcon=0.0, has_reqc=int(has_reqc),
+                        has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
+                        cldovrlp=int(cldovrlp))
+
+
+def sw_config(nx: int, ny: int, nk: int, *, solcon, yr, ghg_input=1, co2vmr=None, n2ovmr=None, ch4vmr=None,
+              icloud=1, has_reqc=1, has_reqi=1, has_reqs=1, cldovrlp=2) -> "_capi.Config":
+    """rrtmg_config of an SW call: the scalar keywords of rrtmg_swrad_wrf_columns."""
+    co2, n2o, ch4, _, _ = _greenhouse(yr, ghg_input, None, co2vmr, n2ovmr, ch4vmr, None, None, lw=False)
+    return _capi.Config(nx=nx, ny=ny, nk=nk, p_top=0.0, co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4, cfc11vmr=0.0,
+                        cfc12vmr=0.0, solcon=float(np.float32(solcon)), has_reqc=int(has_reqc),
+                        has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
+                        cldovrlp=int(cldovrlp))
+
+
 def _as_device(arrays: dict, device: int):
     """numpy or host torch tensors -> torch CUDA float32 (contiguous); torch CUDA
     tensors pass through.  Returns the tensors and whether any input was on the host."""
@@ -239,12 +261,9 @@ def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                       ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d",
                        "re_cloud", "re_ice", "re_snow"), ("p8w", "t8w"),
                       ("tsk", "emiss", "xland", "xice", "snow"))
-        co2, n2o, ch4, cfc11, cfc12 = _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr,
-                                                  cfc11vmr, cfc12vmr, lw=True)
-        cfg = _capi.Config(nx=nx, ny=ny, nk=nk, p_top=float(p_top), co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4,
-                           cfc11vmr=cfc11, cfc12vmr=cfc12, solcon=0.0, has_reqc=int(has_reqc),
-                           has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
-                           cldovrlp=int(cldovrlp))
+        cfg = lw_config(nx, ny, nk, p_top=p_top, yr=yr, ghg_input=ghg_input, case_dir=case_dir, co2vmr=co2vmr,
+                        n2ovmr=n2ovmr, ch4vmr=ch4vmr, cfc11vmr=cfc11vmr, cfc12vmr=cfc12vmr, icloud=icloud,
+                        has_reqc=has_reqc, has_reqi=has_reqi, has_reqs=has_reqs, cldovrlp=cldovrlp)
         outs = out if out is not None else {
             k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), dtype=torch.float32,
                            device=f"cuda:{ctx.device}") for k in _capi.LW_OUT_FIELDS}
@@ -286,11 +305,9 @@ def rrtmg_swrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                       ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d",
                        "re_cloud", "re_ice", "re_snow"), ("p8w", "t8w"),
                       ("tsk", "albedo", "coszr", "xland", "xice", "snow"))
-        co2, n2o, ch4, _, _ = _greenhouse(yr, ghg_input, None, co2vmr, n2ovmr, ch4vmr, None, None, lw=False)
-        cfg = _capi.Config(nx=nx, ny=ny, nk=nk, p_top=0.0, co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4, cfc11vmr=0.0,
-                           cfc12vmr=0.0, solcon=float(np.float32(solcon)), has_reqc=int(has_reqc),
-                           has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
-                           cldovrlp=int(cldovrlp))
+        cfg = sw_config(nx, ny, nk, solcon=solcon, yr=yr, ghg_input=ghg_input, co2vmr=co2vmr, n2ovmr=n2ovmr,
+                        ch4vmr=ch4vmr, icloud=icloud, has_reqc=has_reqc, has_reqi=has_reqi, has_reqs=has_reqs,
+                        cldovrlp=cldovrlp)
         outs = out if out is not None else {
             k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), dtype=torch.float32,
                            device=f"cuda:{ctx.device}") for k in _capi.SW_OUT_FIELDS}

@@ -515,57 +515,120 @@ def _side_stream():
     return _SIDE[dev]
 
 
+_SCALAR_KEYS_LW = ("p_top", "yr", "co2vmr", "n2ovmr", "ch4vmr", "cfc11vmr", "cfc12vmr", "has_reqc", "has_reqi",
+                   "has_reqs", "icloud", "cldovrlp")
+_SCALAR_KEYS_SW = ("solcon", "yr", "co2vmr", "n2ovmr", "ch4vmr", "has_reqc", "has_reqi", "has_reqs", "icloud",
+                   "cldovrlp")
+
+
+class _FallbackPlan:
+    """Persistent buffers and prebuilt C-ABI arguments of the plain-kernel
+    fallback for up to `cap` columns of nk levels: the gathered input fields
+    and the LW/SW outputs of a compact (1, nk, n) domain (n <= cap, each
+    field's first n columns per level), so a call allocates nothing and
+    issues one gather, the LW and SW calls and one scatter."""
+
+    def __init__(self, nk: int, cap: int, lw_scalars: dict, sw_scalars: dict):
+        import torch
+        from . import rrtmg
+        self.nk, self.cap = nk, cap
+        self.ctx = rrtmg.default_context()
+        dev = "cuda"
+        nz = {k: nk for k in _FIELDS_3D}
+        nz.update({k: nk + 1 for k in _FIELDS_LEV})
+        nz.update({k: 1 for k in _FIELDS_2D})
+        self.nz = nz
+        self.sub = {k: torch.empty(z * cap, device=dev) for k, z in nz.items()}
+        self.lw_out = {k: torch.empty((nk if k.startswith("rthraten") else 1) * cap, device=dev)
+                       for k in _capi.LW_OUT_FIELDS}
+        self.sw_out = {k: torch.empty((nk if k.startswith("rthraten") else 1) * cap, device=dev)
+                       for k in _capi.SW_OUT_FIELDS}
+        self.cfg_lw = rrtmg.lw_config(1, 1, nk, **lw_scalars)
+        self.cfg_sw = rrtmg.sw_config(1, 1, nk, **sw_scalars)
+        self.cin_lw = _capi.LwIn(**{k: self.sub[k].data_ptr() for k in _capi.LW_IN_FIELDS})
+        self.cout_lw = _capi.LwOut(**{k: v.data_ptr() for k, v in self.lw_out.items()})
+        self.cin_sw = _capi.SwIn(**{k: self.sub[k].data_ptr() for k in _capi.SW_IN_FIELDS})
+        self.cout_sw = _capi.SwOut(**{k: v.data_ptr() for k, v in self.sw_out.items()})
+        self.gather = _capi.SurFields(nfields=len(nz))
+        for i, (k, z) in enumerate(nz.items()):
+            self.gather.dst[i] = self.sub[k].data_ptr()
+            self.gather.nz[i] = z
+        self.scatter_src = (("rthratenlw", self.lw_out["rthratenlw"], nk), ("rthratensw", self.sw_out["rthratensw"], nk),
+                            ("glw", self.lw_out["glw"], 1), ("lwupb", self.lw_out["lwupb"], 1),
+                            ("swdnb", self.sw_out["swdnb"], 1), ("swupb", self.sw_out["swupb"], 1))
+        self.scatter = _capi.SurFields(nfields=len(self.scatter_src))
+        for i, (_, t, z) in enumerate(self.scatter_src):
+            self.scatter.src[i] = t.data_ptr()
+            self.scatter.nz[i] = z
+
+
+_PLANS: dict = {}
+_LISTS: dict = {}
+
+
+def _fallback_plan(st, n: int) -> _FallbackPlan:
+    import torch
+    cap = 256
+    while cap < n:
+        cap *= 2
+    lw_kw, sw_kw = st.lw_kwargs(), st.sw_kwargs()
+    lw_s = {k: lw_kw[k] for k in _SCALAR_KEYS_LW if k in lw_kw}
+    sw_s = {k: sw_kw[k] for k in _SCALAR_KEYS_SW if k in sw_kw}
+    key = (torch.cuda.current_device(), st.nk, cap, tuple(sorted(lw_s.items())), tuple(sorted(sw_s.items())))
+    plan = _PLANS.get(key)
+    if plan is None:
+        plan = _FallbackPlan(st.nk, cap, lw_s, sw_s)
+        _PLANS.clear()  # keep one plan resident
+        _PLANS[key] = plan
+    return plan
+
+
 def _fallback(st, d: dict, flags, out: dict) -> int:
     """Re-solve the flagged columns with the plain kernels, writing their
-    surrogate outputs over; returns how many columns were re-solved."""
+    surrogate outputs over; returns how many columns were re-solved.  The
+    column count is read on the host (one synchronization); everything after
+    it reuses the buffers and argument blocks of a cached plan."""
     import torch
-    from . import rrtmg
     lib = _capi.load()
     s = _stream()
     nx, ny, nk = st.nx, st.ny, st.nk
     ncol = nx * ny
-    lst = torch.empty(ncol, device="cuda", dtype=torch.int32)
-    cnt = torch.zeros(1, device="cuda", dtype=torch.int32)
+    key = (torch.cuda.current_device(), ncol)
+    if key not in _LISTS:
+        _LISTS.clear()
+        _LISTS[key] = (torch.empty(ncol, device="cuda", dtype=torch.int32),
+                       torch.zeros(1, device="cuda", dtype=torch.int32))
+    lst, cnt = _LISTS[key]
+    cnt.zero_()
     _check(lib.rrtmg_sur_compact(flags.data_ptr(), ncol, lst.data_ptr(), cnt.data_ptr(), s), "compact")
     n = int(cnt.item())
     if n == 0:
         return 0
-    mv = lambda src, dst, nz, to: _check(lib.rrtmg_sur_move_columns(lst.data_ptr(), cnt.data_ptr(), n, nz, ny,
-                                                                     src.data_ptr(), dst.data_ptr(), to, n, 0, s),
-                                         "move")
-    sub = {}
-    for k in _FIELDS_3D:
-        sub[k] = torch.empty(1, nk, n, device="cuda")
-        mv(d[k], sub[k], nk, 1)
-    for k in _FIELDS_LEV:
-        sub[k] = torch.empty(1, nk + 1, n, device="cuda")
-        mv(d[k], sub[k], nk + 1, 1)
-    for k in _FIELDS_2D:
-        sub[k] = torch.empty(1, n, device="cuda")
-        mv(d[k], sub[k], 1, 1)
-    lw_kw = {k: (sub[k] if k in sub else v) for k, v in st.lw_kwargs().items()}
-    sw_kw = {k: (sub[k] if k in sub else v) for k, v in st.sw_kwargs().items()}
-    # LW on a side stream overlaps SW on the current stream.  Every buffer the
-    # side stream touches is allocated on the current stream beforehand, and the
-    # current stream waits for the side stream before it reads or frees them.
+    plan = _fallback_plan(st, n)
+    for i, k in enumerate(plan.nz):
+        plan.gather.src[i] = d[k].data_ptr()
+    _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), n, ny, ctypes.byref(plan.gather), 1, n, 0, s),
+           "gather")
+    plan.cfg_lw.ny = n
+    plan.cfg_sw.ny = n
+    ctx = plan.ctx
+    # LW on a side stream overlaps SW on the current stream; both read the
+    # gathered fields, and the current stream waits for LW before the scatter.
     main, side = torch.cuda.current_stream(), _side_stream()
-    lw_out = {k: torch.empty((1, nk, n) if k.startswith("rthraten") else (1, n), device="cuda")
-              for k in _capi.LW_OUT_FIELDS}
     ready = torch.cuda.Event()
     ready.record(main)
     side.wait_event(ready)
-    with torch.cuda.stream(side):
-        lw = rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw, stream=side.cuda_stream, out=lw_out)
-    sw = rrtmg.rrtmg_swrad_wrf_columns(**sw_kw)
+    ctx.check(ctx.lib.rrtmg_lwrad(ctx.handle, ctypes.byref(plan.cfg_lw), ctypes.byref(plan.cin_lw),
+                                  ctypes.byref(plan.cout_lw), ctypes.c_void_p(side.cuda_stream)))
+    ctx.check(ctx.lib.rrtmg_swrad(ctx.handle, ctypes.byref(plan.cfg_sw), ctypes.byref(plan.cin_sw),
+                                  ctypes.byref(plan.cout_sw), s))
     done = torch.cuda.Event()
     done.record(side)
     main.wait_event(done)
-    mv(lw.rthratenlw, out["rthratenlw"], nk, 0)
-    mv(sw.rthratensw, out["rthratensw"], nk, 0)
-    mv(lw.glw, out["glw"], 1, 0)
-    mv(lw.lwupb, out["lwupb"], 1, 0)
-    mv(sw.swdnb, out["swdnb"], 1, 0)
-    mv(sw.swupb, out["swupb"], 1, 0)
+    for i, (k, _, _) in enumerate(plan.scatter_src):
+        plan.scatter.dst[i] = out[k].data_ptr()
+    _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), n, ny, ctypes.byref(plan.scatter), 0, n, 0, s),
+           "scatter")
     return n
 
 
