@@ -452,24 +452,26 @@ def run_surrogate(args):
     hbm, bf16, peak_kind = _peaks()
     achieved = flops / (kernel_ms / 1e3) / 1e12
 
-    # end to end with host inputs and host outputs
-    # (inputs and outputs in pinned host memory, allocated before the timed region)
+    # end to end with host inputs and host outputs through surrogate.infer_host
+    # (inputs and outputs in page-locked host memory, allocated before the
+    # timed region): the network's fields cross the host link in slabs that
+    # overlap the network and the returning outputs; the fallback reads its
+    # columns' other inputs from host memory in place (counted below)
     e2e_steps = max(0, args.e2e_steps) if args.e2e_steps is not None else 3
-    h2d = sum(v.nbytes for v in st.fields.values())
     pinned_in = {k: torch.from_numpy(v).pin_memory() for k, v in st.fields.items()}
-    dev_in = {k: torch.empty_like(v, device="cuda") for k, v in pinned_in.items()}
-    out_names = ("rthratenlw", "rthratensw", "glw", "lwupb", "swdnb", "swupb")
-    pinned_out = {k: torch.empty(getattr(res, k).shape, pin_memory=True) for k in out_names}
+    pinned_out = {k: torch.empty(getattr(res, k).shape, pin_memory=True) for k in S.OUTPUT_FIELDS}
+    h2d = sum(pinned_in[k].numel() * 4 for k in S.NETWORK_FIELDS)
     d2h = sum(v.numel() * 4 for v in pinned_out.values())
+    if e2e_steps:
+        n_host = S.infer_host(model, st, pinned_in, pinned_out, energy_tol=tol)  # warm-up
+        fb_levels = sum(pinned_in[k].shape[1] if pinned_in[k].dim() == 3 else 1
+                        for k in pinned_in if k not in S.NETWORK_FIELDS)
+        h2d += n_host * fb_levels * 4  # fallback inputs read in place
+        d2h += n_host * (2 * wl["nk"] + 4) * 4  # fallback outputs written in place
     barrier()
     t_e2e = time.perf_counter()
     for _ in range(e2e_steps):
-        for k, v in pinned_in.items():
-            dev_in[k].copy_(v, non_blocking=True)
-        r = S.infer(model, st, dev_in, energy_tol=tol, fallback=True)
-        for k in out_names:
-            pinned_out[k].copy_(getattr(r, k), non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        S.infer_host(model, st, pinned_in, pinned_out, energy_tol=tol)
     barrier()
     t_e2e = max(time.perf_counter() - t_e2e, 1e-9)
     e2e = ws * ncol * e2e_steps / t_e2e if e2e_steps else None

@@ -189,7 +189,9 @@ rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n
 /* Gathers (to_compact = 1) or scatters (0) up to RRTMG_SUR_MAX_FIELDS fields
  * in one launch, each as rrtmg_sur_move_columns does with src[i], dst[i] and
  * nz[i] levels; every compact field has level stride `stride` and column
- * offset `offset`. */
+ * offset `offset`.  Each pointer is device memory or page-locked host memory
+ * mapped at the same address (read or written over the bus in place);
+ * anything else is rejected with RRTMG_BAD_ARG. */
 #define RRTMG_SUR_MAX_FIELDS 32
 typedef struct {
     int nfields;

@@ -41,3 +41,16 @@ def test_product_fails_loudly_without_a_gpu(pkg):
     from wrf_jax_b200 import rrtmg
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         rrtmg.RrtmgContext()
+
+
+def test_infer_host_rejects_pageable_buffers(pkg):
+    """The host-buffer surrogate path reads and writes host memory in place
+    from the GPU, so it accepts page-locked tensors only (checked before any
+    GPU work)."""
+    import torch
+    from wrf_jax_b200 import surrogate as S, synthetic
+    st = synthetic.make_columns(2, 3, S.NK, seed=1)
+    host = {k: torch.from_numpy(v) for k, v in st.fields.items()}
+    out = {k: torch.empty((2, S.NK, 3) if k.startswith("rthraten") else (2, 3)) for k in S.OUTPUT_FIELDS}
+    with pytest.raises(ValueError):
+        S.infer_host(None, st, host, out)

@@ -139,3 +139,24 @@ def test_fused_rejects_other_level_counts(torch_cuda, model):
     lib = _capi.load()
     a = _capi.SurMlpArgs(ncol=128, nk=40, ny=8)
     assert lib.rrtmg_sur_mlp(ctypes.byref(a), None) == 1
+
+
+def test_infer_host_equals_device_path(torch_cuda, model):
+    """Host-buffer pipeline (slabs over the host link, fallback reading and
+    writing host memory in place) against infer() on device fields: the same
+    bits, including the fallback columns (a tight energy gate rejects many)."""
+    torch = torch_cuda
+    from wrf_jax_b200 import surrogate as S, synthetic
+    st = synthetic.make_columns(40, 36, S.NK, seed=9)
+    d = S._device_fields(st, "cuda")
+    ref = S.infer(model, st, d, energy_tol=1.0, fallback=True)
+    torch.cuda.synchronize()
+    host = {k: torch.from_numpy(v).pin_memory() for k, v in st.fields.items()}
+    out = {k: torch.empty(tuple(getattr(ref, k).shape), pin_memory=True) for k in S.OUTPUT_FIELDS}
+    for slabs in (3, 1):
+        for t in out.values():
+            t.fill_(float("nan"))
+        n = S.infer_host(model, st, host, out, energy_tol=1.0, slabs=slabs)
+        assert n == ref.n_fallback and n > 0
+        for k in S.OUTPUT_FIELDS:
+            assert torch.equal(out[k], getattr(ref, k).cpu()), k

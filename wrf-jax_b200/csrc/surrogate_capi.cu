@@ -64,6 +64,18 @@ extern "C" rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag) {
 
 namespace {
 rrtmg_status cuda_status(cudaError_t e) { return e == cudaSuccess ? RRTMG_OK : RRTMG_CUDA; }
+
+// A pointer the kernels may dereference: device memory, managed memory, or
+// page-locked host memory mapped at the same address (unified addressing).
+bool device_reachable(const void *p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky error of an unknown pointer
+    return false;
+  }
+  if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return true;
+  return at.type == cudaMemoryTypeHost && at.devicePointer == p;
+}
 cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 }  // namespace
 
@@ -197,8 +209,10 @@ extern "C" rrtmg_status rrtmg_sur_move_fields(const int *list, const int *count,
   if (!list || !count || !f || max_n < 0 || ny <= 0 || offset < 0 || stride < offset + max_n || f->nfields < 0 ||
       f->nfields > RRTMG_SUR_MAX_FIELDS)
     return RRTMG_BAD_ARG;
-  for (int i = 0; i < f->nfields; ++i)
+  for (int i = 0; i < f->nfields; ++i) {
     if (!f->src[i] || !f->dst[i] || f->nz[i] <= 0) return RRTMG_BAD_ARG;
+    if (!device_reachable(f->src[i]) || !device_reachable(f->dst[i])) return RRTMG_BAD_ARG;
+  }
   return cuda_status(launch_sur_move_fields(list, count, max_n, ny, *f, to_compact, stride, offset,
                                             as_stream(stream)));
 }

@@ -441,6 +441,116 @@ def infer(model: SurrogateModel, st, d: dict | None = None, *, energy_tol: float
     return SurrogateResult(flags=flags, n_fallback=n_fb, **out)
 
 
+# Fields the network reads for every column (features and decode); the
+# plain-kernel fallback also reads the other inputs, for its columns only.
+NETWORK_FIELDS = ("t3d", "p3d", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d", "p8w", "pi3d", "tsk", "albedo",
+                  "coszr", "emiss")
+OUTPUT_FIELDS = ("rthratenlw", "rthratensw", "glw", "lwupb", "swdnb", "swupb")
+
+
+def _network(model: SurrogateModel, d: dict, nx: int, ny: int, nk: int, out: dict, flags, energy_tol: float, X,
+             s) -> None:
+    """Features (tile layout) and the fused network with its decode and
+    energy gate for an (nx, nk, ny) domain: device fields d, device outputs
+    out, per-column flags; X holds at least ceil(nx ny / 128) feature tiles."""
+    lib = _capi.load()
+    ncol = nx * ny
+    fa = _feature_args(d, nk, ny, ncol)
+    fa.mean, fa.rstd = model.norm.in_mean.data_ptr(), model.norm.in_rstd.data_ptr()
+    fa.X, fa.ldx, fa.x_layout = X.data_ptr(), K_IN, 1
+    fa.lo, fa.hi, fa.flags = model.norm.in_lo.data_ptr(), model.norm.in_hi.data_ptr(), flags.data_ptr()
+    _check(lib.rrtmg_sur_features(ctypes.byref(fa), s), "features")
+    ma = _capi.SurMlpArgs(ncol=ncol, nk=nk, ny=ny, X=X.data_ptr(), W=model.weight_image().data_ptr(),
+                          out_mean=model.norm.out_mean.data_ptr(), out_std=model.norm.out_std.data_ptr(),
+                          coszr=d["coszr"].data_ptr(), pi3d=d["pi3d"].data_ptr(), p8w=d["p8w"].data_ptr(),
+                          energy_tol=energy_tol, flags=flags.data_ptr(),
+                          **{k: out[k].data_ptr() for k in OUTPUT_FIELDS})
+    for i in range(4):
+        ma.bias[i] = model.b[i].data_ptr()
+    _check(lib.rrtmg_sur_mlp(ctypes.byref(ma), s), "fused inference")
+
+
+_HOST_WS: dict = {}
+
+
+def _host_workspace(nx: int, nk: int, ny: int, rows: int) -> dict:
+    import torch
+    key = (torch.cuda.current_device(), nx, nk, ny, rows)
+    ws = _HOST_WS.get(key)
+    if ws is None:
+        dev = "cuda"
+        shapes = {k: (nx, nk + 1, ny) if k == "p8w" else ((nx, ny) if k in ("tsk", "albedo", "coszr", "emiss")
+                                                          else (nx, nk, ny)) for k in NETWORK_FIELDS}
+        ws = dict(d={k: torch.empty(v, device=dev) for k, v in shapes.items()},
+                  out={k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), device=dev)
+                       for k in OUTPUT_FIELDS},
+                  flags=torch.empty(nx * ny, device=dev, dtype=torch.int32),
+                  X=torch.zeros((rows * ny + 127) // 128 * 128, K_IN, device=dev, dtype=torch.bfloat16),
+                  h2d=torch.cuda.Stream(), d2h=torch.cuda.Stream())
+        _HOST_WS.clear()  # keep one domain shape resident
+        _HOST_WS[key] = ws
+    return ws
+
+
+def infer_host(model: SurrogateModel, st, host: dict, out: dict, *, energy_tol: float = 5.0, slabs: int = 8,
+               fallback: bool = True) -> int:
+    """Surrogate radiation with host inputs and outputs, pipelined over the
+    host link: `host` holds every input field of the domain as page-locked
+    CPU float32 tensors (st's shapes), `out` the six output fields
+    (rthratenlw, rthratensw, glw, lwupb, swdnb, swupb) as page-locked CPU
+    float32 tensors.  The network's fields go to the GPU in `slabs` slabs of
+    west-east rows on one copy stream, each slab's network runs as soon as it
+    has landed and its outputs return on a second copy stream; the fallback
+    then reads the other inputs of its columns from host memory in place and
+    writes its columns' outputs back to host memory in place.  Results are
+    those of infer() on device fields.  Returns the number of fallback columns;
+    the outputs are complete on return."""
+    import torch
+    if st.nk != NK:
+        raise ValueError(f"the surrogate is built for {NK} levels, got {st.nk}")
+    for name, t in list(host.items()) + list(out.items()):
+        if not (isinstance(t, torch.Tensor) and not t.is_cuda and t.is_pinned() and t.is_contiguous()
+                and t.dtype == torch.float32):
+            raise ValueError(f"{name} must be a contiguous page-locked CPU float32 tensor")
+    nx, ny, nk = st.nx, st.ny, st.nk
+    slabs = max(1, min(int(slabs), nx))
+    bounds = [(nx * q // slabs, nx * (q + 1) // slabs) for q in range(slabs)]
+    ws = _host_workspace(nx, nk, ny, max(i1 - i0 for i0, i1 in bounds))
+    main, h2d, d2h = torch.cuda.current_stream(), ws["h2d"], ws["d2h"]
+    dev, dout, flags = ws["d"], ws["out"], ws["flags"]
+    h2d.wait_stream(main)  # earlier work on these buffers is done
+    d2h.wait_stream(main)
+    landed = []
+    with torch.cuda.stream(h2d):
+        for i0, i1 in bounds:
+            for k in NETWORK_FIELDS:
+                dev[k][i0:i1].copy_(host[k][i0:i1], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(h2d)
+            landed.append(ev)
+    s = _stream()
+    for (i0, i1), ev in zip(bounds, landed):
+        main.wait_event(ev)
+        d_slab = {k: v[i0:i1] for k, v in dev.items()}
+        o_slab = {k: v[i0:i1] for k, v in dout.items()}
+        _network(model, d_slab, i1 - i0, ny, nk, o_slab, flags[i0 * ny:i1 * ny], energy_tol, ws["X"], s)
+        done = torch.cuda.Event()
+        done.record(main)
+        d2h.wait_event(done)
+        with torch.cuda.stream(d2h):
+            for k in OUTPUT_FIELDS:
+                out[k][i0:i1].copy_(dout[k][i0:i1], non_blocking=True)
+    n_fb = 0
+    if fallback:
+        returned = torch.cuda.Event()
+        returned.record(d2h)
+        src = {k: (dev[k] if k in dev else host[k]) for k in host}
+        n_fb = _fallback(st, src, flags, out, before_scatter=returned)
+    main.wait_stream(d2h)
+    main.synchronize()
+    return n_fb
+
+
 def fused_kernel_call(model: SurrogateModel, st, d: dict, *, energy_tol: float = 5.0):
     """Runs the features of a 50-level domain once and returns a callable that
     launches only the fused inference kernel on them (for timing and
@@ -583,11 +693,13 @@ def _fallback_plan(st, n: int) -> _FallbackPlan:
     return plan
 
 
-def _fallback(st, d: dict, flags, out: dict) -> int:
+def _fallback(st, d: dict, flags, out: dict, before_scatter=None) -> int:
     """Re-solve the flagged columns with the plain kernels, writing their
     surrogate outputs over; returns how many columns were re-solved.  The
     column count is read on the host (one synchronization); everything after
-    it reuses the buffers and argument blocks of a cached plan."""
+    it reuses the buffers and argument blocks of a cached plan.  d and out
+    may hold page-locked host tensors, which the gather reads and the scatter
+    writes in place; before_scatter: an event the scatter waits for."""
     import torch
     lib = _capi.load()
     s = _stream()
@@ -625,6 +737,8 @@ def _fallback(st, d: dict, flags, out: dict) -> int:
     done = torch.cuda.Event()
     done.record(side)
     main.wait_event(done)
+    if before_scatter is not None:
+        main.wait_event(before_scatter)
     for i, (k, _, _) in enumerate(plan.scatter_src):
         plan.scatter.dst[i] = out[k].data_ptr()
     _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), n, ny, ctypes.byref(plan.scatter), 0, n, 0, s),
