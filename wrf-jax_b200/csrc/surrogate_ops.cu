@@ -219,6 +219,96 @@ __global__ void __launch_bounds__(kRowThreads) features_rows_kernel(SurFeatureAr
   if (a.flags) a.flags[c] = oob;
 }
 
+// Features of a 50-level column with every index resolved at compile time:
+// word W (features 2W, 2W + 1) of the output row is one expansion of
+// RRTMG_FEAT_WORD(W), W = 0..255, so each load is a register pointer plus a
+// constant level offset, each statistics read a constant shared-memory slot,
+// and words leave four at a time as 16-byte chunks.  The compiler barrier
+// after each chunk keeps all 454 loads from being hoisted.  Values, rounding
+// and range flags are those of features_kernel.
+constexpr int kFeatNk = 50;
+
+// One output word; a macro (not a function) so the 256 expansions stay in one
+// straight-line body with every array index a constant.
+#define RRTMG_FEAT_WORD(W)                                                                        \
+  {                                                                                               \
+    constexpr int W_ = (W), f_ = 2 * W_, NK_ = kFeatNk;                                           \
+    if constexpr (f_ < 9 * NK_ + 4) {                                                             \
+      float r0, r1;                                                                               \
+      if constexpr (f_ < 8 * NK_) {                                                               \
+        constexpr int F_ = f_ / NK_, k_ = f_ % NK_;                                               \
+        r0 = __ldg(pf[F_] + k_ * nys);                                                            \
+        r1 = __ldg(pf[F_] + (k_ + 1) * nys);                                                      \
+        if constexpr (F_ == 1) {                                                                  \
+          r0 = logf(r0);                                                                          \
+          r1 = logf(r1);                                                                          \
+        }                                                                                         \
+      } else if constexpr (f_ < 9 * NK_) {                                                        \
+        constexpr int k_ = f_ - 8 * NK_;                                                          \
+        if constexpr (k_ == 0) {                                                                  \
+          _Pragma("unroll") for (int q_ = 0; q_ <= NK_; ++q_) pw[q_] = __ldg(p8 + q_ * nys);      \
+        }                                                                                         \
+        r0 = pw[k_] - pw[k_ + 1];                                                                 \
+        r1 = pw[k_ + 1] - pw[k_ + 2];                                                             \
+      } else {                                                                                    \
+        constexpr int q_ = f_ - 9 * NK_;                                                          \
+        r0 = __ldg(two[q_]);                                                                      \
+        r1 = __ldg(two[q_ + 1]);                                                                  \
+      }                                                                                           \
+      const float4 s0 = st[f_], s1 = st[f_ + 1];                                                  \
+      oob |= static_cast<unsigned>((r0 < s0.z) | (r0 > s0.w) | (r1 < s1.z) | (r1 > s1.w));        \
+      const __nv_bfloat162 h_ = __floats2bfloat162_rn((r0 - s0.x) * s0.y, (r1 - s1.x) * s1.y);    \
+      ring[W_ % 4] = *reinterpret_cast<const uint32_t *>(&h_);                                    \
+    } else {                                                                                      \
+      ring[W_ % 4] = 0u;                                                                          \
+    }                                                                                             \
+    if constexpr (W_ % 4 == 3) {                                                                  \
+      constexpr int q_ = W_ / 4;                                                                  \
+      const uint4 v_ = make_uint4(ring[0], ring[1], ring[2], ring[3]);                            \
+      if (kTiled)                                                                                 \
+        *reinterpret_cast<uint4 *>(xrow + (q_ >> 3) * 16384 + rr * 128 + (((q_ & 7) ^ (rr & 7)) << 4)) = v_; \
+      else                                                                                        \
+        *reinterpret_cast<uint4 *>(xrow + q_ * 16) = v_;                                          \
+      asm volatile("" ::: "memory");                                                              \
+    }                                                                                             \
+  }
+#define RRTMG_FEAT_W4(b) RRTMG_FEAT_WORD(b) RRTMG_FEAT_WORD((b) + 1) RRTMG_FEAT_WORD((b) + 2) RRTMG_FEAT_WORD((b) + 3)
+#define RRTMG_FEAT_W16(b) RRTMG_FEAT_W4(b) RRTMG_FEAT_W4((b) + 4) RRTMG_FEAT_W4((b) + 8) RRTMG_FEAT_W4((b) + 12)
+#define RRTMG_FEAT_W64(b) RRTMG_FEAT_W16(b) RRTMG_FEAT_W16((b) + 16) RRTMG_FEAT_W16((b) + 32) RRTMG_FEAT_W16((b) + 48)
+
+template <bool kTiled>
+__global__ void __launch_bounds__(kRowThreads) features_nk50_kernel(SurFeatureArgs a) {
+  constexpr int NK = kFeatNk, kNf = 9 * NK + 4;
+  __shared__ float4 st[kNf];
+  for (int f = threadIdx.x; f < kNf; f += blockDim.x)
+    st[f] = make_float4(a.mean[f], a.rstd[f], a.lo ? a.lo[f] : -__int_as_float(0x7f800000),
+                        a.hi ? a.hi[f] : __int_as_float(0x7f800000));
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncol) return;
+  const int ny = a.ny;
+  const size_t nys = static_cast<size_t>(ny);
+  const int i = c / ny, j = c - i * ny;
+  const size_t b3 = static_cast<size_t>(i) * NK * ny + j, bl = static_cast<size_t>(i) * (NK + 1) * ny + j;
+  const float *const pf[8] = {a.t3d + b3, a.p3d + b3, a.qv + b3, a.qc + b3, a.qi + b3, a.qs + b3, a.cldfra + b3,
+                              a.o3 + b3};
+  const float *const p8 = a.p8w + bl;
+  const float *const two[4] = {a.tsk + c, a.albedo + c, a.coszr + c, a.emiss + c};
+  const size_t row = static_cast<size_t>(a.row_offset) + c;
+  uint8_t *xrow = kTiled ? static_cast<uint8_t *>(a.X) + (row >> 7) * 131072u
+                         : static_cast<uint8_t *>(a.X) + row * a.ldx * 2;
+  const int rr = static_cast<int>(row & 127);
+  unsigned oob = 0;
+  uint32_t ring[4];
+  float pw[NK + 1];
+  RRTMG_FEAT_W64(0) RRTMG_FEAT_W64(64) RRTMG_FEAT_W64(128) RRTMG_FEAT_W64(192)
+  if (a.flags) a.flags[c] = oob;
+}
+#undef RRTMG_FEAT_W64
+#undef RRTMG_FEAT_W16
+#undef RRTMG_FEAT_W4
+#undef RRTMG_FEAT_WORD
+
 __global__ void targets_kernel(SurTargetArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.ncol) return;
@@ -515,6 +605,13 @@ cudaError_t launch_sur_features(const SurFeatureArgs &a, cudaStream_t s) {
   const bool rows_ok = a.X && !a.raw && !a.Xt && a.ldx % 8 == 0 && 9 * a.nk + 4 <= kMaxFeatures &&
                        (reinterpret_cast<uintptr_t>(a.X) & 15u) == 0;
   if (a.x_layout == 1 && !rows_ok) return cudaErrorInvalidValue;
+  if (rows_ok && a.nk == kFeatNk && a.ldx == 512) {
+    if (a.x_layout == 1)
+      features_nk50_kernel<true><<<row_blocks, kRowThreads, 0, s>>>(a);
+    else
+      features_nk50_kernel<false><<<row_blocks, kRowThreads, 0, s>>>(a);
+    return cudaGetLastError();
+  }
   if (a.x_layout == 1)
     features_rows_kernel<true><<<row_blocks, kRowThreads, 0, s>>>(a);
   else if (a.x_layout == 0 && rows_ok)
