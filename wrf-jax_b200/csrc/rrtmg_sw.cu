@@ -606,6 +606,242 @@ __device__ __forceinline__ void down_step(Path &P, int r) {
 // kTerms = true: store each level term (type, level, g-point) to `terms` with
 // stride tstride between (type, level, g-point) planes, for the ordered sums
 // of the finish kernel.
+// One g-point of a band: top-down delta-Eddington layers, direct beam and
+// downward adding, then bottom-up adding, level fluxes and their sums (accs)
+// or terms.  o supplies the layer optics of the g-point: tg/tr gas and
+// Rayleigh depths, ct/cs/ca/co the band's cloud optics.
+template <bool kTerms, class Opt>
+__device__ __forceinline__ void sw_gpoint(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
+                                          int clear_only, float *accs, Path &Pc, Path &Pt, float *terms,
+                                          size_t tstride, int G, float sflux_g, const Opt &o) {
+  const int n = C.nlay;
+  const float mu = C.mu;
+  const float repclc = 1.0e-12f;
+  // top-down: layer optics, direct beam, downward adding
+  Pc.tdbt[0] = 1.0f;
+  Pt.tdbt[0] = 1.0f;
+  float tdbtc_nd = 1.0f, tdbt_nd = 1.0f;
+  const float zincflx = ((C.adjflux * sflux_g) * mu) * 1.0f;
+  auto term = [&](int type, int level) -> float & {
+    return terms[((static_cast<size_t>(type) * (n + 1) + level) * kSwGpts + G) * tstride];
+  };
+  float *accfdir = kTerms ? nullptr : accs + 4 * kMaxLev, *acccdir = kTerms ? nullptr : accs + 5 * kMaxLev;
+  if constexpr (kTerms) {
+    term(4, 0) = tdbt_nd * zincflx;
+    term(5, 0) = tdbtc_nd * zincflx;
+  } else {
+    accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
+    acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
+  }
+  // thread-local table values of the next layer are loaded one layer ahead
+  float nx_tr = o.tr(n - 1), nx_tg = o.tg(n - 1);
+  float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
+  if (!clear_only) { nx_ct = o.ct(n - 1); nx_cs = o.cs(n - 1); nx_ca = o.ca(n - 1); nx_co = o.co(n - 1); }
+  uint32_t nx_word = maskbase[(static_cast<size_t>(n - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
+  for (int r = 0; r < n; ++r) {
+    const int l = n - 1 - r;
+    const uint32_t word = nx_word;
+    const float tr = nx_tr, tg = nx_tg;
+    const float ct = nx_ct, cs = nx_cs, ca = nx_ca, co = nx_co;
+    if (l > 0) {
+      nx_tr = o.tr(l - 1);
+      nx_tg = o.tg(l - 1);
+      if (!clear_only) { nx_ct = o.ct(l - 1); nx_cs = o.cs(l - 1); nx_ca = o.ca(l - 1); nx_co = o.co(l - 1); }
+      nx_word = maskbase[(static_cast<size_t>(l - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
+    }
+    const bool cldb = (word >> (G & 31)) & 1u;
+    const float cloud = cldb ? 1.0f : 0.0f;
+    const float clear = 1.0f - cloud;
+    const float ztau = (tr + tg) + 0.0f;
+    float zom = tr + 0.0f * 1.0f;
+    const float zgr = 0.0f * 1.0f * 0.0f / zom;
+    zom = zom / ztau;
+    const float dbtc_nd = exp_lookup(T, ztau / mu);
+    tdbtc_nd = tdbtc_nd * dbtc_nd;
+    const float zf = zgr * zgr;
+    const float zwf = zom * zf;
+    const float ztauc = (1.0f - zwf) * ztau;
+    const float zomcc = (zom - zwf) / (1.0f - zwf);
+    const float zgcc = (zgr - zf) / (1.0f - zf);
+    const RT4 c = reftra(T, true, zgcc, mu, ztauc, zomcc);
+    Pc.ref[r] = c.ref; Pc.refd[r] = c.refd; Pc.tra[r] = c.tra; Pc.trad[r] = c.trad;
+    const float dbtc = exp_lookup(T, ztauc / mu);
+    Pc.dbt[r] = dbtc;
+    Pc.tdbt[r + 1] = Pc.tdbt[r] * dbtc;
+    down_step(Pc, r);
+    if (!clear_only) {
+      const float tcld = cldb ? ct : 0.0f;
+      const float wcld = cldb ? cs : 1.0f;
+      const float gcld = cldb ? ca : 0.0f;
+      const float taor = cldb ? co : 0.0f;
+      const float tauorig = ztau + taor;
+      const float dbtmo_nd = exp_lookup(T, tauorig / mu);
+      const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
+      tdbt_nd = tdbt_nd * dbt_nd;
+      const float ztauo = ztauc + tcld;
+      float zomco = ztauc * zomcc + tcld * wcld;
+      const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
+      zomco = zomco / ztauo;
+      const RT4 o = reftra(T, cloud > repclc, zgco, mu, ztauo, zomco);
+      Pt.ref[r] = clear * c.ref + cloud * o.ref;
+      Pt.refd[r] = clear * c.refd + cloud * o.refd;
+      Pt.tra[r] = clear * c.tra + cloud * o.tra;
+      Pt.trad[r] = clear * c.trad + cloud * o.trad;
+      const float dbtmo = exp_lookup(T, ztauo / mu);
+      const float dbt = clear * dbtc + cloud * dbtmo;
+      Pt.dbt[r] = dbt;
+      Pt.tdbt[r + 1] = Pt.tdbt[r] * dbt;
+      down_step(Pt, r);
+    } else {
+      tdbt_nd = tdbtc_nd;
+    }
+    if constexpr (kTerms) {
+      term(4, r + 1) = tdbt_nd * zincflx;
+      term(5, r + 1) = tdbtc_nd * zincflx;
+    } else {
+      accfdir[r + 1] = accfdir[r + 1] + tdbt_nd * zincflx;
+      acccdir[r + 1] = acccdir[r + 1] + tdbtc_nd * zincflx;
+    }
+  }
+  // surface boundary
+  Pc.ref[n] = C.albedo; Pc.refd[n] = C.albedo; Pc.tra[n] = 0.0f; Pc.trad[n] = 0.0f; Pc.dbt[n] = 0.0f;
+  Pt.ref[n] = C.albedo; Pt.refd[n] = C.albedo; Pt.tra[n] = 0.0f; Pt.trad[n] = 0.0f; Pt.dbt[n] = 0.0f;
+  // bottom-up: upward adding and level fluxes (vrtqdr, sw:3655-3720)
+  float *accfu = accs, *accfd = kTerms ? nullptr : accs + kMaxLev;
+  float *acccu = kTerms ? nullptr : accs + 2 * kMaxLev, *acccd = kTerms ? nullptr : accs + 3 * kMaxLev;
+  float rupc = Pc.ref[n], rupdc = Pc.refd[n];
+  float rupt = Pt.ref[n], rupdt = Pt.refd[n];
+  // level arrays and accumulators of the next level are loaded one level ahead
+  struct Lvl {
+    float ref, refd, tra, trad, dbt, tdbt, tdn, rdnd;
+  };
+  auto load_lvl = [&](const Path &P, int k) {
+    Lvl v;
+    v.ref = P.ref[k]; v.refd = P.refd[k]; v.tra = P.tra[k]; v.trad = P.trad[k]; v.dbt = P.dbt[k];
+    v.tdbt = P.tdbt[k]; v.tdn = P.tdn[k]; v.rdnd = P.rdnd[k];
+    return v;
+  };
+  Lvl nc = load_lvl(Pc, n), nt = nc;
+  if (!clear_only) nt = load_lvl(Pt, n);
+  float nfu = 0.0f, nfd = 0.0f, ncu = 0.0f, ncd = 0.0f;
+  if constexpr (!kTerms) { nfu = accfu[n]; nfd = accfd[n]; ncu = acccu[n]; ncd = acccd[n]; }
+  for (int k = n; k >= 0; --k) {
+    const Lvl c = nc, t = nt;
+    const float afu = nfu, afd = nfd, acu = ncu, acd = ncd;
+    if (k > 0) {
+      nc = load_lvl(Pc, k - 1);
+      if (!clear_only) nt = load_lvl(Pt, k - 1);
+      if constexpr (!kTerms) { nfu = accfu[k - 1]; nfd = accfd[k - 1]; ncu = acccu[k - 1]; ncd = acccd[k - 1]; }
+    }
+    if (k < n) {
+      const float zrc = 1.0f / (1.0f - rupdc * c.refd);
+      const float nrupc = c.ref + c.trad * ((c.tra - c.dbt) * rupdc + c.dbt * rupc) * zrc;
+      const float nrupdc = c.refd + c.trad * c.trad * rupdc * zrc;
+      rupc = nrupc;
+      rupdc = nrupdc;
+      if (!clear_only) {
+        const float zrt = 1.0f / (1.0f - rupdt * t.refd);
+        const float nrupt = t.ref + t.trad * ((t.tra - t.dbt) * rupdt + t.dbt * rupt) * zrt;
+        const float nrupdt = t.refd + t.trad * t.trad * rupdt * zrt;
+        rupt = nrupt;
+        rupdt = nrupdt;
+      }
+    }
+    // clear-sky level fluxes
+    const float zrefc = 1.0f / (1.0f - c.rdnd * rupdc);
+    const float fuc = (c.tdbt * rupc + (c.tdn - c.tdbt) * rupdc) * zrefc;
+    const float fdc = c.tdbt + (c.tdn - c.tdbt + c.tdbt * rupc * c.rdnd) * zrefc;
+    float fut = fuc, fdt = fdc;
+    if (!clear_only) {
+      const float zreft = 1.0f / (1.0f - t.rdnd * rupdt);
+      fut = (t.tdbt * rupt + (t.tdn - t.tdbt) * rupdt) * zreft;
+      fdt = t.tdbt + (t.tdn - t.tdbt + t.tdbt * rupt * t.rdnd) * zreft;
+    }
+    if constexpr (kTerms) {
+      term(0, k) = fut * zincflx;
+      term(1, k) = fdt * zincflx;
+      term(2, k) = fuc * zincflx;
+      term(3, k) = fdc * zincflx;
+    } else {
+      accfu[k] = afu + fut * zincflx;
+      accfd[k] = afd + fdt * zincflx;
+      acccu[k] = acu + fuc * zincflx;
+      acccd[k] = acd + fdc * zincflx;
+    }
+  }
+}
+
+// Layer optics of one g-point from the thread-local band tables of sw_band.
+struct LocalOptics {
+  const float (*taug)[kMaxNgc];
+  const float (*taur)[kMaxNgc];
+  const float *ctau, *cssa, *casm, *ctaor;
+  int g;
+  __device__ float tg(int l) const { return taug[l][g]; }
+  __device__ float tr(int l) const { return taur[l][g]; }
+  __device__ float ct(int l) const { return ctau[l]; }
+  __device__ float cs(int l) const { return cssa[l]; }
+  __device__ float ca(int l) const { return casm[l]; }
+  __device__ float co(int l) const { return ctaor[l]; }
+};
+
+// Solar source of band B (the per-band rules of sw:4430-4450): the source
+// layer from the layers' jp (jp(l)), the spectral interpolation (js0, fs) of
+// the layer (spec(ls, js0, fs), asked only when the band uses it), and the
+// source of each g-point.
+template <int B, class JpFn, class SpecFn>
+__device__ __forceinline__ void sw_source(const Tables &T, const Col &C, JpFn jp, SpecFn spec, float *sflux) {
+  constexpr int ngc = kNgc[B];
+  constexpr int bn = B + 16;
+  const int n = C.nlay;
+  const SwBand &K = T.sw[B];
+  const int layreffr = K.layreffr;
+  int ls = -1;
+  bool found = false;
+  if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
+    // first troposphere crossing of layreffr, one layer up, capped at laytrop-1
+    for (int l = 0; l < n && !found; ++l) {
+      const int jl = jp(l);
+      const int next = l + 1 < n ? jp(l + 1) : jl;
+      if (l < C.laytrop && jl < layreffr && next >= layreffr) {
+        found = true;
+        ls = (l + 1 < C.laytrop - 1) ? l + 1 : C.laytrop - 1;
+      }
+    }
+    if (!found) ls = C.laytrop - 1;
+  }
+  if constexpr (bn == 17 || bn == 28) {
+    for (int l = 1; l < n && !found; ++l) {
+      if (l >= C.laytrop && jp(l - 1) < layreffr && jp(l) >= layreffr) {
+        found = true;
+        ls = l;
+      }
+    }
+    if (!found) ls = n - 1;
+  }
+  bool have = false;
+  if constexpr (bn == 17 || bn == 28) have = C.laytrop < n;
+  if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) have = C.laytrop > 0;
+  float src_fs = 0.0f;
+  int src_js0 = 0;
+  if (have && ls >= 0) spec(ls, src_js0, src_fs);
+#pragma unroll
+  for (int g = 0; g < ngc; ++g) {
+    float sz = 0.0f;
+    if constexpr (bn == 16 || bn == 29) sz = C.laytrop < n ? ld(K.sfluxref + g) : 0.0f;
+    if constexpr (bn == 20 || bn == 23 || bn == 25 || bn == 26) sz = C.laytrop > 0 ? ld(K.sfluxref + g) : 0.0f;
+    if constexpr (bn == 27) sz = C.laytrop < n ? K.scalekur * ld(K.sfluxref + g) : 0.0f;
+    if constexpr (bn == 17 || bn == 28 || bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
+      if (have) {
+        const int c = K.sflux_cols;
+        const float s0 = ld(K.sfluxref + g * c + src_js0), s1 = ld(K.sfluxref + g * c + src_js0 + 1);
+        sz = s0 + src_fs * (s1 - s0);
+      }
+    }
+    sflux[g] = sz;
+  }
+}
+
 // g_only >= 0: only that g-point of the band (the g-point split schedule).
 template <int B, bool kTerms = false>
 __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
@@ -621,12 +857,7 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
   // band's cloud optics for cloudy g-points.
   float taug[kMaxLay][kMaxNgc], taur[kMaxLay][kMaxNgc];
   float ctau[kMaxLay], cssa[kMaxLay], casm[kMaxLay], ctaor[kMaxLay];
-  float src_fs = 0.0f;
-  int src_js0 = 0;
-  // solar-source layer (sw:4430-4450 style rules per band)
-  int ls = -1;
-  const int layreffr = K.layreffr;
-  bool found = false;
+  int jpl[kMaxLay];
   for (int l = 0; l < n; ++l) {
     const SLayer L = make_layer(T, a, C, l);
     SwSpec sp8, sp4;
@@ -641,218 +872,27 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
       const CloudOpt o = sw_cloud(T, L, B, C.iceflg);
       ctau[l] = o.tau; cssa[l] = o.ssa; casm[l] = o.asm_; ctaor[l] = o.taor;
     }
-    // solar source function layer
-    if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
-      // first troposphere crossing of layreffr, one layer up, capped at laytrop-1
-      if (!found) {
-        const int next = l + 1 < n ? make_layer(T, a, C, l + 1).jp : L.jp;
-        if (l < C.laytrop && L.jp < layreffr && next >= layreffr) {
-          found = true;
-          ls = (l + 1 < C.laytrop - 1) ? l + 1 : C.laytrop - 1;
-        }
-      }
-    }
-    if constexpr (bn == 17 || bn == 28) {
-      if (!found && l > 0 && l >= C.laytrop) {
-        const int prev = make_layer(T, a, C, l - 1).jp;
-        if (prev < layreffr && L.jp >= layreffr) { found = true; ls = l; }
-      }
-    }
+    jpl[l] = L.jp;
   }
   float sflux[ngc];
-  {
-    if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
-      if (!found) ls = C.laytrop - 1;
-    }
-    if constexpr (bn == 17 || bn == 28) {
-      if (!found) ls = n - 1;
-    }
-    bool have = false;
-    if constexpr (bn == 17 || bn == 28) have = C.laytrop < n;
-    if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) have = C.laytrop > 0;
-    if (have && ls >= 0) {
-      const SLayer L = make_layer(T, a, C, ls);
-      SwSpec sp8, sp4;
-      sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
-      sp4 = sp8;
-      float tg[ngc], tr[ngc];
-      sw_taumol<B>(T, L, tg, tr, sp8, sp4);
-      if constexpr (bn == 17 || bn == 28) { src_js0 = sp4.js0; src_fs = sp4.fs; }
-      else { src_js0 = sp8.js0; src_fs = sp8.fs; }
-    }
-#pragma unroll
-    for (int g = 0; g < ngc; ++g) {
-      float sz = 0.0f;
-      if constexpr (bn == 16 || bn == 29) sz = C.laytrop < n ? ld(K.sfluxref + g) : 0.0f;
-      if constexpr (bn == 20 || bn == 23 || bn == 25 || bn == 26) sz = C.laytrop > 0 ? ld(K.sfluxref + g) : 0.0f;
-      if constexpr (bn == 27) sz = C.laytrop < n ? K.scalekur * ld(K.sfluxref + g) : 0.0f;
-      if constexpr (bn == 17 || bn == 28 || bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
-        if (have) {
-          const int c = K.sflux_cols;
-          const float s0 = ld(K.sfluxref + g * c + src_js0), s1 = ld(K.sfluxref + g * c + src_js0 + 1);
-          sz = s0 + src_fs * (s1 - s0);
-        }
-      }
-      sflux[g] = sz;
-    }
-  }
-  const float mu = C.mu;
-  const float repclc = 1.0e-12f;
+  sw_source<B>(
+      T, C, [&](int l) { return jpl[l]; },
+      [&](int ls, int &js0, float &fs) {
+        const SLayer L = make_layer(T, a, C, ls);
+        SwSpec sp8, sp4;
+        sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
+        sp4 = sp8;
+        float tg[ngc], tr[ngc];
+        sw_taumol<B>(T, L, tg, tr, sp8, sp4);
+        const SwSpec &sp = (bn == 17 || bn == 28) ? sp4 : sp8;
+        js0 = sp.js0;
+        fs = sp.fs;
+      },
+      sflux);
   for (int g = 0; g < ngc; ++g) {
     if (g_only >= 0 && g != g_only) continue;
-    const int G = gofs + g;
-    // top-down: layer optics, direct beam, downward adding
-    Pc.tdbt[0] = 1.0f;
-    Pt.tdbt[0] = 1.0f;
-    float tdbtc_nd = 1.0f, tdbt_nd = 1.0f;
-    const float zincflx = ((C.adjflux * sflux[g]) * mu) * 1.0f;
-    auto term = [&](int type, int level) -> float & {
-      return terms[((static_cast<size_t>(type) * (n + 1) + level) * kSwGpts + G) * tstride];
-    };
-    float *accfdir = kTerms ? nullptr : accs + 4 * kMaxLev, *acccdir = kTerms ? nullptr : accs + 5 * kMaxLev;
-    if constexpr (kTerms) {
-      term(4, 0) = tdbt_nd * zincflx;
-      term(5, 0) = tdbtc_nd * zincflx;
-    } else {
-      accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
-      acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
-    }
-    // thread-local table values of the next layer are loaded one layer ahead
-    float nx_tr = taur[n - 1][g], nx_tg = taug[n - 1][g];
-    float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
-    if (!clear_only) { nx_ct = ctau[n - 1]; nx_cs = cssa[n - 1]; nx_ca = casm[n - 1]; nx_co = ctaor[n - 1]; }
-    uint32_t nx_word = maskbase[(static_cast<size_t>(n - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
-    for (int r = 0; r < n; ++r) {
-      const int l = n - 1 - r;
-      const uint32_t word = nx_word;
-      const float tr = nx_tr, tg = nx_tg;
-      const float ct = nx_ct, cs = nx_cs, ca = nx_ca, co = nx_co;
-      if (l > 0) {
-        nx_tr = taur[l - 1][g];
-        nx_tg = taug[l - 1][g];
-        if (!clear_only) { nx_ct = ctau[l - 1]; nx_cs = cssa[l - 1]; nx_ca = casm[l - 1]; nx_co = ctaor[l - 1]; }
-        nx_word = maskbase[(static_cast<size_t>(l - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
-      }
-      const bool cldb = (word >> (G & 31)) & 1u;
-      const float cloud = cldb ? 1.0f : 0.0f;
-      const float clear = 1.0f - cloud;
-      const float ztau = (tr + tg) + 0.0f;
-      float zom = tr + 0.0f * 1.0f;
-      const float zgr = 0.0f * 1.0f * 0.0f / zom;
-      zom = zom / ztau;
-      const float dbtc_nd = exp_lookup(T, ztau / mu);
-      tdbtc_nd = tdbtc_nd * dbtc_nd;
-      const float zf = zgr * zgr;
-      const float zwf = zom * zf;
-      const float ztauc = (1.0f - zwf) * ztau;
-      const float zomcc = (zom - zwf) / (1.0f - zwf);
-      const float zgcc = (zgr - zf) / (1.0f - zf);
-      const RT4 c = reftra(T, true, zgcc, mu, ztauc, zomcc);
-      Pc.ref[r] = c.ref; Pc.refd[r] = c.refd; Pc.tra[r] = c.tra; Pc.trad[r] = c.trad;
-      const float dbtc = exp_lookup(T, ztauc / mu);
-      Pc.dbt[r] = dbtc;
-      Pc.tdbt[r + 1] = Pc.tdbt[r] * dbtc;
-      down_step(Pc, r);
-      if (!clear_only) {
-        const float tcld = cldb ? ct : 0.0f;
-        const float wcld = cldb ? cs : 1.0f;
-        const float gcld = cldb ? ca : 0.0f;
-        const float taor = cldb ? co : 0.0f;
-        const float tauorig = ztau + taor;
-        const float dbtmo_nd = exp_lookup(T, tauorig / mu);
-        const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
-        tdbt_nd = tdbt_nd * dbt_nd;
-        const float ztauo = ztauc + tcld;
-        float zomco = ztauc * zomcc + tcld * wcld;
-        const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
-        zomco = zomco / ztauo;
-        const RT4 o = reftra(T, cloud > repclc, zgco, mu, ztauo, zomco);
-        Pt.ref[r] = clear * c.ref + cloud * o.ref;
-        Pt.refd[r] = clear * c.refd + cloud * o.refd;
-        Pt.tra[r] = clear * c.tra + cloud * o.tra;
-        Pt.trad[r] = clear * c.trad + cloud * o.trad;
-        const float dbtmo = exp_lookup(T, ztauo / mu);
-        const float dbt = clear * dbtc + cloud * dbtmo;
-        Pt.dbt[r] = dbt;
-        Pt.tdbt[r + 1] = Pt.tdbt[r] * dbt;
-        down_step(Pt, r);
-      } else {
-        tdbt_nd = tdbtc_nd;
-      }
-      if constexpr (kTerms) {
-        term(4, r + 1) = tdbt_nd * zincflx;
-        term(5, r + 1) = tdbtc_nd * zincflx;
-      } else {
-        accfdir[r + 1] = accfdir[r + 1] + tdbt_nd * zincflx;
-        acccdir[r + 1] = acccdir[r + 1] + tdbtc_nd * zincflx;
-      }
-    }
-    // surface boundary
-    Pc.ref[n] = C.albedo; Pc.refd[n] = C.albedo; Pc.tra[n] = 0.0f; Pc.trad[n] = 0.0f; Pc.dbt[n] = 0.0f;
-    Pt.ref[n] = C.albedo; Pt.refd[n] = C.albedo; Pt.tra[n] = 0.0f; Pt.trad[n] = 0.0f; Pt.dbt[n] = 0.0f;
-    // bottom-up: upward adding and level fluxes (vrtqdr, sw:3655-3720)
-    float *accfu = accs, *accfd = kTerms ? nullptr : accs + kMaxLev;
-    float *acccu = kTerms ? nullptr : accs + 2 * kMaxLev, *acccd = kTerms ? nullptr : accs + 3 * kMaxLev;
-    float rupc = Pc.ref[n], rupdc = Pc.refd[n];
-    float rupt = Pt.ref[n], rupdt = Pt.refd[n];
-    // level arrays and accumulators of the next level are loaded one level ahead
-    struct Lvl {
-      float ref, refd, tra, trad, dbt, tdbt, tdn, rdnd;
-    };
-    auto load_lvl = [&](const Path &P, int k) {
-      Lvl v;
-      v.ref = P.ref[k]; v.refd = P.refd[k]; v.tra = P.tra[k]; v.trad = P.trad[k]; v.dbt = P.dbt[k];
-      v.tdbt = P.tdbt[k]; v.tdn = P.tdn[k]; v.rdnd = P.rdnd[k];
-      return v;
-    };
-    Lvl nc = load_lvl(Pc, n), nt = nc;
-    if (!clear_only) nt = load_lvl(Pt, n);
-    float nfu = 0.0f, nfd = 0.0f, ncu = 0.0f, ncd = 0.0f;
-    if constexpr (!kTerms) { nfu = accfu[n]; nfd = accfd[n]; ncu = acccu[n]; ncd = acccd[n]; }
-    for (int k = n; k >= 0; --k) {
-      const Lvl c = nc, t = nt;
-      const float afu = nfu, afd = nfd, acu = ncu, acd = ncd;
-      if (k > 0) {
-        nc = load_lvl(Pc, k - 1);
-        if (!clear_only) nt = load_lvl(Pt, k - 1);
-        if constexpr (!kTerms) { nfu = accfu[k - 1]; nfd = accfd[k - 1]; ncu = acccu[k - 1]; ncd = acccd[k - 1]; }
-      }
-      if (k < n) {
-        const float zrc = 1.0f / (1.0f - rupdc * c.refd);
-        const float nrupc = c.ref + c.trad * ((c.tra - c.dbt) * rupdc + c.dbt * rupc) * zrc;
-        const float nrupdc = c.refd + c.trad * c.trad * rupdc * zrc;
-        rupc = nrupc;
-        rupdc = nrupdc;
-        if (!clear_only) {
-          const float zrt = 1.0f / (1.0f - rupdt * t.refd);
-          const float nrupt = t.ref + t.trad * ((t.tra - t.dbt) * rupdt + t.dbt * rupt) * zrt;
-          const float nrupdt = t.refd + t.trad * t.trad * rupdt * zrt;
-          rupt = nrupt;
-          rupdt = nrupdt;
-        }
-      }
-      // clear-sky level fluxes
-      const float zrefc = 1.0f / (1.0f - c.rdnd * rupdc);
-      const float fuc = (c.tdbt * rupc + (c.tdn - c.tdbt) * rupdc) * zrefc;
-      const float fdc = c.tdbt + (c.tdn - c.tdbt + c.tdbt * rupc * c.rdnd) * zrefc;
-      float fut = fuc, fdt = fdc;
-      if (!clear_only) {
-        const float zreft = 1.0f / (1.0f - t.rdnd * rupdt);
-        fut = (t.tdbt * rupt + (t.tdn - t.tdbt) * rupdt) * zreft;
-        fdt = t.tdbt + (t.tdn - t.tdbt + t.tdbt * rupt * t.rdnd) * zreft;
-      }
-      if constexpr (kTerms) {
-        term(0, k) = fut * zincflx;
-        term(1, k) = fdt * zincflx;
-        term(2, k) = fuc * zincflx;
-        term(3, k) = fdc * zincflx;
-      } else {
-        accfu[k] = afu + fut * zincflx;
-        accfd[k] = afd + fdt * zincflx;
-        acccu[k] = acu + fuc * zincflx;
-        acccd[k] = acd + fdc * zincflx;
-      }
-    }
+    const LocalOptics o{taug, taur, ctau, cssa, casm, ctaor, g};
+    sw_gpoint<kTerms>(T, a, C, maskbase, clear_only, accs, Pc, Pt, terms, tstride, gofs + g, sflux[g], o);
   }
 }
 
@@ -995,30 +1035,156 @@ __global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, 
   sw_outputs(a, C, col, accs);
 }
 
-// g-point split schedule for small domains: thread (day column, g-point G =
-// blockIdx.y) runs one g-point of its band and stores its level terms, so a
-// column's latency drops to one g-point.  The terms (type, level, g-point) are
-// summed by sw_gsum_kernel and finished by sw_split_finish_kernel.
+// g-point split schedule for small domains, from layer records:
+//   sw_colprep_kernel  thread = day slot: the column set-up once;
+//   sw_optics_kernel   thread = (day slot, layer, band): the band's gas and
+//                      Rayleigh depths of every g-point, its cloud optics, the
+//                      spectral interpolation its solar source uses, and jp;
+//   sw_source_kernel   thread = (day slot, band): the band's solar source;
+//   sw_gsplit_kernel   thread = (day slot, g-point): one g-point's sweeps.
+// The operations are those of sw_band, so the level terms (type, level,
+// g-point) are bit-identical; sw_gsum_kernel and sw_split_finish_kernel sum
+// and finish them.  Scratch after the terms: column records, then layer
+// records of kSwRec floats.
+constexpr int kSwRec = 312;  // taug[112], taur[112], cloud[14][4], spec[14][2], jp, padding
+constexpr int kSwRecTaur = kSwGpts, kSwRecCloud = 2 * kSwGpts, kSwRecSpec = kSwRecCloud + 4 * kSwBands,
+              kSwRecJp = kSwRecSpec + 2 * kSwBands;
+static_assert(kSwRecJp < kSwRec, "record layout");
+
+struct SwColRec {
+  Col C;
+  float sflux[kSwGpts];
+};
+constexpr size_t kSwColRecFloats = (sizeof(SwColRec) + 15) / 16 * 4;
+
+__host__ __device__ __forceinline__ size_t sw_terms_only_floats(int nk, int ncol) {
+  return static_cast<size_t>(6) * (nk + 2) * kSwGpts * static_cast<size_t>(ncol);
+}
+__device__ __forceinline__ SwColRec *sw_colrecs(const SwArgs &a) {
+  return reinterpret_cast<SwColRec *>(a.split_terms + sw_terms_only_floats(a.nk, a.ncol));
+}
+__device__ __forceinline__ float *sw_layrecs(const SwArgs &a) {
+  return a.split_terms + sw_terms_only_floats(a.nk, a.ncol) + kSwColRecFloats * static_cast<size_t>(a.ncol);
+}
+
+__constant__ int kSwGofsDev[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
+
+__global__ void __launch_bounds__(128) sw_colprep_kernel(Tables T, SwArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.ncol || t >= *a.nday) return;
+  Col C;
+  sw_setup(T, a, a.daylist[t], C);
+  sw_colrecs(a)[t].C = C;
+}
+
+template <int B>
+__device__ __forceinline__ void sw_layer_optics(const Tables &T, const SwArgs &a, const Col &C, int l, int clear_only,
+                                                float *rec) {
+  constexpr int ngc = kNgc[B], gofs = kGofs[B], bn = B + 16;
+  const SLayer L = make_layer(T, a, C, l);
+  SwSpec sp8, sp4;
+  sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
+  sp4 = sp8;
+  float tg[ngc], tr[ngc];
+  sw_taumol<B>(T, L, tg, tr, sp8, sp4);
+#pragma unroll
+  for (int g = 0; g < ngc; ++g) {
+    rec[gofs + g] = tg[g];
+    rec[kSwRecTaur + gofs + g] = tr[g];
+  }
+  if (!clear_only) {
+    const CloudOpt o = sw_cloud(T, L, B, C.iceflg);
+    float *cq = rec + kSwRecCloud + 4 * B;
+    cq[0] = o.tau; cq[1] = o.ssa; cq[2] = o.asm_; cq[3] = o.taor;
+  }
+  const SwSpec &sp = (bn == 17 || bn == 28) ? sp4 : sp8;
+  rec[kSwRecSpec + 2 * B] = __int_as_float(sp.js0);
+  rec[kSwRecSpec + 2 * B + 1] = sp.fs;
+  if (B == 0) rec[kSwRecJp] = __int_as_float(L.jp);
+}
+
+#define RRTMG_SW_BAND_SWITCH(band, CALL) \
+  switch (band) {                        \
+    case 0: CALL(0); break;              \
+    case 1: CALL(1); break;              \
+    case 2: CALL(2); break;              \
+    case 3: CALL(3); break;              \
+    case 4: CALL(4); break;              \
+    case 5: CALL(5); break;              \
+    case 6: CALL(6); break;              \
+    case 7: CALL(7); break;              \
+    case 8: CALL(8); break;              \
+    case 9: CALL(9); break;              \
+    case 10: CALL(10); break;            \
+    case 11: CALL(11); break;            \
+    case 12: CALL(12); break;            \
+    default: CALL(13); break;            \
+  }
+
+// grid.y = band: every block runs one band's code
+__global__ void __launch_bounds__(128) sw_optics_kernel(Tables T, SwArgs a) {
+  const int n = a.nk + 1;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = idx / n, l = idx - t * n;
+  if (t >= a.ncol || t >= *a.nday) return;
+  const Col &C = sw_colrecs(a)[t].C;
+  float *rec = sw_layrecs(a) + static_cast<size_t>(idx) * kSwRec;
+  const int clear_only = a.icld == 0;
+#define RRTMG_SW_OPT(B) sw_layer_optics<B>(T, a, C, l, clear_only, rec)
+  RRTMG_SW_BAND_SWITCH(blockIdx.y, RRTMG_SW_OPT)
+#undef RRTMG_SW_OPT
+}
+
+__global__ void __launch_bounds__(128) sw_source_kernel(Tables T, SwArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.ncol || t >= *a.nday) return;
+  const int n = a.nk + 1;
+  SwColRec &R = sw_colrecs(a)[t];
+  const float *recs = sw_layrecs(a) + static_cast<size_t>(t) * n * kSwRec;
+  const int band = blockIdx.y;
+  auto jp = [&](int l) { return __float_as_int(recs[static_cast<size_t>(l) * kSwRec + kSwRecJp]); };
+  auto spec = [&](int ls, int &js0, float &fs) {
+    const float *q = recs + static_cast<size_t>(ls) * kSwRec + kSwRecSpec + 2 * band;
+    js0 = __float_as_int(q[0]);
+    fs = q[1];
+  };
+#define RRTMG_SW_SRC(B)                                 \
+  {                                                     \
+    constexpr int gofs_ = kGofs[B];                     \
+    sw_source<B>(T, R.C, jp, spec, R.sflux + gofs_);    \
+  }
+  RRTMG_SW_BAND_SWITCH(band, RRTMG_SW_SRC)
+#undef RRTMG_SW_SRC
+}
+#undef RRTMG_SW_BAND_SWITCH
+
+// Layer optics of one g-point from the layer records of its column.
+struct RecordOptics {
+  const float *recs;
+  int G, cloud;  // cloud = record offset of the band's cloud optics
+  __device__ float tg(int l) const { return recs[static_cast<size_t>(l) * kSwRec + G]; }
+  __device__ float tr(int l) const { return recs[static_cast<size_t>(l) * kSwRec + kSwRecTaur + G]; }
+  __device__ float ct(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud]; }
+  __device__ float cs(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud + 1]; }
+  __device__ float ca(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud + 2]; }
+  __device__ float co(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud + 3]; }
+};
+
+// grid.y = g-point
 __global__ void __launch_bounds__(128) sw_gsplit_kernel(Tables T, SwArgs a, int first, int count) {
   const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= first + count || t >= *a.nday) return;
   const int col = a.daylist[t];
-  Col C;
-  sw_setup(T, a, col, C);
-  const int clear_only = a.icld == 0;
-  Path Pc, Pt;
-  const uint32_t *maskbase = a.mask + col;
-  float *terms = a.split_terms + (t - first);
-  const size_t ts = static_cast<size_t>(count);
+  const int n = a.nk + 1;
+  const SwColRec &R = sw_colrecs(a)[t];
+  const Col C = R.C;
   const int G = blockIdx.y;
-#define RRTMG_SW_G(B)                                                                                       \
-  {                                                                                                         \
-    constexpr int lo_ = kGofs[B], n_ = kNgc[B];                                                             \
-    if (G >= lo_ && G < lo_ + n_) sw_band<B, true>(T, a, C, maskbase, clear_only, nullptr, Pc, Pt, terms, ts, G - lo_); \
-  }
-  RRTMG_SW_G(0) RRTMG_SW_G(1) RRTMG_SW_G(2) RRTMG_SW_G(3) RRTMG_SW_G(4) RRTMG_SW_G(5) RRTMG_SW_G(6)
-  RRTMG_SW_G(7) RRTMG_SW_G(8) RRTMG_SW_G(9) RRTMG_SW_G(10) RRTMG_SW_G(11) RRTMG_SW_G(12) RRTMG_SW_G(13)
-#undef RRTMG_SW_G
+  int band = kSwBands - 1;
+  while (G < kSwGofsDev[band]) --band;
+  const RecordOptics o{sw_layrecs(a) + static_cast<size_t>(t) * n * kSwRec, G, kSwRecCloud + 4 * band};
+  Path Pc, Pt;
+  sw_gpoint<true>(T, a, C, a.mask + col, a.icld == 0, nullptr, Pc, Pt, a.split_terms + (t - first),
+                  static_cast<size_t>(count), G, R.sflux[G], o);
 }
 
 // Ordered g-point sums of the split schedules: thread (day-list slot t, plane
@@ -1074,7 +1240,9 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
 }
 
 size_t sw_split_terms_floats(int nk, int ncol) {
-  return static_cast<size_t>(6) * (nk + 2) * kSwGpts * static_cast<size_t>(ncol);
+  // terms, column records, layer records
+  return sw_terms_only_floats(nk, ncol) +
+         (kSwColRecFloats + static_cast<size_t>(kSwRec) * (nk + 1)) * static_cast<size_t>(ncol);
 }
 
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream) {
@@ -1083,8 +1251,19 @@ cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t str
     // small domain: g-point split schedule over all ncol list slots, ordered
     // g-point sums, then the column outputs
     const int blocks = (a.ncol + threads - 1) / threads;
-    sw_gsplit_kernel<<<dim3(blocks, kSwGpts), threads, 0, stream>>>(T, a, 0, a.ncol);
+    sw_colprep_kernel<<<blocks, threads, 0, stream>>>(T, a);
     cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const long long layers = static_cast<long long>(a.ncol) * (a.nk + 1);
+    sw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kSwBands), threads, 0, stream>>>(
+        T, a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sw_source_kernel<<<dim3(blocks, kSwBands), threads, 0, stream>>>(T, a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sw_gsplit_kernel<<<dim3(blocks, kSwGpts), threads, 0, stream>>>(T, a, 0, a.ncol);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     sw_gsum_kernel<<<dim3(blocks, 6 * (a.nk + 2)), threads, 0, stream>>>(a, 0, a.ncol);
     e = cudaGetLastError();
