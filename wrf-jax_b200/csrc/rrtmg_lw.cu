@@ -1050,7 +1050,8 @@ __device__ __forceinline__ void surface_band(const Tables &T, const Layer &L0, f
 // Column prologue of both schedules: buffer layers, laytrop, pwvcm, the band
 // diffusivities (lw:5520-5539) and whether any layer is cloudy.
 // Column set-up shared by both prologues: buffer layers, laytrop and pwvcm.
-__device__ __forceinline__ void column_core(const Tables &T, const LwArgs &a, int col, Col &C) {
+// Fields of the column context taken from the call and the 2-D inputs.
+__device__ __forceinline__ void column_head(const LwArgs &a, int col, Col &C) {
   C.i = col / a.ny;
   C.j = col - C.i * a.ny;
   C.nk = a.nk;
@@ -1062,38 +1063,53 @@ __device__ __forceinline__ void column_core(const Tables &T, const LwArgs &a, in
   C.has_reqc = a.has_reqc; C.has_reqi = a.has_reqi; C.has_reqs = a.has_reqs; C.icloud = a.icloud;
   C.tsfc = ld(a.in.tsk + col);
   C.semiss = ld(a.in.emiss + col);
-  column_setup(T, a, C);
-  const int nlay = C.nlay;
-
-  // column integrals: laytrop (lw:1263-1264) and pwvcm (lw:1037-1064)
-  {
-    int laytrop = 0;
-    float amttl = 0.0f, wvttl = 0.0f;
-    const float amd = 28.9660f, amw = 18.0160f, avogad = 6.02214199e23f, grav = 9.8066f;
-    for (int l = 0; l < nlay; ++l) {
-      const float pavel = play_at(a, C, l);
-      laytrop += glibc_logf(T, pavel) > 4.56f;
-      const float h2o = h2o_at(a, C, l);
-      const float amm = (1.0f - h2o) * amd + h2o * amw;
-      const float pm = ((plev_at(a, C, l) - plev_at(a, C, l + 1)) * 1.0e3f) * avogad;
-      float md = 1.0e2f * grav;
-      md = md * amm;
-      md = md * (1.0f + h2o);
-      const float coldry = pm / md;
-      const float wk0 = h2o * coldry;
-      amttl = (amttl + coldry) + wk0;
-      wvttl = wvttl + wk0;
-    }
-    C.laytrop = laytrop;
-    const float wvsh = (amw * wvttl) / (amd * amttl);
-    C.pwvcm = (wvsh * (1.0e3f * plev_at(a, C, 0))) / (1.0e2f * grav);
-  }
 }
 
-__device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a, int col, Col &C, float *secdiff,
-                                                bool &has_cloud) {
-  column_core(T, a, col, C);
+constexpr float kAmd = 28.9660f, kAmw = 18.0160f, kAvogad = 6.02214199e23f, kGrav = 9.8066f;
+
+// Layer l's share of the column integrals: whether it is below the
+// tropopause test pressure, its dry-air column and its water column
+// (lw:1037-1064, 1263-1264).
+__device__ __forceinline__ void column_layer(const Tables &T, const LwArgs &a, const Col &C, int l, bool &trop,
+                                             float &coldry, float &wk0) {
+  const float pavel = play_at(a, C, l);
+  trop = glibc_logf(T, pavel) > 4.56f;
+  const float h2o = h2o_at(a, C, l);
+  const float amm = (1.0f - h2o) * kAmd + h2o * kAmw;
+  const float pm = ((plev_at(a, C, l) - plev_at(a, C, l + 1)) * 1.0e3f) * kAvogad;
+  float md = 1.0e2f * kGrav;
+  md = md * amm;
+  md = md * (1.0f + h2o);
+  coldry = pm / md;
+  wk0 = h2o * coldry;
+}
+
+__device__ __forceinline__ float column_pwvcm(const LwArgs &a, const Col &C, float amttl, float wvttl) {
+  const float wvsh = (kAmw * wvttl) / (kAmd * amttl);
+  return (wvsh * (1.0e3f * plev_at(a, C, 0))) / (1.0e2f * kGrav);
+}
+
+__device__ __forceinline__ void column_core(const Tables &T, const LwArgs &a, int col, Col &C) {
+  column_head(a, col, C);
+  column_setup(T, a, C);
   const int nlay = C.nlay;
+  // column integrals: laytrop and pwvcm, summed in layer order
+  int laytrop = 0;
+  float amttl = 0.0f, wvttl = 0.0f;
+  for (int l = 0; l < nlay; ++l) {
+    bool trop;
+    float coldry, wk0;
+    column_layer(T, a, C, l, trop, coldry, wk0);
+    laytrop += trop;
+    amttl = (amttl + coldry) + wk0;
+    wvttl = wvttl + wk0;
+  }
+  C.laytrop = laytrop;
+  C.pwvcm = column_pwvcm(a, C, amttl, wvttl);
+}
+
+// Band diffusivities from the column water (lw:5520-5539).
+__device__ __forceinline__ void column_secdiff(const Tables &T, const Col &C, float *secdiff) {
 #pragma unroll
   for (int b = 0; b < kLwBands; ++b) {
     const bool variable = !(b == 0 || b == 3 || b >= 9);
@@ -1105,6 +1121,13 @@ __device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a
       secdiff[b] = 1.66f;
     }
   }
+}
+
+__device__ __forceinline__ void column_prologue(const Tables &T, const LwArgs &a, int col, Col &C, float *secdiff,
+                                                bool &has_cloud) {
+  column_core(T, a, col, C);
+  const int nlay = C.nlay;
+  column_secdiff(T, C, secdiff);
 
   // cloudy layers and whether any layer is cloudy (lw:5566-5567, 5656)
   has_cloud = false;
@@ -1347,14 +1370,45 @@ __device__ __forceinline__ float *layer_records(const LwArgs &a) {
   return a.optics + kColRecFloats * static_cast<size_t>(a.chunk_count);
 }
 
+// A warp per column: the lanes take the layers of the column integrals, whose
+// sums are then taken in layer order from shared memory (the operations and
+// order of column_prologue).
 __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
-  const int lc = blockIdx.x * blockDim.x + threadIdx.x;
-  if (lc >= a.chunk_count) return;
+  __shared__ float s_cd[4][kMaxLay], s_wk[4][kMaxLay];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lc = blockIdx.x * 4 + w;
+  if (lc >= a.chunk_count) return;  // whole warps
+  const int col = a.chunk_first + lc;
   ColRec r;
-  bool has_cloud;
-  column_prologue(T, a, a.chunk_first + lc, r.C, r.secdiff, has_cloud);
+  Col &C = r.C;
+  column_head(a, col, C);
+  column_setup(T, a, C);
+  const int nlay = C.nlay;
+  int trop_count = 0;
+  bool cloud = false;
+  for (int l = lane; l < nlay; l += 32) {
+    bool trop;
+    column_layer(T, a, C, l, trop, s_cd[w][l], s_wk[w][l]);
+    trop_count += trop;
+    uint32_t any = 0;
+#pragma unroll
+    for (int q = 0; q < kLwMaskWords; ++q) any |= a.mask[(static_cast<size_t>(l) * kLwMaskWords + q) * a.ncol + col];
+    cloud = cloud || any != 0u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) trop_count += __shfl_xor_sync(0xffffffffu, trop_count, o);
+  const bool has_cloud = __any_sync(0xffffffffu, cloud);
+  __syncwarp();
+  float amttl = 0.0f, wvttl = 0.0f;
+  for (int l = 0; l < nlay; ++l) {
+    amttl = (amttl + s_cd[w][l]) + s_wk[w][l];
+    wvttl = wvttl + s_wk[w][l];
+  }
+  C.laytrop = trop_count;
+  C.pwvcm = column_pwvcm(a, C, amttl, wvttl);
+  column_secdiff(T, C, r.secdiff);
   r.has_cloud = has_cloud ? 1 : 0;
-  reinterpret_cast<ColRec *>(a.optics)[lc] = r;
+  if (lane == 0) reinterpret_cast<ColRec *>(a.optics)[lc] = r;
 }
 
 template <int B>
@@ -1610,6 +1664,76 @@ __global__ void __launch_bounds__(128) lw_finish_kernel(LwArgs a) {
   for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
 }
 
+// lw_finish_kernel for the split schedule's small domains: a block per column,
+// its threads over flux levels.  Each level's four totals are the band terms
+// added in band order, as in lw_finish_kernel; then each layer's heating rate
+// and the 2-D outputs, with the same operations.
+constexpr int kFinishThreads = 64;
+
+__global__ void __launch_bounds__(kFinishThreads) lw_finish_block_kernel(LwArgs a) {
+  __shared__ float tot[4][kMaxLay + 2];
+  const int col = a.chunk_first + blockIdx.x;
+  const int i = col / a.ny, j = col - i * a.ny;
+  const int nk = a.nk, nlay = a.nlay;
+  const float pi = 3.1415926535897932384626433832795f;
+  const float fluxfac = pi * 2.0e4f;
+  const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
+  // upward totals at slots 0 .. nk + 1, downward at 0 .. nk
+  for (int slot = threadIdx.x; slot <= nk + 1; slot += blockDim.x) {
+    for (int type = 0; type < 4; ++type) {
+      if (type >= 2 && slot > nk) continue;
+      float total = 0.0f;
+#pragma unroll
+      for (int b = 0; b < kLwBands; ++b) total = total + a.terms[term_index(a, type, slot, b, col)];
+      tot[type][slot] = total * fluxfac;
+    }
+  }
+  __syncthreads();
+  const size_t rbase = static_cast<size_t>(i) * nk * a.ny + j;
+  const size_t wbase = static_cast<size_t>(i) * (nk + 1) * a.ny + j;
+  for (int l = threadIdx.x; l < nk; l += blockDim.x) {
+    const int lev = l + 1;
+    const float ufl0 = tot[0][l], uflc0 = tot[1][l], dfl0 = tot[2][l], dflc0 = tot[3][l];
+    const float ufl1 = tot[0][lev], uflc1 = tot[1][lev];
+    float dfl1, dflc1;
+    if (lev == nlay) {
+      dfl1 = 0.0f * fluxfac;
+      dflc1 = 0.0f * fluxfac;
+    } else {
+      dfl1 = tot[2][lev];
+      dflc1 = tot[3][lev];
+    }
+    const float fnet0 = ufl0 - dfl0, fnet1 = ufl1 - dfl1;
+    const float fnetc0 = uflc0 - dflc0, fnetc1 = uflc1 - dflc1;
+    const float plev0 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l) * a.ny));
+    const float plev1 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l + 1) * a.ny));
+    const float dp = plev0 - plev1;
+    const float htr = heatfac * (fnet0 - fnet1) / dp;
+    const float htrc = heatfac * (fnetc0 - fnetc1) / dp;
+    const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * a.ny);
+    a.rthraten[rbase + static_cast<size_t>(l) * a.ny] = (htr / 86400.0f) / pi3d;
+    a.rthratenc[rbase + static_cast<size_t>(l) * a.ny] = (htrc / 86400.0f) / pi3d;
+  }
+  if (threadIdx.x == 0) {
+    const int top = nlay == nk ? nk : nk + 1;
+    const float uflt = tot[0][top], ufltc = tot[1][top];
+    const float dflt = 0.0f * fluxfac;
+    a.upt[col] = uflt;
+    a.uptc[col] = ufltc;
+    a.dnt[col] = dflt;
+    a.dntc[col] = dflt;
+    a.upb[col] = tot[0][0];
+    a.upbc[col] = tot[1][0];
+    a.dnb[col] = tot[2][0];
+    a.dnbc[col] = tot[3][0];
+    a.glw[col] = tot[2][0];
+    a.olr[col] = uflt;
+    a.lwcf[col] = ufltc - uflt;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream) {
@@ -1636,7 +1760,7 @@ size_t lw_optics_floats(int nlay, int ncol) {
 
 cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
-  lw_colprep_kernel<<<(a.chunk_count + threads - 1) / threads, threads, 0, stream>>>(T, a);
+  lw_colprep_kernel<<<(a.chunk_count + 3) / 4, threads, 0, stream>>>(T, a);
   cudaError_t e0 = cudaGetLastError();
   if (e0 != cudaSuccess) return e0;
   const long long layers = static_cast<long long>(a.chunk_count) * a.nlay;
@@ -1651,6 +1775,10 @@ cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stre
 }
 
 cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream) {
+  if (a.optics) {  // split schedule: small domain
+    lw_finish_block_kernel<<<a.chunk_count, kFinishThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+  }
   const int threads = 128;
   const int blocks = (a.chunk_count + threads - 1) / threads;
   lw_finish_kernel<<<blocks, threads, 0, stream>>>(a);
