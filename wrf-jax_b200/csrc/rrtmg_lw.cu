@@ -1508,51 +1508,48 @@ __device__ __forceinline__ void gpoint_step(const Tables &T, const float *rec, i
   rA = rn;
 }
 
-// Band term of a level from the half-warp's g-point radiances (g order), by
-// the lane of g-point 0 (g < 0: store nothing).
-__device__ __forceinline__ void store_band_term(const LwArgs &a, float rn, float rcn, int ngc, int g, int band,
-                                                int type, int slot, int col) {
-  const int base = threadIdx.x & 16;
-  float s = 0.0f, sc = 0.0f;
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const float v = __shfl_sync(0xffffffffu, rn, base + q);
-    const float vc = __shfl_sync(0xffffffffu, rcn, base + q);
-    if (q < ngc) {
-      s = s + v;
-      sc = sc + vc;
-    }
-  }
-  if (g == 0 && slot >= 0) {
-    a.terms[term_index(a, type, slot, band, col)] = (s * 0.5f) * kDelwave[band];
-    a.terms[term_index(a, type + 1, slot, band, col)] = (sc * 0.5f) * kDelwave[band];
-  }
-}
-
 __constant__ int kNgcDev[kLwBands] = {10, 12, 16, 14, 16, 8, 12, 8, 12, 6, 8, 8, 4, 2, 2, 2};
 __constant__ int kGofsDev[kLwBands] = {0, 10, 22, 38, 52, 68, 76, 88, 96, 108, 114, 122, 130, 134, 136, 138};
 
-// Band-major grid (blockIdx.y = band), two columns per warp (one per half-warp).
-__global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int band = blockIdx.y;
-  const int lane16 = t & 15;
-  if ((t & ~31) >> 4 >= a.chunk_count) return;  // the whole warp is past the end
-  // a half-warp past the last column repeats it and stores nothing
-  const int lraw = t >> 4;
-  const bool valid = lraw < a.chunk_count;
-  const int lc = valid ? lraw : a.chunk_count - 1;
+constexpr int kGsplitThreads = 160;  // 140 g-points of one column, padded to whole warps
+
+// A block per column, thread G = g-point.  After each level the g-point
+// radiances go to shared memory (double-buffered by level, one barrier per
+// level) and 32 threads take the band sums in g order, total and clear, and
+// store the band terms.
+__global__ void __launch_bounds__(kGsplitThreads) lw_gsplit_kernel(Tables T, LwArgs a) {
+  __shared__ float s_rad[2][2][kLwGpts];  // [level parity][total, clear][g-point]
+  const int lc = blockIdx.x;
   const int col = a.chunk_first + lc;
-  const int ngc = kNgcDev[band];
-  // lanes past the band's g-points repeat its last one and are not summed
-  const int G = kGofsDev[band] + (lane16 < ngc ? lane16 : ngc - 1);
-  const int store_g = valid ? lane16 : -1;
+  const int tid = threadIdx.x;
+  const int G = tid < kLwGpts ? tid : kLwGpts - 1;  // the padding threads repeat the last g-point
+  int band = kLwBands - 1;
+  while (G < kGofsDev[band]) --band;
   const ColRec &R = col_records(a)[lc];
   const float sd = R.secdiff[band];
   const bool has_cloud = R.has_cloud != 0;
   const float tsfc = R.C.tsfc, semiss = R.C.semiss;
   const int nlay = R.C.nlay, nk = R.C.nk;
   const float *recs = layer_records(a) + static_cast<size_t>(lc) * nlay * kLwOpticsFloats;
+  // band sums of a level: thread q < 16 the total of band q, 16 + q its clear sum
+  int step = 0;
+  auto level_terms = [&](float rA, float rB, int type, int slot) {
+    float(*buf)[kLwGpts] = s_rad[step & 1];
+    if (tid < kLwGpts) {
+      buf[0][tid] = rA;
+      buf[1][tid] = rB;
+    }
+    __syncthreads();
+    if (tid < 2 * kLwBands && slot >= 0) {
+      const int b = tid & 15, which = tid >> 4;
+      const float *v = buf[which] + kGofsDev[b];
+      const int ngc = kNgcDev[b];
+      float sum = 0.0f;
+      for (int q = 0; q < ngc; ++q) sum = sum + v[q];
+      a.terms[term_index(a, type + which, slot, b, col)] = (sum * 0.5f) * kDelwave[b];
+    }
+    ++step;
+  };
   float rA = 0.0f, rB = 0.0f;
   bool iclddn = false;
   for (int l = nlay - 1; l >= 0; --l) {
@@ -1560,7 +1557,7 @@ __global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
     const bool cloudy = load_mask(a, l, col, mask);
     iclddn = iclddn || cloudy;
     gpoint_step<true>(T, recs + static_cast<size_t>(l) * kLwOpticsFloats, G, band, mask, cloudy, sd, rA, rB, iclddn);
-    store_band_term(a, rA, rB, ngc, store_g, band, 2, l <= nk ? l : -1, col);
+    level_terms(rA, rB, 2, l <= nk ? l : -1);
   }
   {
     // surface emission and reflection (surface_sums)
@@ -1572,7 +1569,7 @@ __global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
     const float rad0 = recs[kLwGpts + G] * plankbnd;
     rA = rad0 + reflect * rA;
     rB = rad0 + reflect * rB;
-    store_band_term(a, rA, rB, ngc, store_g, band, 0, 0, col);
+    level_terms(rA, rB, 0, 0);
   }
   for (int l = 0; l < nlay; ++l) {
     uint32_t mask[kLwMaskWords];
@@ -1580,7 +1577,7 @@ __global__ void __launch_bounds__(128) lw_gsplit_kernel(Tables T, LwArgs a) {
     gpoint_step<false>(T, recs + static_cast<size_t>(l) * kLwOpticsFloats, G, band, mask, cloudy, sd, rA, rB,
                        has_cloud);
     const int lev = l + 1;
-    store_band_term(a, rA, rB, ngc, store_g, band, 0, lev <= nk ? lev : (lev == nlay ? nk + 1 : -1), col);
+    level_terms(rA, rB, 0, lev <= nk ? lev : (lev == nlay ? nk + 1 : -1));
   }
 }
 
@@ -1768,9 +1765,7 @@ cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stre
       T, a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const long long total = static_cast<long long>(a.chunk_count) * 16;
-  const dim3 grid(static_cast<unsigned>((total + threads - 1) / threads), kLwBands);
-  lw_gsplit_kernel<<<grid, threads, 0, stream>>>(T, a);
+  lw_gsplit_kernel<<<a.chunk_count, kGsplitThreads, 0, stream>>>(T, a);
   return cudaGetLastError();
 }
 

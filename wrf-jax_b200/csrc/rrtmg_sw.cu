@@ -930,8 +930,12 @@ __global__ void __launch_bounds__(256) sw_daylist_kernel(SwArgs a) {
   a.swddif[col] = 0.0f; a.swdownc[col] = 0.0f; a.swddnic[col] = 0.0f; a.swddirc[col] = 0.0f;
 }
 
-// Column set-up of a day column (buffer ozone, laytrop; sw:2491-2508, 7101-7306).
-__device__ __forceinline__ void sw_setup(const Tables &T, const SwArgs &a, int col, Col &C) {
+__device__ __forceinline__ float sw_pavel(const SwArgs &a, const Col &C, int l) {
+  return l < C.nk ? pa_to_hpa(in3(a.in.p3d, C, l)) : 0.5f * pa_to_hpa(in3w(a.in.p8w, C, C.nk));
+}
+
+// Column set-up of a day column without laytrop (buffer ozone; sw:2491-2508).
+__device__ __forceinline__ void sw_setup_head(const Tables &T, const SwArgs &a, int col, Col &C) {
   C.i = col / a.ny;
   C.j = col - C.i * a.ny;
   C.nk = a.nk;
@@ -956,38 +960,45 @@ __device__ __forceinline__ void sw_setup(const Tables &T, const SwArgs &a, int c
     if (top <= 0.0f) top = mmr_t * amdo;
     C.o3top = top;
   }
-  {
-    int laytrop = 0;
-    for (int l = 0; l < n; ++l) {
-      const float pavel = l < nk ? pa_to_hpa(in3(a.in.p3d, C, l)) : 0.5f * pa_to_hpa(in3w(a.in.p8w, C, nk));
-      laytrop += glibc_logf(T, pavel) > 4.56f;
-    }
-    C.laytrop = laytrop;
-  }
+  (void)n;
 }
 
-// Heating rates, theta tendencies and 2-D outputs of a day column from its
-// level sums accs (six arrays of kMaxLev, top-down; sw:2285-2301, 2536-2719).
-__device__ __forceinline__ void sw_outputs(const SwArgs &a, const Col &C, int col, const float *accs) {
+// Column set-up of a day column (buffer ozone, laytrop; sw:2491-2508, 7101-7306).
+__device__ __forceinline__ void sw_setup(const Tables &T, const SwArgs &a, int col, Col &C) {
+  sw_setup_head(T, a, col, C);
+  int laytrop = 0;
+  for (int l = 0; l < C.nlay; ++l) laytrop += glibc_logf(T, sw_pavel(a, C, l)) > 4.56f;
+  C.laytrop = laytrop;
+}
+
+// Heating rate and theta tendency of layer l of a day column from its level
+// sums accs (six arrays of stride `stride`, top-down; sw:2285-2301).
+__device__ __forceinline__ void sw_layer_output(const SwArgs &a, const Col &C, int l, const float *accs,
+                                                int stride) {
   const int nk = C.nk, n = C.nlay;
-  const float coszen = C.coszen;
   const size_t rbase = static_cast<size_t>(C.i) * nk * C.ny + C.j;
-  const float *fu = accs, *fd = accs + kMaxLev, *cu = accs + 2 * kMaxLev, *cd = accs + 3 * kMaxLev;
-  const float *fdir = accs + 4 * kMaxLev, *cdir = accs + 5 * kMaxLev;
+  const float *fu = accs, *fd = accs + stride, *cu = accs + 2 * stride, *cd = accs + 3 * stride;
   const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
-  for (int l = 0; l < nk; ++l) {
-    // bottom-up level l is top-down index n - l
-    const float n1 = fd[n - (l + 1)] - fu[n - (l + 1)], n0 = fd[n - l] - fu[n - l];
-    const float c1 = cd[n - (l + 1)] - cu[n - (l + 1)], c0 = cd[n - l] - cu[n - l];
-    const float plev0 = pa_to_hpa(in3w(a.in.p8w, C, l));
-    const float plev1 = pa_to_hpa(in3w(a.in.p8w, C, l + 1));
-    const float zdpgcp = heatfac / (plev0 - plev1);
-    const float hr = (n1 - n0) * zdpgcp;
-    const float hrc = (c1 - c0) * zdpgcp;
-    const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * C.ny);
-    a.rthraten[rbase + static_cast<size_t>(l) * C.ny] = (hr / 86400.0f) / pi3d;
-    a.rthratenc[rbase + static_cast<size_t>(l) * C.ny] = (hrc / 86400.0f) / pi3d;
-  }
+  // bottom-up level l is top-down index n - l
+  const float n1 = fd[n - (l + 1)] - fu[n - (l + 1)], n0 = fd[n - l] - fu[n - l];
+  const float c1 = cd[n - (l + 1)] - cu[n - (l + 1)], c0 = cd[n - l] - cu[n - l];
+  const float plev0 = pa_to_hpa(in3w(a.in.p8w, C, l));
+  const float plev1 = pa_to_hpa(in3w(a.in.p8w, C, l + 1));
+  const float zdpgcp = heatfac / (plev0 - plev1);
+  const float hr = (n1 - n0) * zdpgcp;
+  const float hrc = (c1 - c0) * zdpgcp;
+  const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * C.ny);
+  a.rthraten[rbase + static_cast<size_t>(l) * C.ny] = (hr / 86400.0f) / pi3d;
+  a.rthratenc[rbase + static_cast<size_t>(l) * C.ny] = (hrc / 86400.0f) / pi3d;
+}
+
+// 2-D outputs of a day column from its level sums (sw:2536-2719).
+__device__ __forceinline__ void sw_column_outputs(const SwArgs &a, const Col &C, int col, const float *accs,
+                                                  int stride) {
+  const int n = C.nlay;
+  const float coszen = C.coszen;
+  const float *fu = accs, *fd = accs + stride, *cu = accs + 2 * stride, *cd = accs + 3 * stride;
+  const float *fdir = accs + 4 * stride, *cdir = accs + 5 * stride;
   a.upt[col] = fu[0];
   a.uptc[col] = cu[0];
   a.dnt[col] = fd[0];
@@ -1004,6 +1015,13 @@ __device__ __forceinline__ void sw_outputs(const SwArgs &a, const Col &C, int co
   a.swdownc[col] = cd[n];
   a.swddirc[col] = cdir[n];
   a.swddnic[col] = cdir[n] / coszen;
+}
+
+// Heating rates, theta tendencies and 2-D outputs of a day column from its
+// level sums accs (six arrays of kMaxLev, top-down).
+__device__ __forceinline__ void sw_outputs(const SwArgs &a, const Col &C, int col, const float *accs) {
+  for (int l = 0; l < C.nk; ++l) sw_layer_output(a, C, l, accs, kMaxLev);
+  sw_column_outputs(a, C, col, accs, kMaxLev);
 }
 
 
@@ -1069,12 +1087,19 @@ __device__ __forceinline__ float *sw_layrecs(const SwArgs &a) {
 
 __constant__ int kSwGofsDev[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
 
+// A warp per day column; the lanes take the layers of the laytrop count.
 __global__ void __launch_bounds__(128) sw_colprep_kernel(Tables T, SwArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.ncol || t >= *a.nday) return;
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (t >= a.ncol || t >= *a.nday) return;  // whole warps
   Col C;
-  sw_setup(T, a, a.daylist[t], C);
-  sw_colrecs(a)[t].C = C;
+  sw_setup_head(T, a, a.daylist[t], C);
+  int count = 0;
+  for (int l = lane; l < C.nlay; l += 32) count += glibc_logf(T, sw_pavel(a, C, l)) > 4.56f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+  C.laytrop = count;
+  if (lane == 0) sw_colrecs(a)[t].C = C;
 }
 
 template <int B>
@@ -1207,9 +1232,12 @@ __global__ void __launch_bounds__(128) sw_gsum_kernel(SwArgs a, int first, int c
   p[0] = acc;
 }
 
-__global__ void __launch_bounds__(128) sw_split_finish_kernel(Tables T, SwArgs a, int first, int count) {
-  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= first + count || t >= *a.nday) return;
+// Outputs of the split schedule: a block per day slot, its threads over
+// layers; the level sums are the g-point-0 slots sw_gsum_kernel wrote.
+__global__ void __launch_bounds__(64) sw_split_finish_kernel(Tables T, SwArgs a, int first, int count) {
+  __shared__ float accs[6 * kMaxLev];
+  const int t = first + blockIdx.x;
+  if (t >= first + count || t >= *a.nday) return;  // whole blocks
   const int col = a.daylist[t];
   Col C;
   C.i = col / a.ny;
@@ -1221,13 +1249,14 @@ __global__ void __launch_bounds__(128) sw_split_finish_kernel(Tables T, SwArgs a
   const int n = C.nlay;
   const float *terms = a.split_terms + (t - first);
   const size_t ts = static_cast<size_t>(count);
-  float accs[6 * kMaxLev];
-  for (int type = 0; type < 6; ++type) {
-    for (int level = 0; level <= n; ++level)
-      accs[type * kMaxLev + level] = terms[(static_cast<size_t>(type) * (n + 1) + level) * kSwGpts * ts];
+  for (int q = threadIdx.x; q < 6 * (n + 1); q += blockDim.x) {
+    const int type = q / (n + 1), level = q - type * (n + 1);
+    accs[type * kMaxLev + level] = terms[(static_cast<size_t>(type) * (n + 1) + level) * kSwGpts * ts];
   }
+  __syncthreads();
+  for (int l = threadIdx.x; l < C.nk; l += blockDim.x) sw_layer_output(a, C, l, accs, kMaxLev);
+  if (threadIdx.x == 0) sw_column_outputs(a, C, col, accs, kMaxLev);
   (void)T;
-  sw_outputs(a, C, col, accs);
 }
 
 }  // namespace
@@ -1251,7 +1280,7 @@ cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t str
     // small domain: g-point split schedule over all ncol list slots, ordered
     // g-point sums, then the column outputs
     const int blocks = (a.ncol + threads - 1) / threads;
-    sw_colprep_kernel<<<blocks, threads, 0, stream>>>(T, a);
+    sw_colprep_kernel<<<(a.ncol + 3) / 4, threads, 0, stream>>>(T, a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const long long layers = static_cast<long long>(a.ncol) * (a.nk + 1);
@@ -1268,7 +1297,7 @@ cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t str
     sw_gsum_kernel<<<dim3(blocks, 6 * (a.nk + 2)), threads, 0, stream>>>(a, 0, a.ncol);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    sw_split_finish_kernel<<<blocks, threads, 0, stream>>>(T, a, 0, a.ncol);
+    sw_split_finish_kernel<<<a.ncol, 64, 0, stream>>>(T, a, 0, a.ncol);
     return cudaGetLastError();
   }
   // The day count is known only on the device: launch over ncol list slots in
