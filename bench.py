@@ -356,9 +356,12 @@ def run_plain(args):
 
 def _surrogate_launches(n_fallback: int, fused: bool) -> int:
     """Kernel launches of one surrogate step: features, the fused network
-    kernel (or 4 GEMMs and a decode), compact; with fallback columns also 22
-    gathers, 6 scatters and the plain LW (3) and SW (3) launches."""
-    return (3 if fused else 7) + (34 if n_fallback > 0 else 0)
+    kernel (or 4 GEMMs and a decode), compact; with fallback columns also one
+    batched gather and one scatter, the LW split schedule (McICA, column
+    set-up, layer optics, g-point sweep, finish) and the SW split schedule
+    (McICA, day list, column set-up, layer optics, solar source, g-point sweep,
+    g-point sums, finish)."""
+    return (3 if fused else 7) + (15 if n_fallback > 0 else 0)
 
 
 def run_surrogate(args):
