@@ -83,8 +83,6 @@ class EnsembleRunner:
                 ncol = nx * ny
                 mpad = (ncol + 127) // 128 * 128
                 m.buf = dict(X=torch.zeros(mpad, S.K_IN, device="cuda", dtype=torch.bfloat16),
-                             H=[torch.empty(mpad, S.HIDDEN, device="cuda", dtype=torch.bfloat16) for _ in range(3)],
-                             Y=torch.empty(mpad, S.N_OUT, device="cuda"),
                              flags=torch.empty(ncol, device="cuda", dtype=torch.int32),
                              list=torch.empty(ncol, device="cuda", dtype=torch.int32),
                              count=torch.zeros(1, device="cuda", dtype=torch.int32))
@@ -112,24 +110,10 @@ class EnsembleRunner:
             rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw, context=self.ctx, stream=sid, out=m.out["lw"])
             rrtmg.rrtmg_swrad_wrf_columns(**sw_kw, context=self.ctx, stream=sid, out=m.out["sw"])
             return
-        st, b, model = m.st, m.buf, self.model
+        st, b = m.st, m.buf
         s = ctypes.c_void_p(sid)
-        fa = S._feature_args(m.d, st.nk, st.ny, m.columns)
-        fa.mean, fa.rstd = model.norm.in_mean.data_ptr(), model.norm.in_rstd.data_ptr()
-        fa.X, fa.ldx = b["X"].data_ptr(), S.K_IN
-        fa.lo, fa.hi, fa.flags = model.norm.in_lo.data_ptr(), model.norm.in_hi.data_ptr(), b["flags"].data_ptr()
-        S._check(lib.rrtmg_sur_features(ctypes.byref(fa), s), "features")
-        inp = b["X"]
-        for i in range(3):
-            S.gemm_bf16(inp, model.wb[i], epilogue=_capi.EPI_GELU, bias=model.b[i], H=b["H"][i], stream=sid)
-            inp = b["H"][i]
-        S.gemm_bf16(inp, model.wb[3], epilogue=_capi.EPI_F32, bias=model.b[3], C=b["Y"], stream=sid)
-        da = _capi.SurDecodeArgs(ncol=m.columns, nk=st.nk, ny=st.ny, Y=b["Y"].data_ptr(), ldy=S.N_OUT,
-                                 out_mean=model.norm.out_mean.data_ptr(), out_std=model.norm.out_std.data_ptr(),
-                                 coszr=m.d["coszr"].data_ptr(), pi3d=m.d["pi3d"].data_ptr(),
-                                 p8w=m.d["p8w"].data_ptr(), energy_tol=self.energy_tol,
-                                 **{k: v.data_ptr() for k, v in m.out.items()}, flags=b["flags"].data_ptr())
-        S._check(lib.rrtmg_sur_decode(ctypes.byref(da), s), "decode")
+        # features in the tile layout, then the fused network and gated decode
+        S._network(self.model, m.d, st.nx, st.ny, st.nk, m.out, b["flags"], self.energy_tol, b["X"], s)
         b["count"].zero_()
         S._check(lib.rrtmg_sur_compact(b["flags"].data_ptr(), m.columns, b["list"].data_ptr(),
                                        b["count"].data_ptr(), s), "compact")
@@ -179,20 +163,21 @@ class EnsembleRunner:
         sub.update({k: torch.empty(1, nk + 1, total, device="cuda") for k in S._FIELDS_LEV})
         sub.update({k: torch.empty(1, total, device="cuda") for k in S._FIELDS_2D})
 
-        def move(m, src, dst, nz, to, off, n):
-            S._check(lib.rrtmg_sur_move_columns(m.buf["list"].data_ptr(), m.buf["count"].data_ptr(), n, nz, m.st.ny,
-                                                src.data_ptr(), dst.data_ptr(), to, total, off, ctypes.c_void_p(s)),
-                     "move columns")
+        nz = {k: nk for k in S._FIELDS_3D}
+        nz.update({k: nk + 1 for k in S._FIELDS_LEV})
+        nz.update({k: 1 for k in S._FIELDS_2D})
+
+        def move(m, pairs, to, off, n):
+            f = _capi.SurFields(nfields=len(pairs))
+            for i, (src, dst, z) in enumerate(pairs):
+                f.src[i], f.dst[i], f.nz[i] = src.data_ptr(), dst.data_ptr(), z
+            S._check(lib.rrtmg_sur_move_fields(m.buf["list"].data_ptr(), m.buf["count"].data_ptr(), n, m.st.ny,
+                                               ctypes.byref(f), to, total, off, ctypes.c_void_p(s)), "move fields")
 
         off = 0
         for m, n in zip(sur, counts):
             if n:
-                for k in S._FIELDS_3D:
-                    move(m, m.d[k], sub[k], nk, 1, off, n)
-                for k in S._FIELDS_LEV:
-                    move(m, m.d[k], sub[k], nk + 1, 1, off, n)
-                for k in S._FIELDS_2D:
-                    move(m, m.d[k], sub[k], 1, 1, off, n)
+                move(m, [(m.d[k], sub[k], z) for k, z in nz.items()], 1, off, n)
             off += n
         ref = sur[0].st  # scalars (gases, solar constant, flags) are common to the generator's domains
         lw_kw = {k: (sub[k] if k in sub else v) for k, v in ref.lw_kwargs().items()}
@@ -202,12 +187,9 @@ class EnsembleRunner:
         off = 0
         for m, n in zip(sur, counts):
             if n:
-                move(m, lw.rthratenlw, m.out["rthratenlw"], nk, 0, off, n)
-                move(m, sw.rthratensw, m.out["rthratensw"], nk, 0, off, n)
-                move(m, lw.glw, m.out["glw"], 1, 0, off, n)
-                move(m, lw.lwupb, m.out["lwupb"], 1, 0, off, n)
-                move(m, sw.swdnb, m.out["swdnb"], 1, 0, off, n)
-                move(m, sw.swupb, m.out["swupb"], 1, 0, off, n)
+                move(m, [(lw.rthratenlw, m.out["rthratenlw"], nk), (sw.rthratensw, m.out["rthratensw"], nk),
+                         (lw.glw, m.out["glw"], 1), (lw.lwupb, m.out["lwupb"], 1), (sw.swdnb, m.out["swdnb"], 1),
+                         (sw.swupb, m.out["swupb"], 1)], 0, off, n)
             off += n
         return total
 
