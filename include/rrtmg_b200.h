@@ -105,6 +105,18 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
 rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in,
                          rrtmg_sw_out *out, void *stream);
 
+/* LW / SW over the first *live_count columns of a domain, the count read on
+ * the GPU when the kernels run (live_count: device memory, written earlier on
+ * the same stream); no counterpart in the reference.  Columns c = i * ny + j
+ * at or past the count are skipped and their outputs left as they were; the
+ * results of the others are those of rrtmg_lwrad / rrtmg_swrad.  The
+ * radiation surrogate uses it to re-solve the columns its gate
+ * rejects without reading their number on the host. */
+rrtmg_status rrtmg_lwrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in,
+                              rrtmg_lw_out *out, const int *live_count, void *stream);
+rrtmg_status rrtmg_swrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in,
+                              rrtmg_sw_out *out, const int *live_count, void *stream);
+
 /* LW with no allocation inside the call; no counterpart in the reference.
  * Same arguments and results as rrtmg_lwrad, but the McICA scratch lives in
  * fixed file-scope device arrays (32 MiB of mask words) instead of a per-call

@@ -181,8 +181,8 @@ rrtmg_status rrtmg_sur_compact(const unsigned *flags, int ncol, int *list, int *
 
 /* Gathers (to_compact = 1) or scatters (0) a field of nz levels between a
  * domain with south_north size ny and columns offset .. offset + count - 1 of
- * a compact (1, nz, stride) domain holding the listed columns; max_n bounds
- * the device-side count. */
+ * a compact (1, nz, stride) domain holding the listed columns; only the first
+ * min(count, max_n) listed columns move (count is read on the device). */
 rrtmg_status rrtmg_sur_move_columns(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
                                     float *dst, int to_compact, int stride, int offset, void *stream);
 

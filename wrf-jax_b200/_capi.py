@@ -116,8 +116,9 @@ STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "
           4: "RRTMG_TIMEOUT"}
 
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
-           "rrtmg_lwrad_static_scratch", "rrtmg_timing_enable", "rrtmg_timing_read", "rrtmg_set_schedule",
-           "rrtmg_get_schedule", "rrtmg_lw_nlayers", "rrtmg_last_error", "rrtmg_status_string")
+           "rrtmg_lwrad_static_scratch", "rrtmg_lwrad_live", "rrtmg_swrad_live", "rrtmg_timing_enable",
+           "rrtmg_timing_read", "rrtmg_set_schedule", "rrtmg_get_schedule", "rrtmg_lw_nlayers",
+           "rrtmg_last_error", "rrtmg_status_string")
 SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile", "rrtmg_sur_features", "rrtmg_sur_targets",
                      "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
                      "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
@@ -151,6 +152,12 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.rrtmg_swrad.restype = ctypes.c_int
     lib.rrtmg_swrad.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(SwIn),
                                 ctypes.POINTER(SwOut), ctypes.c_void_p]
+    lib.rrtmg_lwrad_live.restype = ctypes.c_int
+    lib.rrtmg_lwrad_live.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(LwIn),
+                                     ctypes.POINTER(LwOut), ctypes.c_void_p, ctypes.c_void_p]
+    lib.rrtmg_swrad_live.restype = ctypes.c_int
+    lib.rrtmg_swrad_live.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(SwIn),
+                                     ctypes.POINTER(SwOut), ctypes.c_void_p, ctypes.c_void_p]
     lib.rrtmg_lwrad_static_scratch.restype = ctypes.c_int
     lib.rrtmg_lwrad_static_scratch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.POINTER(LwIn),
                                                ctypes.POINTER(LwOut), ctypes.c_void_p]

@@ -503,8 +503,9 @@ const char *rrtmg_status_string(rrtmg_status s) {
   return "unknown status";
 }
 
-rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
-                         void *stream_ptr) {
+// live: null, or a device count; columns at or past it are skipped.
+static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
+                               void *stream_ptr, const int *live) {
   rrtmg_status st = check_config(ctx, cfg);
   if (st != RRTMG_OK) return st;
   if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
@@ -566,6 +567,7 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kLwGpts; m.words = kLwMaskWords;
   m.enabled = icld >= 1;
+  m.live = live;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
   timing_mark(ctx, 0, tslot, 1, stream);
@@ -576,6 +578,7 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
   LwArgs a{};
+  a.live = live;
   a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
   a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.cfc11 = cfg->cfc11vmr; a.cfc12 = cfg->cfc12vmr;
   a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
@@ -615,8 +618,8 @@ rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw
   return RRTMG_OK;
 }
 
-rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
-                         void *stream_ptr) {
+static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
+                               void *stream_ptr, const int *live) {
   rrtmg_status st = check_config(ctx, cfg);
   if (st != RRTMG_OK) return st;
   if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
@@ -659,6 +662,7 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kSwGpts; m.words = kSwMaskWords;
   m.enabled = icld >= 1;
+  m.live = live;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
   timing_mark(ctx, 1, tslot, 1, stream);
@@ -668,6 +672,7 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
   SwArgs a{};
+  a.live = live;
   a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
   a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.solcon = cfg->solcon;
   a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
@@ -723,6 +728,37 @@ rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+rrtmg_status rrtmg_lwrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
+                         void *stream) {
+  return lwrad_impl(ctx, cfg, in, out, stream, nullptr);
+}
+
+rrtmg_status rrtmg_swrad(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
+                         void *stream) {
+  return swrad_impl(ctx, cfg, in, out, stream, nullptr);
+}
+
+static bool device_count(const int *p) {
+  cudaPointerAttributes at{};
+  if (!p || cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+rrtmg_status rrtmg_lwrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
+                              const int *live_count, void *stream) {
+  if (!device_count(live_count)) return fail(ctx, RRTMG_BAD_ARG, "live_count must be a device pointer");
+  return lwrad_impl(ctx, cfg, in, out, stream, live_count);
+}
+
+rrtmg_status rrtmg_swrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
+                              const int *live_count, void *stream) {
+  if (!device_count(live_count)) return fail(ctx, RRTMG_BAD_ARG, "live_count must be a device pointer");
+  return swrad_impl(ctx, cfg, in, out, stream, live_count);
+}
+
 // rrtmg_lwrad_static_scratch: the LW call with its McICA scratch in fixed
 // file-scope device arrays instead of a per-call stream-ordered allocation.
 //

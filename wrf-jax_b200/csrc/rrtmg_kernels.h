@@ -7,11 +7,15 @@
 
 namespace rrtmg {
 
+// Columns at or past a device-side live count are skipped (null: all).
+__device__ __forceinline__ bool dead_column(const int *live, int col) { return live && col >= *live; }
+
 struct McicaArgs {
   int ncol, ny, nk, nlay, nsub, words, enabled;
   const float *p3d, *cldfra;
   const KissJump *jumps;  // one per subcolumn
   uint32_t *mask;         // (nlay, words, ncol)
+  const int *live;        // null, or a device count of leading columns to process
 };
 
 // Per-column inputs shared by LW and SW (WRF layout, device pointers).
@@ -35,6 +39,7 @@ struct LwArgs {
   float *terms;     // band-group schedule scratch, lw_terms_floats(nk, chunk_count) floats
   float *optics;    // g-point split schedule: lw_optics_floats(nlay, chunk_count) floats, else null
   int chunk_first, chunk_count;  // columns of one band-group/finish launch pair
+  const int *live;  // null, or a device count of leading columns to process
 };
 
 // default columns per band-group/finish launch pair (the term scratch holds one chunk)
@@ -58,6 +63,7 @@ struct SwArgs {
   int *daylist;  // scratch: ncol entries, day column indices
   float *split_terms;  // small domains: sw_split_terms_floats(nk, ncol) floats, else null
   int chunk_columns;   // day-list slots per launch of the column kernel
+  const int *live;     // null, or a device count of leading columns to process
 };
 
 // defaults: columns per SW column-kernel launch, and the largest domain that

@@ -1377,7 +1377,7 @@ __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
   __shared__ float s_cd[4][kMaxLay], s_wk[4][kMaxLay];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lc = blockIdx.x * 4 + w;
-  if (lc >= a.chunk_count) return;  // whole warps
+  if (lc >= a.chunk_count || dead_column(a.live, a.chunk_first + lc)) return;  // whole warps
   const int col = a.chunk_first + lc;
   ColRec r;
   Col &C = r.C;
@@ -1443,6 +1443,7 @@ __global__ void __launch_bounds__(128) lw_optics_kernel(Tables T, LwArgs a) {
   if (t >= a.chunk_count * a.nlay) return;
   const int lc = t / a.nlay, l = t - lc * a.nlay;
   const int col = a.chunk_first + lc;
+  if (dead_column(a.live, col)) return;
   const Col &C = col_records(a)[lc].C;
   uint32_t mask[kLwMaskWords];
   const bool cloudy = load_mask(a, l, col, mask);
@@ -1521,6 +1522,7 @@ __global__ void __launch_bounds__(kGsplitThreads) lw_gsplit_kernel(Tables T, LwA
   __shared__ float s_rad[2][2][kLwGpts];  // [level parity][total, clear][g-point]
   const int lc = blockIdx.x;
   const int col = a.chunk_first + lc;
+  if (dead_column(a.live, col)) return;  // whole block
   const int tid = threadIdx.x;
   const int G = tid < kLwGpts ? tid : kLwGpts - 1;  // the padding threads repeat the last g-point
   int band = kLwBands - 1;
@@ -1586,7 +1588,7 @@ constexpr int kLwGroups = 9;
 
 __global__ void __launch_bounds__(128, 3) lw_group_kernel(Tables T, LwArgs a) {
   const int col = a.chunk_first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.chunk_first + a.chunk_count) return;
+  if (col >= a.chunk_first + a.chunk_count || dead_column(a.live, col)) return;
   switch (blockIdx.y) {
     case 0: lw_group<2>(T, a, col); break;
     case 1: lw_group<4>(T, a, col); break;
@@ -1604,7 +1606,7 @@ __global__ void __launch_bounds__(128, 3) lw_group_kernel(Tables T, LwArgs a) {
 // 7040-7057) and the 2-D outputs (lw:7059-7077).
 __global__ void __launch_bounds__(128) lw_finish_kernel(LwArgs a) {
   const int col = a.chunk_first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.chunk_first + a.chunk_count) return;
+  if (col >= a.chunk_first + a.chunk_count || dead_column(a.live, col)) return;
   const int i = col / a.ny, j = col - i * a.ny;
   const int nk = a.nk, nlay = a.nlay;
   const float pi = 3.1415926535897932384626433832795f;
@@ -1670,6 +1672,7 @@ constexpr int kFinishThreads = 64;
 __global__ void __launch_bounds__(kFinishThreads) lw_finish_block_kernel(LwArgs a) {
   __shared__ float tot[4][kMaxLay + 2];
   const int col = a.chunk_first + blockIdx.x;
+  if (dead_column(a.live, col)) return;  // whole block
   const int i = col / a.ny, j = col - i * a.ny;
   const int nk = a.nk, nlay = a.nlay;
   const float pi = 3.1415926535897932384626433832795f;

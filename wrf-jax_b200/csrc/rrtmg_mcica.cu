@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(256) mcica_mask_kernel(McicaArgs a) {
   const int lane = threadIdx.x & 31;
   const int col = gwarp / warps_per_col;
   const int w = gwarp - col * warps_per_col;
-  if (col >= a.ncol) return;  // whole warp exits together
+  if (col >= a.ncol || dead_column(a.live, col)) return;  // whole warp exits together
   const int g = w * 32 + lane;
   const bool active = g < a.nsub;
   const int i = col / a.ny, j = col - i * a.ny;

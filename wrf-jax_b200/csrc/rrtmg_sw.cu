@@ -903,7 +903,7 @@ __device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const 
 __global__ void __launch_bounds__(256) sw_daylist_kernel(SwArgs a) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  const bool inside = col < a.ncol;
+  const bool inside = col < a.ncol && !dead_column(a.live, col);
   const float coszen = inside ? ld(a.in.coszr + col) : 0.0f;
   const bool day = coszen > 0.0f;
   const unsigned ballot = __ballot_sync(0xffffffffu, inside && day);

@@ -552,9 +552,9 @@ __global__ void compact_kernel(const unsigned *flags, int ncol, int *list, int *
 
 // Gather (to_compact = 1) or scatter (0) a field between a domain and the
 // compact (1, nz, n) domain of listed columns.
-__global__ void move_columns_kernel(const int *list, const int *count, int nz, int ny, const float *src, float *dst,
-                                    int to_compact, int stride, int offset) {
-  const int n = *count;
+__global__ void move_columns_kernel(const int *list, const int *count, int max_n, int nz, int ny, const float *src,
+                                    float *dst, int to_compact, int stride, int offset) {
+  const int n = min(*count, max_n);  // the compact side holds max_n columns
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * nz) return;
   const int k = t / n, j = t - k * n;
@@ -567,10 +567,10 @@ __global__ void move_columns_kernel(const int *list, const int *count, int nz, i
 
 // Several fields in one launch: blockIdx.y = field, grid-stride over its
 // (level, listed column) pairs.
-__global__ void move_fields_kernel(const int *list, const int *count, int ny, rrtmg_sur_fields f, int to_compact,
-                                   int stride, int offset) {
+__global__ void move_fields_kernel(const int *list, const int *count, int max_n, int ny, rrtmg_sur_fields f,
+                                   int to_compact, int stride, int offset) {
   const int field = blockIdx.y;
-  const int n = *count, nz = f.nz[field];
+  const int n = min(*count, max_n), nz = f.nz[field];  // the compact side holds max_n columns
   const float *src = f.src[field];
   float *dst = f.dst[field];
   const long long total = static_cast<long long>(n) * nz;
@@ -595,8 +595,8 @@ cudaError_t launch_sur_move_fields(const int *list, const int *count, int max_n,
   if (total == 0 || f.nfields == 0) return cudaSuccess;
   long long blocks = (total + 255) / 256;
   if (blocks > 4096) blocks = 4096;
-  move_fields_kernel<<<dim3(static_cast<unsigned>(blocks), f.nfields), 256, 0, s>>>(list, count, ny, f, to_compact,
-                                                                                     stride, offset);
+  move_fields_kernel<<<dim3(static_cast<unsigned>(blocks), f.nfields), 256, 0, s>>>(list, count, max_n, ny, f,
+                                                                                     to_compact, stride, offset);
   return cudaGetLastError();
 }
 
@@ -684,8 +684,8 @@ cudaError_t launch_sur_move_columns(const int *list, const int *count, int max_n
                                     float *dst, int to_compact, int stride, int offset, cudaStream_t s) {
   const long long total = static_cast<long long>(max_n) * nz;
   if (total == 0) return cudaSuccess;
-  move_columns_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(list, count, nz, ny, src, dst,
-                                                                                 to_compact, stride, offset);
+  move_columns_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(list, count, max_n, nz, ny, src,
+                                                                                 dst, to_compact, stride, offset);
   return cudaGetLastError();
 }
 

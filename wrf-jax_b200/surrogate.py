@@ -688,18 +688,27 @@ def _fallback_plan(st, n: int) -> _FallbackPlan:
     plan = _PLANS.get(key)
     if plan is None:
         plan = _FallbackPlan(st.nk, cap, lw_s, sw_s)
-        _PLANS.clear()  # keep one plan resident
+        while len(_PLANS) >= 2:  # keep the capacity plan and one exact-size plan resident
+            _PLANS.pop(next(iter(_PLANS)))
         _PLANS[key] = plan
     return plan
+
+
+# Columns the fallback re-solves without reading their number on the host;
+# when the gate rejects more, those steps take the synchronous path as well.
+FALLBACK_CAPACITY = 2048
 
 
 def _fallback(st, d: dict, flags, out: dict, before_scatter=None) -> int:
     """Re-solve the flagged columns with the plain kernels, writing their
     surrogate outputs over; returns how many columns were re-solved.  The
-    column count is read on the host (one synchronization); everything after
-    it reuses the buffers and argument blocks of a cached plan.  d and out
-    may hold page-locked host tensors, which the gather reads and the scatter
-    writes in place; before_scatter: an event the scatter waits for."""
+    gather, the LW and SW calls and the scatter are queued with the column
+    count left on the device (rrtmg_lwrad_live / rrtmg_swrad_live over a
+    compact domain of a fixed capacity); the count is read once at the end.
+    Steps with more rejected columns than the capacity re-solve all of them
+    again on a domain of the exact size.  d and out may hold page-locked host
+    tensors, which the gathers read and the scatters write in place;
+    before_scatter: an event the scatters wait for."""
     import torch
     lib = _capi.load()
     s = _stream()
@@ -713,16 +722,27 @@ def _fallback(st, d: dict, flags, out: dict, before_scatter=None) -> int:
     lst, cnt = _LISTS[key]
     cnt.zero_()
     _check(lib.rrtmg_sur_compact(flags.data_ptr(), ncol, lst.data_ptr(), cnt.data_ptr(), s), "compact")
+    plan = _fallback_plan(st, min(ncol, FALLBACK_CAPACITY))
+    _solve_listed(plan, lib, s, lst, cnt, ny, d, out, before_scatter, live=True)
     n = int(cnt.item())
-    if n == 0:
-        return 0
-    plan = _fallback_plan(st, n)
+    if n > plan.cap:
+        _solve_listed(_fallback_plan(st, n), lib, s, lst, cnt, ny, d, out, before_scatter, live=False, n=n)
+    return n
+
+
+def _solve_listed(plan, lib, s, lst, cnt, ny, d, out, before_scatter, *, live: bool, n: int | None = None) -> None:
+    """Gather the listed columns into the plan's compact domain, run LW (side
+    stream) and SW (current stream) on it, scatter the results back.  live:
+    the domain has plan.cap slots and the count stays on the device; else
+    exactly n columns."""
+    import torch
+    m = plan.cap if live else n
     for i, k in enumerate(plan.nz):
         plan.gather.src[i] = d[k].data_ptr()
-    _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), n, ny, ctypes.byref(plan.gather), 1, n, 0, s),
+    _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), m, ny, ctypes.byref(plan.gather), 1, m, 0, s),
            "gather")
-    plan.cfg_lw.ny = n
-    plan.cfg_sw.ny = n
+    plan.cfg_lw.ny = m
+    plan.cfg_sw.ny = m
     ctx = plan.ctx
     # LW on a side stream overlaps SW on the current stream; both read the
     # gathered fields, and the current stream waits for LW before the scatter.
@@ -730,10 +750,17 @@ def _fallback(st, d: dict, flags, out: dict, before_scatter=None) -> int:
     ready = torch.cuda.Event()
     ready.record(main)
     side.wait_event(ready)
-    ctx.check(ctx.lib.rrtmg_lwrad(ctx.handle, ctypes.byref(plan.cfg_lw), ctypes.byref(plan.cin_lw),
-                                  ctypes.byref(plan.cout_lw), ctypes.c_void_p(side.cuda_stream)))
-    ctx.check(ctx.lib.rrtmg_swrad(ctx.handle, ctypes.byref(plan.cfg_sw), ctypes.byref(plan.cin_sw),
-                                  ctypes.byref(plan.cout_sw), s))
+    side_s = ctypes.c_void_p(side.cuda_stream)
+    if live:
+        ctx.check(ctx.lib.rrtmg_lwrad_live(ctx.handle, ctypes.byref(plan.cfg_lw), ctypes.byref(plan.cin_lw),
+                                           ctypes.byref(plan.cout_lw), ctypes.c_void_p(cnt.data_ptr()), side_s))
+        ctx.check(ctx.lib.rrtmg_swrad_live(ctx.handle, ctypes.byref(plan.cfg_sw), ctypes.byref(plan.cin_sw),
+                                           ctypes.byref(plan.cout_sw), ctypes.c_void_p(cnt.data_ptr()), s))
+    else:
+        ctx.check(ctx.lib.rrtmg_lwrad(ctx.handle, ctypes.byref(plan.cfg_lw), ctypes.byref(plan.cin_lw),
+                                      ctypes.byref(plan.cout_lw), side_s))
+        ctx.check(ctx.lib.rrtmg_swrad(ctx.handle, ctypes.byref(plan.cfg_sw), ctypes.byref(plan.cin_sw),
+                                      ctypes.byref(plan.cout_sw), s))
     done = torch.cuda.Event()
     done.record(side)
     main.wait_event(done)
@@ -741,9 +768,8 @@ def _fallback(st, d: dict, flags, out: dict, before_scatter=None) -> int:
         main.wait_event(before_scatter)
     for i, (k, _, _) in enumerate(plan.scatter_src):
         plan.scatter.dst[i] = out[k].data_ptr()
-    _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), n, ny, ctypes.byref(plan.scatter), 0, n, 0, s),
+    _check(lib.rrtmg_sur_move_fields(lst.data_ptr(), cnt.data_ptr(), m, ny, ctypes.byref(plan.scatter), 0, m, 0, s),
            "scatter")
-    return n
 
 
 def heating_kday(rthraten, pi3d):
