@@ -160,3 +160,66 @@ def test_infer_host_equals_device_path(torch_cuda, model):
         assert n == ref.n_fallback and n > 0
         for k in S.OUTPUT_FIELDS:
             assert torch.equal(out[k], getattr(ref, k).cpu()), k
+
+
+def test_fallback_overflow_takes_the_exact_size_pass(torch_cuda, model):
+    """More rejected columns than the sync-free capacity: every one of them
+    still carries the plain kernels' bits."""
+    torch = torch_cuda
+    from wrf_jax_b200 import surrogate as S, synthetic
+    st = synthetic.make_columns(100, 100, S.NK, seed=8)
+    d = S._device_fields(st, "cuda")
+    res = S.infer(model, st, d, energy_tol=0.5, fallback=True)
+    lw, sw = S._plain(st, d)
+    torch.cuda.synchronize()
+    assert res.n_fallback > S.FALLBACK_CAPACITY
+    rej = (res.flags != 0).view(st.nx, st.ny)
+    assert int(rej.sum()) == res.n_fallback
+    m3 = rej[:, None, :].expand(st.nx, st.nk, st.ny)
+    assert torch.equal(res.rthratenlw[m3], lw.rthratenlw[m3])
+    assert torch.equal(res.rthratensw[m3], sw.rthratensw[m3])
+    assert torch.equal(res.lwupb[rej], lw.lwupb[rej]) and torch.equal(res.swupb[rej], sw.swupb[rej])
+
+
+def test_live_count_calls_match_full_calls(torch_cuda):
+    """rrtmg_lwrad_live / rrtmg_swrad_live with a device count below the
+    domain size: the counted columns equal the full call's, the others keep
+    what the output buffers held."""
+    torch = torch_cuda
+    from wrf_jax_b200 import _capi, rrtmg, surrogate as S, synthetic
+    st = synthetic.make_columns(1, 300, 47, seed=12)
+    d = S._device_fields(st, "cuda")
+    lw_ref, sw_ref = S._plain(st, d)
+    ctx = rrtmg.default_context()
+    live = torch.tensor([173], device="cuda", dtype=torch.int32)
+    lw_kw, sw_kw = st.lw_kwargs(), st.sw_kwargs()
+    scal = lambda kw, keys: {k: kw[k] for k in keys if k in kw}
+    cfg_lw = rrtmg.lw_config(1, 300, 47, **scal(lw_kw, S._SCALAR_KEYS_LW))
+    cfg_sw = rrtmg.sw_config(1, 300, 47, **scal(sw_kw, S._SCALAR_KEYS_SW))
+    lw_out = {k: torch.full(tuple(getattr(lw_ref, k).shape), -7.0, device="cuda") for k in _capi.LW_OUT_FIELDS}
+    sw_out = {k: torch.full(tuple(getattr(sw_ref, k).shape), -7.0, device="cuda") for k in _capi.SW_OUT_FIELDS}
+    s = torch.cuda.current_stream().cuda_stream
+    ctx.check(ctx.lib.rrtmg_lwrad_live(ctx.handle, ctypes.byref(cfg_lw),
+                                       ctypes.byref(_capi.LwIn(**{k: d[k].data_ptr() for k in _capi.LW_IN_FIELDS})),
+                                       ctypes.byref(_capi.LwOut(**{k: v.data_ptr() for k, v in lw_out.items()})),
+                                       ctypes.c_void_p(live.data_ptr()), ctypes.c_void_p(s)))
+    ctx.check(ctx.lib.rrtmg_swrad_live(ctx.handle, ctypes.byref(cfg_sw),
+                                       ctypes.byref(_capi.SwIn(**{k: d[k].data_ptr() for k in _capi.SW_IN_FIELDS})),
+                                       ctypes.byref(_capi.SwOut(**{k: v.data_ptr() for k, v in sw_out.items()})),
+                                       ctypes.c_void_p(live.data_ptr()), ctypes.c_void_p(s)))
+    torch.cuda.synchronize()
+    for name, ref, got in [(k, getattr(lw_ref, k), lw_out[k]) for k in _capi.LW_OUT_FIELDS] + \
+                          [(k, getattr(sw_ref, k), sw_out[k]) for k in _capi.SW_OUT_FIELDS]:
+        if got.dim() == 3:
+            assert torch.equal(got[:, :, :173], ref[:, :, :173]), name
+            assert bool((got[:, :, 173:] == -7.0).all()), name
+        else:
+            assert torch.equal(got[:, :173], ref[:, :173]), name
+            assert bool((got[:, 173:] == -7.0).all()), name
+    # a host pointer is refused before anything runs
+    host_count = ctypes.c_int(5)
+    st_code = ctx.lib.rrtmg_lwrad_live(ctx.handle, ctypes.byref(cfg_lw),
+                                       ctypes.byref(_capi.LwIn(**{k: d[k].data_ptr() for k in _capi.LW_IN_FIELDS})),
+                                       ctypes.byref(_capi.LwOut(**{k: v.data_ptr() for k, v in lw_out.items()})),
+                                       ctypes.cast(ctypes.byref(host_count), ctypes.c_void_p), ctypes.c_void_p(s))
+    assert st_code == 1
