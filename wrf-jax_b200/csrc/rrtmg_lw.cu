@@ -1338,7 +1338,8 @@ __device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int c
 
 // ---------------------------------------------------------------------------
 // g-point split schedule for small domains, in two launches.
-// lw_colprep_kernel: thread (column) computes the column set-up once.
+// lw_colprep_kernel: thread (column) computes the column set-up once;
+// lw_layer_kernel: thread (column, layer) the layer set-up (make_layer) once.
 // lw_optics_kernel: thread (column, layer, band) computes the layer's gas
 //   optics of the band (taumol), its Planck terms and the band cloud optical
 //   depth into a per-column record (kLwOpticsFloats per layer).
@@ -1368,6 +1369,21 @@ __device__ __forceinline__ const ColRec *col_records(const LwArgs &a) {
 }
 __device__ __forceinline__ float *layer_records(const LwArgs &a) {
   return a.optics + kColRecFloats * static_cast<size_t>(a.chunk_count);
+}
+// the layers' set-up (make_layer), computed once per column and layer
+constexpr size_t kLayerFloats = (sizeof(Layer) + 15) / 16 * 4;
+__device__ __forceinline__ Layer *layer_setups(const LwArgs &a) {
+  return reinterpret_cast<Layer *>(layer_records(a) +
+                                   static_cast<size_t>(kLwOpticsFloats) * a.nlay * static_cast<size_t>(a.chunk_count));
+}
+
+// thread = (column, layer): the layer's set-up for every band's optics
+__global__ void __launch_bounds__(128) lw_layer_kernel(Tables T, LwArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.chunk_count * a.nlay) return;
+  const int lc = t / a.nlay, l = t - lc * a.nlay;
+  if (dead_column(a.live, a.chunk_first + lc)) return;
+  layer_setups(a)[t] = make_layer(T, a, col_records(a)[lc].C, l);
 }
 
 // A warp per column: the lanes take the layers of the column integrals, whose
@@ -1447,7 +1463,7 @@ __global__ void __launch_bounds__(128) lw_optics_kernel(Tables T, LwArgs a) {
   const Col &C = col_records(a)[lc].C;
   uint32_t mask[kLwMaskWords];
   const bool cloudy = load_mask(a, l, col, mask);
-  const Layer L = make_layer(T, a, C, l);
+  const Layer &L = layer_setups(a)[t];
   float *rec = layer_records(a) + static_cast<size_t>(t) * kLwOpticsFloats;
   switch (band) {
     case 0: band_optics<0>(T, L, cloudy, C.iceflg, rec); break;
@@ -1755,7 +1771,7 @@ cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stre
 }
 
 size_t lw_optics_floats(int nlay, int ncol) {
-  return (static_cast<size_t>(kLwOpticsFloats) * nlay + kColRecFloats) * static_cast<size_t>(ncol);
+  return ((static_cast<size_t>(kLwOpticsFloats) + kLayerFloats) * nlay + kColRecFloats) * static_cast<size_t>(ncol);
 }
 
 cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream) {
@@ -1764,6 +1780,9 @@ cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stre
   cudaError_t e0 = cudaGetLastError();
   if (e0 != cudaSuccess) return e0;
   const long long layers = static_cast<long long>(a.chunk_count) * a.nlay;
+  lw_layer_kernel<<<static_cast<unsigned>((layers + threads - 1) / threads), threads, 0, stream>>>(T, a);
+  e0 = cudaGetLastError();
+  if (e0 != cudaSuccess) return e0;
   lw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kLwBands), threads, 0, stream>>>(
       T, a);
   cudaError_t e = cudaGetLastError();
