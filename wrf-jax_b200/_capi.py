@@ -112,6 +112,24 @@ class SurFields(ctypes.Structure):
     """rrtmg_sur_fields (include/rrtmg_surrogate.h)."""
     _fields_ = [("nfields", _I), ("src", _F * MAX_FIELDS), ("dst", _F * MAX_FIELDS), ("nz", _I * MAX_FIELDS)]
 
+class PrologueScalars(ctypes.Structure):
+    """rrtmg_prologue_scalars (include/rrtmg_prologue.h)."""
+    _fields_ = [("tloctm0", _FL), ("sin_declin", _FL), ("cos_declin", _FL), ("month_lo", _I), ("month_hi", _I),
+                ("fact_lo", _FL), ("fact_hi", _FL)]
+
+
+PROLOGUE_IN_FIELDS = ("qv3d", "qc3d", "qi3d", "qs3d", "t3d", "p3d", "xlat", "xlong")
+PROLOGUE_OUT_FIELDS = ("cldfra3d", "o33d", "coszr", "condensate_present")
+
+
+class PrologueIn(ctypes.Structure):
+    _fields_ = [(n, _F) for n in PROLOGUE_IN_FIELDS]
+
+
+class PrologueOut(ctypes.Structure):
+    _fields_ = [(n, _F) for n in PROLOGUE_OUT_FIELDS]
+
+
 STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
           4: "RRTMG_TIMEOUT"}
 
@@ -124,6 +142,8 @@ SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile
                      "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
                      "rrtmg_sur_compact", "rrtmg_sur_move_columns", "rrtmg_sur_timestamp",
                      "rrtmg_sur_pack_weights", "rrtmg_sur_mlp", "rrtmg_sur_move_fields")
+PROLOGUE_EXPORTS = ("rrtmg_radconst", "rrtmg_prologue_scalars_from_calendar", "rrtmg_set_ozone_climatology",
+                    "rrtmg_radiation_prologue", "rrtmg_cal_cldfra1", "rrtmg_calc_coszen", "rrtmg_cam_o3rad")
 
 _lib = None
 
@@ -189,6 +209,14 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_sur_mlp": [ctypes.POINTER(SurMlpArgs), V],
         "rrtmg_sur_move_fields": [P, P, I, I, ctypes.POINTER(SurFields), I, I, I, V],
         "rrtmg_set_schedule": [V, ctypes.POINTER(Schedule)],
+        "rrtmg_radconst": [ctypes.c_double, ctypes.POINTER(FL), ctypes.POINTER(FL)],
+        "rrtmg_prologue_scalars_from_calendar": [ctypes.c_double] * 4 + [ctypes.POINTER(PrologueScalars)],
+        "rrtmg_set_ozone_climatology": [V, P, I, P, I, P],
+        "rrtmg_radiation_prologue": [V, I, I, I, ctypes.POINTER(PrologueScalars), ctypes.POINTER(PrologueIn),
+                                     ctypes.POINTER(PrologueOut), V],
+        "rrtmg_cal_cldfra1": [V, I, I, I, P, P, P, P, P, P, P, V],
+        "rrtmg_calc_coszen": [V, I, I, P, P, ctypes.POINTER(PrologueScalars), P, V],
+        "rrtmg_cam_o3rad": [V, I, I, I, P, P, ctypes.POINTER(PrologueScalars), P, V],
         "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
     }
     for name, argtypes in sigs.items():

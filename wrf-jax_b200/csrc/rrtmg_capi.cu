@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/rrtmg_b200.h"
+#include "../../include/rrtmg_prologue.h"
 #include "rrtmg_device.cuh"
 #include "rrtmg_kernels.h"
 
@@ -51,6 +52,15 @@ struct rrtmg_ctx {
   std::vector<cudaEvent_t> events[2];
   int timing_next[2] = {0, 0};
   int timing_count[2] = {0, 0};
+  // radiation prologue: SVML sin/cos constants from the blob, and the CAM
+  // ozone climatology (plev, lat, then the (12, latsiz, levsiz) table in one
+  // allocation); replaced climatologies stay allocated until destroy because
+  // queued launches may still read them
+  SvmlConsts svml{};
+  bool have_svml = false;
+  float *ozone = nullptr;
+  int oz_levsiz = 0, oz_latsiz = 0;
+  std::vector<float *> retired_ozone;
 };
 
 namespace {
@@ -294,6 +304,14 @@ bool fill_tables(rrtmg_ctx *ctx, std::string &err) {
   T.expf_c0 = ep[1];
   T.expf_c1 = ep[2];
   T.expf_c2 = ep[3];
+  int ns = 0, nc = 0;
+  const float *ss = host_ptr<float>(ctx, "svml.sinf", &ns);
+  const float *sc = host_ptr<float>(ctx, "svml.cosf", &nc);
+  if (ss && sc && ns == 12 && nc == 14) {
+    std::memcpy(ctx->svml.s, ss, sizeof(ctx->svml.s));
+    std::memcpy(ctx->svml.c, sc, sizeof(ctx->svml.c));
+    ctx->have_svml = true;
+  }
   return true;
 }
 
@@ -479,6 +497,8 @@ void rrtmg_destroy(rrtmg_ctx *ctx) {
   cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
   for (auto &kv : ctx->jumps) cudaFree(kv.second);
+  cudaFree(ctx->ozone);
+  for (float *p : ctx->retired_ozone) cudaFree(p);
   cudaFree(ctx->dev_blob);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   for (auto &side : ctx->events)
@@ -954,4 +974,134 @@ extern "C" rrtmg_status rrtmg_get_schedule(const rrtmg_ctx *ctx, rrtmg_schedule 
   sch->sw_split_max_columns = ctx->sw_split_max;
   sch->lw_split_max_columns = ctx->lw_split_max;
   return RRTMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// radiation prologue (include/rrtmg_prologue.h)
+// ---------------------------------------------------------------------------
+extern "C" rrtmg_status rrtmg_set_ozone_climatology(rrtmg_ctx *ctx, const float *plev_pa, int levsiz,
+                                                    const float *lat, int latsiz, const float *ozone) {
+  if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
+  if (!plev_pa || !lat || !ozone) return fail(ctx, RRTMG_BAD_ARG, "null climatology array");
+  if (levsiz < 2 || levsiz > 128 || latsiz < 2 || latsiz > 256 || latsiz * levsiz > 12288)
+    return fail(ctx, RRTMG_BAD_ARG, "climatology size outside 2..128 levels, 2..256 latitudes, 12288 points");
+  for (int i = 0; i + 1 < levsiz; ++i)
+    if (!(plev_pa[i] < plev_pa[i + 1])) return fail(ctx, RRTMG_BAD_ARG, "ozone pressures must be ascending");
+  for (int i = 0; i + 1 < latsiz; ++i)
+    if (!(lat[i] < lat[i + 1])) return fail(ctx, RRTMG_BAD_ARG, "ozone latitudes must be ascending");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  const size_t tab = static_cast<size_t>(12) * latsiz * levsiz;
+  float *buf = nullptr;
+  e = cudaMalloc(&buf, sizeof(float) * (levsiz + latsiz + tab));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(ozone climatology)");
+  if ((e = cudaMemcpy(buf, plev_pa, sizeof(float) * levsiz, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(buf + levsiz, lat, sizeof(float) * latsiz, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(buf + levsiz + latsiz, ozone, sizeof(float) * tab, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaFree(buf);
+    return cuda_fail(ctx, e, "cudaMemcpy(ozone climatology)");
+  }
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  if (ctx->ozone) ctx->retired_ozone.push_back(ctx->ozone);
+  ctx->ozone = buf;
+  ctx->oz_levsiz = levsiz;
+  ctx->oz_latsiz = latsiz;
+  return RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_radiation_prologue(rrtmg_ctx *ctx, int nx, int nk, int ny,
+                                                 const rrtmg_prologue_scalars *sc, const rrtmg_prologue_in *in,
+                                                 rrtmg_prologue_out *out, void *stream_ptr) {
+  if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
+  if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
+  if (nx <= 0 || ny <= 0 || nk <= 0) return fail(ctx, RRTMG_BAD_ARG, "nx, nk and ny must be positive");
+  if (static_cast<long long>(nx) * ny > (1ll << 30)) return fail(ctx, RRTMG_BAD_ARG, "too many columns in one call");
+  const bool cld = out->cldfra3d, oz = out->o33d, cz = out->coszr, flag = out->condensate_present;
+  if (cld && any_null({in->qv3d, in->qc3d, in->qi3d, in->qs3d, in->t3d, in->p3d}))
+    return fail(ctx, RRTMG_BAD_ARG, "cloud fraction needs qv3d, qc3d, qi3d, qs3d, t3d and p3d");
+  if (flag && any_null({in->qc3d, in->qi3d, in->qs3d}))
+    return fail(ctx, RRTMG_BAD_ARG, "the condensate flag needs qc3d, qi3d and qs3d");
+  if (oz && any_null({in->xlat, in->p3d})) return fail(ctx, RRTMG_BAD_ARG, "ozone needs xlat and p3d");
+  if (cz && any_null({in->xlat, in->xlong})) return fail(ctx, RRTMG_BAD_ARG, "cos zenith needs xlat and xlong");
+  if ((oz || cz) && !sc) return fail(ctx, RRTMG_BAD_ARG, "ozone and cos zenith need the step scalars");
+  if (cz && !ctx->have_svml)
+    return fail(ctx, RRTMG_BAD_ARG, "the table blob has no SVML sin/cos constants (rebuild it)");
+  if (oz && (sc->month_lo < 0 || sc->month_lo > 11 || sc->month_hi < 0 || sc->month_hi > 11))
+    return fail(ctx, RRTMG_BAD_ARG, "ozone months must be in 0..11");
+  PrologueArgs a{};
+  a.nx = nx;
+  a.nk = nk;
+  a.ny = ny;
+  a.qv = in->qv3d; a.qc = in->qc3d; a.qi = in->qi3d; a.qs = in->qs3d; a.t = in->t3d; a.p = in->p3d;
+  a.xlat = in->xlat;
+  a.xlong = in->xlong;
+  a.cldfra = out->cldfra3d;
+  a.o33d = out->o33d;
+  a.coszr = out->coszr;
+  a.condensate = out->condensate_present;
+  if (sc) {
+    a.tloctm0 = sc->tloctm0;
+    a.sin_declin = sc->sin_declin;
+    a.cos_declin = sc->cos_declin;
+    a.month_lo = sc->month_lo;
+    a.month_hi = sc->month_hi;
+    a.fact_lo = sc->fact_lo;
+    a.fact_hi = sc->fact_hi;
+  }
+  bool have_ozone = false;
+  {
+    // fail() takes this mutex too: record under it, report after it
+    std::lock_guard<std::mutex> lk(ctx->mutex);
+    a.svml = ctx->svml;
+    have_ozone = ctx->ozone != nullptr;
+    if (oz && have_ozone) {
+      a.levsiz = ctx->oz_levsiz;
+      a.latsiz = ctx->oz_latsiz;
+      a.oz_plev = ctx->ozone;
+      a.oz_lat = ctx->ozone + a.levsiz;
+      a.oz_tab = ctx->ozone + a.levsiz + a.latsiz;
+    }
+  }
+  if (oz && !have_ozone) return fail(ctx, RRTMG_BAD_ARG, "no ozone climatology (rrtmg_set_ozone_climatology)");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  if (flag && (e = cudaMemsetAsync(out->condensate_present, 0, sizeof(int), stream)) != cudaSuccess)
+    return cuda_fail(ctx, e, "cudaMemsetAsync(condensate flag)");
+  e = launch_prologue(a, stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "prologue kernel launch");
+  return RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_cal_cldfra1(rrtmg_ctx *ctx, int nx, int nk, int ny, const float *qv, const float *qc,
+                                         const float *qi, const float *qs, const float *t_phy, const float *p_phy,
+                                         float *cldfra, void *stream) {
+  rrtmg_prologue_in in{};
+  in.qv3d = qv; in.qc3d = qc; in.qi3d = qi; in.qs3d = qs; in.t3d = t_phy; in.p3d = p_phy;
+  rrtmg_prologue_out out{};
+  out.cldfra3d = cldfra;
+  if (!cldfra) return fail(ctx, RRTMG_BAD_ARG, "null cldfra output");
+  return rrtmg_radiation_prologue(ctx, nx, nk, ny, nullptr, &in, &out, stream);
+}
+
+extern "C" rrtmg_status rrtmg_calc_coszen(rrtmg_ctx *ctx, int nx, int ny, const float *xlat, const float *xlong,
+                                         const rrtmg_prologue_scalars *sc, float *coszen, void *stream) {
+  rrtmg_prologue_in in{};
+  in.xlat = xlat;
+  in.xlong = xlong;
+  rrtmg_prologue_out out{};
+  out.coszr = coszen;
+  if (!coszen) return fail(ctx, RRTMG_BAD_ARG, "null coszen output");
+  return rrtmg_radiation_prologue(ctx, nx, 1, ny, sc, &in, &out, stream);
+}
+
+extern "C" rrtmg_status rrtmg_cam_o3rad(rrtmg_ctx *ctx, int nx, int nk, int ny, const float *xlat, const float *p3d,
+                                       const rrtmg_prologue_scalars *sc, float *o33d, void *stream) {
+  rrtmg_prologue_in in{};
+  in.xlat = xlat;
+  in.p3d = p3d;
+  rrtmg_prologue_out out{};
+  out.o33d = o33d;
+  if (!o33d) return fail(ctx, RRTMG_BAD_ARG, "null o33d output");
+  return rrtmg_radiation_prologue(ctx, nx, nk, ny, sc, &in, &out, stream);
 }

@@ -89,4 +89,28 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);
 size_t sw_split_terms_floats(int nk, int ncol);
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
+// Radiation prologue (cloud fraction, cos zenith, CAM ozone).  Constants of
+// the SVML sin/cos emulation in the reference's order (svml.sinf: 12,
+// svml.cosf: 14 values).
+struct SvmlConsts {
+  float s[12];
+  float c[14];
+};
+
+struct PrologueArgs {
+  int nx, nk, ny;
+  const float *qv, *qc, *qi, *qs, *t, *p;  // (nx, nk, ny)
+  const float *xlat, *xlong;               // (nx, ny)
+  float *cldfra, *o33d, *coszr;            // outputs; null: not computed
+  int *condensate;                         // null, or a zeroed device flag
+  float tloctm0, sin_declin, cos_declin;
+  SvmlConsts svml;
+  const float *oz_plev, *oz_lat, *oz_tab;  // device climatology: (levsiz), (latsiz), (12, latsiz, levsiz)
+  int levsiz, latsiz, month_lo, month_hi;
+  float fact_lo, fact_hi;
+};
+
+size_t prologue_smem_bytes(int levsiz, int latsiz);
+cudaError_t launch_prologue(const PrologueArgs &a, cudaStream_t stream);
+
 }  // namespace rrtmg

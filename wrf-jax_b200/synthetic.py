@@ -179,6 +179,46 @@ def make_columns(nx: int, ny: int, nk: int, *, seed: int = 0, t_noise: float = 2
     return ColumnState(fields=fields, scalars=scalars, nx=nx, ny=ny, nk=nk)
 
 
+
+def lat_lon(nx: int, ny: int, *, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """(xlat, xlong) in degrees on an (nx, ny) grid: latitudes U(-90, 90) and
+    longitudes U(-180, 180), float32."""
+    rng = np.random.default_rng(seed + 1000)
+    lat = rng.uniform(-90.0, 90.0, (nx, ny)).astype(np.float32)
+    lon = rng.uniform(-180.0, 180.0, (nx, ny)).astype(np.float32)
+    return lat, lon
+
+
+def cam_ozone_climatology(*, seed: int = 0, levsiz: int = 59, latsiz: int = 64):
+    """Seeded stand-in for a case's CAM ozone files (ozone_plev.formatted,
+    ozone_lat.formatted, ozone.formatted): ``levsiz`` pressure levels in hPa,
+    geometric from 0.35 to 1000 hPa; ``latsiz`` latitudes evenly spaced
+    within +-87.9 degrees; (12, latsiz, levsiz) volume mixing ratios, a
+    log-pressure Gaussian of 2-10 ppmv near 10 hPa varying with latitude and
+    month over a 20 ppbv floor, with 5 % multiplicative noise."""
+    rng = np.random.default_rng(seed + 2000)
+    plev = np.geomspace(0.35, 1000.0, levsiz).astype(np.float32)
+    lat = np.linspace(-87.9, 87.9, latsiz).astype(np.float32)
+    month = np.arange(12)[:, None, None]
+    phi = np.deg2rad(lat)[None, :, None]
+    lp = np.log(plev.astype(np.float64))[None, None, :]
+    peak = 6.0e-6 + 3.0e-6 * np.cos(phi) ** 2 + 1.0e-6 * np.sin(phi) * np.cos(2 * np.pi * month / 12)
+    oz = 2.0e-8 + peak * np.exp(-0.5 * ((lp - np.log(10.0)) / 1.1) ** 2)
+    oz *= rng.uniform(0.95, 1.05, oz.shape)
+    return plev, lat, oz.astype(np.float32)
+
+
+def write_cam_ozone_files(directory, plev_hpa, lat, ozone) -> None:
+    """Write a climatology in the three text files of a WRF case directory
+    (values exact in binary32: nine significant digits; one row per month and
+    latitude)."""
+    from pathlib import Path
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    np.savetxt(d / "ozone_plev.formatted", np.asarray(plev_hpa, np.float32), fmt="%.9e")
+    np.savetxt(d / "ozone_lat.formatted", np.asarray(lat, np.float32), fmt="%.9e")
+    np.savetxt(d / "ozone.formatted", np.asarray(ozone, np.float32).reshape(-1, np.shape(ozone)[-1]), fmt="%.9e")
+
 # Named workloads (grid sizes and spreads).
 WORKLOADS = {
     "cpu_64x64x44": dict(nx=64, ny=64, nk=44, seed=0),

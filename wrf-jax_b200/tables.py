@@ -102,6 +102,29 @@ def _glibc_math_tables(path: Path) -> dict:
     }
 
 
+
+def _svml_trig_constants(runtime_py: Path) -> dict:
+    """Constants of the four-lane SVML sin/cos emulation the zenith-angle code
+    uses (src/wrf_jax/runtime.py, ``_svml_sinf_np`` / ``_svml_cosf_np``): the
+    bit patterns passed to ``_svml_float32_from_bits_np`` in source order,
+    stored as binary32 (12 for sin, 14 for cos)."""
+    tree = ast.parse(runtime_py.read_text())
+    out = {}
+    for fname, key, count in (("_svml_sinf_np", "svml.sinf", 12), ("_svml_cosf_np", "svml.cosf", 14)):
+        node = next((n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == fname), None)
+        if node is None:
+            raise ValueError(f"{runtime_py}: {fname} not found")
+        calls = sorted(
+            (sub.lineno, sub.col_offset, int(sub.args[0].value)) for sub in ast.walk(node)
+            if isinstance(sub, ast.Call) and isinstance(sub.func, ast.Name)
+            and sub.func.id == "_svml_float32_from_bits_np" and sub.args
+            and isinstance(sub.args[0], ast.Constant))
+        bits = [b for _, _, b in calls]
+        if len(bits) != count:
+            raise ValueError(f"{fname}: expected {count} constants, found {len(bits)}")
+        out[key] = np.asarray(bits, np.uint32).view(np.float32).copy()
+    return out
+
 # ---------------------------------------------------------------------------
 # Fortran record parsing
 # ---------------------------------------------------------------------------
@@ -343,6 +366,7 @@ def build_tables(physics_dir: str | Path) -> dict:
     t["lw_buffer_tprof"] = f32(lwlit["_LW_BUFFER_TPROF"])
     t["sw.preflog"] = f32(swlit["_PREFLOG_VALUES"])
     t.update(_glibc_math_tables(phys.parent / "core" / "wrf_math.py"))
+    t.update(_svml_trig_constants(phys.parent / "runtime.py"))
     t["sw.tref"] = f32(swlit["_TREF_VALUES"])
 
     for side, counts, ngs, ngm, ngn, nb, first, records, fname in (
@@ -433,12 +457,24 @@ def read_blob(path: str | Path) -> dict:
 
 
 DEFAULT_BLOB = Path(__file__).resolve().parent / "data" / "rrtmg_tables.bin"
+# entries added after the first blob layout: a blob without them is rebuilt
+REQUIRED_ENTRIES = frozenset({"svml.sinf", "svml.cosf"})
+
+
+def _blob_names(path: Path) -> set:
+    try:
+        raw = Path(path).read_bytes()
+        _, count = struct.unpack_from("<II", raw, 8)
+        return {raw[16 + 88 * i:16 + 88 * i + 48].split(b"\0", 1)[0].decode() for i in range(count)}
+    except (OSError, struct.error, UnicodeDecodeError):
+        return set()
 
 
 def ensure_blob(physics_dir: str | Path | None = None, path: str | Path = DEFAULT_BLOB) -> Path:
-    """Build the blob from a WRF-JAX physics directory if it is not there yet."""
+    """Build the blob from a WRF-JAX physics directory if it is missing or lacks an entry
+    of REQUIRED_ENTRIES."""
     path = Path(path)
-    if path.exists():
+    if path.exists() and (physics_dir is None or REQUIRED_ENTRIES <= _blob_names(path)):
         return path
     if physics_dir is None:
         raise FileNotFoundError(
