@@ -14,7 +14,7 @@
 namespace rrtmg {
 namespace {
 
-constexpr int kPrologueThreads = 128;
+constexpr int kPrologueThreads = 256;
 
 // ---------------------------------------------------------------------------
 // sin / cos as the reference's zenith-angle code evaluates them
@@ -135,33 +135,31 @@ __device__ float glibc_sinf_cosf(float y, bool cosine) {
 // saturated.  One binary32 operation per reference operation; exp and power
 // are CUDA's expf/powf.
 __device__ __forceinline__ float cal_cldfra1(float qv, float qc, float qi, float qs, float t, float p) {
-  const float svpt0 = 273.15f;
   const float es0 = __fmul_rn(1000.0f, 0.61078f);
   const float ep_2 = static_cast<float>(287.0 / 461.6);
+  // the reference's final mask first: every other element is 0 whatever the
+  // intermediate values (the saturation terms of invalid T or p are never used)
   const bool valid = (t > 100.0f) & (p > 100.0f);
-  const float ts = valid ? t : svpt0;
-  const float tc = __fsub_rn(ts, svpt0);
-  float esw = __fmul_rn(es0, expf(__fdiv_rn(__fmul_rn(17.2693882f, tc), __fsub_rn(ts, 35.86f))));
-  float esi = __fmul_rn(es0, expf(__fdiv_rn(__fmul_rn(21.8745584f, tc), __fsub_rn(ts, 7.66f))));
-  esw = valid ? esw : 0.0f;
-  esi = valid ? esi : 0.0f;
-  const float dw = __fsub_rn(p, esw), di = __fsub_rn(p, esi);
-  const float qvsw = (valid & (dw > 1.0f)) ? __fdiv_rn(__fmul_rn(ep_2, esw), dw) : 0.0f;
-  const float qvsi = (valid & (di > 1.0f)) ? __fdiv_rn(__fmul_rn(ep_2, esi), di) : 0.0f;
   const float qcld = __fadd_rn(__fadd_rn(qi, qc), qs);
-  const bool cloudy = qcld >= 1.0e-12f;
-  const float w = cloudy ? __fdiv_rn(__fadd_rn(qi, qs), qcld) : 0.0f;
+  if (!(valid & (qcld >= 1.0e-12f))) return 0.0f;
+  const float tc = __fsub_rn(t, 273.15f);
+  const float esw = __fmul_rn(es0, expf(__fdiv_rn(__fmul_rn(17.2693882f, tc), __fsub_rn(t, 35.86f))));
+  const float esi = __fmul_rn(es0, expf(__fdiv_rn(__fmul_rn(21.8745584f, tc), __fsub_rn(t, 7.66f))));
+  const float dw = __fsub_rn(p, esw), di = __fsub_rn(p, esi);
+  const float qvsw = (dw > 1.0f) ? __fdiv_rn(__fmul_rn(ep_2, esw), dw) : 0.0f;
+  const float qvsi = (di > 1.0f) ? __fdiv_rn(__fmul_rn(ep_2, esi), di) : 0.0f;
+  const float w = __fdiv_rn(__fadd_rn(qi, qs), qcld);
   const float qvs = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, w), qvsw), __fmul_rn(w, qvsi));
-  const float rhum = (valid & (qvs > 0.0f)) ? __fdiv_rn(qv, qvs) : 0.0f;
+  const float rhum = (qvs > 0.0f) ? __fdiv_rn(qv, qvs) : 0.0f;
+  if (rhum >= 1.0f) return 1.0f;
   // numpy maximum keeps NaN; so do these selects
   float subsat = __fsub_rn(qvs, qv);
   subsat = (subsat < 1.0e-10f) ? 1.0e-10f : subsat;
   float arg = __fdiv_rn(__fmul_rn(-100.0f, qcld), powf(subsat, 0.49f));
   arg = (arg < -6.9f) ? -6.9f : arg;
   const float rpos = (rhum < 1.0e-10f) ? 1.0e-10f : rhum;
-  float partial = __fmul_rn(powf(rpos, 0.25f), __fsub_rn(1.0f, expf(arg)));
-  partial = (partial < 0.01f) ? 0.0f : partial;
-  return (valid & cloudy) ? ((rhum >= 1.0f) ? 1.0f : partial) : 0.0f;
+  const float partial = __fmul_rn(powf(rpos, 0.25f), __fsub_rn(1.0f, expf(arg)));
+  return (partial < 0.01f) ? 0.0f : partial;
 }
 
 // Index of the last entry < v in an ascending table (numpy searchsorted
@@ -189,7 +187,7 @@ struct OzoneColumn {
 };
 
 template <bool kCld, bool kOz, bool kCz, bool kFlag>
-__global__ void __launch_bounds__(kPrologueThreads)
+__global__ void __launch_bounds__(kPrologueThreads, 5)
 prologue_kernel(const PrologueArgs a) {
   extern __shared__ float smem[];
   float *s_plev = smem;                       // levsiz
@@ -254,18 +252,32 @@ prologue_kernel(const PrologueArgs a) {
     const size_t base = static_cast<size_t>(i) * a.nk * a.ny + j;
     const float ptop = kOz ? s_plev[0] : 0.0f;
     const float pbot = kOz ? s_plev[a.levsiz - 1] : 0.0f;
+    // pressure bracket, walked from the previous level's (levels go up, so
+    // it mostly stays or steps down), and the climatology at its two ends
+    int kk = kOz ? a.levsiz - 2 : 0, cached = -1;
+    float v_lo = 0.0f, v_hi = 0.0f;
+    constexpr bool kQ = kCld || kFlag, kP = kCld || kOz;
+    float n_qc = 0.0f, n_qi = 0.0f, n_qs = 0.0f, n_qv = 0.0f, n_t = 0.0f, n_p = 0.0f;
+    auto load = [&](size_t e) {
+      if (kQ) {
+        n_qc = __ldg(a.qc + e);
+        n_qi = __ldg(a.qi + e);
+        n_qs = __ldg(a.qs + e);
+      }
+      if (kCld) {
+        n_qv = __ldg(a.qv + e);
+        n_t = __ldg(a.t + e);
+      }
+      if (kP) n_p = __ldg(a.p + e);
+    };
+    load(base);
     for (int k = 0; k < a.nk; ++k) {
       const size_t e = base + static_cast<size_t>(k) * a.ny;
-      float qc = 0.0f, qi = 0.0f, qs = 0.0f;
-      if (kCld || kFlag) {
-        qc = __ldg(a.qc + e);
-        qi = __ldg(a.qi + e);
-        qs = __ldg(a.qs + e);
-      }
+      const float qc = n_qc, qi = n_qi, qs = n_qs, qv = n_qv, t = n_t, p = n_p;
+      if (k + 1 < a.nk) load(e + a.ny);
       if (kFlag)
         any_condensate |= ((__float_as_uint(qc) | __float_as_uint(qi) | __float_as_uint(qs)) & 0x7fffffffu) != 0u;
-      const float p = (kCld || kOz) ? __ldg(a.p + e) : 0.0f;
-      if (kCld) a.cldfra[e] = cal_cldfra1(__ldg(a.qv + e), qc, qi, qs, __ldg(a.t + e), p);
+      if (kCld) a.cldfra[e] = cal_cldfra1(qv, qc, qi, qs, t, p);
       if (kOz) {
         // runtime.py:5788-5801: pressure bracket, linear in pressure; above
         // the top level scaled by p / plev[0], below the bottom the last value
@@ -275,10 +287,22 @@ prologue_kernel(const PrologueArgs a) {
         } else if (p > pbot) {
           v = oz.at(a.levsiz - 1);
         } else {
-          const int kk = bracket(s_plev, a.levsiz, p);
+          // largest kk with plev[kk] < p, clamped to [0, levsiz-2]
+          while (kk > 0 && !(s_plev[kk] < p)) --kk;
+          while (kk < a.levsiz - 2 && s_plev[kk + 1] < p) ++kk;
+          if (kk != cached) {
+            if (kk == cached - 1) {
+              v_hi = v_lo;
+              v_lo = oz.at(kk);
+            } else {
+              v_lo = oz.at(kk);
+              v_hi = oz.at(kk + 1);
+            }
+            cached = kk;
+          }
           const float dpu = __fsub_rn(p, s_plev[kk]);
           const float dpl = __fsub_rn(s_plev[kk + 1], p);
-          const float num = __fadd_rn(__fmul_rn(oz.at(kk), dpl), __fmul_rn(oz.at(kk + 1), dpu));
+          const float num = __fadd_rn(__fmul_rn(v_lo, dpl), __fmul_rn(v_hi, dpu));
           v = __fdiv_rn(num, __fadd_rn(dpl, dpu));
         }
         a.o33d[e] = v;
@@ -317,7 +341,7 @@ cudaError_t launch_prologue(const PrologueArgs &a, cudaStream_t stream) {
   // the ozone tables are staged once per block: a persistent grid of a few
   // blocks per SM when they are needed, one thread per column otherwise
   const int need = (ncol + kPrologueThreads - 1) / kPrologueThreads;
-  const int blocks = oz ? std::min(need, sms * 6) : need;
+  const int blocks = oz ? std::min(need, sms * 5) : need;
   const int key = (cld ? 8 : 0) | (oz ? 4 : 0) | (cz ? 2 : 0) | (flag ? 1 : 0);
   switch (key) {
 #define RRTMG_PROLOGUE_CASE(K)                                                              \
