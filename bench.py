@@ -12,7 +12,9 @@ the surrogate path against the plain kernels and the fallback fraction.
 domain (180,625 columns) with per-launch kernel times and their roofline.
 
 `--workload prologue` measures the radiation prologue (cloud fraction, CAM
-ozone, cos zenith) on the 1000 x 1000 x 50 domain against the HBM roofline.
+ozone, cos zenith) on the 1000 x 1000 x 50 domain against the HBM roofline;
+`--workload tendency` the fused radiation tendency chain (LW + SW sum, mass
+coupling, accumulation into t_tendf) on 1000 x 51 x 1000 memory arrays.
 
 `e2e` repeats the step with host (numpy) inputs: the host->device copies of
 the inputs and the device->host copies of the outputs are inside the timed
@@ -680,13 +682,131 @@ def run_prologue(args):
         torch.distributed.destroy_process_group()
 
 
+def run_tendency(args):
+    """Radiation tendency chain (LW + SW heating, mass coupling over the tile,
+    accumulation into t_tendf) in one pass over a 1000 x 51 x 1000 memory
+    domain (WRF mass arrays: 50 levels plus the unused top slot), tile = the
+    whole domain.  HBM-bound: per element it reads rthratenlw, rthratensw and
+    rt_tendf and writes rthraten, and rt_tendf on the tile's levels (20 bytes,
+    16 on the unused top slot)."""
+    import torch
+
+    _package()
+    from wrf_jax_b200 import tendency as TD
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    nx = args.nx or 1000
+    ny = args.ny or 1000
+    nk = (args.nk or 50) + 1
+    b = dict(ids=1, ide=nx + 1, jds=1, jde=ny + 1, kds=1, kde=nk, ims=1, ime=nx, jms=1, jme=ny, kms=1, kme=nk,
+             its=1, ite=nx, jts=1, jte=ny, kts=1, kte=nk - 1)
+    tb = TD.bounds({}, **b)
+    rng = np.random.default_rng(5 + rank)
+    shape = (nx, nk, ny)
+    host = {
+        "lw": torch.from_numpy(rng.normal(-2e-5, 1e-5, shape).astype(np.float32)).pin_memory(),
+        "sw": torch.from_numpy(rng.normal(1e-5, 1e-5, shape).astype(np.float32)).pin_memory(),
+        "t": torch.from_numpy(rng.normal(0, 3, shape).astype(np.float32)).pin_memory(),
+    }
+    c1 = torch.from_numpy(rng.uniform(0, 1, nk).astype(np.float32)).cuda()
+    c2 = torch.from_numpy(rng.uniform(0, 5000, nk).astype(np.float32)).cuda()
+    mut = torch.from_numpy(rng.uniform(5e4, 9.5e4, (nx, ny)).astype(np.float32)).cuda()
+    dev = {k: v.cuda() for k, v in host.items()}
+    r = torch.empty(shape, device="cuda")
+    from wrf_jax_b200 import _capi
+    lib = _capi.load()
+
+    def step(src):
+        st = lib.rrtmg_radiation_tendency(ctypes.byref(tb), src["lw"].data_ptr(), src["sw"].data_ptr(),
+                                          c1.data_ptr(), c2.data_ptr(), mut.data_ptr(), 1, r.data_ptr(),
+                                          src["t"].data_ptr(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if st != 0:
+            raise RuntimeError(f"rrtmg_radiation_tendency failed: {st}")
+
+    for _ in range(max(3, args.warmup)):
+        step(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for a, b_ in ev:   # 1 GB of arrays per step: larger than L2
+            a.record()
+            step(dev)
+            b_.record()
+        t1.record()
+        torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    kernel_ms = statistics.median(a.elapsed_time(b_) for a, b_ in ev)
+    if ws > 1:
+        tt = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms = total_ms / args.steps
+    ncol = nx * ny
+    h_r = torch.empty(shape, pin_memory=True)
+    h_t = torch.empty(shape, pin_memory=True)
+    e2e_steps = args.e2e_steps or max(2, min(args.steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        step({k: v.cuda(non_blocking=True) for k, v in host.items()})
+        h_r.copy_(r, non_blocking=True)
+        h_t.copy_(dev["t"], non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    hbm, _, src = _peaks()
+    # reads lw, sw, rt_tendf and writes rthraten everywhere; rt_tendf is written
+    # back on the tile's levels only (kts..kde-1: not the unused top slot)
+    alg = nx * ny * (16 * nk + 4 * (nk - 1))
+    achieved = alg / (kernel_ms * 1e-3) / 1e9
+    line = {
+        "metric": "radiation tendency columns/s on 1 B200 (LW+SW sum, mass coupling, t_tendf accumulation)",
+        "value": ncol * ws / (ms / 1e3), "unit": "columns/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"tendency_{nx}x{nk}x{ny}", "memory_levels": nk, "columns_per_gpu": ncol,
+                   "l2": "arrays (1 GB) larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_source": src,
+                     "kernel": "tendency_kernel_vec4" if ny % 4 == 0 else "tendency_kernel",
+                     "algorithmic_bytes_per_column": 16 * nk + 4 * (nk - 1), "kernel_ms": kernel_ms},
+        "e2e": {"value": ncol / (e2e_ms / 1e3), "unit": "columns/s", "h2d_bytes_per_step": 3 * 4 * nx * nk * ny,
+                "d2h_bytes_per_step": 2 * 4 * nx * nk * ny},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(REPO / "oracle"))
+        import tendency_oracle as TO
+        rows = 100
+        bb = dict(b, ime=rows, ite=rows, ide=rows + 1)
+        lw, sw, tt = (host[k].numpy()[:rows] for k in ("lw", "sw", "t"))
+        t = time.perf_counter()
+        TO.radiation_tendency(lw, sw, c1.cpu().numpy(), c2.cpu().numpy(), mut.cpu().numpy()[:rows], tt, bb)
+        dt = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": rows * ny / dt, "unit": "columns/s", "cores": 1, "kind": "port",
+                                "sample": f"{rows} x {nk} x {ny} through the numpy oracle"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
-    ap.add_argument("--workload", choices=("surrogate", "plain", "ensemble", "prologue"), default="surrogate")
+    ap.add_argument("--workload", choices=("surrogate", "plain", "ensemble", "prologue", "tendency"), default="surrogate")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=None, help="override the plain domain (profiling cases)")
     ap.add_argument("--ny", type=int, default=None)
@@ -702,6 +822,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "prologue":
         run_prologue(args)
+    elif args.workload == "tendency":
+        run_tendency(args)
     else:
         run_surrogate(args)
 

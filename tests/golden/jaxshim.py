@@ -527,6 +527,16 @@ def _make_lax():
         return fn(*args)
 
     lax.platform_dependent = platform_dependent
+
+    def dynamic_update_slice(operand, update, start_indices):
+        # JAX clamps the start so that the update fits inside the operand
+        out = np.array(_plain(operand), copy=True)
+        upd = np.asarray(_plain(update))
+        starts = [min(max(int(s), 0), out.shape[d] - upd.shape[d]) for d, s in enumerate(start_indices)]
+        out[tuple(slice(s, s + n) for s, n in zip(starts, upd.shape))] = upd
+        return wrap(out)
+
+    lax.dynamic_update_slice = dynamic_update_slice
     lax.optimization_barrier = lambda x: x
 
     def bitcast_convert_type(x, new_dtype):

@@ -130,6 +130,13 @@ class PrologueOut(ctypes.Structure):
     _fields_ = [(n, _F) for n in PROLOGUE_OUT_FIELDS]
 
 
+class TendencyBounds(ctypes.Structure):
+    """rrtmg_tendency_bounds (include/rrtmg_tendency.h)."""
+    _fields_ = [(n, _I) for n in ("ids", "ide", "jds", "jde", "kds", "kde", "ims", "ime", "jms", "jme", "kms",
+                                  "kme", "its", "ite", "jts", "jte", "kts", "kte", "specified", "nested",
+                                  "periodic_x")]
+
+
 STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "RRTMG_CUDA",
           4: "RRTMG_TIMEOUT"}
 
@@ -144,6 +151,7 @@ SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile
                      "rrtmg_sur_pack_weights", "rrtmg_sur_mlp", "rrtmg_sur_move_fields")
 PROLOGUE_EXPORTS = ("rrtmg_radconst", "rrtmg_prologue_scalars_from_calendar", "rrtmg_set_ozone_climatology",
                     "rrtmg_radiation_prologue", "rrtmg_cal_cldfra1", "rrtmg_calc_coszen", "rrtmg_cam_o3rad")
+TENDENCY_EXPORTS = ("rrtmg_radiation_tendency", "rrtmg_phy_ra_ten")
 
 _lib = None
 
@@ -217,6 +225,8 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_cal_cldfra1": [V, I, I, I, P, P, P, P, P, P, P, V],
         "rrtmg_calc_coszen": [V, I, I, P, P, ctypes.POINTER(PrologueScalars), P, V],
         "rrtmg_cam_o3rad": [V, I, I, I, P, P, ctypes.POINTER(PrologueScalars), P, V],
+        "rrtmg_radiation_tendency": [ctypes.POINTER(TendencyBounds), P, P, P, P, P, I, P, P, V],
+        "rrtmg_phy_ra_ten": [ctypes.POINTER(TendencyBounds), P, P, V],
         "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
     }
     for name, argtypes in sigs.items():
