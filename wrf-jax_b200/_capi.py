@@ -152,6 +152,7 @@ SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile
 PROLOGUE_EXPORTS = ("rrtmg_radconst", "rrtmg_prologue_scalars_from_calendar", "rrtmg_set_ozone_climatology",
                     "rrtmg_radiation_prologue", "rrtmg_cal_cldfra1", "rrtmg_calc_coszen", "rrtmg_cam_o3rad")
 TENDENCY_EXPORTS = ("rrtmg_radiation_tendency", "rrtmg_phy_ra_ten")
+TABLES_EXPORTS = ("rrtmg_blob_with_wrf_data", "rrtmg_create_with_wrf_data")
 
 _lib = None
 
@@ -227,6 +228,8 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_cam_o3rad": [V, I, I, I, P, P, ctypes.POINTER(PrologueScalars), P, V],
         "rrtmg_radiation_tendency": [ctypes.POINTER(TendencyBounds), P, P, P, P, P, I, P, P, V],
         "rrtmg_phy_ra_ten": [ctypes.POINTER(TendencyBounds), P, P, V],
+        "rrtmg_blob_with_wrf_data": [ctypes.c_char_p] * 4,
+        "rrtmg_create_with_wrf_data": [ctypes.c_char_p] * 3 + [I, ctypes.POINTER(ctypes.c_void_p)],
         "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
     }
     for name, argtypes in sigs.items():

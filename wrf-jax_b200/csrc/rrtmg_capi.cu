@@ -95,6 +95,14 @@ rrtmg_status fail(rrtmg_ctx *ctx, rrtmg_status st, const std::string &msg) {
   return st;
 }
 
+}  // namespace
+
+rrtmg_status rrtmg::create_error(rrtmg_status status, const std::string &message) {
+  return fail(nullptr, status, message);
+}
+
+namespace {
+
 rrtmg_status cuda_fail(rrtmg_ctx *ctx, cudaError_t e, const char *what) {
   return fail(ctx, RRTMG_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }

@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
+#include "../../include/rrtmg_b200.h"
 #include "rrtmg_device.cuh"
 
 namespace rrtmg {
@@ -111,6 +114,9 @@ struct PrologueArgs {
 };
 
 size_t prologue_smem_bytes(int levsiz, int latsiz);
+
+// Records an error of a call without a context (text for rrtmg_last_error(NULL)).
+rrtmg_status create_error(rrtmg_status status, const std::string &message);
 cudaError_t launch_prologue(const PrologueArgs &a, cudaStream_t stream);
 
 }  // namespace rrtmg

@@ -103,6 +103,27 @@ class RrtmgContext:
             raise RrtmgError(st, self.lib.rrtmg_last_error(None).decode())
         self.handle = handle
 
+    @classmethod
+    def from_wrf_data(cls, lw_data, sw_data, base_blob=None, device: int | None = None) -> "RrtmgContext":
+        """A context whose absorption tables are read natively from the
+        reference's RRTMG_LW_DATA / RRTMG_SW_DATA files (include/rrtmg_tables.h);
+        the other tables come from ``base_blob`` (default: the package's blob)."""
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("rrtmg_b200 needs a CUDA device; there is no CPU fallback")
+        self = cls.__new__(cls)
+        self.lib = _capi.load()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        base = Path(base_blob) if base_blob is not None else tables.DEFAULT_BLOB
+        handle = ctypes.c_void_p()
+        st = self.lib.rrtmg_create_with_wrf_data(str(base).encode(), str(lw_data).encode(), str(sw_data).encode(),
+                                                 self.device, ctypes.byref(handle))
+        if st != 0:
+            raise RrtmgError(st, self.lib.rrtmg_last_error(None).decode())
+        self.handle = handle
+        return self
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self.lib.rrtmg_destroy(self.handle)

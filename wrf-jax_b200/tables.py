@@ -379,6 +379,7 @@ def build_tables(physics_dir: str | Path) -> dict:
         t[f"{side}.rwgt"] = rwgt
         t[f"{side}.ngc"] = i32(counts)
         t[f"{side}.ngs"] = i32(ngs)
+        t[f"{side}.ngn"] = i32(ngn)
         raw = _read_records(data / "rrtmg" / fname, records)
         for ib in range(nb):
             t.update(_compress(raw[first + ib], ib, counts, ngs, ngn, rwgt, f"{side}{first + ib}"))
@@ -458,7 +459,7 @@ def read_blob(path: str | Path) -> dict:
 
 DEFAULT_BLOB = Path(__file__).resolve().parent / "data" / "rrtmg_tables.bin"
 # entries added after the first blob layout: a blob without them is rebuilt
-REQUIRED_ENTRIES = frozenset({"svml.sinf", "svml.cosf"})
+REQUIRED_ENTRIES = frozenset({"svml.sinf", "svml.cosf", "lw.ngn", "sw.ngn"})
 
 
 def _blob_names(path: Path) -> set:
