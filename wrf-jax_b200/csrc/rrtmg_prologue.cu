@@ -206,10 +206,29 @@ prologue_kernel(const PrologueArgs a) {
   const int ncol = a.nx * a.ny;
   const float degrad = static_cast<float>(3.14159265358979323846 / 180.0);
   const int vec_rows = (a.nx / 4) * 4;
+  const int lane = threadIdx.x & 31;
   bool any_condensate = false;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += gridDim.x * blockDim.x) {
-    const int i = c / a.ny, j = c - i * a.ny;
-    if (kCz) {
+  // Cloudy levels (the only ones whose cloud fraction is not 0 by the final
+  // mask) are queued per warp and evaluated 32 at a time with every lane
+  // busy, instead of in place with most lanes idle: up to 63 element indices
+  // per warp (31 left over plus one level's 32).
+  __shared__ unsigned long long s_queue[kPrologueThreads / 32][64];
+  unsigned long long *q = s_queue[threadIdx.x >> 5];
+  int qn = 0;  // warp-uniform
+  auto drain = [&](int n) {
+    if (lane < n) {
+      const size_t e = q[lane];
+      a.cldfra[e] = cal_cldfra1(__ldg(a.qv + e), __ldg(a.qc + e), __ldg(a.qi + e), __ldg(a.qs + e),
+                                __ldg(a.t + e), __ldg(a.p + e));
+    }
+  };
+  // whole warps take the same columns' iterations (the queue is warp-synchronous)
+  for (int c0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); c0 < ncol; c0 += gridDim.x * blockDim.x) {
+    const int c = c0 + lane;
+    const bool live = c < ncol;
+    const int cc = live ? c : ncol - 1;  // in-range addresses for idle lanes; nothing stored for them
+    const int i = cc / a.ny, j = cc - i * a.ny;
+    if (kCz && live) {
       // runtime.py:6233-6243
       const float lat = __ldg(a.xlat + c), lon = __ldg(a.xlong + c);
       const float tloc = __fadd_rn(a.tloctm0, __fdiv_rn(lon, 15.0f));
@@ -236,7 +255,7 @@ prologue_kernel(const PrologueArgs a) {
     OzoneColumn oz;
     if (kOz) {
       // runtime.py:5767-5773: latitude bracket and offsets
-      const float lat = __ldg(a.xlat + c);
+      const float lat = __ldg(a.xlat + cc);
       const int li = bracket(s_lat, a.latsiz, lat);
       oz.dlat = __fsub_rn(lat, s_lat[li]);
       oz.span = __fsub_rn(s_lat[li + 1], s_lat[li]);
@@ -257,28 +276,43 @@ prologue_kernel(const PrologueArgs a) {
     int kk = kOz ? a.levsiz - 2 : 0, cached = -1;
     float v_lo = 0.0f, v_hi = 0.0f;
     constexpr bool kQ = kCld || kFlag, kP = kCld || kOz;
-    float n_qc = 0.0f, n_qi = 0.0f, n_qs = 0.0f, n_qv = 0.0f, n_t = 0.0f, n_p = 0.0f;
+    float n_qc = 0.0f, n_qi = 0.0f, n_qs = 0.0f, n_t = 0.0f, n_p = 0.0f;
     auto load = [&](size_t e) {
       if (kQ) {
         n_qc = __ldg(a.qc + e);
         n_qi = __ldg(a.qi + e);
         n_qs = __ldg(a.qs + e);
       }
-      if (kCld) {
-        n_qv = __ldg(a.qv + e);
-        n_t = __ldg(a.t + e);
-      }
+      if (kCld) n_t = __ldg(a.t + e);
       if (kP) n_p = __ldg(a.p + e);
     };
     load(base);
     for (int k = 0; k < a.nk; ++k) {
       const size_t e = base + static_cast<size_t>(k) * a.ny;
-      const float qc = n_qc, qi = n_qi, qs = n_qs, qv = n_qv, t = n_t, p = n_p;
+      const float qc = n_qc, qi = n_qi, qs = n_qs, t = n_t, p = n_p;
       if (k + 1 < a.nk) load(e + a.ny);
       if (kFlag)
-        any_condensate |= ((__float_as_uint(qc) | __float_as_uint(qi) | __float_as_uint(qs)) & 0x7fffffffu) != 0u;
-      if (kCld) a.cldfra[e] = cal_cldfra1(qv, qc, qi, qs, t, p);
-      if (kOz) {
+        any_condensate |= live && ((__float_as_uint(qc) | __float_as_uint(qi) | __float_as_uint(qs)) & 0x7fffffffu) != 0u;
+      if (kCld) {
+        // the final mask of runtime.py:5964 first: valid T and p, condensate >= 1e-12
+        bool heavy = false;
+        if (live) {
+          heavy = ((t > 100.0f) & (p > 100.0f)) && __fadd_rn(__fadd_rn(qi, qc), qs) >= 1.0e-12f;
+          if (!heavy) a.cldfra[e] = 0.0f;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, heavy);
+        if (heavy) q[qn + __popc(m & ((1u << lane) - 1u))] = e;
+        qn += __popc(m);
+        if (qn >= 32) {
+          __syncwarp();
+          drain(32);
+          __syncwarp();
+          if (lane < qn - 32) q[lane] = q[32 + lane];
+          qn -= 32;
+          __syncwarp();
+        }
+      }
+      if (kOz && live) {
         // runtime.py:5788-5801: pressure bracket, linear in pressure; above
         // the top level scaled by p / plev[0], below the bottom the last value
         float v;
@@ -309,7 +343,11 @@ prologue_kernel(const PrologueArgs a) {
       }
     }
   }
-  if (kFlag && __any_sync(0xffffffffu, any_condensate) && (threadIdx.x & 31) == 0) atomicOr(a.condensate, 1);
+  if (kCld) {
+    __syncwarp();
+    drain(qn);
+  }
+  if (kFlag && __any_sync(0xffffffffu, any_condensate) && lane == 0) atomicOr(a.condensate, 1);
 }
 
 template <bool kCld, bool kOz, bool kCz, bool kFlag>
