@@ -17,7 +17,10 @@ import pytest
 
 REPO = Path(__file__).resolve().parents[1]
 GOLDEN = REPO / "tests" / "golden"
-REFERENCE_PHYSICS = Path("/root/reference/src/wrf_jax/physics")
+# WRF-JAX sources (only used to build the table blob and the golden fixtures):
+# $WRF_JAX_REFERENCE, else a "reference" checkout beside this repository
+REFERENCE_ROOT = Path(os.environ.get("WRF_JAX_REFERENCE", str(Path(__file__).resolve().parents[2] / "reference")))
+REFERENCE_PHYSICS = REFERENCE_ROOT / "src" / "wrf_jax" / "physics"
 
 
 def load_package():

@@ -27,6 +27,7 @@ import ast
 import ctypes
 import ctypes.util
 import importlib.util
+import os
 import sys
 import tempfile
 from datetime import datetime
@@ -152,4 +153,5 @@ def main(reference_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "WRF_JAX_REFERENCE", str(Path(__file__).resolve().parents[3] / "reference")))

@@ -28,6 +28,7 @@ Output: tendency_golden.npz.
 from __future__ import annotations
 
 import ast
+import os
 import sys
 from collections.abc import Mapping
 from pathlib import Path
@@ -135,4 +136,5 @@ def main(reference_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "WRF_JAX_REFERENCE", str(Path(__file__).resolve().parents[3] / "reference")))

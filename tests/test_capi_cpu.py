@@ -59,3 +59,30 @@ def test_create_rejects_missing_blob(pkg):
     st = lib.rrtmg_create(b"/nonexistent/blob.bin", 0, ctypes.byref(h))
     assert st == 1  # RRTMG_BAD_ARG, before any CUDA call
     assert b"cannot open" in lib.rrtmg_last_error(None)
+
+
+def _one_entry_blob(dtype: int, ndim: int, shape, offset: int, nbytes: int, payload: bytes = b"") -> bytes:
+    import struct
+    head = b"RRTMGB2\0" + struct.pack("<II", 1, 1)
+    entry = b"x".ljust(48, b"\0") + struct.pack("<II4IQQ", dtype, ndim, *shape, offset, nbytes)
+    return head + entry + payload
+
+
+@pytest.mark.parametrize("desc,blob", [
+    # offset + nbytes wraps past 2**64: must not pass the range check
+    ("wrapping range", _one_entry_blob(0, 1, (4, 1, 1, 1), 104, 2**64 - 8, b"\0" * 16)),
+    # inside the buffer, but nbytes is not 4 * (3 x 2) floats
+    ("size vs shape", _one_entry_blob(0, 2, (3, 2, 1, 1), 104, 16, b"\0" * 16)),
+    ("unknown dtype", _one_entry_blob(7, 1, (4, 1, 1, 1), 104, 16, b"\0" * 16)),
+])
+def test_create_rejects_malformed_blob_before_any_cuda_call(pkg, desc, blob):
+    """rrtmg_create_from_memory parses the blob on the host first; a malformed
+    entry is RRTMG_BAD_ARG, never an out-of-range read."""
+    from wrf_jax_b200 import _capi
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    buf = ctypes.create_string_buffer(blob, len(blob))
+    st = lib.rrtmg_create_from_memory(buf, len(blob), 0, ctypes.byref(h))
+    assert st == 1, desc
+    msg = lib.rrtmg_last_error(None)
+    assert b"table entry" in msg, (desc, msg)

@@ -97,3 +97,24 @@ def test_gather_rejects_more_ranks_than_batches(pkg):
     assert sharding.rank_rows(3, 4, 3) == (3, 3)
     assert sharding.slice_rows(np.zeros((2, 5, 3)), 2, 3, 1, 2).shape == (2, 5, 1)
     assert sharding.slice_rows(np.zeros((2, 3)), 2, 3, 0, 2).shape == (2, 2)
+
+
+@pytest.mark.gpu
+def test_rank_slabs_on_one_gpu_equal_whole_domain(pkg):
+    """The CUDA kernels through sharded_call: both ranks' row ranges of a
+    two-rank split (run one after the other on one GPU, gather=False, so no
+    process group is needed) concatenated in row order equal the whole-domain
+    call bit for bit."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from wrf_jax_b200 import rrtmg, sharding, synthetic
+    st = synthetic.make_columns(12, 9, 44, seed=23, fractional_clouds=True)
+    for call, kw in ((rrtmg.rrtmg_lwrad_wrf_columns, st.lw_kwargs()), (rrtmg.rrtmg_swrad_wrf_columns, st.sw_kwargs())):
+        whole = call(**kw)._asdict()
+        slabs = [sharding.sharded_call(call, kw, rank=r, world=2, rows_per_batch=2, gather=False, device=0)
+                 for r in range(2)]
+        assert slabs[0][0][0] == 0 and slabs[0][0][1] == slabs[1][0][0] and slabs[1][0][1] == 9
+        for name, value in whole.items():
+            got = np.concatenate([np.asarray(s[1][name]) for s in slabs], axis=-1)
+            np.testing.assert_array_equal(got, value, err_msg=name)

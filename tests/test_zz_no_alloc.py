@@ -72,6 +72,23 @@ def test_static_scratch_matches_allocating_call_twice(env, pkg, nx, ny, nk, seed
     _assert_same(second, ref, "second call")
 
 
+def test_static_scratch_alternating_layer_counts(env, pkg):
+    """Calls with different model tops (so different LW layer counts) in turn:
+    each selects its own slot of the jump table written at set-up, nothing is
+    copied per call, and every call equals rrtmg_lwrad bit for bit."""
+    from wrf_jax_b200 import synthetic
+    a = synthetic.make_columns(20, 12, 50, seed=31, fractional_clouds=True)               # p_top 50 hPa: nlay 63
+    b = synthetic.make_columns(20, 12, 50, seed=32, fractional_clouds=True, p_top=1000.0)  # nlay 53
+    ctx = env[0]
+    assert ctx.lib.rrtmg_lw_nlayers(float(a.lw_kwargs()["p_top"]), 50) != \
+        ctx.lib.rrtmg_lw_nlayers(float(b.lw_kwargs()["p_top"]), 50)
+    ref_a = _device_call(env, a, "rrtmg_lwrad")
+    ref_b = _device_call(env, b, "rrtmg_lwrad")
+    for rep in range(2):
+        _assert_same(_device_call(env, a, "rrtmg_lwrad_static_scratch"), ref_a, f"round {rep} top 50 hPa")
+        _assert_same(_device_call(env, b, "rrtmg_lwrad_static_scratch"), ref_b, f"round {rep} top 10 hPa")
+
+
 def test_static_scratch_rejects_domain_beyond_capacity(env, pkg):
     ctx, _capi, torch = env
     nk, p_top = 50, 5000.0

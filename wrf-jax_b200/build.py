@@ -21,7 +21,7 @@ LIB = HERE / "librrtmg_b200.so"
 SOURCES = ("rrtmg_capi.cu", "rrtmg_mcica.cu", "rrtmg_lw.cu", "rrtmg_sw.cu", "surrogate_gemm.cu",
            "surrogate_ops.cu", "surrogate_capi.cu", "surrogate_mlp.cu", "rrtmg_prologue.cu",
            "rrtmg_tendency.cu", "rrtmg_tables.cu")
-HEADERS = ("rrtmg_device.cuh", "rrtmg_kernels.h", "surrogate_kernels.h", "umma_common.cuh")
+HEADERS = ("rrtmg_device.cuh", "rrtmg_kernels.h", "surrogate_kernels.h", "umma_common.cuh", "kiss_jump_host.h")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-ftz=false",

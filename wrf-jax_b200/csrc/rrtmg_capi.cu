@@ -16,6 +16,7 @@
 #include "../../include/rrtmg_prologue.h"
 #include "rrtmg_device.cuh"
 #include "rrtmg_kernels.h"
+#include "kiss_jump_host.h"
 
 using namespace rrtmg;
 
@@ -107,6 +108,19 @@ rrtmg_status cuda_fail(rrtmg_ctx *ctx, cudaError_t e, const char *what) {
   return fail(ctx, RRTMG_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// nbytes equals the element size of dtype (0 f32, 1 i32, 2 f64, 3 u64) times
+// the product of the first ndim extents (ndim <= 4).
+bool entry_size_matches(uint32_t dtype, uint32_t ndim, const uint32_t *shape, uint64_t nbytes) {
+  static const uint64_t kSize[4] = {4, 4, 8, 8};
+  if (dtype > 3 || ndim > 4) return false;
+  uint64_t count = 1;
+  for (uint32_t d = 0; d < ndim; ++d) {
+    if (shape[d] != 0 && count > UINT64_MAX / 8 / shape[d]) return false;
+    count *= shape[d];
+  }
+  return count * kSize[dtype] == nbytes;
+}
+
 bool parse_blob(rrtmg_ctx *ctx, std::string &err) {
   const auto &raw = ctx->host_blob;
   if (raw.size() < 16 || std::memcmp(raw.data(), "RRTMGB2\0", 8) != 0) {
@@ -134,8 +148,12 @@ bool parse_blob(rrtmg_ctx *ctx, std::string &err) {
     std::memcpy(e.shape, raw.data() + pos + 56, 16);
     std::memcpy(&e.offset, raw.data() + pos + 72, 8);
     std::memcpy(&e.nbytes, raw.data() + pos + 80, 8);
-    if (e.offset + e.nbytes > raw.size()) {
+    if (e.offset > raw.size() || e.nbytes > raw.size() - e.offset) {
       err = std::string("table entry out of range: ") + name;
+      return false;
+    }
+    if (!entry_size_matches(e.dtype, e.ndim, e.shape, e.nbytes)) {
+      err = std::string("table entry size does not match its shape and type: ") + name;
       return false;
     }
     ctx->entries[name] = e;
@@ -323,42 +341,6 @@ bool fill_tables(rrtmg_ctx *ctx, std::string &err) {
   return true;
 }
 
-// Jump of `k` KISS steps (module_ra_rrtmg_common.py:1008-1064).
-KissJump make_jump(uint64_t k) {
-  KissJump J{};
-  uint32_t mul = 1, add = 0;
-  uint32_t basis[32];
-  for (int b = 0; b < 32; ++b) basis[b] = 1u << b;
-  for (uint64_t s = 0; s < k; ++s) {
-    mul = 69069u * mul;
-    add = 69069u * add + 1327217885u;
-    for (int b = 0; b < 32; ++b) {
-      uint32_t x = basis[b];
-      x ^= x << 13;
-      x ^= x >> 17;
-      x ^= x << 5;
-      basis[b] = x;
-    }
-  }
-  J.lcg_mul = mul;
-  J.lcg_add = add;
-  for (int b = 0; b < 32; ++b) J.xs[b] = basis[b];
-  auto powmod = [](uint64_t a, uint64_t e, uint64_t m) {
-    uint64_t r = 1 % m, base = a % m;
-    while (e) {
-      if (e & 1) r = (r * base) % m;
-      base = (base * base) % m;
-      e >>= 1;
-    }
-    return r;
-  };
-  const uint64_t e = k >= 2 ? k - 2 : 0;
-  J.mwc3_pow = static_cast<uint32_t>(powmod(18000, e, 18000ull * 65536 - 1));
-  J.mwc4_pow = static_cast<uint32_t>(powmod(30903, e, 30903ull * 65536 - 1));
-  J.steps = static_cast<uint32_t>(k);
-  return J;
-}
-
 rrtmg_status get_jumps(rrtmg_ctx *ctx, int nlay, int nsub, int skip, const KissJump **out) {
   std::lock_guard<std::mutex> lk(ctx->mutex);
   auto key = std::make_tuple(nlay, nsub, skip);
@@ -367,9 +349,9 @@ rrtmg_status get_jumps(rrtmg_ctx *ctx, int nlay, int nsub, int skip, const KissJ
     *out = it->second;
     return RRTMG_OK;
   }
-  // offsets skip + g * nlay, built incrementally
+  // offsets skip + g * nlay
   std::vector<KissJump> host(nsub);
-  for (int g = 0; g < nsub; ++g) host[g] = make_jump(static_cast<uint64_t>(skip) + static_cast<uint64_t>(g) * nlay);
+  kiss_jumps(static_cast<uint64_t>(skip), nlay, nsub, host.data());
   KissJump *dev = nullptr;
   cudaError_t e = cudaMalloc(&dev, sizeof(KissJump) * nsub);
   if (e != cudaSuccess) {
@@ -393,7 +375,8 @@ rrtmg_status finish_create(rrtmg_ctx *ctx, int device, rrtmg_ctx **out) {
     delete ctx;
     return fail(nullptr, RRTMG_BAD_ARG, err);
   }
-  cudaError_t e = cudaSetDevice(device);
+  DeviceGuard guard(device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) {
     delete ctx;
     return cuda_fail(nullptr, e, "cudaSetDevice");
@@ -500,9 +483,7 @@ rrtmg_status rrtmg_create(const char *path, int device, rrtmg_ctx **out) {
 
 void rrtmg_destroy(rrtmg_ctx *ctx) {
   if (!ctx) return;
-  int prev = 0;
-  cudaGetDevice(&prev);
-  cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
   cudaDeviceSynchronize();
   for (auto &kv : ctx->jumps) cudaFree(kv.second);
   cudaFree(ctx->ozone);
@@ -511,7 +492,6 @@ void rrtmg_destroy(rrtmg_ctx *ctx) {
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   for (auto &side : ctx->events)
     for (cudaEvent_t ev : side) cudaEventDestroy(ev);
-  cudaSetDevice(prev);
   delete ctx;
 }
 
@@ -554,7 +534,8 @@ static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   if (icld >= 1 && (inflg < 2 || iceflg < 3 || liqflg != 1))
     return fail(ctx, RRTMG_UNSUPPORTED_OPTION, "cloud optics option not supported by cldprmc_lw");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   const int ncol = cfg->nx * cfg->ny;
   const KissJump *jumps = nullptr;
@@ -668,7 +649,8 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   if (icld >= 1 && (inflg < 2 || iceflg < 3 || liqflg != 1))
     return fail(ctx, RRTMG_UNSUPPORTED_OPTION, "cloud optics option not supported by cldprmc_sw");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   const int ncol = cfg->nx * cfg->ny;
   const KissJump *jumps = nullptr;
@@ -792,34 +774,52 @@ rrtmg_status rrtmg_swrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrt
 //
 // Scratch: g_static_mask holds kStaticMaskWords 32-bit words (32 MiB); a call
 // needs nlay * 5 * nx * ny of them and is rejected with RRTMG_BAD_ARG above
-// that.  g_static_jumps holds the 140 KISS jumps for the call's nlay; they are
-// uploaded (a plain copy from a static host table) only when nlay differs from
-// the last upload on that device.  Nothing has to start at zero: the McICA
-// kernel writes every mask word the LW kernel then reads.
+// that.  g_static_jumps holds the 140 KISS jumps of every layer count the
+// kernels accept (slot nlay, 2.7 MB); they are written once per device, so a
+// call only selects its slot and copies nothing.  Nothing has to start at
+// zero: the McICA kernel writes every mask word the LW kernel then reads.
 //
-// Set-up: the first call on each device looks up both symbols with that
-// device current (cudaGetSymbolAddress); that first call should come before
-// any stream capture begins.  The scratch is shared by every context and
-// stream on a device, so calls that overlap in time on one device race.
+// Set-up: the first call on each device, with that device current, looks up
+// both symbols (cudaGetSymbolAddress) and fills the jump table with one
+// synchronous copy; that first call should come before any stream capture
+// begins.  Later calls, with any nlay, enqueue only the two kernels.  The
+// scratch is shared by every context and stream on a device, so calls that
+// overlap in time on one device race.
 namespace {
 
 constexpr size_t kStaticMaskWords = size_t(8) << 20;  // 32 MiB of mask words
 constexpr int kStaticMaxDevices = 64;
+constexpr int kStaticMinLay = 4;  // nlay >= nk >= 4
 
 __device__ __align__(256) uint32_t g_static_mask[kStaticMaskWords];
-__device__ __align__(256) KissJump g_static_jumps[kLwGpts];
+__device__ __align__(256) KissJump g_static_jumps[kMaxLay + 1][kLwGpts];
 
 struct StaticScratch {
   bool ready = false;
   uint32_t *mask = nullptr;
-  KissJump *jumps = nullptr;
-  int loaded_nlay = -1;  // nlay of the jumps last enqueued into g_static_jumps
+  KissJump *jumps = nullptr;  // slot nlay at jumps + nlay * kLwGpts
 };
 
 std::mutex g_static_mutex;
 StaticScratch g_static_scratch[kStaticMaxDevices];
-KissJump g_static_host_jumps[kMaxLay + 1][kLwGpts];  // host copies per nlay (static storage)
-bool g_static_host_built[kMaxLay + 1];
+
+// One-time set-up of the current device's scratch (caller holds g_static_mutex).
+cudaError_t static_scratch_setup(StaticScratch &s) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_static_mask);
+  if (e != cudaSuccess) return e;
+  s.mask = static_cast<uint32_t *>(p);
+  e = cudaGetSymbolAddress(&p, g_static_jumps);
+  if (e != cudaSuccess) return e;
+  s.jumps = static_cast<KissJump *>(p);
+  std::vector<KissJump> host(static_cast<size_t>(kMaxLay + 1) * kLwGpts, KissJump{});
+  for (int nlay = kStaticMinLay; nlay <= kMaxLay; ++nlay)
+    kiss_jumps(150ull, nlay, kLwGpts, host.data() + static_cast<size_t>(nlay) * kLwGpts);
+  e = cudaMemcpy(s.jumps, host.data(), host.size() * sizeof(KissJump), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  s.ready = true;
+  return cudaSuccess;
+}
 
 }  // namespace
 
@@ -854,7 +854,8 @@ extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_c
   if (ctx->device < 0 || ctx->device >= kStaticMaxDevices)
     return fail(ctx, RRTMG_BAD_ARG, "device ordinal beyond the static scratch's device slots");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
 
   uint32_t *mask = nullptr;
@@ -863,29 +864,11 @@ extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_c
     std::lock_guard<std::mutex> lk(g_static_mutex);
     StaticScratch &s = g_static_scratch[ctx->device];
     if (!s.ready) {  // once per device, with that device current
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_static_mask);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(static mcica mask)");
-      s.mask = static_cast<uint32_t *>(p);
-      e = cudaGetSymbolAddress(&p, g_static_jumps);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(static jump table)");
-      s.jumps = static_cast<KissJump *>(p);
-      s.ready = true;
-    }
-    if (!g_static_host_built[nlay]) {
-      for (int g = 0; g < kLwGpts; ++g)
-        g_static_host_jumps[nlay][g] = make_jump(150ull + static_cast<uint64_t>(g) * nlay);
-      g_static_host_built[nlay] = true;
-    }
-    if (s.loaded_nlay != nlay) {
-      s.loaded_nlay = -1;
-      e = cudaMemcpyAsync(s.jumps, g_static_host_jumps[nlay], sizeof(KissJump) * kLwGpts, cudaMemcpyHostToDevice,
-                          stream);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(static jump table)");
-      s.loaded_nlay = nlay;
+      e = static_scratch_setup(s);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "static McICA scratch set-up");
     }
     mask = s.mask;
-    jumps = s.jumps;
+    jumps = s.jumps + static_cast<size_t>(nlay) * kLwGpts;
   }
 
   McicaArgs m{};
@@ -916,7 +899,8 @@ extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_c
 
 extern "C" rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable) {
   if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   std::lock_guard<std::mutex> lk(ctx->mutex);
   if (enable && ctx->events[0].empty()) {
@@ -939,7 +923,8 @@ extern "C" rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable) {
 
 extern "C" int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_calls) {
   if (!ctx || side < 0 || side > 1 || !ms || max_calls <= 0) return -1;
-  if (cudaSetDevice(ctx->device) != cudaSuccess) return -1;
+  DeviceGuard guard(ctx->device);
+  if (guard.status() != cudaSuccess) return -1;
   std::lock_guard<std::mutex> lk(ctx->mutex);
   const int count = ctx->timing_count[side] < max_calls ? ctx->timing_count[side] : max_calls;
   const int newest = (ctx->timing_next[side] + kTimingSlots - 1) % kTimingSlots;
@@ -997,7 +982,8 @@ extern "C" rrtmg_status rrtmg_set_ozone_climatology(rrtmg_ctx *ctx, const float 
     if (!(plev_pa[i] < plev_pa[i + 1])) return fail(ctx, RRTMG_BAD_ARG, "ozone pressures must be ascending");
   for (int i = 0; i + 1 < latsiz; ++i)
     if (!(lat[i] < lat[i + 1])) return fail(ctx, RRTMG_BAD_ARG, "ozone latitudes must be ascending");
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   const size_t tab = static_cast<size_t>(12) * latsiz * levsiz;
   float *buf = nullptr;
@@ -1072,7 +1058,8 @@ extern "C" rrtmg_status rrtmg_radiation_prologue(rrtmg_ctx *ctx, int nx, int nk,
   }
   if (oz && !have_ozone) return fail(ctx, RRTMG_BAD_ARG, "no ozone climatology (rrtmg_set_ozone_climatology)");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   if (flag && (e = cudaMemsetAsync(out->condensate_present, 0, sizeof(int), stream)) != cudaSuccess)
     return cuda_fail(ctx, e, "cudaMemsetAsync(condensate flag)");

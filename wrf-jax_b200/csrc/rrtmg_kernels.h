@@ -115,6 +115,32 @@ struct PrologueArgs {
 
 size_t prologue_smem_bytes(int levsiz, int latsiz);
 
+// Makes `device` current for the guard's lifetime and restores the caller's
+// current device when it goes out of scope, so an entry point leaves the
+// calling thread's device as it found it.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&prev_) != cudaSuccess) {
+      cudaGetLastError();
+      prev_ = -1;
+    }
+    status_ = prev_ == device ? cudaSuccess : cudaSetDevice(device);
+    switched_ = status_ == cudaSuccess && prev_ >= 0 && prev_ != device;
+  }
+  ~DeviceGuard() {
+    if (switched_) cudaSetDevice(prev_);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+  cudaError_t status() const { return status_; }
+
+ private:
+  int prev_ = -1;
+  bool switched_ = false;
+  cudaError_t status_ = cudaSuccess;
+};
+
 // Records an error of a call without a context (text for rrtmg_last_error(NULL)).
 rrtmg_status create_error(rrtmg_status status, const std::string &message);
 cudaError_t launch_prologue(const PrologueArgs &a, cudaStream_t stream);

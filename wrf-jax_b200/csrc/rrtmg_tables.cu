@@ -178,8 +178,19 @@ bool parse_blob(const std::vector<unsigned char> &raw, Blob &blob, std::string &
     std::memcpy(shape, raw.data() + pos + 56, 16);
     std::memcpy(&offset, raw.data() + pos + 72, 8);
     std::memcpy(&nbytes, raw.data() + pos + 80, 8);
-    if (ndim > 4 || offset + nbytes > raw.size()) {
+    if (ndim > 4 || e.dtype > 3 || offset > raw.size() || nbytes > raw.size() - offset) {
       err = std::string("bad table entry ") + name;
+      return false;
+    }
+    // nbytes must equal the element size (f32, i32: 4; f64, u64: 8) times the extents
+    uint64_t count = 1;
+    bool overflow = false;
+    for (uint32_t d = 0; d < ndim; ++d) {
+      if (shape[d] != 0 && count > UINT64_MAX / 8 / shape[d]) overflow = true;
+      count *= shape[d];
+    }
+    if (overflow || count * (e.dtype >= 2 ? 8u : 4u) != nbytes) {
+      err = std::string("table entry size does not match its shape and type: ") + name;
       return false;
     }
     e.shape.assign(shape, shape + ndim);

@@ -95,12 +95,25 @@ def max_over_ranks(value: float, group=None, device=None) -> float:
 
 
 def sharded_call(call: Callable[..., Any], kwargs: Mapping[str, Any], *, rank: int, world: int,
-                 rows_per_batch: int = 1, gather: bool = True, group=None):
+                 rows_per_batch: int = 1, gather: bool = True, group=None, device: int | None = None):
     """Run ``call`` (e.g. ``rrtmg.rrtmg_lwrad_wrf_columns``) on this rank's rows of
     the domain in ``kwargs``.  Returns (rows, result): result holds this rank's
     slab of every output field, or with ``gather`` the whole fields on every rank.
     A gather needs rows on every rank; the check is the same on all ranks, so
-    they all raise before any collective."""
+    they all raise before any collective.
+
+    Device: the radiation calls run on the context they are given, else on
+    the process's current CUDA device (``rrtmg.default_context``).  With one
+    process per GPU, pass ``device`` (normally the local rank) or call
+    ``torch.cuda.set_device(local_rank)`` first; otherwise every rank uses
+    GPU 0.  With ``device`` the call runs under ``torch.cuda.device(device)``
+    and the caller's current device is restored afterwards."""
+    if device is not None:
+        import torch
+
+        with torch.cuda.device(int(device)):
+            return sharded_call(call, kwargs, rank=rank, world=world, rows_per_batch=rows_per_batch,
+                                gather=gather, group=group)
     t3d = kwargs["t3d"]
     nx, ny = int(t3d.shape[0]), int(t3d.shape[2])
     ranges = batch_partitions(ny, rows_per_batch, world)
