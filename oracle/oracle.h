@@ -65,6 +65,9 @@ typedef struct {
 int ora_lw_nlayers(double p_top, int nk);
 int ora_lw_columns(const ora_tables *t, const ora_in *in, ora_out *out, int nthreads);
 int ora_sw_columns(const ora_tables *t, const ora_in *in, ora_out *out, int nthreads);
+/* Test knob: move the LW cloud-absorptance expf and minor-gas powf results by
+ * the given numbers of ulps (0, 0 = glibc, the default); process-wide. */
+void ora_set_libm_perturbation(int exp_ulps, int pow_ulps);
 
 #ifdef __cplusplus
 }

@@ -472,7 +472,38 @@ static inline float frac_interp(const float *tab, int ncols, int jpl, float fpl,
     return interpf(tab[g * ncols + j0], tab[g * ncols + j0 + 1], fpl);
 }
 
-static inline float active_pow(float base, float exponent) { return powf(base, exponent); }
+/* Test knob (ora_set_libm_perturbation): move the two results the reference
+ * takes from XLA's binary32 libm rather than glibc -- the minor-gas scaling
+ * power (lw:134-144) and the cloud absorptance exponential (lw:5564) -- by a
+ * given number of ulps, to bound what a last-place libm difference does to
+ * the outputs.  Zero (the default) leaves glibc's results untouched. */
+static int g_pow_ulps = 0, g_exp_ulps = 0;
+
+void ora_set_libm_perturbation(int exp_ulps, int pow_ulps)
+{
+    g_exp_ulps = exp_ulps;
+    g_pow_ulps = pow_ulps;
+}
+
+static inline float nudge_ulps(float v, int ulps)
+{
+    for (; ulps > 0; --ulps) v = nextafterf(v, INFINITY);
+    for (; ulps < 0; ++ulps) v = nextafterf(v, -INFINITY);
+    return v;
+}
+
+static inline float active_pow(float base, float exponent)
+{
+    float r = powf(base, exponent);
+    return g_pow_ulps && exponent != 0.0f && base != 1.0f ? nudge_ulps(r, g_pow_ulps) : r;
+}
+
+/* exp of a cloud optical depth; exp(0) = 1 is exact in every libm */
+static inline float cloud_expf(float x)
+{
+    float r = expf(x);
+    return g_exp_ulps && x != 0.0f ? nudge_ulps(r, g_exp_ulps) : r;
+}
 
 /* ------------------------------------------------------------------------ */
 /* taumol per band (lw:1597-4684)                                            */
@@ -1112,7 +1143,7 @@ static void lw_rtrnmc(const ora_lw_cache *L, lw_col *S)
             if (odepth < 0.0f) odepth = 0.0f;
             int cldf = S->cldf[g][l];
             float odcld_raw = sd * S->taucmc[g][l];
-            float abscld = 1.0f - expf(-odcld_raw);
+            float abscld = 1.0f - cloud_expf(-odcld_raw);
             float odcld = cldf ? odcld_raw : 0.0f;
             float efclfrac = cldf ? abscld * (float)cldf : 0.0f;
             efcl[l] = efclfrac;
