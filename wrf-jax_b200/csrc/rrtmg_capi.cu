@@ -701,30 +701,27 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
   a.nday = daylist + ncol;
   a.daylist = daylist;
-  int sw_split_max, sw_chunk;
+  int sw_chunk;
   {
     std::lock_guard<std::mutex> lk(ctx->mutex);
-    sw_split_max = ctx->sw_split_max;
     sw_chunk = ctx->sw_chunk;
   }
-  a.chunk_columns = sw_chunk;
-  float *split_terms = nullptr;
-  if (ncol <= sw_split_max) {
-    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&split_terms),
-                                sw_split_terms_floats(cfg->nk, ncol) * sizeof(float), ctx->pool, stream);
-    if (e != cudaSuccess) {
-      cudaFreeAsync(daylist, stream);
-      cudaFreeAsync(mask, stream);
-      return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(sw band terms)");
-    }
+  a.chunk_capacity = ncol < sw_chunk ? ncol : sw_chunk;
+  float *records = nullptr;
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&records),
+                              sw_record_floats(cfg->nk, a.chunk_capacity) * sizeof(float), ctx->pool, stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(daylist, stream);
+    cudaFreeAsync(mask, stream);
+    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(sw layer records)");
   }
-  a.split_terms = split_terms;
+  a.records = records;
   e = launch_sw_daylist(a, stream);
   timing_mark(ctx, 1, tslot, 2, stream);
   if (e == cudaSuccess) e = launch_sw_columns(ctx->tables, a, stream);
   timing_mark(ctx, 1, tslot, 3, stream);
-  if (split_terms) {
-    cudaError_t es = cudaFreeAsync(split_terms, stream);
+  {
+    cudaError_t es = cudaFreeAsync(records, stream);
     if (e == cudaSuccess) e = es;
   }
   cudaError_t ef = cudaFreeAsync(daylist, stream);

@@ -64,14 +64,17 @@ struct SwArgs {
   float *zero2[4];
   int *nday;     // scratch: number of day columns (set by the compaction kernel)
   int *daylist;  // scratch: ncol entries, day column indices
-  float *split_terms;  // small domains: sw_split_terms_floats(nk, ncol) floats, else null
-  int chunk_columns;   // day-list slots per launch of the column kernel
+  float *records;      // scratch: sw_record_floats(nk, chunk_capacity) floats
+  int chunk_capacity;  // day-list slots per chunk of the sweep schedule
+  int chunk_first, chunk_count;  // the chunk being launched (set by launch_sw_columns)
   const int *live;     // null, or a device count of leading columns to process
 };
 
-// defaults: columns per SW column-kernel launch, and the largest domain that
-// uses the g-point split SW schedule
-constexpr int kSwChunkColumns = 131072;
+// default day-list slots per chunk of the SW sweep schedule (its records take
+// about 64 KB per slot at nk = 50)
+constexpr int kSwChunkColumns = 32768;
+// no longer used by the SW path (every domain runs the sweep schedule); kept
+// as the default of the schedule field that used to select it
 constexpr int kSwSplitMaxColumns = 4096;
 
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
@@ -89,7 +92,7 @@ size_t lw_optics_floats(int nlay, int ncol);
 // day-column compaction (writes the night columns), then the column kernel over
 // the day columns; both need a.nday and a.daylist (1 + ncol ints)
 cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);
-size_t sw_split_terms_floats(int nk, int ncol);
+size_t sw_record_floats(int nk, int chunk);
 cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
 // Radiation prologue (cloud fraction, cos zenith, CAM ozone).  Constants of

@@ -24,7 +24,6 @@ namespace {
 
 constexpr int kNgc[kSwBands] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};
 constexpr int kGofs[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
-constexpr int kMaxNgc = 12;
 constexpr int kMaxLev = kMaxLay + 1;
 constexpr float kOneMinus = 1.0f - 1.0e-6f;
 
@@ -582,209 +581,6 @@ __device__ __forceinline__ RT4 reftra(const Tables &T, bool lrt, float zg, float
   return r;
 }
 
-// One adding-method path (clear or total) of one g-point: level arrays top-down.
-struct Path {
-  float ref[kMaxLev], refd[kMaxLev], tra[kMaxLev], trad[kMaxLev], dbt[kMaxLev];
-  float tdbt[kMaxLev], tdn[kMaxLev], rdnd[kMaxLev];
-};
-
-// Downward recurrence of vrtqdr (sw:3681-3702) for level r+1 once layer r is known.
-__device__ __forceinline__ void down_step(Path &P, int r) {
-  if (r == 0) {
-    P.tdn[0] = 1.0f;
-    P.rdnd[0] = 0.0f;
-    P.tdn[1] = P.tra[0];
-    P.rdnd[1] = P.refd[0];
-    return;
-  }
-  const float zreflect = 1.0f / (1.0f - P.refd[r] * P.rdnd[r]);
-  P.tdn[r + 1] = P.tdbt[r] * P.tra[r] + P.trad[r] * ((P.tdn[r] - P.tdbt[r]) + P.tdbt[r] * P.ref[r] * P.rdnd[r]) * zreflect;
-  P.rdnd[r + 1] = P.refd[r] + P.trad[r] * P.trad[r] * P.rdnd[r] * zreflect;
-}
-
-// kTerms = false: add each level term into the thread's accumulators (accs).
-// kTerms = true: store each level term (type, level, g-point) to `terms` with
-// stride tstride between (type, level, g-point) planes, for the ordered sums
-// of the finish kernel.
-// One g-point of a band: top-down delta-Eddington layers, direct beam and
-// downward adding, then bottom-up adding, level fluxes and their sums (accs)
-// or terms.  o supplies the layer optics of the g-point: tg/tr gas and
-// Rayleigh depths, ct/cs/ca/co the band's cloud optics.
-template <bool kTerms, class Opt>
-__device__ __forceinline__ void sw_gpoint(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
-                                          int clear_only, float *accs, Path &Pc, Path &Pt, float *terms,
-                                          size_t tstride, int G, float sflux_g, const Opt &o) {
-  const int n = C.nlay;
-  const float mu = C.mu;
-  const float repclc = 1.0e-12f;
-  // top-down: layer optics, direct beam, downward adding
-  Pc.tdbt[0] = 1.0f;
-  Pt.tdbt[0] = 1.0f;
-  float tdbtc_nd = 1.0f, tdbt_nd = 1.0f;
-  const float zincflx = ((C.adjflux * sflux_g) * mu) * 1.0f;
-  auto term = [&](int type, int level) -> float & {
-    return terms[((static_cast<size_t>(type) * (n + 1) + level) * kSwGpts + G) * tstride];
-  };
-  float *accfdir = kTerms ? nullptr : accs + 4 * kMaxLev, *acccdir = kTerms ? nullptr : accs + 5 * kMaxLev;
-  if constexpr (kTerms) {
-    term(4, 0) = tdbt_nd * zincflx;
-    term(5, 0) = tdbtc_nd * zincflx;
-  } else {
-    accfdir[0] = accfdir[0] + tdbt_nd * zincflx;
-    acccdir[0] = acccdir[0] + tdbtc_nd * zincflx;
-  }
-  // thread-local table values of the next layer are loaded one layer ahead
-  float nx_tr = o.tr(n - 1), nx_tg = o.tg(n - 1);
-  float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
-  if (!clear_only) { nx_ct = o.ct(n - 1); nx_cs = o.cs(n - 1); nx_ca = o.ca(n - 1); nx_co = o.co(n - 1); }
-  uint32_t nx_word = maskbase[(static_cast<size_t>(n - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
-  for (int r = 0; r < n; ++r) {
-    const int l = n - 1 - r;
-    const uint32_t word = nx_word;
-    const float tr = nx_tr, tg = nx_tg;
-    const float ct = nx_ct, cs = nx_cs, ca = nx_ca, co = nx_co;
-    if (l > 0) {
-      nx_tr = o.tr(l - 1);
-      nx_tg = o.tg(l - 1);
-      if (!clear_only) { nx_ct = o.ct(l - 1); nx_cs = o.cs(l - 1); nx_ca = o.ca(l - 1); nx_co = o.co(l - 1); }
-      nx_word = maskbase[(static_cast<size_t>(l - 1) * kSwMaskWords + (G >> 5)) * a.ncol];
-    }
-    const bool cldb = (word >> (G & 31)) & 1u;
-    const float cloud = cldb ? 1.0f : 0.0f;
-    const float clear = 1.0f - cloud;
-    const float ztau = (tr + tg) + 0.0f;
-    float zom = tr + 0.0f * 1.0f;
-    const float zgr = 0.0f * 1.0f * 0.0f / zom;
-    zom = zom / ztau;
-    const float dbtc_nd = exp_lookup(T, ztau / mu);
-    tdbtc_nd = tdbtc_nd * dbtc_nd;
-    const float zf = zgr * zgr;
-    const float zwf = zom * zf;
-    const float ztauc = (1.0f - zwf) * ztau;
-    const float zomcc = (zom - zwf) / (1.0f - zwf);
-    const float zgcc = (zgr - zf) / (1.0f - zf);
-    const RT4 c = reftra(T, true, zgcc, mu, ztauc, zomcc);
-    Pc.ref[r] = c.ref; Pc.refd[r] = c.refd; Pc.tra[r] = c.tra; Pc.trad[r] = c.trad;
-    const float dbtc = exp_lookup(T, ztauc / mu);
-    Pc.dbt[r] = dbtc;
-    Pc.tdbt[r + 1] = Pc.tdbt[r] * dbtc;
-    down_step(Pc, r);
-    if (!clear_only) {
-      const float tcld = cldb ? ct : 0.0f;
-      const float wcld = cldb ? cs : 1.0f;
-      const float gcld = cldb ? ca : 0.0f;
-      const float taor = cldb ? co : 0.0f;
-      const float tauorig = ztau + taor;
-      const float dbtmo_nd = exp_lookup(T, tauorig / mu);
-      const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
-      tdbt_nd = tdbt_nd * dbt_nd;
-      const float ztauo = ztauc + tcld;
-      float zomco = ztauc * zomcc + tcld * wcld;
-      const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
-      zomco = zomco / ztauo;
-      const RT4 o = reftra(T, cloud > repclc, zgco, mu, ztauo, zomco);
-      Pt.ref[r] = clear * c.ref + cloud * o.ref;
-      Pt.refd[r] = clear * c.refd + cloud * o.refd;
-      Pt.tra[r] = clear * c.tra + cloud * o.tra;
-      Pt.trad[r] = clear * c.trad + cloud * o.trad;
-      const float dbtmo = exp_lookup(T, ztauo / mu);
-      const float dbt = clear * dbtc + cloud * dbtmo;
-      Pt.dbt[r] = dbt;
-      Pt.tdbt[r + 1] = Pt.tdbt[r] * dbt;
-      down_step(Pt, r);
-    } else {
-      tdbt_nd = tdbtc_nd;
-    }
-    if constexpr (kTerms) {
-      term(4, r + 1) = tdbt_nd * zincflx;
-      term(5, r + 1) = tdbtc_nd * zincflx;
-    } else {
-      accfdir[r + 1] = accfdir[r + 1] + tdbt_nd * zincflx;
-      acccdir[r + 1] = acccdir[r + 1] + tdbtc_nd * zincflx;
-    }
-  }
-  // surface boundary
-  Pc.ref[n] = C.albedo; Pc.refd[n] = C.albedo; Pc.tra[n] = 0.0f; Pc.trad[n] = 0.0f; Pc.dbt[n] = 0.0f;
-  Pt.ref[n] = C.albedo; Pt.refd[n] = C.albedo; Pt.tra[n] = 0.0f; Pt.trad[n] = 0.0f; Pt.dbt[n] = 0.0f;
-  // bottom-up: upward adding and level fluxes (vrtqdr, sw:3655-3720)
-  float *accfu = accs, *accfd = kTerms ? nullptr : accs + kMaxLev;
-  float *acccu = kTerms ? nullptr : accs + 2 * kMaxLev, *acccd = kTerms ? nullptr : accs + 3 * kMaxLev;
-  float rupc = Pc.ref[n], rupdc = Pc.refd[n];
-  float rupt = Pt.ref[n], rupdt = Pt.refd[n];
-  // level arrays and accumulators of the next level are loaded one level ahead
-  struct Lvl {
-    float ref, refd, tra, trad, dbt, tdbt, tdn, rdnd;
-  };
-  auto load_lvl = [&](const Path &P, int k) {
-    Lvl v;
-    v.ref = P.ref[k]; v.refd = P.refd[k]; v.tra = P.tra[k]; v.trad = P.trad[k]; v.dbt = P.dbt[k];
-    v.tdbt = P.tdbt[k]; v.tdn = P.tdn[k]; v.rdnd = P.rdnd[k];
-    return v;
-  };
-  Lvl nc = load_lvl(Pc, n), nt = nc;
-  if (!clear_only) nt = load_lvl(Pt, n);
-  float nfu = 0.0f, nfd = 0.0f, ncu = 0.0f, ncd = 0.0f;
-  if constexpr (!kTerms) { nfu = accfu[n]; nfd = accfd[n]; ncu = acccu[n]; ncd = acccd[n]; }
-  for (int k = n; k >= 0; --k) {
-    const Lvl c = nc, t = nt;
-    const float afu = nfu, afd = nfd, acu = ncu, acd = ncd;
-    if (k > 0) {
-      nc = load_lvl(Pc, k - 1);
-      if (!clear_only) nt = load_lvl(Pt, k - 1);
-      if constexpr (!kTerms) { nfu = accfu[k - 1]; nfd = accfd[k - 1]; ncu = acccu[k - 1]; ncd = acccd[k - 1]; }
-    }
-    if (k < n) {
-      const float zrc = 1.0f / (1.0f - rupdc * c.refd);
-      const float nrupc = c.ref + c.trad * ((c.tra - c.dbt) * rupdc + c.dbt * rupc) * zrc;
-      const float nrupdc = c.refd + c.trad * c.trad * rupdc * zrc;
-      rupc = nrupc;
-      rupdc = nrupdc;
-      if (!clear_only) {
-        const float zrt = 1.0f / (1.0f - rupdt * t.refd);
-        const float nrupt = t.ref + t.trad * ((t.tra - t.dbt) * rupdt + t.dbt * rupt) * zrt;
-        const float nrupdt = t.refd + t.trad * t.trad * rupdt * zrt;
-        rupt = nrupt;
-        rupdt = nrupdt;
-      }
-    }
-    // clear-sky level fluxes
-    const float zrefc = 1.0f / (1.0f - c.rdnd * rupdc);
-    const float fuc = (c.tdbt * rupc + (c.tdn - c.tdbt) * rupdc) * zrefc;
-    const float fdc = c.tdbt + (c.tdn - c.tdbt + c.tdbt * rupc * c.rdnd) * zrefc;
-    float fut = fuc, fdt = fdc;
-    if (!clear_only) {
-      const float zreft = 1.0f / (1.0f - t.rdnd * rupdt);
-      fut = (t.tdbt * rupt + (t.tdn - t.tdbt) * rupdt) * zreft;
-      fdt = t.tdbt + (t.tdn - t.tdbt + t.tdbt * rupt * t.rdnd) * zreft;
-    }
-    if constexpr (kTerms) {
-      term(0, k) = fut * zincflx;
-      term(1, k) = fdt * zincflx;
-      term(2, k) = fuc * zincflx;
-      term(3, k) = fdc * zincflx;
-    } else {
-      accfu[k] = afu + fut * zincflx;
-      accfd[k] = afd + fdt * zincflx;
-      acccu[k] = acu + fuc * zincflx;
-      acccd[k] = acd + fdc * zincflx;
-    }
-  }
-}
-
-// Layer optics of one g-point from the thread-local band tables of sw_band.
-struct LocalOptics {
-  const float (*taug)[kMaxNgc];
-  const float (*taur)[kMaxNgc];
-  const float *ctau, *cssa, *casm, *ctaor;
-  int g;
-  __device__ float tg(int l) const { return taug[l][g]; }
-  __device__ float tr(int l) const { return taur[l][g]; }
-  __device__ float ct(int l) const { return ctau[l]; }
-  __device__ float cs(int l) const { return cssa[l]; }
-  __device__ float ca(int l) const { return casm[l]; }
-  __device__ float co(int l) const { return ctaor[l]; }
-};
-
 // Solar source of band B (the per-band rules of sw:4430-4450): the source
 // layer from the layers' jp (jp(l)), the spectral interpolation (js0, fs) of
 // the layer (spec(ls, js0, fs), asked only when the band uses it), and the
@@ -839,60 +635,6 @@ __device__ __forceinline__ void sw_source(const Tables &T, const Col &C, JpFn jp
       }
     }
     sflux[g] = sz;
-  }
-}
-
-// g_only >= 0: only that g-point of the band (the g-point split schedule).
-template <int B, bool kTerms = false>
-__device__ __forceinline__ void sw_band(const Tables &T, const SwArgs &a, const Col &C, const uint32_t *maskbase,
-                                        int clear_only, float *accs, Path &Pc, Path &Pt, float *terms = nullptr,
-                                        size_t tstride = 0, int g_only = -1) {
-  constexpr int ngc = kNgc[B];
-  constexpr int gofs = kGofs[B];
-  constexpr int bn = B + 16;
-  const int n = C.nlay;
-  const int col = C.i * C.ny + C.j;
-  const SwBand &K = T.sw[B];
-  // Per-layer band optics, thread-local: taug/taur of every g-point and the
-  // band's cloud optics for cloudy g-points.
-  float taug[kMaxLay][kMaxNgc], taur[kMaxLay][kMaxNgc];
-  float ctau[kMaxLay], cssa[kMaxLay], casm[kMaxLay], ctaor[kMaxLay];
-  int jpl[kMaxLay];
-  for (int l = 0; l < n; ++l) {
-    const SLayer L = make_layer(T, a, C, l);
-    SwSpec sp8, sp4;
-    sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
-    sp4 = sp8;
-    float tg[ngc], tr[ngc];
-    sw_taumol<B>(T, L, tg, tr, sp8, sp4);
-#pragma unroll
-    for (int g = 0; g < ngc; ++g) { taug[l][g] = tg[g]; taur[l][g] = tr[g]; }
-    // cloud optics of the band at this layer (used by cloudy g-points)
-    if (!clear_only) {
-      const CloudOpt o = sw_cloud(T, L, B, C.iceflg);
-      ctau[l] = o.tau; cssa[l] = o.ssa; casm[l] = o.asm_; ctaor[l] = o.taor;
-    }
-    jpl[l] = L.jp;
-  }
-  float sflux[ngc];
-  sw_source<B>(
-      T, C, [&](int l) { return jpl[l]; },
-      [&](int ls, int &js0, float &fs) {
-        const SLayer L = make_layer(T, a, C, ls);
-        SwSpec sp8, sp4;
-        sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
-        sp4 = sp8;
-        float tg[ngc], tr[ngc];
-        sw_taumol<B>(T, L, tg, tr, sp8, sp4);
-        const SwSpec &sp = (bn == 17 || bn == 28) ? sp4 : sp8;
-        js0 = sp.js0;
-        fs = sp.fs;
-      },
-      sflux);
-  for (int g = 0; g < ngc; ++g) {
-    if (g_only >= 0 && g != g_only) continue;
-    const LocalOptics o{taug, taur, ctau, cssa, casm, ctaor, g};
-    sw_gpoint<kTerms>(T, a, C, maskbase, clear_only, accs, Pc, Pt, terms, tstride, gofs + g, sflux[g], o);
   }
 }
 
@@ -963,14 +705,6 @@ __device__ __forceinline__ void sw_setup_head(const Tables &T, const SwArgs &a, 
   (void)n;
 }
 
-// Column set-up of a day column (buffer ozone, laytrop; sw:2491-2508, 7101-7306).
-__device__ __forceinline__ void sw_setup(const Tables &T, const SwArgs &a, int col, Col &C) {
-  sw_setup_head(T, a, col, C);
-  int laytrop = 0;
-  for (int l = 0; l < C.nlay; ++l) laytrop += glibc_logf(T, sw_pavel(a, C, l)) > 4.56f;
-  C.laytrop = laytrop;
-}
-
 // Heating rate and theta tendency of layer l of a day column from its level
 // sums accs (six arrays of stride `stride`, top-down; sw:2285-2301).
 __device__ __forceinline__ void sw_layer_output(const SwArgs &a, const Col &C, int l, const float *accs,
@@ -1017,53 +751,24 @@ __device__ __forceinline__ void sw_column_outputs(const SwArgs &a, const Col &C,
   a.swddnic[col] = cdir[n] / coszen;
 }
 
-// Heating rates, theta tendencies and 2-D outputs of a day column from its
-// level sums accs (six arrays of kMaxLev, top-down).
-__device__ __forceinline__ void sw_outputs(const SwArgs &a, const Col &C, int col, const float *accs) {
-  for (int l = 0; l < C.nk; ++l) sw_layer_output(a, C, l, accs, kMaxLev);
-  sw_column_outputs(a, C, col, accs, kMaxLev);
-}
-
-
-__global__ void __launch_bounds__(128) sw_kernel(Tables T, SwArgs a, int first, int count) {
-  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= first + count || t >= *a.nday) return;
-  const int col = a.daylist[t];
-  Col C;
-  sw_setup(T, a, col, C);
-  const int clear_only = a.icld == 0;
-  float accs[6 * kMaxLev];
-  for (int k = 0; k < 6 * kMaxLev; ++k) accs[k] = 0.0f;
-  Path Pc, Pt;
-  const uint32_t *maskbase = a.mask + col;
-  sw_band<0>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<1>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<2>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<3>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<4>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<5>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<6>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<7>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<8>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<9>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<10>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<11>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<12>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_band<13>(T, a, C, maskbase, clear_only, accs, Pc, Pt);
-  sw_outputs(a, C, col, accs);
-}
-
-// g-point split schedule for small domains, from layer records:
-//   sw_colprep_kernel  thread = day slot: the column set-up once;
+// ---------------------------------------------------------------------------
+// Sweep schedule, every domain size.  Day-list slots are processed in chunks;
+// per chunk:
+//   sw_colprep_kernel  warp = day slot: the column set-up once (laytrop by a
+//                      warp vote over the layers);
 //   sw_optics_kernel   thread = (day slot, layer, band): the band's gas and
 //                      Rayleigh depths of every g-point, its cloud optics, the
-//                      spectral interpolation its solar source uses, and jp;
+//                      spectral interpolation its solar source uses, and jp,
+//                      into a layer record;
 //   sw_source_kernel   thread = (day slot, band): the band's solar source;
-//   sw_gsplit_kernel   thread = (day slot, g-point): one g-point's sweeps.
-// The operations are those of sw_band, so the level terms (type, level,
-// g-point) are bit-identical; sw_gsum_kernel and sw_split_finish_kernel sum
-// and finish them.  Scratch after the terms: column records, then layer
-// records of kSwRec floats.
+//   sw_sweep_kernel    block = kSweepCols day slots x 112 g-points, thread =
+//                      one g-point: the top-down pass (delta-Eddington layers,
+//                      direct beam, downward adding) and the bottom-up pass
+//                      (upward adding, level fluxes) of spcvmc, the
+//                      per-level spectral sums in g-point order in shared
+//                      memory, then heating and the 2-D outputs.
+// Records: per chunk slot a column record, then nlay layer records of kSwRec
+// floats (about 64 KB per day column at nk = 50).
 constexpr int kSwRec = 312;  // taug[112], taur[112], cloud[14][4], spec[14][2], jp, padding
 constexpr int kSwRecTaur = kSwGpts, kSwRecCloud = 2 * kSwGpts, kSwRecSpec = kSwRecCloud + 4 * kSwBands,
               kSwRecJp = kSwRecSpec + 2 * kSwBands;
@@ -1075,23 +780,18 @@ struct SwColRec {
 };
 constexpr size_t kSwColRecFloats = (sizeof(SwColRec) + 15) / 16 * 4;
 
-__host__ __device__ __forceinline__ size_t sw_terms_only_floats(int nk, int ncol) {
-  return static_cast<size_t>(6) * (nk + 2) * kSwGpts * static_cast<size_t>(ncol);
-}
-__device__ __forceinline__ SwColRec *sw_colrecs(const SwArgs &a) {
-  return reinterpret_cast<SwColRec *>(a.split_terms + sw_terms_only_floats(a.nk, a.ncol));
-}
+// chunk-relative slot u = t - a.chunk_first
+__device__ __forceinline__ SwColRec *sw_colrecs(const SwArgs &a) { return reinterpret_cast<SwColRec *>(a.records); }
 __device__ __forceinline__ float *sw_layrecs(const SwArgs &a) {
-  return a.split_terms + sw_terms_only_floats(a.nk, a.ncol) + kSwColRecFloats * static_cast<size_t>(a.ncol);
+  return a.records + kSwColRecFloats * static_cast<size_t>(a.chunk_capacity);
 }
-
-__constant__ int kSwGofsDev[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
 
 // A warp per day column; the lanes take the layers of the laytrop count.
 __global__ void __launch_bounds__(128) sw_colprep_kernel(Tables T, SwArgs a) {
   const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (t >= a.ncol || t >= *a.nday) return;  // whole warps
+  const int u = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int t = a.chunk_first + u;
+  if (u >= a.chunk_count || t >= *a.nday) return;  // whole warps
   Col C;
   sw_setup_head(T, a, a.daylist[t], C);
   int count = 0;
@@ -1099,7 +799,7 @@ __global__ void __launch_bounds__(128) sw_colprep_kernel(Tables T, SwArgs a) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
   C.laytrop = count;
-  if (lane == 0) sw_colrecs(a)[t].C = C;
+  if (lane == 0) sw_colrecs(a)[u].C = C;
 }
 
 template <int B>
@@ -1150,9 +850,9 @@ __device__ __forceinline__ void sw_layer_optics(const Tables &T, const SwArgs &a
 __global__ void __launch_bounds__(128) sw_optics_kernel(Tables T, SwArgs a) {
   const int n = a.nk + 1;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = idx / n, l = idx - t * n;
-  if (t >= a.ncol || t >= *a.nday) return;
-  const Col &C = sw_colrecs(a)[t].C;
+  const int u = idx / n, l = idx - u * n;
+  if (u >= a.chunk_count || a.chunk_first + u >= *a.nday) return;
+  const Col &C = sw_colrecs(a)[u].C;
   float *rec = sw_layrecs(a) + static_cast<size_t>(idx) * kSwRec;
   const int clear_only = a.icld == 0;
 #define RRTMG_SW_OPT(B) sw_layer_optics<B>(T, a, C, l, clear_only, rec)
@@ -1161,11 +861,11 @@ __global__ void __launch_bounds__(128) sw_optics_kernel(Tables T, SwArgs a) {
 }
 
 __global__ void __launch_bounds__(128) sw_source_kernel(Tables T, SwArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.ncol || t >= *a.nday) return;
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= a.chunk_count || a.chunk_first + u >= *a.nday) return;
   const int n = a.nk + 1;
-  SwColRec &R = sw_colrecs(a)[t];
-  const float *recs = sw_layrecs(a) + static_cast<size_t>(t) * n * kSwRec;
+  SwColRec &R = sw_colrecs(a)[u];
+  const float *recs = sw_layrecs(a) + static_cast<size_t>(u) * n * kSwRec;
   const int band = blockIdx.y;
   auto jp = [&](int l) { return __float_as_int(recs[static_cast<size_t>(l) * kSwRec + kSwRecJp]); };
   auto spec = [&](int ls, int &js0, float &fs) {
@@ -1183,80 +883,256 @@ __global__ void __launch_bounds__(128) sw_source_kernel(Tables T, SwArgs a) {
 }
 #undef RRTMG_SW_BAND_SWITCH
 
-// Layer optics of one g-point from the layer records of its column.
-struct RecordOptics {
-  const float *recs;
-  int G, cloud;  // cloud = record offset of the band's cloud optics
-  __device__ float tg(int l) const { return recs[static_cast<size_t>(l) * kSwRec + G]; }
-  __device__ float tr(int l) const { return recs[static_cast<size_t>(l) * kSwRec + kSwRecTaur + G]; }
-  __device__ float ct(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud]; }
-  __device__ float cs(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud + 1]; }
-  __device__ float ca(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud + 2]; }
-  __device__ float co(int l) const { return recs[static_cast<size_t>(l) * kSwRec + cloud + 3]; }
+__constant__ int kSwGofsDev[kSwBands] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
+
+constexpr int kSweepCols = 2;                         // day columns per block
+constexpr int kSweepThreads = kSweepCols * kSwGpts;   // 224: one thread per g-point
+constexpr int kRing = 8;                              // levels of terms per ordered-sum round
+
+// Shared memory of a sweep block: the level terms of the last kRing levels of
+// the current pass, awaiting their g-ordered sums, and the sums themselves.
+struct SweepShared {
+  float ring[kRing][kSweepCols][4][kSwGpts];
+  float sums[kSweepCols][6][kMaxLev];  // type: fu, fd, cu, cd, fdir, cdir; level top-down
+};
+static_assert(sizeof(SweepShared) <= 48 * 1024, "sweep shared memory within the default limit");
+
+// One level of one adding path, as the bottom-up pass reads it back: the
+// layer's reflectances/transmittances and direct-beam transmittance, and the
+// level's cumulative direct beam and downward recurrence (vrtqdr, sw:3655-3702).
+struct SwLevel {
+  float4 rt;   // ref, refd, tra, trad
+  float4 dn;   // dbt, tdbt, tdn, rdnd
 };
 
-// grid.y = g-point
-__global__ void __launch_bounds__(128) sw_gsplit_kernel(Tables T, SwArgs a, int first, int count) {
-  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= first + count || t >= *a.nday) return;
-  const int col = a.daylist[t];
-  const int n = a.nk + 1;
-  const SwColRec &R = sw_colrecs(a)[t];
-  const Col C = R.C;
-  const int G = blockIdx.y;
-  int band = kSwBands - 1;
-  while (G < kSwGofsDev[band]) --band;
-  const RecordOptics o{sw_layrecs(a) + static_cast<size_t>(t) * n * kSwRec, G, kSwRecCloud + 4 * band};
-  Path Pc, Pt;
-  sw_gpoint<true>(T, a, C, a.mask + col, a.icld == 0, nullptr, Pc, Pt, a.split_terms + (t - first),
-                  static_cast<size_t>(count), G, R.sflux[G], o);
-}
-
-// Ordered g-point sums of the split schedules: thread (day-list slot t, plane
-// (type, level) = blockIdx.y) adds the plane's 112 terms in g-point order,
-// starting from zero as the accumulators of sw_kernel do, and stores the sum
-// over the plane's g-point-0 term.
-__global__ void __launch_bounds__(128) sw_gsum_kernel(SwArgs a, int first, int count) {
-  const int t = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= first + count || t >= *a.nday) return;
-  const size_t ts = static_cast<size_t>(count);
-  float *p = a.split_terms + (t - first) + static_cast<size_t>(blockIdx.y) * kSwGpts * ts;
-  float acc = 0.0f;
-  for (int G0 = 0; G0 < kSwGpts; G0 += 16) {
-    float v[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = p[static_cast<size_t>(G0 + q) * ts];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc = acc + v[q];
-  }
-  p[0] = acc;
-}
-
-// Outputs of the split schedule: a block per day slot, its threads over
-// layers; the level sums are the g-point-0 slots sw_gsum_kernel wrote.
-__global__ void __launch_bounds__(64) sw_split_finish_kernel(Tables T, SwArgs a, int first, int count) {
-  __shared__ float accs[6 * kMaxLev];
-  const int t = first + blockIdx.x;
-  if (t >= first + count || t >= *a.nday) return;  // whole blocks
-  const int col = a.daylist[t];
-  Col C;
-  C.i = col / a.ny;
-  C.j = col - C.i * a.ny;
-  C.nk = a.nk;
-  C.ny = a.ny;
-  C.nlay = a.nk + 1;
-  C.coszen = ld(a.in.coszr + col);
-  const int n = C.nlay;
-  const float *terms = a.split_terms + (t - first);
-  const size_t ts = static_cast<size_t>(count);
-  for (int q = threadIdx.x; q < 6 * (n + 1); q += blockDim.x) {
-    const int type = q / (n + 1), level = q - type * (n + 1);
-    accs[type * kMaxLev + level] = terms[(static_cast<size_t>(type) * (n + 1) + level) * kSwGpts * ts];
+// Adds ring rounds into the sums: chain (column, type, level) adds the 112
+// terms of its level in g-point order, starting from zero as the
+// reference's ordered sums do (sw:153-177).  `levels[j]` is the level of ring
+// slot j, `types` the sums' type indices of the pass's ring types.
+__device__ __forceinline__ void sweep_flush(SweepShared &S, int count, int ntypes, const int *types, int level0,
+                                            int dir) {
+  __syncthreads();
+  const int chains = kSweepCols * ntypes * count;
+  for (int ch = threadIdx.x; ch < chains; ch += kSweepThreads) {
+    const int j = ch % count;
+    const int rest = ch / count;
+    const int q = rest % ntypes;
+    const int c = rest / ntypes;
+    const float *v = S.ring[j][c][q];
+    float acc = 0.0f;
+#pragma unroll 16
+    for (int G = 0; G < kSwGpts; ++G) acc = acc + v[G];
+    S.sums[c][types[q]][level0 + dir * j] = acc;
   }
   __syncthreads();
-  for (int l = threadIdx.x; l < C.nk; l += blockDim.x) sw_layer_output(a, C, l, accs, kMaxLev);
-  if (threadIdx.x == 0) sw_column_outputs(a, C, col, accs, kMaxLev);
-  (void)T;
+}
+
+// Block = kSweepCols consecutive slots of the chunk; thread = (slot, g-point).
+// A slot past the day count repeats the block's first slot so that every
+// thread takes the same barriers; its results are not written.
+__global__ void __launch_bounds__(kSweepThreads, 3) sw_sweep_kernel(Tables T, SwArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SweepShared &S = *reinterpret_cast<SweepShared *>(smem_raw);
+  const int nday = *a.nday;
+  const int u0 = blockIdx.x * kSweepCols;
+  if (u0 >= a.chunk_count || a.chunk_first + u0 >= nday) return;  // whole block
+  const int cslot = threadIdx.x / kSwGpts;
+  const int G = threadIdx.x - cslot * kSwGpts;
+  const int u_own = u0 + cslot;
+  const bool live = u_own < a.chunk_count && a.chunk_first + u_own < nday;
+  const int u = live ? u_own : u0;
+  const int col = a.daylist[a.chunk_first + u];
+  const SwColRec &R = sw_colrecs(a)[u];
+  const Col C = R.C;
+  const float sflux_g = R.sflux[G];
+  const int n = C.nlay;
+  const float mu = C.mu;
+  const float repclc = 1.0e-12f;
+  const int clear_only = a.icld == 0;
+  int band = kSwBands - 1;
+  while (G < kSwGofsDev[band]) --band;
+  const float *recs = sw_layrecs(a) + static_cast<size_t>(u) * n * kSwRec;
+  const float *crec = recs + kSwRecCloud + 4 * band;
+  const uint32_t *maskbase = a.mask + col + static_cast<size_t>(G >> 5) * a.ncol;
+  const size_t mstride = static_cast<size_t>(kSwMaskWords) * a.ncol;
+  const uint32_t bit = 1u << (G & 31);
+
+  // per-thread stack of the top-down pass, read back bottom-up
+  SwLevel stc[kMaxLev], stt[kMaxLev];
+
+  // ---- top-down pass: layer optics, direct beam, downward adding (sw:6887-7041)
+  const int dtypes[2] = {4, 5};
+  float tdbtc_nd = 1.0f, tdbt_nd = 1.0f;
+  const float zincflx = ((C.adjflux * sflux_g) * mu) * 1.0f;
+  S.ring[0][cslot][0][G] = tdbt_nd * zincflx;
+  S.ring[0][cslot][1][G] = tdbtc_nd * zincflx;
+  int filled = 1, level0 = 0;
+  // carry of the downward recurrence: level r values of each path
+  float c_tdbt = 1.0f, c_tdn = 1.0f, c_rdnd = 0.0f;
+  float t_tdbt = 1.0f, t_tdn = 1.0f, t_rdnd = 0.0f;
+  // layer values are loaded one layer ahead
+  const float *rl = recs + static_cast<size_t>(n - 1) * kSwRec;
+  float nx_tg = rl[G], nx_tr = rl[kSwRecTaur + G];
+  float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
+  const float *cl = crec + static_cast<size_t>(n - 1) * kSwRec;
+  if (!clear_only) { nx_ct = cl[0]; nx_cs = cl[1]; nx_ca = cl[2]; nx_co = cl[3]; }
+  uint32_t nx_word = maskbase[static_cast<size_t>(n - 1) * mstride];
+  for (int r = 0; r < n; ++r) {
+    const int l = n - 1 - r;
+    const uint32_t word = nx_word;
+    const float tr = nx_tr, tg = nx_tg;
+    const float ct = nx_ct, cs = nx_cs, ca = nx_ca, co = nx_co;
+    if (l > 0) {
+      const float *q = recs + static_cast<size_t>(l - 1) * kSwRec;
+      nx_tg = q[G];
+      nx_tr = q[kSwRecTaur + G];
+      if (!clear_only) {
+        const float *cq = crec + static_cast<size_t>(l - 1) * kSwRec;
+        nx_ct = cq[0]; nx_cs = cq[1]; nx_ca = cq[2]; nx_co = cq[3];
+      }
+      nx_word = maskbase[static_cast<size_t>(l - 1) * mstride];
+    }
+    const bool cldb = (word & bit) != 0u;
+    const float cloud = cldb ? 1.0f : 0.0f;
+    const float clear = 1.0f - cloud;
+    const float ztau = (tr + tg) + 0.0f;
+    float zom = tr + 0.0f * 1.0f;
+    const float zgr = 0.0f * 1.0f * 0.0f / zom;
+    zom = zom / ztau;
+    const float dbtc_nd = exp_lookup(T, ztau / mu);
+    tdbtc_nd = tdbtc_nd * dbtc_nd;
+    const float zf = zgr * zgr;
+    const float zwf = zom * zf;
+    const float ztauc = (1.0f - zwf) * ztau;
+    const float zomcc = (zom - zwf) / (1.0f - zwf);
+    const float zgcc = (zgr - zf) / (1.0f - zf);
+    const RT4 c = reftra(T, true, zgcc, mu, ztauc, zomcc);
+    const float dbtc = exp_lookup(T, ztauc / mu);
+    stc[r].rt = make_float4(c.ref, c.refd, c.tra, c.trad);
+    stc[r].dn = make_float4(dbtc, c_tdbt, c_tdn, c_rdnd);
+    // downward recurrence of vrtqdr (sw:3681-3702) for level r + 1
+    {
+      const float tdbt_next = c_tdbt * dbtc;
+      float tdn_next, rdnd_next;
+      if (r == 0) {
+        tdn_next = c.tra;
+        rdnd_next = c.refd;
+      } else {
+        const float zreflect = 1.0f / (1.0f - c.refd * c_rdnd);
+        tdn_next = c_tdbt * c.tra + c.trad * ((c_tdn - c_tdbt) + c_tdbt * c.ref * c_rdnd) * zreflect;
+        rdnd_next = c.refd + c.trad * c.trad * c_rdnd * zreflect;
+      }
+      c_tdbt = tdbt_next;
+      c_tdn = tdn_next;
+      c_rdnd = rdnd_next;
+    }
+    if (!clear_only) {
+      const float tcld = cldb ? ct : 0.0f;
+      const float wcld = cldb ? cs : 1.0f;
+      const float gcld = cldb ? ca : 0.0f;
+      const float taor = cldb ? co : 0.0f;
+      const float tauorig = ztau + taor;
+      const float dbtmo_nd = exp_lookup(T, tauorig / mu);
+      const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
+      tdbt_nd = tdbt_nd * dbt_nd;
+      const float ztauo = ztauc + tcld;
+      float zomco = ztauc * zomcc + tcld * wcld;
+      const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
+      zomco = zomco / ztauo;
+      const RT4 o = reftra(T, cloud > repclc, zgco, mu, ztauo, zomco);
+      const float ref = clear * c.ref + cloud * o.ref;
+      const float refd = clear * c.refd + cloud * o.refd;
+      const float tra = clear * c.tra + cloud * o.tra;
+      const float trad = clear * c.trad + cloud * o.trad;
+      const float dbtmo = exp_lookup(T, ztauo / mu);
+      const float dbt = clear * dbtc + cloud * dbtmo;
+      stt[r].rt = make_float4(ref, refd, tra, trad);
+      stt[r].dn = make_float4(dbt, t_tdbt, t_tdn, t_rdnd);
+      const float tdbt_next = t_tdbt * dbt;
+      float tdn_next, rdnd_next;
+      if (r == 0) {
+        tdn_next = tra;
+        rdnd_next = refd;
+      } else {
+        const float zreflect = 1.0f / (1.0f - refd * t_rdnd);
+        tdn_next = t_tdbt * tra + trad * ((t_tdn - t_tdbt) + t_tdbt * ref * t_rdnd) * zreflect;
+        rdnd_next = refd + trad * trad * t_rdnd * zreflect;
+      }
+      t_tdbt = tdbt_next;
+      t_tdn = tdn_next;
+      t_rdnd = rdnd_next;
+    } else {
+      tdbt_nd = tdbtc_nd;
+    }
+    S.ring[filled][cslot][0][G] = tdbt_nd * zincflx;
+    S.ring[filled][cslot][1][G] = tdbtc_nd * zincflx;
+    if (++filled == kRing || r == n - 1) {
+      sweep_flush(S, filled, 2, dtypes, level0, 1);
+      level0 += filled;
+      filled = 0;
+    }
+  }
+
+  // ---- bottom-up pass: upward adding and level fluxes (vrtqdr, sw:3655-3720)
+  const int utypes[4] = {0, 1, 2, 3};
+  float rupc = C.albedo, rupdc = C.albedo;
+  float rupt = C.albedo, rupdt = C.albedo;
+  level0 = n;
+  // surface level n: albedo reflection, no transmission; the recurrence's level-n values
+  SwLevel c = {make_float4(C.albedo, C.albedo, 0.0f, 0.0f), make_float4(0.0f, c_tdbt, c_tdn, c_rdnd)};
+  SwLevel t = {make_float4(C.albedo, C.albedo, 0.0f, 0.0f), make_float4(0.0f, t_tdbt, t_tdn, t_rdnd)};
+  if (clear_only) t = c;
+  for (int k = n; k >= 0; --k) {
+    SwLevel nc = c, nt = t;
+    if (k > 0) {
+      nc = stc[k - 1];
+      if (!clear_only) nt = stt[k - 1];
+    }
+    if (k < n) {
+      const float zrc = 1.0f / (1.0f - rupdc * c.rt.y);
+      const float nrupc = c.rt.x + c.rt.w * ((c.rt.z - c.dn.x) * rupdc + c.dn.x * rupc) * zrc;
+      const float nrupdc = c.rt.y + c.rt.w * c.rt.w * rupdc * zrc;
+      rupc = nrupc;
+      rupdc = nrupdc;
+      if (!clear_only) {
+        const float zrt = 1.0f / (1.0f - rupdt * t.rt.y);
+        const float nrupt = t.rt.x + t.rt.w * ((t.rt.z - t.dn.x) * rupdt + t.dn.x * rupt) * zrt;
+        const float nrupdt = t.rt.y + t.rt.w * t.rt.w * rupdt * zrt;
+        rupt = nrupt;
+        rupdt = nrupdt;
+      }
+    }
+    // level fluxes; tdbt = dn.y, tdn = dn.z, rdnd = dn.w
+    const float zrefc = 1.0f / (1.0f - c.dn.w * rupdc);
+    const float fuc = (c.dn.y * rupc + (c.dn.z - c.dn.y) * rupdc) * zrefc;
+    const float fdc = c.dn.y + (c.dn.z - c.dn.y + c.dn.y * rupc * c.dn.w) * zrefc;
+    float fut = fuc, fdt = fdc;
+    if (!clear_only) {
+      const float zreft = 1.0f / (1.0f - t.dn.w * rupdt);
+      fut = (t.dn.y * rupt + (t.dn.z - t.dn.y) * rupdt) * zreft;
+      fdt = t.dn.y + (t.dn.z - t.dn.y + t.dn.y * rupt * t.dn.w) * zreft;
+    }
+    S.ring[filled][cslot][0][G] = fut * zincflx;
+    S.ring[filled][cslot][1][G] = fdt * zincflx;
+    S.ring[filled][cslot][2][G] = fuc * zincflx;
+    S.ring[filled][cslot][3][G] = fdc * zincflx;
+    if (++filled == kRing || k == 0) {
+      sweep_flush(S, filled, 4, utypes, level0, -1);
+      level0 -= filled;
+      filled = 0;
+    }
+    c = nc;
+    t = nt;
+  }
+
+  // ---- outputs of the block's live columns (sw:2285-2301, 2536-2719)
+  for (int q = threadIdx.x; q < kSweepCols * kMaxLay; q += kSweepThreads) {
+    const int cs = q / kMaxLay, l = q - cs * kMaxLay;
+    const int uq = u0 + cs;
+    if (l >= a.nk || uq >= a.chunk_count || a.chunk_first + uq >= nday) continue;
+    sw_layer_output(a, sw_colrecs(a)[uq].C, l, &S.sums[cs][0][0], kMaxLev);
+  }
+  if (G == 0 && live) sw_column_outputs(a, C, col, &S.sums[cslot][0][0], kMaxLev);
 }
 
 }  // namespace
@@ -1268,45 +1144,33 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-size_t sw_split_terms_floats(int nk, int ncol) {
-  // terms, column records, layer records
-  return sw_terms_only_floats(nk, ncol) +
-         (kSwColRecFloats + static_cast<size_t>(kSwRec) * (nk + 1)) * static_cast<size_t>(ncol);
+size_t sw_record_floats(int nk, int chunk) {
+  return (kSwColRecFloats + static_cast<size_t>(kSwRec) * (nk + 1)) * static_cast<size_t>(chunk);
 }
 
-cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+cudaError_t launch_sw_columns(const Tables &T, const SwArgs &args, cudaStream_t stream) {
+  SwArgs a = args;
   const int threads = 128;
-  if (a.split_terms) {
-    // small domain: g-point split schedule over all ncol list slots, ordered
-    // g-point sums, then the column outputs
-    const int blocks = (a.ncol + threads - 1) / threads;
-    sw_colprep_kernel<<<(a.ncol + 3) / 4, threads, 0, stream>>>(T, a);
+  const int n = a.nk + 1;
+  // The day count is known only on the device: chunks cover all ncol list
+  // slots; slots at or beyond the day count exit at once.
+  for (int first = 0; first < a.ncol; first += a.chunk_capacity) {
+    a.chunk_first = first;
+    a.chunk_count = a.ncol - first < a.chunk_capacity ? a.ncol - first : a.chunk_capacity;
+    sw_colprep_kernel<<<(a.chunk_count + 3) / 4, threads, 0, stream>>>(T, a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const long long layers = static_cast<long long>(a.ncol) * (a.nk + 1);
-    sw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kSwBands), threads, 0, stream>>>(
+    const long long layers = static_cast<long long>(a.chunk_count) * n;
+    sw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kSwBands), threads, 0,
+                       stream>>>(T, a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sw_source_kernel<<<dim3((a.chunk_count + threads - 1) / threads, kSwBands), threads, 0, stream>>>(T, a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sw_sweep_kernel<<<(a.chunk_count + kSweepCols - 1) / kSweepCols, kSweepThreads, sizeof(SweepShared), stream>>>(
         T, a);
     e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    sw_source_kernel<<<dim3(blocks, kSwBands), threads, 0, stream>>>(T, a);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    sw_gsplit_kernel<<<dim3(blocks, kSwGpts), threads, 0, stream>>>(T, a, 0, a.ncol);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    sw_gsum_kernel<<<dim3(blocks, 6 * (a.nk + 2)), threads, 0, stream>>>(a, 0, a.ncol);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    sw_split_finish_kernel<<<a.ncol, 64, 0, stream>>>(T, a, 0, a.ncol);
-    return cudaGetLastError();
-  }
-  // The day count is known only on the device: launch over ncol list slots in
-  // chunks; slots at or beyond the day count exit at once.
-  const int chunk = a.chunk_columns > 0 ? a.chunk_columns : kSwChunkColumns;
-  for (int first = 0; first < a.ncol; first += chunk) {
-    const int count = a.ncol - first < chunk ? a.ncol - first : chunk;
-    sw_kernel<<<(count + threads - 1) / threads, threads, 0, stream>>>(T, a, first, count);
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
