@@ -46,20 +46,32 @@ class _Out(ctypes.Structure):
     _fields_ = [(n, _F) for n in _OUT_FIELDS]
 
 
-def build(force: bool = False) -> Path:
-    """Compile the oracle with its Makefile (gcc, no GPU needed)."""
+COUNT_LIB_PATH = HERE / "liboracle_rrtmg_count.so"
+
+
+def build(force: bool = False, counted: bool = False) -> Path:
+    """Compile the oracle with its Makefile (gcc, no GPU needed); ``counted``
+    builds the FLOP-counting variant (flop_count.h) instead."""
     srcs = [HERE / n for n in ("oracle_common.c", "oracle_lw.c", "oracle_sw.c", "oracle.h",
                                 "oracle_internal.h")]
-    if force or not LIB_PATH.exists() or any(s.stat().st_mtime > LIB_PATH.stat().st_mtime for s in srcs):
-        subprocess.run(["make", "-s", "-C", str(HERE), "liboracle_rrtmg.so"], check=True)
-    return LIB_PATH
+    lib = COUNT_LIB_PATH if counted else LIB_PATH
+    if counted:
+        srcs += [HERE / "flop_count.h", HERE / "flop_count.cc"]
+    if force or not lib.exists() or any(s.stat().st_mtime > lib.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE), lib.name], check=True)
+    return lib
 
 
 class Oracle:
     """Loaded oracle library plus one table blob."""
 
-    def __init__(self, blob_path: str | os.PathLike, nthreads: int | None = None):
-        self.lib = ctypes.CDLL(str(build()))
+    def __init__(self, blob_path: str | os.PathLike, nthreads: int | None = None, counted: bool = False):
+        self.lib = ctypes.CDLL(str(build(counted=counted)))
+        self.counted = counted
+        if counted:
+            nthreads = 1  # the counters are per thread
+            self.lib.ora_flop_counts_take.restype = None
+            self.lib.ora_flop_counts_take.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
         self.lib.ora_tables_load.restype = ctypes.c_void_p
         self.lib.ora_tables_load.argtypes = [ctypes.c_char_p]
         self.lib.ora_tables_free.argtypes = [ctypes.c_void_p]
@@ -79,6 +91,13 @@ class Oracle:
         if tables:
             self.lib.ora_tables_free(tables)
             self.tables = None
+
+    def take_counts(self) -> dict:
+        """Operations counted since the last call (counted build only): binary32
+        add (incl. subtract), mul, div, sqrt, exp, log, pow."""
+        buf = (ctypes.c_ulonglong * 7)()
+        self.lib.ora_flop_counts_take(buf)
+        return dict(zip(("add", "mul", "div", "sqrt", "exp", "log", "pow"), (int(v) for v in buf)))
 
     # ------------------------------------------------------------------
     @staticmethod
