@@ -47,10 +47,12 @@ struct rrtmg_ctx {
   // launch schedule (rrtmg_set_schedule)
   int lw_chunk = kLwChunkColumns, sw_chunk = kSwChunkColumns, sw_split_max = kSwSplitMaxColumns;
   int lw_split_max = kLwSplitMaxColumns;
-  // optional per-launch timing: a ring of calls per side (0 LW, 1 SW), each
-  // with kTimingMarks events recorded around the call's three launches
+  // optional per-phase timing: a ring of calls per side (0 LW, 1 SW); each
+  // call records events between its phases (McICA, then per chunk the optics
+  // launches and the sweep launch), marks[side][slot] of them
   bool timing = false;
-  std::vector<cudaEvent_t> events[2];
+  std::vector<std::vector<cudaEvent_t>> events[2];
+  std::vector<int> marks[2];
   int timing_next[2] = {0, 0};
   int timing_count[2] = {0, 0};
   // radiation prologue: SVML sin/cos constants from the blob, and the CAM
@@ -66,7 +68,6 @@ struct rrtmg_ctx {
 
 namespace {
 constexpr int kTimingSlots = 256;
-constexpr int kTimingMarks = 4;
 
 // Claims the next timing slot of `side`, or -1 when timing is off.
 int timing_slot(rrtmg_ctx *ctx, int side) {
@@ -75,11 +76,30 @@ int timing_slot(rrtmg_ctx *ctx, int side) {
   const int slot = ctx->timing_next[side];
   ctx->timing_next[side] = (slot + 1) % kTimingSlots;
   if (ctx->timing_count[side] < kTimingSlots) ++ctx->timing_count[side];
+  ctx->marks[side][slot] = 0;
   return slot;
 }
 
-void timing_mark(rrtmg_ctx *ctx, int side, int slot, int mark, cudaStream_t stream) {
-  if (slot >= 0) cudaEventRecord(ctx->events[side][slot * kTimingMarks + mark], stream);
+// Records the slot's next event on `stream` (events are created on first use).
+void timing_mark(rrtmg_ctx *ctx, int side, int slot, cudaStream_t stream) {
+  if (slot < 0) return;
+  cudaEvent_t ev = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mutex);
+    std::vector<cudaEvent_t> &v = ctx->events[side][slot];
+    const int m = ctx->marks[side][slot];
+    if (m == static_cast<int>(v.size())) {
+      cudaEvent_t fresh = nullptr;
+      if (cudaEventCreate(&fresh) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+      }
+      v.push_back(fresh);
+    }
+    ev = v[m];
+    ctx->marks[side][slot] = m + 1;
+  }
+  cudaEventRecord(ev, stream);
 }
 }  // namespace
 
@@ -491,7 +511,8 @@ void rrtmg_destroy(rrtmg_ctx *ctx) {
   cudaFree(ctx->dev_blob);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   for (auto &side : ctx->events)
-    for (cudaEvent_t ev : side) cudaEventDestroy(ev);
+    for (auto &slot : side)
+      for (cudaEvent_t ev : slot) cudaEventDestroy(ev);
   delete ctx;
 }
 
@@ -542,47 +563,34 @@ static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   st = get_jumps(ctx, nlay, kLwGpts, 150, &jumps);
   if (st != RRTMG_OK) return st;
   uint32_t *mask = nullptr;
-  float *terms = nullptr;
+  float *scratch = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
-  int lw_chunk_setting, lw_split_max;
+  int lw_chunk_setting;
   {
     std::lock_guard<std::mutex> lk(ctx->mutex);
     lw_chunk_setting = ctx->lw_chunk;
-    lw_split_max = ctx->lw_split_max;
   }
-  const bool gsplit = ncol <= lw_split_max;
-  const int chunk = gsplit || ncol < lw_chunk_setting ? ncol : lw_chunk_setting;
-  const size_t terms_bytes = lw_terms_floats(cfg->nk, chunk) * sizeof(float);
+  const int chunk = ncol < lw_chunk_setting ? ncol : lw_chunk_setting;
   e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
-  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&terms), terms_bytes, ctx->pool, stream);
+  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&scratch), lw_scratch_floats(nlay, chunk) * sizeof(float),
+                              ctx->pool, stream);
   if (e != cudaSuccess) {
     cudaFreeAsync(mask, stream);
-    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw band terms)");
-  }
-  float *optics = nullptr;
-  if (gsplit) {
-    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&optics), lw_optics_floats(nlay, ncol) * sizeof(float),
-                                ctx->pool, stream);
-    if (e != cudaSuccess) {
-      cudaFreeAsync(terms, stream);
-      cudaFreeAsync(mask, stream);
-      return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw layer optics)");
-    }
+    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw layer records)");
   }
 
   const int tslot = timing_slot(ctx, 0);
-  timing_mark(ctx, 0, tslot, 0, stream);
+  timing_mark(ctx, 0, tslot, stream);
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kLwGpts; m.words = kLwMaskWords;
   m.enabled = icld >= 1;
   m.live = live;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
-  timing_mark(ctx, 0, tslot, 1, stream);
+  timing_mark(ctx, 0, tslot, stream);
   if (e != cudaSuccess) {
-    if (optics) cudaFreeAsync(optics, stream);
-    cudaFreeAsync(terms, stream);
+    cudaFreeAsync(scratch, stream);
     cudaFreeAsync(mask, stream);
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
@@ -602,27 +610,21 @@ static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   a.upb = out->lwupb; a.upbc = out->lwupbc; a.dnb = out->lwdnb; a.dnbc = out->lwdnbc;
   a.glw = out->glw; a.olr = out->olr; a.lwcf = out->lwcf;
   a.zero2[0] = out->lwuptcln; a.zero2[1] = out->lwdntcln; a.zero2[2] = out->lwupbcln; a.zero2[3] = out->lwdnbcln;
-  a.terms = terms;
-  a.optics = optics;
-  // chunks of columns: band groups then finish per chunk, reusing the term
-  // scratch; timing mark 2 follows the last chunk's band groups, so the
-  // finish launches of the earlier chunks count with the band groups
+  a.scratch = scratch;
+  a.chunk_capacity = chunk;
+  // chunks of columns, each through its optics and then its sweep, reusing the scratch
   for (int first = 0; first < ncol && e == cudaSuccess; first += chunk) {
     a.chunk_first = first;
     a.chunk_count = ncol - first < chunk ? ncol - first : chunk;
-    e = gsplit ? launch_lw_gsplit(ctx->tables, a, stream) : launch_lw_groups(ctx->tables, a, stream);
-    if (first + chunk >= ncol) timing_mark(ctx, 0, tslot, 2, stream);
-    if (e == cudaSuccess) e = launch_lw_finish(a, stream);
+    e = launch_lw_chunk_optics(ctx->tables, a, stream);
+    timing_mark(ctx, 0, tslot, stream);
+    if (e == cudaSuccess) e = launch_lw_chunk_sweep(ctx->tables, a, stream);
+    timing_mark(ctx, 0, tslot, stream);
   }
-  timing_mark(ctx, 0, tslot, 3, stream);
-  if (optics) {
-    cudaError_t eo = cudaFreeAsync(optics, stream);
-    if (e == cudaSuccess && eo != cudaSuccess) e = eo;
-  }
-  cudaError_t ef = cudaFreeAsync(terms, stream);
+  cudaError_t ef = cudaFreeAsync(scratch, stream);
   cudaError_t ef2 = cudaFreeAsync(mask, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
-  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(lw band terms)");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(lw layer records)");
   if (ef2 != cudaSuccess) return cuda_fail(ctx, ef2, "cudaFreeAsync(mcica mask)");
   return RRTMG_OK;
 }
@@ -668,14 +670,14 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
     return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(day list)");
   }
   const int tslot = timing_slot(ctx, 1);
-  timing_mark(ctx, 1, tslot, 0, stream);
+  timing_mark(ctx, 1, tslot, stream);
   McicaArgs m{};
   m.ncol = ncol; m.ny = cfg->ny; m.nk = cfg->nk; m.nlay = nlay; m.nsub = kSwGpts; m.words = kSwMaskWords;
   m.enabled = icld >= 1;
   m.live = live;
   m.p3d = in->p3d; m.cldfra = in->cldfra3d; m.jumps = jumps; m.mask = mask;
   e = launch_mcica(m, stream);
-  timing_mark(ctx, 1, tslot, 1, stream);
+  timing_mark(ctx, 1, tslot, stream);
   if (e != cudaSuccess) {
     cudaFreeAsync(daylist, stream);
     cudaFreeAsync(mask, stream);
@@ -716,10 +718,18 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
     return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(sw layer records)");
   }
   a.records = records;
+  // the day count is known only on the device: the chunks cover all ncol
+  // list slots, and slots at or beyond the day count exit at once; the day
+  // list counts with the first chunk's optics
   e = launch_sw_daylist(a, stream);
-  timing_mark(ctx, 1, tslot, 2, stream);
-  if (e == cudaSuccess) e = launch_sw_columns(ctx->tables, a, stream);
-  timing_mark(ctx, 1, tslot, 3, stream);
+  for (int first = 0; first < ncol && e == cudaSuccess; first += a.chunk_capacity) {
+    a.chunk_first = first;
+    a.chunk_count = ncol - first < a.chunk_capacity ? ncol - first : a.chunk_capacity;
+    e = launch_sw_chunk_optics(ctx->tables, a, stream);
+    timing_mark(ctx, 1, tslot, stream);
+    if (e == cudaSuccess) e = launch_sw_chunk_sweep(ctx->tables, a, stream);
+    timing_mark(ctx, 1, tslot, stream);
+  }
   {
     cudaError_t es = cudaFreeAsync(records, stream);
     if (e == cudaSuccess) e = es;
@@ -896,20 +906,11 @@ extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_c
 
 extern "C" rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable) {
   if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
-  DeviceGuard guard(ctx->device);
-  cudaError_t e = guard.status();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   std::lock_guard<std::mutex> lk(ctx->mutex);
   if (enable && ctx->events[0].empty()) {
-    for (auto &side : ctx->events) {
-      side.resize(static_cast<size_t>(kTimingSlots) * kTimingMarks);
-      for (cudaEvent_t &ev : side) {
-        e = cudaEventCreate(&ev);
-        if (e != cudaSuccess) {
-          ctx->last_error = std::string("cudaEventCreate: ") + cudaGetErrorString(e);
-          return RRTMG_CUDA;
-        }
-      }
+    for (int side = 0; side < 2; ++side) {
+      ctx->events[side].resize(kTimingSlots);
+      ctx->marks[side].assign(kTimingSlots, 0);
     }
   }
   ctx->timing = enable != 0;
@@ -923,18 +924,23 @@ extern "C" int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_ca
   DeviceGuard guard(ctx->device);
   if (guard.status() != cudaSuccess) return -1;
   std::lock_guard<std::mutex> lk(ctx->mutex);
+  if (ctx->events[side].empty()) return 0;
   const int count = ctx->timing_count[side] < max_calls ? ctx->timing_count[side] : max_calls;
   const int newest = (ctx->timing_next[side] + kTimingSlots - 1) % kTimingSlots;
   for (int q = 0; q < count; ++q) {
     // oldest of the returned calls first
     const int slot = (newest - (count - 1 - q) + kTimingSlots) % kTimingSlots;
-    const cudaEvent_t *ev = &ctx->events[side][static_cast<size_t>(slot) * kTimingMarks];
-    if (cudaEventSynchronize(ev[kTimingMarks - 1]) != cudaSuccess) return -1;
-    for (int m = 0; m + 1 < kTimingMarks; ++m) {
+    const std::vector<cudaEvent_t> &ev = ctx->events[side][slot];
+    const int n = ctx->marks[side][slot];
+    if (n < 2 || cudaEventSynchronize(ev[n - 1]) != cudaSuccess) return -1;
+    // interval 0: McICA; odd intervals: a chunk's optics; even ones: its sweep
+    float phase[3] = {0.0f, 0.0f, 0.0f};
+    for (int m = 0; m + 1 < n; ++m) {
       float t = 0.0f;
       if (cudaEventElapsedTime(&t, ev[m], ev[m + 1]) != cudaSuccess) return -1;
-      ms[q * (kTimingMarks - 1) + m] = t;
+      phase[m == 0 ? 0 : (m % 2 == 1 ? 1 : 2)] += t;
     }
+    for (int k = 0; k < 3; ++k) ms[q * 3 + k] = phase[k];
   }
   return count;
 }

@@ -39,16 +39,17 @@ struct LwArgs {
   float *rthraten, *rthratenc;
   float *upt, *uptc, *dnt, *dntc, *upb, *upbc, *dnb, *dnbc, *glw, *olr, *lwcf;
   float *zero2[4];  // *cln fields, written as zeros
-  float *terms;     // band-group schedule scratch, lw_terms_floats(nk, chunk_count) floats
-  float *optics;    // g-point split schedule: lw_optics_floats(nlay, chunk_count) floats, else null
-  int chunk_first, chunk_count;  // columns of one band-group/finish launch pair
+  float *scratch;       // sweep schedule: lw_scratch_floats(nlay, chunk_capacity) floats
+  int chunk_capacity;   // columns per chunk of the sweep schedule
+  int chunk_first, chunk_count;  // the chunk being launched
   const int *live;  // null, or a device count of leading columns to process
 };
 
-// default columns per band-group/finish launch pair (the term scratch holds one chunk)
-constexpr int kLwChunkColumns = 131072;
-// Domains of at most this many columns run the LW g-point split schedule
-// (its optics scratch: 1,376 bytes per column and layer).
+// default columns per chunk of the LW sweep schedule (its scratch takes about
+// 107 KB per column at nk = 50 and a 50 hPa top)
+constexpr int kLwChunkColumns = 16384;
+// no longer used by the LW path (every domain runs the sweep schedule); kept
+// as the default of the schedule field that used to select the split schedule
 constexpr int kLwSplitMaxColumns = 2048;
 
 struct SwArgs {
@@ -80,20 +81,19 @@ constexpr int kSwSplitMaxColumns = 4096;
 cudaError_t launch_mcica(const McicaArgs &a, cudaStream_t stream);
 // fused schedule (one thread per column, no scratch)
 cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream);
-// band-group schedule (thread per column and band group), then the finish
-// kernel (ordered band sums, fluxes, heating); both need a.terms
-size_t lw_terms_floats(int nk, int ncol);
-cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stream);
-cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream);
-// g-point split schedule for small domains (columns chunk_first ..): fills the
-// same band terms as launch_lw_groups.
-cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream);
-size_t lw_optics_floats(int nlay, int ncol);
-// day-column compaction (writes the night columns), then the column kernel over
-// the day columns; both need a.nday and a.daylist (1 + ncol ints)
+// sweep schedule, one chunk of columns (a.chunk_first, a.chunk_count) at a
+// time: the optics launches (column set-up, layer set-up, gas optics), then
+// the sweep launch (radiative transfer, flux sums, heating, outputs)
+size_t lw_scratch_floats(int nlay, int chunk);
+cudaError_t launch_lw_chunk_optics(const Tables &T, const LwArgs &a, cudaStream_t stream);
+cudaError_t launch_lw_chunk_sweep(const Tables &T, const LwArgs &a, cudaStream_t stream);
+// day-column compaction (writes the night columns; needs a.nday and a.daylist,
+// 1 + ncol ints), then per chunk of day-list slots the optics launches (column
+// set-up, layer optics, solar source) and the sweep launch
 cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);
 size_t sw_record_floats(int nk, int chunk);
-cudaError_t launch_sw_columns(const Tables &T, const SwArgs &a, cudaStream_t stream);
+cudaError_t launch_sw_chunk_optics(const Tables &T, const SwArgs &a, cudaStream_t stream);
+cudaError_t launch_sw_chunk_sweep(const Tables &T, const SwArgs &a, cudaStream_t stream);
 
 // Radiation prologue (cloud fraction, cos zenith, CAM ozone).  Constants of
 // the SVML sin/cos emulation in the reference's order (svml.sinf: 12,

@@ -1238,52 +1238,72 @@ __global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Band-group schedule.  Thread (column, group) sweeps its column for the bands
-// of one group only, so the group's <= 16 g-point radiances stay in registers
-// and a CTA runs the gas optics of one group.  Each band's level term
-// (bandsum * 0.5) * delwave (lw:170-199) goes to a scratch array; the finish
-// kernel adds the 16 terms of a level in band order, which is the reference's
-// sum, then forms fluxes and heating rates.
+// Sweep schedule, every domain size.  Columns are processed in chunks; per
+// chunk:
+//   lw_colprep_kernel  warp = column: buffer layers, column integrals (laytrop,
+//                      pwvcm, summed in layer order), band diffusivities, and
+//                      whether any layer is cloudy;
+//   lw_layer_kernel    thread = (layer, column): the layer set-up (make_layer)
+//                      once; the inputs of the gas optics go to a
+//                      structure-of-arrays record, each band's Planck terms and
+//                      cloud optical depth and the layer's cloud flag to the
+//                      layer record;
+//   lw_gas_kernel      thread = (layer, column), grid.y = band: the band's gas
+//                      optical depths and Planck fractions (taumol) into the
+//                      layer record, so every warp runs one band's code;
+//   lw_sweep_kernel    block = kLwSweepCols columns x 140 g-points, thread =
+//                      one g-point: the downward and upward radiance sweeps of
+//                      rtrnmc (lw:5476-5722) from the layer records; each
+//                      level's radiances go to shared memory, where they are
+//                      summed in g-point order per band and the band terms in
+//                      band order (lw:170-199); then fluxes, heating rates and
+//                      the 2-D outputs.
+// Operation for operation these are the reference's statements in its order,
+// the same as the fused lw_kernel's, so the results are bit-identical.
 // ---------------------------------------------------------------------------
 
-// Scratch index of a band term: type 0/1 upward total/clear, 2/3 downward
-// total/clear; slot = flux level 0..nk, or nk + 1 for the top of the
-// atmosphere (level nlay) when nlay > nk.
-__device__ __forceinline__ size_t term_index(const LwArgs &a, int type, int slot, int band, int col) {
-  return ((static_cast<size_t>(type) * (a.nk + 2) + slot) * kLwBands + band) * a.chunk_count + (col - a.chunk_first);
-}
+// Layer record (kLwRec floats): taug of each band's g-points from a 16-byte
+// boundary (kLwPadOfs), the Planck fractions likewise from kLwRecFracs, per
+// band (blay, dplankup, dplankdn, cloud optical depth) from kLwRecBand, and
+// the layer's cloud flag at kLwRecFlags.
+constexpr int kLwPadOfs[kLwBands] = {0, 12, 24, 40, 56, 72, 80, 92, 100, 112, 120, 128, 136, 140, 144, 148};
+constexpr int kLwPadG = 152;
+constexpr int kLwRecFracs = kLwPadG, kLwRecBand = 2 * kLwPadG, kLwRecFlags = kLwRecBand + 4 * kLwBands;
+constexpr int kLwRec = kLwRecFlags + 4;
+static_assert(kLwRec % 4 == 0, "layer records are float4 aligned");
+__constant__ int kLwPadOfsDev[kLwBands] = {0, 12, 24, 40, 56, 72, 80, 92, 100, 112, 120, 128, 136, 140, 144, 148};
+__constant__ int kNgcDev[kLwBands] = {10, 12, 16, 14, 16, 8, 12, 8, 12, 6, 8, 8, 4, 2, 2, 2};
+__constant__ int kGofsDev[kLwBands] = {0, 10, 22, 38, 52, 68, 76, 88, 96, 108, 114, 122, 130, 134, 136, 138};
 
-template <int B>
-__device__ __forceinline__ void zero_band(float *radA, float *radB) {
-  constexpr int ngc = kNgc[B];
-  constexpr int gofs = kGofs[B];
-#pragma unroll
-  for (int g = 0; g < ngc; ++g) {
-    radA[gofs + g] = 0.0f;
-    radB[gofs + g] = 0.0f;
-  }
-}
+// The Layer fields taumol reads, stored field by field ([field][layer][column]).
+#define RRTMG_LW_GAS_FLOATS(X)                                                                                   \
+  X(pavel) X(coldry) X(wx0) X(wx1) X(wx2) X(wx3) X(colh2o) X(colco2) X(colo3) X(coln2o) X(colco) X(colch4)      \
+  X(colo2) X(colbrd) X(fac00) X(fac01) X(fac10) X(fac11) X(rat_h2oco2) X(rat_h2oco2_1) X(rat_h2oo3)             \
+  X(rat_h2oo3_1) X(rat_h2on2o) X(rat_h2on2o_1) X(rat_h2och4) X(rat_h2och4_1) X(rat_n2oco2) X(rat_n2oco2_1)      \
+  X(rat_o3co2) X(rat_o3co2_1) X(selffac) X(selffrac) X(forfac) X(forfrac) X(minorfrac) X(scaleminor)            \
+  X(scaleminorn2)
+#define RRTMG_LW_GAS_INTS(X) X(jp) X(jt) X(jt1) X(indself) X(indfor) X(indminor) X(trop)
+#define RRTMG_LW_COUNT(name) +1
+constexpr int kLwGasFields = 0 RRTMG_LW_GAS_FLOATS(RRTMG_LW_COUNT) RRTMG_LW_GAS_INTS(RRTMG_LW_COUNT);
+#undef RRTMG_LW_COUNT
 
-template <int B, bool kDown>
-__device__ __forceinline__ void band_term(const Tables &T, const LwArgs &a, const Layer &L, const uint32_t *mask,
-                                          bool cloudy, int iceflag, const float *secdiff, float *radA, float *radB,
-                                          bool sep, int type, int slot, int col) {
-  float bs, bsc;
-  band_sums<B, kDown>(T, L, mask, cloudy, iceflag, secdiff[B], radA, radB, sep, bs, bsc);
-  if (slot >= 0) {
-    a.terms[term_index(a, type, slot, B, col)] = (bs * 0.5f) * kDelwave[B];
-    a.terms[term_index(a, type + 1, slot, B, col)] = (bsc * 0.5f) * kDelwave[B];
-  }
-}
+// Per-column record, computed once per column.
+struct ColRec {
+  Col C;
+  float secdiff[kLwBands];
+  int has_cloud;
+};
+constexpr size_t kColRecFloats = (sizeof(ColRec) + 15) / 16 * 4;
 
-template <int B>
-__device__ __forceinline__ void surface_term(const Tables &T, const LwArgs &a, const Layer &L0, const Col &C,
-                                             int indbound, float tbndfrac, float reflect, float *radA, float *radB,
-                                             int col) {
-  float bs, bsc;
-  surface_sums<B>(T, L0, C.semiss * planck(T, indbound, tbndfrac, B), reflect, radA, radB, bs, bsc);
-  a.terms[term_index(a, 0, 0, B, col)] = (bs * 0.5f) * kDelwave[B];
-  a.terms[term_index(a, 1, 0, B, col)] = (bsc * 0.5f) * kDelwave[B];
+// scratch of one chunk: column records, then the gas fields, then the layer records
+__device__ __forceinline__ const ColRec *col_records(const LwArgs &a) {
+  return reinterpret_cast<const ColRec *>(a.scratch);
+}
+__device__ __forceinline__ float *gas_fields(const LwArgs &a) {
+  return a.scratch + kColRecFloats * static_cast<size_t>(a.chunk_capacity);
+}
+__device__ __forceinline__ float *layer_records(const LwArgs &a) {
+  return gas_fields(a) + static_cast<size_t>(kLwGasFields) * a.nlay * a.chunk_capacity;
 }
 
 __device__ __forceinline__ bool load_mask(const LwArgs &a, int l, int col, uint32_t *mask) {
@@ -1294,96 +1314,6 @@ __device__ __forceinline__ bool load_mask(const LwArgs &a, int l, int col, uint3
     any |= mask[w];
   }
   return any != 0u;
-}
-
-template <int... Bs>
-__device__ __forceinline__ void lw_group(const Tables &T, const LwArgs &a, int col) {
-  Col C;
-  float secdiff[kLwBands];
-  bool has_cloud;
-  column_prologue(T, a, col, C, secdiff, has_cloud);
-  const int nlay = C.nlay, nk = C.nk;
-  float radA[kLwGpts], radB[kLwGpts];
-  (zero_band<Bs>(radA, radB), ...);
-
-  // downward sweep, top to bottom: level l gets the downward terms
-  bool iclddn = false;
-  for (int l = nlay - 1; l >= 0; --l) {
-    uint32_t mask[kLwMaskWords];
-    const bool cloudy = load_mask(a, l, col, mask);
-    iclddn = iclddn || cloudy;
-    const Layer L = make_layer(T, a, C, l);
-    const int slot = l <= nk ? l : -1;
-    (band_term<Bs, true>(T, a, L, mask, cloudy, C.iceflg, secdiff, radA, radB, iclddn, 2, slot, col), ...);
-  }
-  // surface emission and reflection: level 0 upward terms
-  {
-    const Layer L0 = make_layer(T, a, C, 0);
-    const float bt = C.tsfc - 159.0f;
-    const int indbound = clampi(static_cast<int>(bt), 1, 180);
-    const float tbndfrac = bt - static_cast<float>(indbound);
-    const float reflect = 1.0f - C.semiss;
-    (surface_term<Bs>(T, a, L0, C, indbound, tbndfrac, reflect, radA, radB, col), ...);
-  }
-  // upward sweep, bottom to top: level l + 1 gets the upward terms
-  for (int l = 0; l < nlay; ++l) {
-    uint32_t mask[kLwMaskWords];
-    const bool cloudy = load_mask(a, l, col, mask);
-    const Layer L = make_layer(T, a, C, l);
-    const int lev = l + 1;
-    const int slot = lev <= nk ? lev : (lev == nlay ? nk + 1 : -1);
-    (band_term<Bs, false>(T, a, L, mask, cloudy, C.iceflg, secdiff, radA, radB, has_cloud, 0, slot, col), ...);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// g-point split schedule for small domains, in two launches.
-// lw_colprep_kernel: thread (column) computes the column set-up once;
-// lw_layer_kernel: thread (column, layer) the layer set-up (make_layer) once.
-// lw_optics_kernel: thread (column, layer, band) computes the layer's gas
-//   optics of the band (taumol), its Planck terms and the band cloud optical
-//   depth into a per-column record (kLwOpticsFloats per layer).
-// lw_gsplit_kernel: thread (column, band, g-point) runs the two sweeps of one
-//   g-point from those records.  A half-warp owns one (column, band), lane g
-//   its g-point; the band's radiance sum of a level is taken in g order
-//   through shuffles and stored as the band term the finish kernel adds in
-//   band order: the operations and order of band_sums, so the results are
-//   bit-identical to the band-group schedule's while a column's latency drops
-//   from its largest band group to one g-point.
-// Record of a layer: taug[140], fracs[140], then per band blay, dplankup,
-// dplankdn and the cloud optical depth the band's cloudy g-points use.
-// ---------------------------------------------------------------------------
-constexpr int kLwOpticsFloats = 2 * kLwGpts + 4 * kLwBands;
-
-// Per-column record of the split schedule, computed once per column.
-struct ColRec {
-  Col C;
-  float secdiff[kLwBands];
-  int has_cloud;
-};
-// column records first, 16-byte aligned, then the layer records
-constexpr size_t kColRecFloats = (sizeof(ColRec) + 15) / 16 * 4;
-
-__device__ __forceinline__ const ColRec *col_records(const LwArgs &a) {
-  return reinterpret_cast<const ColRec *>(a.optics);
-}
-__device__ __forceinline__ float *layer_records(const LwArgs &a) {
-  return a.optics + kColRecFloats * static_cast<size_t>(a.chunk_count);
-}
-// the layers' set-up (make_layer), computed once per column and layer
-constexpr size_t kLayerFloats = (sizeof(Layer) + 15) / 16 * 4;
-__device__ __forceinline__ Layer *layer_setups(const LwArgs &a) {
-  return reinterpret_cast<Layer *>(layer_records(a) +
-                                   static_cast<size_t>(kLwOpticsFloats) * a.nlay * static_cast<size_t>(a.chunk_count));
-}
-
-// thread = (column, layer): the layer's set-up for every band's optics
-__global__ void __launch_bounds__(128) lw_layer_kernel(Tables T, LwArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.chunk_count * a.nlay) return;
-  const int lc = t / a.nlay, l = t - lc * a.nlay;
-  if (dead_column(a.live, a.chunk_first + lc)) return;
-  layer_setups(a)[t] = make_layer(T, a, col_records(a)[lc].C, l);
 }
 
 // A warp per column: the lanes take the layers of the column integrals, whose
@@ -1406,10 +1336,8 @@ __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
     bool trop;
     column_layer(T, a, C, l, trop, s_cd[w][l], s_wk[w][l]);
     trop_count += trop;
-    uint32_t any = 0;
-#pragma unroll
-    for (int q = 0; q < kLwMaskWords; ++q) any |= a.mask[(static_cast<size_t>(l) * kLwMaskWords + q) * a.ncol + col];
-    cloud = cloud || any != 0u;
+    uint32_t mask[kLwMaskWords];
+    cloud = load_mask(a, l, col, mask) || cloud;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) trop_count += __shfl_xor_sync(0xffffffffu, trop_count, o);
@@ -1424,85 +1352,122 @@ __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
   C.pwvcm = column_pwvcm(a, C, amttl, wvttl);
   column_secdiff(T, C, r.secdiff);
   r.has_cloud = has_cloud ? 1 : 0;
-  if (lane == 0) reinterpret_cast<ColRec *>(a.optics)[lc] = r;
+  if (lane == 0) reinterpret_cast<ColRec *>(a.scratch)[lc] = r;
 }
 
-template <int B>
-__device__ __forceinline__ void band_optics(const Tables &T, const Layer &L, bool cloudy_layer, int iceflag,
-                                            float *rec) {
-  constexpr int ngc = kNgc[B];
-  constexpr int gofs = kGofs[B];
-  float taug[ngc], fracs[ngc];
-  taumol<B>(T, L, taug, fracs);
-#pragma unroll
-  for (int g = 0; g < ngc; ++g) {
-    rec[gofs + g] = taug[g];
-    rec[kLwGpts + gofs + g] = fracs[g];
-  }
-  const float blay = planck(T, L.indlay, L.tlayfrac, B);
-  float *bq = rec + 2 * kLwGpts + 4 * B;
-  bq[0] = blay;
-  bq[1] = planck(T, L.indlev1, L.tlev1frac, B) - blay;
-  bq[2] = planck(T, L.indlev0, L.tlev0frac, B) - blay;
-  float teff = 0.0f;
-  if (cloudy_layer) {
-    bool active = false;
-    const float tauc = cloud_tau(T, L, B, iceflag, active);
-    teff = active ? tauc : 0.0f;
-  }
-  bq[3] = teff;
-}
-
-__global__ void __launch_bounds__(128) lw_optics_kernel(Tables T, LwArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int band = blockIdx.y;
-  if (t >= a.chunk_count * a.nlay) return;
-  const int lc = t / a.nlay, l = t - lc * a.nlay;
+// thread = (layer, chunk column), columns fastest
+__global__ void __launch_bounds__(128) lw_layer_kernel(Tables T, LwArgs a) {
+  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int l = static_cast<int>(idx / a.chunk_count);
+  const int lc = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
+  if (l >= a.nlay) return;
   const int col = a.chunk_first + lc;
   if (dead_column(a.live, col)) return;
   const Col &C = col_records(a)[lc].C;
+  const Layer L = make_layer(T, a, C, l);
+  float *gas = gas_fields(a) + static_cast<size_t>(l) * a.chunk_capacity + lc;
+  const size_t fstride = static_cast<size_t>(a.nlay) * a.chunk_capacity;
+  int f = 0;
+#define RRTMG_LW_PUT(name) gas[static_cast<size_t>(f++) * fstride] = L.name;
+#define RRTMG_LW_PUTI(name) gas[static_cast<size_t>(f++) * fstride] = __int_as_float(L.name);
+  RRTMG_LW_GAS_FLOATS(RRTMG_LW_PUT)
+  RRTMG_LW_GAS_INTS(RRTMG_LW_PUTI)
+#undef RRTMG_LW_PUT
+#undef RRTMG_LW_PUTI
   uint32_t mask[kLwMaskWords];
   const bool cloudy = load_mask(a, l, col, mask);
-  const Layer &L = layer_setups(a)[t];
-  float *rec = layer_records(a) + static_cast<size_t>(t) * kLwOpticsFloats;
-  switch (band) {
-    case 0: band_optics<0>(T, L, cloudy, C.iceflg, rec); break;
-    case 1: band_optics<1>(T, L, cloudy, C.iceflg, rec); break;
-    case 2: band_optics<2>(T, L, cloudy, C.iceflg, rec); break;
-    case 3: band_optics<3>(T, L, cloudy, C.iceflg, rec); break;
-    case 4: band_optics<4>(T, L, cloudy, C.iceflg, rec); break;
-    case 5: band_optics<5>(T, L, cloudy, C.iceflg, rec); break;
-    case 6: band_optics<6>(T, L, cloudy, C.iceflg, rec); break;
-    case 7: band_optics<7>(T, L, cloudy, C.iceflg, rec); break;
-    case 8: band_optics<8>(T, L, cloudy, C.iceflg, rec); break;
-    case 9: band_optics<9>(T, L, cloudy, C.iceflg, rec); break;
-    case 10: band_optics<10>(T, L, cloudy, C.iceflg, rec); break;
-    case 11: band_optics<11>(T, L, cloudy, C.iceflg, rec); break;
-    case 12: band_optics<12>(T, L, cloudy, C.iceflg, rec); break;
-    case 13: band_optics<13>(T, L, cloudy, C.iceflg, rec); break;
-    case 14: band_optics<14>(T, L, cloudy, C.iceflg, rec); break;
-    default: band_optics<15>(T, L, cloudy, C.iceflg, rec); break;
+  float4 *rec = reinterpret_cast<float4 *>(layer_records(a) + (static_cast<size_t>(lc) * a.nlay + l) * kLwRec);
+  const int iceflag = C.iceflg;
+#pragma unroll 1
+  for (int b = 0; b < kLwBands; ++b) {
+    const float blay = planck(T, L.indlay, L.tlayfrac, b);
+    const float dplankup = planck(T, L.indlev1, L.tlev1frac, b) - blay;
+    const float dplankdn = planck(T, L.indlev0, L.tlev0frac, b) - blay;
+    float teff = 0.0f;
+    if (cloudy) {
+      bool active = false;
+      const float tauc = cloud_tau(T, L, b, iceflag, active);
+      teff = active ? tauc : 0.0f;
+    }
+    rec[kLwRecBand / 4 + b] = make_float4(blay, dplankup, dplankdn, teff);
+  }
+  rec[kLwRecFlags / 4] = make_float4(cloudy ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// ngc values of v to float4s at dst (the tail padded with zeros).
+template <int NGC>
+__device__ __forceinline__ void store_padded(float4 *dst, const float *v) {
+#pragma unroll
+  for (int q = 0; q < (NGC + 3) / 4; ++q) {
+    const int g = 4 * q;
+    dst[q] = make_float4(v[g], g + 1 < NGC ? v[g + 1] : 0.0f, g + 2 < NGC ? v[g + 2] : 0.0f,
+                         g + 3 < NGC ? v[g + 3] : 0.0f);
   }
 }
 
-// One g-point of band_sums from a layer record: the new radiances (rA, rB).
+template <int B>
+__device__ __forceinline__ void gas_band(const Tables &T, const Layer &L, float4 *rec) {
+  constexpr int ngc = kNgc[B], pofs = kLwPadOfs[B];
+  float taug[ngc], fracs[ngc];
+  taumol<B>(T, L, taug, fracs);
+  store_padded<ngc>(rec + pofs / 4, taug);
+  store_padded<ngc>(rec + (kLwRecFracs + pofs) / 4, fracs);
+}
+
+// thread = (layer, chunk column), grid.y = band
+__global__ void __launch_bounds__(128) lw_gas_kernel(Tables T, LwArgs a) {
+  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int l = static_cast<int>(idx / a.chunk_count);
+  const int lc = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
+  if (l >= a.nlay || dead_column(a.live, a.chunk_first + lc)) return;
+  const float *gas = gas_fields(a) + static_cast<size_t>(l) * a.chunk_capacity + lc;
+  const size_t fstride = static_cast<size_t>(a.nlay) * a.chunk_capacity;
+  Layer L{};
+  int f = 0;
+#define RRTMG_LW_GET(name) L.name = gas[static_cast<size_t>(f++) * fstride];
+#define RRTMG_LW_GETI(name) L.name = __float_as_int(gas[static_cast<size_t>(f++) * fstride]);
+  RRTMG_LW_GAS_FLOATS(RRTMG_LW_GET)
+  RRTMG_LW_GAS_INTS(RRTMG_LW_GETI)
+#undef RRTMG_LW_GET
+#undef RRTMG_LW_GETI
+  float4 *rec = reinterpret_cast<float4 *>(layer_records(a) + (static_cast<size_t>(lc) * a.nlay + l) * kLwRec);
+  switch (blockIdx.y) {
+    case 0: gas_band<0>(T, L, rec); break;
+    case 1: gas_band<1>(T, L, rec); break;
+    case 2: gas_band<2>(T, L, rec); break;
+    case 3: gas_band<3>(T, L, rec); break;
+    case 4: gas_band<4>(T, L, rec); break;
+    case 5: gas_band<5>(T, L, rec); break;
+    case 6: gas_band<6>(T, L, rec); break;
+    case 7: gas_band<7>(T, L, rec); break;
+    case 8: gas_band<8>(T, L, rec); break;
+    case 9: gas_band<9>(T, L, rec); break;
+    case 10: gas_band<10>(T, L, rec); break;
+    case 11: gas_band<11>(T, L, rec); break;
+    case 12: gas_band<12>(T, L, rec); break;
+    case 13: gas_band<13>(T, L, rec); break;
+    case 14: gas_band<14>(T, L, rec); break;
+    default: gas_band<15>(T, L, rec); break;
+  }
+}
+
+// One g-point of band_sums: the new radiances (rA, rB) after one layer, from
+// the g-point's gas optical depth tg and Planck fraction fr, its band's
+// (blay, dplankup, dplankdn, cloud optical depth) bq, its McICA bit cld and
+// the layer's cloud flag.
 template <bool kDown>
-__device__ __forceinline__ void gpoint_step(const Tables &T, const float *rec, int G, int band, const uint32_t *mask,
-                                            bool cloudy_layer, float secdiff, float &rA, float &rB, bool sep_clear) {
-  const float tg = rec[G], fr = rec[kLwGpts + G];
-  const float *bq = rec + 2 * kLwGpts + 4 * band;
-  const float blay = bq[0], dplankup = bq[1], dplankdn = bq[2], teff = bq[3];
-  const bool cld = (mask[G >> 5] >> (G & 31)) & 1u;
+__device__ __forceinline__ void lw_step(const Tables &T, float tg, float fr, float4 bq, bool cld, bool cloudy_layer,
+                                        float secdiff, float &rA, float &rB, bool sep_clear) {
   float odepth = secdiff * tg;
   if (odepth < 0.0f) odepth = 0.0f;
   float odcld = 0.0f, efcl = 0.0f;
   if (cld) {
-    const float odcld_raw = secdiff * teff;
+    const float odcld_raw = secdiff * bq.w;
     const float abscld = 1.0f - glibc_expf(T, -odcld_raw);
     odcld = odcld_raw;
     efcl = abscld * 1.0f;
   }
-  const Terms tm = layer_terms(T, cloudy_layer, odepth, odcld, fr, blay, dplankdn, dplankup);
+  const Terms tm = layer_terms(T, cloudy_layer, odepth, odcld, fr, bq.x, bq.z, bq.y);
   const float cf = cld ? 1.0f : 0.0f;
   const float r = rA, rc = rB;
   float rn;
@@ -1525,202 +1490,170 @@ __device__ __forceinline__ void gpoint_step(const Tables &T, const float *rec, i
   rA = rn;
 }
 
-__constant__ int kNgcDev[kLwBands] = {10, 12, 16, 14, 16, 8, 12, 8, 12, 6, 8, 8, 4, 2, 2, 2};
-__constant__ int kGofsDev[kLwBands] = {0, 10, 22, 38, 52, 68, 76, 88, 96, 108, 114, 122, 130, 134, 136, 138};
+constexpr int kLwSweepCols = 2;                            // columns per block
+constexpr int kLwSweepThreads = 288;                       // 2 x 140 g-points in 9 warps; 8 padding threads
+constexpr int kLwRing = 8;                                 // levels of radiances per ordered-sum round
+static_assert(kLwSweepThreads >= kLwSweepCols * kLwGpts && kLwSweepThreads % 32 == 0, "sweep block shape");
 
-constexpr int kGsplitThreads = 160;  // 140 g-points of one column, padded to whole warps
+struct LwSweepShared {
+  float ring[kLwRing][kLwSweepCols][2][kLwGpts];  // total, clear radiance of each g-point
+  float flux[kLwSweepCols][4][kMaxLay + 1];       // up total, up clear, down total, down clear per level
+};
 
-// A block per column, thread G = g-point.  After each level the g-point
-// radiances go to shared memory (double-buffered by level, one barrier per
-// level) and 32 threads take the band sums in g order, total and clear, and
-// store the band terms.
-__global__ void __launch_bounds__(kGsplitThreads) lw_gsplit_kernel(Tables T, LwArgs a) {
-  __shared__ float s_rad[2][2][kLwGpts];  // [level parity][total, clear][g-point]
-  const int lc = blockIdx.x;
-  const int col = a.chunk_first + lc;
-  if (dead_column(a.live, col)) return;  // whole block
+// Sums the ring's levels: chain (column, total/clear, level) adds each band's
+// radiances in g-point order, then the band terms (bandsum * 0.5) * delwave in
+// band order (band_step, lw:170-199), times fluxfac.
+__device__ __forceinline__ void lw_flush(LwSweepShared &S, int count, int type0, int level0, int dir) {
+  __syncthreads();
+  const float pi = 3.1415926535897932384626433832795f;
+  const float fluxfac = pi * 2.0e4f;
+  const int chains = kLwSweepCols * 2 * count;
+  for (int ch = threadIdx.x; ch < chains; ch += kLwSweepThreads) {
+    const int j = ch % count;
+    const int rest = ch / count;
+    const int q = rest & 1;
+    const int c = rest >> 1;
+    const float *v = S.ring[j][c][q];
+    float total = 0.0f;
+#pragma unroll
+    for (int b = 0; b < kLwBands; ++b) {
+      float bandsum = 0.0f;
+      const float *vb = v + kGofsDev[b];
+      const int ngc = kNgcDev[b];
+      for (int g = 0; g < ngc; ++g) bandsum = bandsum + vb[g];
+      total = total + (bandsum * 0.5f) * kDelwave[b];
+    }
+    S.flux[c][type0 + q][level0 + dir * j] = total * fluxfac;
+  }
+  __syncthreads();
+}
+
+// Block = kLwSweepCols consecutive columns of the chunk.  A column past the
+// chunk or the live count repeats the block's first column so that every
+// thread takes the same barriers; its results are not written.
+__global__ void __launch_bounds__(kLwSweepThreads, 3) lw_sweep_kernel(Tables T, LwArgs a) {
+  __shared__ __align__(16) LwSweepShared S;
+  const int lc0 = blockIdx.x * kLwSweepCols;
+  if (lc0 >= a.chunk_count || dead_column(a.live, a.chunk_first + lc0)) return;  // whole block
   const int tid = threadIdx.x;
-  const int G = tid < kLwGpts ? tid : kLwGpts - 1;  // the padding threads repeat the last g-point
+  const bool writer = tid < kLwSweepCols * kLwGpts;
+  const int cslot = writer ? tid / kLwGpts : kLwSweepCols - 1;
+  const int G = writer ? tid - cslot * kLwGpts : kLwGpts - 1;
+  const int lc_own = lc0 + cslot;
+  const bool live = lc_own < a.chunk_count && !dead_column(a.live, a.chunk_first + lc_own);
+  const int lc = live ? lc_own : lc0;
+  const int col = a.chunk_first + lc;
   int band = kLwBands - 1;
   while (G < kGofsDev[band]) --band;
+  const int P = kLwPadOfsDev[band] + (G - kGofsDev[band]);
   const ColRec &R = col_records(a)[lc];
   const float sd = R.secdiff[band];
   const bool has_cloud = R.has_cloud != 0;
-  const float tsfc = R.C.tsfc, semiss = R.C.semiss;
-  const int nlay = R.C.nlay, nk = R.C.nk;
-  const float *recs = layer_records(a) + static_cast<size_t>(lc) * nlay * kLwOpticsFloats;
-  // band sums of a level: thread q < 16 the total of band q, 16 + q its clear sum
-  int step = 0;
-  auto level_terms = [&](float rA, float rB, int type, int slot) {
-    float(*buf)[kLwGpts] = s_rad[step & 1];
-    if (tid < kLwGpts) {
-      buf[0][tid] = rA;
-      buf[1][tid] = rB;
-    }
-    __syncthreads();
-    if (tid < 2 * kLwBands && slot >= 0) {
-      const int b = tid & 15, which = tid >> 4;
-      const float *v = buf[which] + kGofsDev[b];
-      const int ngc = kNgcDev[b];
-      float sum = 0.0f;
-      for (int q = 0; q < ngc; ++q) sum = sum + v[q];
-      a.terms[term_index(a, type + which, slot, b, col)] = (sum * 0.5f) * kDelwave[b];
-    }
-    ++step;
-  };
+  const int nlay = a.nlay, nk = a.nk;
+  const float *recs = layer_records(a) + static_cast<size_t>(lc) * nlay * kLwRec;
+  const uint32_t *mword = a.mask + col + static_cast<size_t>(G >> 5) * a.ncol;
+  const size_t mstride = static_cast<size_t>(kLwMaskWords) * a.ncol;
+  const uint32_t bit = 1u << (G & 31);
+  const float pi = 3.1415926535897932384626433832795f;
+  const float fluxfac = pi * 2.0e4f;
+  if (tid < kLwSweepCols * 2) S.flux[tid >> 1][2 + (tid & 1)][nlay] = 0.0f * fluxfac;  // no downward flux at the top
+
+  // downward sweep, top to bottom: layer l gives level l; next layer loaded ahead
   float rA = 0.0f, rB = 0.0f;
   bool iclddn = false;
+  int filled = 0, level0 = nlay - 1;
+  const float *q = recs + static_cast<size_t>(nlay - 1) * kLwRec;
+  float nx_tg = q[P], nx_fr = q[kLwRecFracs + P];
+  float4 nx_bq = *reinterpret_cast<const float4 *>(q + kLwRecBand + 4 * band);
+  float nx_flag = q[kLwRecFlags];
+  uint32_t nx_word = mword[static_cast<size_t>(nlay - 1) * mstride];
   for (int l = nlay - 1; l >= 0; --l) {
-    uint32_t mask[kLwMaskWords];
-    const bool cloudy = load_mask(a, l, col, mask);
+    const float tg = nx_tg, fr = nx_fr, flag = nx_flag;
+    const float4 bq = nx_bq;
+    const uint32_t word = nx_word;
+    if (l > 0) {
+      q = recs + static_cast<size_t>(l - 1) * kLwRec;
+      nx_tg = q[P];
+      nx_fr = q[kLwRecFracs + P];
+      nx_bq = *reinterpret_cast<const float4 *>(q + kLwRecBand + 4 * band);
+      nx_flag = q[kLwRecFlags];
+      nx_word = mword[static_cast<size_t>(l - 1) * mstride];
+    }
+    const bool cloudy = flag != 0.0f;
     iclddn = iclddn || cloudy;
-    gpoint_step<true>(T, recs + static_cast<size_t>(l) * kLwOpticsFloats, G, band, mask, cloudy, sd, rA, rB, iclddn);
-    level_terms(rA, rB, 2, l <= nk ? l : -1);
+    lw_step<true>(T, tg, fr, bq, (word & bit) != 0u, cloudy, sd, rA, rB, iclddn);
+    if (writer) {
+      S.ring[filled][cslot][0][G] = rA;
+      S.ring[filled][cslot][1][G] = rB;
+    }
+    if (++filled == kLwRing || l == 0) {
+      lw_flush(S, filled, 2, level0, -1);
+      level0 -= filled;
+      filled = 0;
+    }
   }
+  // surface emission and reflection: level 0 upward (surface_sums, lw:5648-5655)
   {
-    // surface emission and reflection (surface_sums)
-    const float bt = tsfc - 159.0f;
+    const float bt = R.C.tsfc - 159.0f;
     const int indbound = clampi(static_cast<int>(bt), 1, 180);
     const float tbndfrac = bt - static_cast<float>(indbound);
-    const float reflect = 1.0f - semiss;
-    const float plankbnd = semiss * planck(T, indbound, tbndfrac, band);
-    const float rad0 = recs[kLwGpts + G] * plankbnd;
+    const float reflect = 1.0f - R.C.semiss;
+    const float plankbnd = R.C.semiss * planck(T, indbound, tbndfrac, band);
+    const float rad0 = recs[kLwRecFracs + P] * plankbnd;
     rA = rad0 + reflect * rA;
     rB = rad0 + reflect * rB;
-    level_terms(rA, rB, 0, 0);
+    if (writer) {
+      S.ring[0][cslot][0][G] = rA;
+      S.ring[0][cslot][1][G] = rB;
+    }
+    filled = 1;
+    level0 = 0;
   }
+  // upward sweep, bottom to top: layer l gives level l + 1
+  q = recs;
+  nx_tg = q[P];
+  nx_fr = q[kLwRecFracs + P];
+  nx_bq = *reinterpret_cast<const float4 *>(q + kLwRecBand + 4 * band);
+  nx_flag = q[kLwRecFlags];
+  nx_word = mword[0];
   for (int l = 0; l < nlay; ++l) {
-    uint32_t mask[kLwMaskWords];
-    const bool cloudy = load_mask(a, l, col, mask);
-    gpoint_step<false>(T, recs + static_cast<size_t>(l) * kLwOpticsFloats, G, band, mask, cloudy, sd, rA, rB,
-                       has_cloud);
-    const int lev = l + 1;
-    level_terms(rA, rB, 0, lev <= nk ? lev : (lev == nlay ? nk + 1 : -1));
+    const float tg = nx_tg, fr = nx_fr, flag = nx_flag;
+    const float4 bq = nx_bq;
+    const uint32_t word = nx_word;
+    if (l + 1 < nlay) {
+      q = recs + static_cast<size_t>(l + 1) * kLwRec;
+      nx_tg = q[P];
+      nx_fr = q[kLwRecFracs + P];
+      nx_bq = *reinterpret_cast<const float4 *>(q + kLwRecBand + 4 * band);
+      nx_flag = q[kLwRecFlags];
+      nx_word = mword[static_cast<size_t>(l + 1) * mstride];
+    }
+    lw_step<false>(T, tg, fr, bq, (word & bit) != 0u, flag != 0.0f, sd, rA, rB, has_cloud);
+    if (writer) {
+      S.ring[filled][cslot][0][G] = rA;
+      S.ring[filled][cslot][1][G] = rB;
+    }
+    if (++filled == kLwRing || l == nlay - 1) {
+      lw_flush(S, filled, 0, level0, 1);
+      level0 += filled;
+      filled = 0;
+    }
   }
-}
 
-// Groups of whole bands with at most 16 g-points each (140 in total).
-constexpr int kLwGroups = 9;
-
-__global__ void __launch_bounds__(128, 3) lw_group_kernel(Tables T, LwArgs a) {
-  const int col = a.chunk_first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.chunk_first + a.chunk_count || dead_column(a.live, col)) return;
-  switch (blockIdx.y) {
-    case 0: lw_group<2>(T, a, col); break;
-    case 1: lw_group<4>(T, a, col); break;
-    case 2: lw_group<3, 13>(T, a, col); break;
-    case 3: lw_group<1, 12>(T, a, col); break;
-    case 4: lw_group<0, 9>(T, a, col); break;
-    case 5: lw_group<5, 7>(T, a, col); break;
-    case 6: lw_group<6, 14, 15>(T, a, col); break;
-    case 7: lw_group<8>(T, a, col); break;
-    default: lw_group<10, 11>(T, a, col); break;
-  }
-}
-
-// Ordered band sums of every level, fluxes, heating rates (lw:5702-5712,
-// 7040-7057) and the 2-D outputs (lw:7059-7077).
-__global__ void __launch_bounds__(128) lw_finish_kernel(LwArgs a) {
-  const int col = a.chunk_first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= a.chunk_first + a.chunk_count || dead_column(a.live, col)) return;
-  const int i = col / a.ny, j = col - i * a.ny;
-  const int nk = a.nk, nlay = a.nlay;
-  const float pi = 3.1415926535897932384626433832795f;
-  const float fluxfac = pi * 2.0e4f;
+  // heating rates and theta tendencies (lw:5706-5712, 7040-7057) and the 2-D
+  // outputs (lw:7059-7077) of the block's live columns
   const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
-  auto level = [&](int type, int slot) {
-    float total = 0.0f;
-#pragma unroll
-    for (int b = 0; b < kLwBands; ++b) total = total + a.terms[term_index(a, type, slot, b, col)];
-    return total * fluxfac;
-  };
-  const int top = nlay == nk ? nk : nk + 1;
-  float ufl0 = level(0, 0), uflc0 = level(1, 0), dfl0 = level(2, 0), dflc0 = level(3, 0);
-  const float upb = ufl0, upbc = uflc0, dnb = dfl0, dnbc = dflc0;
-  const size_t rbase = static_cast<size_t>(i) * nk * a.ny + j;
-  const size_t wbase = static_cast<size_t>(i) * (nk + 1) * a.ny + j;
-  for (int l = 0; l < nk; ++l) {
-    const int lev = l + 1;
-    const float ufl1 = level(0, lev), uflc1 = level(1, lev);
-    float dfl1, dflc1;
-    if (lev == nlay) {
-      dfl1 = 0.0f * fluxfac;
-      dflc1 = 0.0f * fluxfac;
-    } else {
-      dfl1 = level(2, lev);
-      dflc1 = level(3, lev);
-    }
-    const float fnet0 = ufl0 - dfl0, fnet1 = ufl1 - dfl1;
-    const float fnetc0 = uflc0 - dflc0, fnetc1 = uflc1 - dflc1;
-    const float plev0 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l) * a.ny));
-    const float plev1 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l + 1) * a.ny));
-    const float dp = plev0 - plev1;
-    const float htr = heatfac * (fnet0 - fnet1) / dp;
-    const float htrc = heatfac * (fnetc0 - fnetc1) / dp;
-    const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * a.ny);
-    a.rthraten[rbase + static_cast<size_t>(l) * a.ny] = (htr / 86400.0f) / pi3d;
-    a.rthratenc[rbase + static_cast<size_t>(l) * a.ny] = (htrc / 86400.0f) / pi3d;
-    ufl0 = ufl1; uflc0 = uflc1; dfl0 = dfl1; dflc0 = dflc1;
-  }
-  const float uflt = level(0, top), ufltc = level(1, top);
-  const float dflt = 0.0f * fluxfac;
-  a.upt[col] = uflt;
-  a.uptc[col] = ufltc;
-  a.dnt[col] = dflt;
-  a.dntc[col] = dflt;
-  a.upb[col] = upb;
-  a.upbc[col] = upbc;
-  a.dnb[col] = dnb;
-  a.dnbc[col] = dnbc;
-  a.glw[col] = dnb;
-  a.olr[col] = uflt;
-  a.lwcf[col] = ufltc - uflt;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
-}
-
-// lw_finish_kernel for the split schedule's small domains: a block per column,
-// its threads over flux levels.  Each level's four totals are the band terms
-// added in band order, as in lw_finish_kernel; then each layer's heating rate
-// and the 2-D outputs, with the same operations.
-constexpr int kFinishThreads = 64;
-
-__global__ void __launch_bounds__(kFinishThreads) lw_finish_block_kernel(LwArgs a) {
-  __shared__ float tot[4][kMaxLay + 2];
-  const int col = a.chunk_first + blockIdx.x;
-  if (dead_column(a.live, col)) return;  // whole block
-  const int i = col / a.ny, j = col - i * a.ny;
-  const int nk = a.nk, nlay = a.nlay;
-  const float pi = 3.1415926535897932384626433832795f;
-  const float fluxfac = pi * 2.0e4f;
-  const float heatfac = (9.8066f * 8.6400e4f) / (1004.5f * 1.0e2f);
-  // upward totals at slots 0 .. nk + 1, downward at 0 .. nk
-  for (int slot = threadIdx.x; slot <= nk + 1; slot += blockDim.x) {
-    for (int type = 0; type < 4; ++type) {
-      if (type >= 2 && slot > nk) continue;
-      float total = 0.0f;
-#pragma unroll
-      for (int b = 0; b < kLwBands; ++b) total = total + a.terms[term_index(a, type, slot, b, col)];
-      tot[type][slot] = total * fluxfac;
-    }
-  }
-  __syncthreads();
-  const size_t rbase = static_cast<size_t>(i) * nk * a.ny + j;
-  const size_t wbase = static_cast<size_t>(i) * (nk + 1) * a.ny + j;
-  for (int l = threadIdx.x; l < nk; l += blockDim.x) {
-    const int lev = l + 1;
-    const float ufl0 = tot[0][l], uflc0 = tot[1][l], dfl0 = tot[2][l], dflc0 = tot[3][l];
-    const float ufl1 = tot[0][lev], uflc1 = tot[1][lev];
-    float dfl1, dflc1;
-    if (lev == nlay) {
-      dfl1 = 0.0f * fluxfac;
-      dflc1 = 0.0f * fluxfac;
-    } else {
-      dfl1 = tot[2][lev];
-      dflc1 = tot[3][lev];
-    }
-    const float fnet0 = ufl0 - dfl0, fnet1 = ufl1 - dfl1;
-    const float fnetc0 = uflc0 - dflc0, fnetc1 = uflc1 - dflc1;
+  for (int qq = tid; qq < kLwSweepCols * nk; qq += kLwSweepThreads) {
+    const int cs = qq / nk, l = qq - cs * nk;
+    const int lcq = lc0 + cs;
+    if (lcq >= a.chunk_count || dead_column(a.live, a.chunk_first + lcq)) continue;
+    const int cq = a.chunk_first + lcq;
+    const int i = cq / a.ny, j = cq - i * a.ny;
+    const float(*fx)[kMaxLay + 1] = S.flux[cs];
+    const float fnet0 = fx[0][l] - fx[2][l], fnet1 = fx[0][l + 1] - fx[2][l + 1];
+    const float fnetc0 = fx[1][l] - fx[3][l], fnetc1 = fx[1][l + 1] - fx[3][l + 1];
+    const size_t rbase = static_cast<size_t>(i) * nk * a.ny + j;
+    const size_t wbase = static_cast<size_t>(i) * (nk + 1) * a.ny + j;
     const float plev0 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l) * a.ny));
     const float plev1 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l + 1) * a.ny));
     const float dp = plev0 - plev1;
@@ -1730,23 +1663,23 @@ __global__ void __launch_bounds__(kFinishThreads) lw_finish_block_kernel(LwArgs 
     a.rthraten[rbase + static_cast<size_t>(l) * a.ny] = (htr / 86400.0f) / pi3d;
     a.rthratenc[rbase + static_cast<size_t>(l) * a.ny] = (htrc / 86400.0f) / pi3d;
   }
-  if (threadIdx.x == 0) {
-    const int top = nlay == nk ? nk : nk + 1;
-    const float uflt = tot[0][top], ufltc = tot[1][top];
+  if (G == 0 && writer && live) {
+    const float(*fx)[kMaxLay + 1] = S.flux[cslot];
+    const float uflt = fx[0][nlay], ufltc = fx[1][nlay];
     const float dflt = 0.0f * fluxfac;
     a.upt[col] = uflt;
     a.uptc[col] = ufltc;
     a.dnt[col] = dflt;
     a.dntc[col] = dflt;
-    a.upb[col] = tot[0][0];
-    a.upbc[col] = tot[1][0];
-    a.dnb[col] = tot[2][0];
-    a.dnbc[col] = tot[3][0];
-    a.glw[col] = tot[2][0];
+    a.upb[col] = fx[0][0];
+    a.upbc[col] = fx[1][0];
+    a.dnb[col] = fx[2][0];
+    a.dnbc[col] = fx[3][0];
+    a.glw[col] = fx[2][0];
     a.olr[col] = uflt;
     a.lwcf[col] = ufltc - uflt;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) a.zero2[q][col] = 0.0f;
+    for (int z = 0; z < 4; ++z) a.zero2[z][col] = 0.0f;
   }
 }
 
@@ -1759,46 +1692,26 @@ cudaError_t launch_lw(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-size_t lw_terms_floats(int nk, int ncol) {
-  return static_cast<size_t>(4) * (nk + 2) * kLwBands * static_cast<size_t>(ncol);
+size_t lw_scratch_floats(int nlay, int chunk) {
+  return (kColRecFloats + (static_cast<size_t>(kLwGasFields) + kLwRec) * nlay) * static_cast<size_t>(chunk);
 }
 
-cudaError_t launch_lw_groups(const Tables &T, const LwArgs &a, cudaStream_t stream) {
-  const int threads = 128;
-  const int blocks = (a.chunk_count + threads - 1) / threads;
-  lw_group_kernel<<<dim3(blocks, kLwGroups), threads, 0, stream>>>(T, a);
-  return cudaGetLastError();
-}
-
-size_t lw_optics_floats(int nlay, int ncol) {
-  return ((static_cast<size_t>(kLwOpticsFloats) + kLayerFloats) * nlay + kColRecFloats) * static_cast<size_t>(ncol);
-}
-
-cudaError_t launch_lw_gsplit(const Tables &T, const LwArgs &a, cudaStream_t stream) {
+cudaError_t launch_lw_chunk_optics(const Tables &T, const LwArgs &a, cudaStream_t stream) {
   const int threads = 128;
   lw_colprep_kernel<<<(a.chunk_count + 3) / 4, threads, 0, stream>>>(T, a);
-  cudaError_t e0 = cudaGetLastError();
-  if (e0 != cudaSuccess) return e0;
-  const long long layers = static_cast<long long>(a.chunk_count) * a.nlay;
-  lw_layer_kernel<<<static_cast<unsigned>((layers + threads - 1) / threads), threads, 0, stream>>>(T, a);
-  e0 = cudaGetLastError();
-  if (e0 != cudaSuccess) return e0;
-  lw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kLwBands), threads, 0, stream>>>(
-      T, a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  lw_gsplit_kernel<<<a.chunk_count, kGsplitThreads, 0, stream>>>(T, a);
+  const long long layers = static_cast<long long>(a.chunk_count) * a.nlay;
+  const unsigned blocks = static_cast<unsigned>((layers + threads - 1) / threads);
+  lw_layer_kernel<<<blocks, threads, 0, stream>>>(T, a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  lw_gas_kernel<<<dim3(blocks, kLwBands), threads, 0, stream>>>(T, a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_lw_finish(const LwArgs &a, cudaStream_t stream) {
-  if (a.optics) {  // split schedule: small domain
-    lw_finish_block_kernel<<<a.chunk_count, kFinishThreads, 0, stream>>>(a);
-    return cudaGetLastError();
-  }
-  const int threads = 128;
-  const int blocks = (a.chunk_count + threads - 1) / threads;
-  lw_finish_kernel<<<blocks, threads, 0, stream>>>(a);
+cudaError_t launch_lw_chunk_sweep(const Tables &T, const LwArgs &a, cudaStream_t stream) {
+  lw_sweep_kernel<<<(a.chunk_count + kLwSweepCols - 1) / kLwSweepCols, kLwSweepThreads, 0, stream>>>(T, a);
   return cudaGetLastError();
 }
 

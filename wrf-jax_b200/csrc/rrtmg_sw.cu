@@ -16,6 +16,8 @@
 // transmittance, direct beam, downward adding recurrence) and a bottom-up pass
 // (upward adding recurrence, level fluxes) that accumulates the spectral sums
 // in g-point order.
+#include <atomic>
+
 #include "rrtmg_device.cuh"
 #include "rrtmg_kernels.h"
 
@@ -512,27 +514,45 @@ struct RT4 {
   float ref, refd, tra, trad;
 };
 
-// Delta-Eddington layer reflectance/transmittance (reftra_sw_columns, sw:3490-3601)
-__device__ __forceinline__ RT4 reftra(const Tables &T, bool lrt, float zg, float mu, float zto1, float zw) {
+// exp_lookup of min(v, 500) given ex_v = exp_lookup(v) (reftra's clamp of
+// its exponent arguments, sw:3530-3545)
+__device__ __forceinline__ float lookup_clamped(const Tables &T, float v, float ex_v) {
+  return v > 500.0f ? exp_lookup(T, 500.0f) : ex_v;
+}
+
+// x / d, or x itself when d is exactly 1 (then the quotient is x exactly).
+__device__ __forceinline__ float div_or_same(float x, float d) { return d == 1.0f ? x : x / d; }
+
+// 0 / x as IEEE binary32 division computes it: a zero with the sign of x, or
+// the canonical NaN when x is zero or NaN.
+__device__ __forceinline__ float zero_over(float x) {
+  if (x == 0.0f || x != x) return __int_as_float(0x7fffffff);
+  return __int_as_float(__float_as_int(x) & static_cast<int>(0x80000000u));
+}
+
+// Delta-Eddington layer reflectance/transmittance (reftra_sw_columns,
+// sw:3490-3601) of a layer that scatters (the reference's lrt = true).
+// zto1_mu = zto1 / mu and ex_zto1_mu = exp_lookup(zto1_mu) come from the
+// caller, which needs the same quotient and lookup for its direct beam.
+// Divisions whose divisor is exactly 1 are skipped: their quotient is the
+// dividend, bit for bit.
+__device__ __forceinline__ RT4 reftra(const Tables &T, float zg, float mu, float zto1, float zw, float zto1_mu,
+                                      float ex_zto1_mu) {
   RT4 r;
-  r.ref = 0.0f; r.refd = 0.0f; r.tra = 1.0f; r.trad = 1.0f;
-  if (!lrt) return r;
   const float eps = 1.0e-8f, zwcrit = 0.9999995f;
   const float zg3 = 3.0f * zg;
   const float g1 = (8.0f - zw * (5.0f + zg3)) * 0.25f;
   const float g2 = 3.0f * (zw * (1.0f - zg)) * 0.25f;
   const float g3 = (2.0f - zg3 * mu) * 0.25f;
   const float g4 = 1.0f - g3;
-  const float sr = zg != 1.0f ? zg / (1.0f - zg) : 0.0f;
+  const float sr = zg != 1.0f ? div_or_same(zg, 1.0f - zg) : 0.0f;
   const float denom = zg != 1.0f ? 1.0f - (1.0f - zw) * sr * sr : 1.0f;
-  const float zwo = (zw > 0.0f && denom != 0.0f) ? zw / denom : 0.0f;
+  const float zwo = (zw > 0.0f && denom != 0.0f) ? div_or_same(zw, denom) : 0.0f;
   if (zwo >= zwcrit) {
     const float za = g1 * mu;
     const float za1 = za - g3;
     const float zgt = g1 * zto1;
-    float ze = zto1 / mu;
-    if (ze > 500.0f) ze = 500.0f;
-    const float ex = exp_lookup(T, ze);
+    const float ex = lookup_clamped(T, zto1_mu, ex_zto1_mu);
     r.ref = (zgt - za1 * (1.0f - ex)) / (1.0f + zgt);
     r.tra = 1.0f - r.ref;
     r.refd = zgt / (1.0f + zgt);
@@ -559,11 +579,9 @@ __device__ __forceinline__ RT4 reftra(const Tables &T, bool lrt, float zg, float
   const float zbeta = (g1 - zrk) / zrkg;
   float ze1 = zrk * zto1;
   if (ze1 > 500.0f) ze1 = 500.0f;
-  float ze2 = zto1 / mu;
-  if (ze2 > 500.0f) ze2 = 500.0f;
   const float zem1 = exp_lookup(T, ze1);
   const float zep1 = 1.0f / zem1;
-  const float zem2 = exp_lookup(T, ze2);
+  const float zem2 = lookup_clamped(T, zto1_mu, ex_zto1_mu);
   const float zep2 = 1.0f / zem2;
   const float zdenr = zr4 * zep1 + zr5 * zem1;
   const float zdent = zr4 * zep1 + zr5 * zem1;
@@ -768,11 +786,16 @@ __device__ __forceinline__ void sw_column_outputs(const SwArgs &a, const Col &C,
 //                      per-level spectral sums in g-point order in shared
 //                      memory, then heating and the 2-D outputs.
 // Records: per chunk slot a column record, then nlay layer records of kSwRec
-// floats (about 64 KB per day column at nk = 50).
-constexpr int kSwRec = 312;  // taug[112], taur[112], cloud[14][4], spec[14][2], jp, padding
-constexpr int kSwRecTaur = kSwGpts, kSwRecCloud = 2 * kSwGpts, kSwRecSpec = kSwRecCloud + 4 * kSwBands,
-              kSwRecJp = kSwRecSpec + 2 * kSwBands;
-static_assert(kSwRecJp < kSwRec, "record layout");
+// floats (1,376 bytes per layer, 70 KB per day column at nk = 50).  Each
+// band's g-points start on a 16-byte boundary (kPadOfs) so the optics kernel
+// writes whole float4s: taug at [0, 128), taur at [128, 256), the cloud optics
+// (tau, ssa, asm, unscaled tau) of band B at 256 + 4 B, the solar-source
+// interpolation (js0, fs) of band B at 312 + 2 B, jp at 340.
+constexpr int kSwRec = 344;
+constexpr int kSwRecTaur = 128, kSwRecCloud = 256, kSwRecSpec = 312, kSwRecJp = 340;
+constexpr int kPadOfs[kSwBands] = {0, 8, 20, 28, 36, 48, 60, 64, 76, 84, 92, 100, 108, 116};
+static_assert(kSwRecJp < kSwRec && kSwRec % 4 == 0, "record layout");
+__constant__ int kPadOfsDev[kSwBands] = {0, 8, 20, 28, 36, 48, 60, 64, 76, 84, 92, 100, 108, 116};
 
 struct SwColRec {
   Col C;
@@ -802,30 +825,76 @@ __global__ void __launch_bounds__(128) sw_colprep_kernel(Tables T, SwArgs a) {
   if (lane == 0) sw_colrecs(a)[u].C = C;
 }
 
+// ngc values of v to float4s at dst (the tail padded with zeros).
+template <int NGC>
+__device__ __forceinline__ void store_padded(float4 *dst, const float *v) {
+#pragma unroll
+  for (int q = 0; q < (NGC + 3) / 4; ++q) {
+    const int g = 4 * q;
+    dst[q] = make_float4(v[g], g + 1 < NGC ? v[g + 1] : 0.0f, g + 2 < NGC ? v[g + 2] : 0.0f,
+                         g + 3 < NGC ? v[g + 3] : 0.0f);
+  }
+}
+
+// Band B of one layer record: gas and Rayleigh depths of every g-point, the
+// band's cloud optics (cldprmc_sw only where the layer holds cloud water; a
+// layer without any has the reference's inactive values 0, 1, 0, 0), and the
+// spectral interpolation its solar source uses (into spec[2 B], spec[2 B + 1]).
 template <int B>
-__device__ __forceinline__ void sw_layer_optics(const Tables &T, const SwArgs &a, const Col &C, int l, int clear_only,
-                                                float *rec) {
-  constexpr int ngc = kNgc[B], gofs = kGofs[B], bn = B + 16;
-  const SLayer L = make_layer(T, a, C, l);
+__device__ __forceinline__ void sw_band_record(const Tables &T, const SLayer &L, bool cloud_water, int iceflg,
+                                               float4 *rec, float *spec) {
+  constexpr int ngc = kNgc[B], bn = B + 16, pofs = kPadOfs[B];
   SwSpec sp8, sp4;
   sp8.sc = 0.0f; sp8.fs = 0.0f; sp8.js0 = 0;
   sp4 = sp8;
   float tg[ngc], tr[ngc];
   sw_taumol<B>(T, L, tg, tr, sp8, sp4);
-#pragma unroll
-  for (int g = 0; g < ngc; ++g) {
-    rec[gofs + g] = tg[g];
-    rec[kSwRecTaur + gofs + g] = tr[g];
+  store_padded<ngc>(rec + pofs / 4, tg);
+  store_padded<ngc>(rec + (kSwRecTaur + pofs) / 4, tr);
+  float4 cq = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+  if (cloud_water) {
+    const CloudOpt o = sw_cloud(T, L, B, iceflg);
+    cq = make_float4(o.tau, o.ssa, o.asm_, o.taor);
   }
-  if (!clear_only) {
-    const CloudOpt o = sw_cloud(T, L, B, C.iceflg);
-    float *cq = rec + kSwRecCloud + 4 * B;
-    cq[0] = o.tau; cq[1] = o.ssa; cq[2] = o.asm_; cq[3] = o.taor;
-  }
+  rec[kSwRecCloud / 4 + B] = cq;
   const SwSpec &sp = (bn == 17 || bn == 28) ? sp4 : sp8;
-  rec[kSwRecSpec + 2 * B] = __int_as_float(sp.js0);
-  rec[kSwRecSpec + 2 * B + 1] = sp.fs;
-  if (B == 0) rec[kSwRecJp] = __int_as_float(L.jp);
+  spec[2 * B] = __int_as_float(sp.js0);
+  spec[2 * B + 1] = sp.fs;
+}
+
+// thread = (layer, chunk slot), slots fastest: the layer set-up once, then the
+// records of all 14 bands.
+__global__ void __launch_bounds__(128) sw_optics_kernel(Tables T, SwArgs a) {
+  const int n = a.nk + 1;
+  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int l = static_cast<int>(idx / a.chunk_count);
+  const int u = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
+  if (l >= n || a.chunk_first + u >= *a.nday) return;
+  const Col C = sw_colrecs(a)[u].C;
+  float4 *rec = reinterpret_cast<float4 *>(sw_layrecs(a) + (static_cast<size_t>(u) * n + l) * kSwRec);
+  const SLayer L = make_layer(T, a, C, l);
+  // the activity test of cldprmc_sw (sw:1409-1440), the same for every band
+  const float cswp = C.iceflg == 5 ? L.cswp : 0.0f;
+  const bool cloud_water = a.icld != 0 && ((L.ciwp + L.clwp) + cswp) >= 1.0e-20f;
+  float spec[2 * kSwBands];
+  sw_band_record<0>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<1>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<2>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<3>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<4>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<5>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<6>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<7>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<8>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<9>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<10>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<11>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<12>(T, L, cloud_water, C.iceflg, rec, spec);
+  sw_band_record<13>(T, L, cloud_water, C.iceflg, rec, spec);
+#pragma unroll
+  for (int q = 0; q < kSwBands / 2; ++q)
+    rec[kSwRecSpec / 4 + q] = make_float4(spec[4 * q], spec[4 * q + 1], spec[4 * q + 2], spec[4 * q + 3]);
+  rec[kSwRecJp / 4] = make_float4(__int_as_float(L.jp), 0.0f, 0.0f, 0.0f);
 }
 
 #define RRTMG_SW_BAND_SWITCH(band, CALL) \
@@ -845,20 +914,6 @@ __device__ __forceinline__ void sw_layer_optics(const Tables &T, const SwArgs &a
     case 12: CALL(12); break;            \
     default: CALL(13); break;            \
   }
-
-// grid.y = band: every block runs one band's code
-__global__ void __launch_bounds__(128) sw_optics_kernel(Tables T, SwArgs a) {
-  const int n = a.nk + 1;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int u = idx / n, l = idx - u * n;
-  if (u >= a.chunk_count || a.chunk_first + u >= *a.nday) return;
-  const Col &C = sw_colrecs(a)[u].C;
-  float *rec = sw_layrecs(a) + static_cast<size_t>(idx) * kSwRec;
-  const int clear_only = a.icld == 0;
-#define RRTMG_SW_OPT(B) sw_layer_optics<B>(T, a, C, l, clear_only, rec)
-  RRTMG_SW_BAND_SWITCH(blockIdx.y, RRTMG_SW_OPT)
-#undef RRTMG_SW_OPT
-}
 
 __global__ void __launch_bounds__(128) sw_source_kernel(Tables T, SwArgs a) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -895,7 +950,6 @@ struct SweepShared {
   float ring[kRing][kSweepCols][4][kSwGpts];
   float sums[kSweepCols][6][kMaxLev];  // type: fu, fd, cu, cd, fdir, cdir; level top-down
 };
-static_assert(sizeof(SweepShared) <= 48 * 1024, "sweep shared memory within the default limit");
 
 // One level of one adding path, as the bottom-up pass reads it back: the
 // layer's reflectances/transmittances and direct-beam transmittance, and the
@@ -930,7 +984,17 @@ __device__ __forceinline__ void sweep_flush(SweepShared &S, int count, int ntype
 // Block = kSweepCols consecutive slots of the chunk; thread = (slot, g-point).
 // A slot past the day count repeats the block's first slot so that every
 // thread takes the same barriers; its results are not written.
-__global__ void __launch_bounds__(kSweepThreads, 3) sw_sweep_kernel(Tables T, SwArgs a) {
+//
+// Work per g-point layer follows spcvmc (sw:6887-7041) statement by statement;
+// three kinds of operation are shared or skipped where the result is known
+// bit for bit: the quotient tau / mu and its Pade lookup, computed once for
+// the direct beam and reftra's exponent; divisions by a divisor that is
+// exactly 1; and, in a g-point layer without cloud, the cloudy
+// reflectance/transmittance inputs, whose only consumer is a reftra call the
+// reference skips (lrt = false).  The total-sky stack slot of such a layer is
+// not stored: the bottom-up pass re-forms it from the clear-sky slot with the
+// reference's mixing expression.
+__global__ void __launch_bounds__(kSweepThreads, 4) sw_sweep_kernel(Tables T, SwArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SweepShared &S = *reinterpret_cast<SweepShared *>(smem_raw);
   const int nday = *a.nday;
@@ -947,10 +1011,10 @@ __global__ void __launch_bounds__(kSweepThreads, 3) sw_sweep_kernel(Tables T, Sw
   const float sflux_g = R.sflux[G];
   const int n = C.nlay;
   const float mu = C.mu;
-  const float repclc = 1.0e-12f;
   const int clear_only = a.icld == 0;
   int band = kSwBands - 1;
   while (G < kSwGofsDev[band]) --band;
+  const int P = kPadOfsDev[band] + (G - kSwGofsDev[band]);  // record position of the g-point
   const float *recs = sw_layrecs(a) + static_cast<size_t>(u) * n * kSwRec;
   const float *crec = recs + kSwRecCloud + 4 * band;
   const uint32_t *maskbase = a.mask + col + static_cast<size_t>(G >> 5) * a.ncol;
@@ -972,42 +1036,42 @@ __global__ void __launch_bounds__(kSweepThreads, 3) sw_sweep_kernel(Tables T, Sw
   float t_tdbt = 1.0f, t_tdn = 1.0f, t_rdnd = 0.0f;
   // layer values are loaded one layer ahead
   const float *rl = recs + static_cast<size_t>(n - 1) * kSwRec;
-  float nx_tg = rl[G], nx_tr = rl[kSwRecTaur + G];
-  float nx_ct = 0.0f, nx_cs = 1.0f, nx_ca = 0.0f, nx_co = 0.0f;
-  const float *cl = crec + static_cast<size_t>(n - 1) * kSwRec;
-  if (!clear_only) { nx_ct = cl[0]; nx_cs = cl[1]; nx_ca = cl[2]; nx_co = cl[3]; }
+  float nx_tg = rl[P], nx_tr = rl[kSwRecTaur + P];
+  float4 nx_cld = *reinterpret_cast<const float4 *>(crec + static_cast<size_t>(n - 1) * kSwRec);
   uint32_t nx_word = maskbase[static_cast<size_t>(n - 1) * mstride];
   for (int r = 0; r < n; ++r) {
     const int l = n - 1 - r;
     const uint32_t word = nx_word;
     const float tr = nx_tr, tg = nx_tg;
-    const float ct = nx_ct, cs = nx_cs, ca = nx_ca, co = nx_co;
+    const float4 cld = nx_cld;
     if (l > 0) {
       const float *q = recs + static_cast<size_t>(l - 1) * kSwRec;
-      nx_tg = q[G];
-      nx_tr = q[kSwRecTaur + G];
-      if (!clear_only) {
-        const float *cq = crec + static_cast<size_t>(l - 1) * kSwRec;
-        nx_ct = cq[0]; nx_cs = cq[1]; nx_ca = cq[2]; nx_co = cq[3];
-      }
+      nx_tg = q[P];
+      nx_tr = q[kSwRecTaur + P];
+      nx_cld = *reinterpret_cast<const float4 *>(crec + static_cast<size_t>(l - 1) * kSwRec);
       nx_word = maskbase[static_cast<size_t>(l - 1) * mstride];
     }
-    const bool cldb = (word & bit) != 0u;
+    const bool cldb = !clear_only && (word & bit) != 0u;
     const float cloud = cldb ? 1.0f : 0.0f;
     const float clear = 1.0f - cloud;
+    // clear sky: gas + Rayleigh, no aerosol (sw:6923-6927)
     const float ztau = (tr + tg) + 0.0f;
-    float zom = tr + 0.0f * 1.0f;
-    const float zgr = 0.0f * 1.0f * 0.0f / zom;
-    zom = zom / ztau;
-    const float dbtc_nd = exp_lookup(T, ztau / mu);
+    const float zom0 = tr + 0.0f * 1.0f;
+    const float zgr = zero_over(zom0);  // 0 * 1 * 0 / zom
+    const float zom = zom0 / ztau;
+    const float v_nd = ztau / mu;
+    const float dbtc_nd = exp_lookup(T, v_nd);
     tdbtc_nd = tdbtc_nd * dbtc_nd;
     const float zf = zgr * zgr;
     const float zwf = zom * zf;
-    const float ztauc = (1.0f - zwf) * ztau;
-    const float zomcc = (zom - zwf) / (1.0f - zwf);
-    const float zgcc = (zgr - zf) / (1.0f - zf);
-    const RT4 c = reftra(T, true, zgcc, mu, ztauc, zomcc);
-    const float dbtc = exp_lookup(T, ztauc / mu);
+    const float d_w = 1.0f - zwf;
+    const float ztauc = d_w * ztau;
+    const float zomcc = div_or_same(zom - zwf, d_w);
+    const float zgcc = div_or_same(zgr - zf, 1.0f - zf);
+    // ztauc is ztau exactly when d_w == 1
+    const float v_c = d_w == 1.0f ? v_nd : ztauc / mu;
+    const float dbtc = d_w == 1.0f ? dbtc_nd : exp_lookup(T, v_c);
+    const RT4 c = reftra(T, zgcc, mu, ztauc, zomcc, v_c, dbtc);
     stc[r].rt = make_float4(c.ref, c.refd, c.tra, c.trad);
     stc[r].dn = make_float4(dbtc, c_tdbt, c_tdn, c_rdnd);
     // downward recurrence of vrtqdr (sw:3681-3702) for level r + 1
@@ -1027,26 +1091,43 @@ __global__ void __launch_bounds__(kSweepThreads, 3) sw_sweep_kernel(Tables T, Sw
       c_rdnd = rdnd_next;
     }
     if (!clear_only) {
-      const float tcld = cldb ? ct : 0.0f;
-      const float wcld = cldb ? cs : 1.0f;
-      const float gcld = cldb ? ca : 0.0f;
-      const float taor = cldb ? co : 0.0f;
-      const float tauorig = ztau + taor;
-      const float dbtmo_nd = exp_lookup(T, tauorig / mu);
-      const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
-      tdbt_nd = tdbt_nd * dbt_nd;
-      const float ztauo = ztauc + tcld;
-      float zomco = ztauc * zomcc + tcld * wcld;
-      const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
-      zomco = zomco / ztauo;
-      const RT4 o = reftra(T, cloud > repclc, zgco, mu, ztauo, zomco);
-      const float ref = clear * c.ref + cloud * o.ref;
-      const float refd = clear * c.refd + cloud * o.refd;
-      const float tra = clear * c.tra + cloud * o.tra;
-      const float trad = clear * c.trad + cloud * o.trad;
-      const float dbtmo = exp_lookup(T, ztauo / mu);
-      const float dbt = clear * dbtc + cloud * dbtmo;
-      stt[r].rt = make_float4(ref, refd, tra, trad);
+      float ref, refd, tra, trad, dbt;
+      if (cldb) {
+        const float tcld = cld.x, wcld = cld.y, gcld = cld.z, taor = cld.w;
+        const float tauorig = ztau + taor;
+        const float dbtmo_nd = exp_lookup(T, tauorig / mu);
+        const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
+        tdbt_nd = tdbt_nd * dbt_nd;
+        const float ztauo = ztauc + tcld;
+        float zomco = ztauc * zomcc + tcld * wcld;
+        const float zgco = (tcld * wcld * gcld + ztauc * zomcc * zgcc) / zomco;
+        zomco = zomco / ztauo;
+        const float v_o = ztauo / mu;
+        const float dbtmo = exp_lookup(T, v_o);
+        const RT4 o = reftra(T, zgco, mu, ztauo, zomco, v_o, dbtmo);
+        ref = clear * c.ref + cloud * o.ref;
+        refd = clear * c.refd + cloud * o.refd;
+        tra = clear * c.tra + cloud * o.tra;
+        trad = clear * c.trad + cloud * o.trad;
+        dbt = clear * dbtc + cloud * dbtmo;
+        stt[r].rt = make_float4(ref, refd, tra, trad);
+      } else {
+        // no cloud in this g-point layer: taor = tcld = 0, so tauorig and
+        // ztauo are ztau and ztauc plus zero, and the cloudy reftra is the
+        // reference's lrt = false constant set (0, 0, 1, 1)
+        const float tauorig = ztau + 0.0f;
+        const float dbtmo_nd = __float_as_uint(tauorig) == __float_as_uint(ztau) ? dbtc_nd
+                                                                                 : exp_lookup(T, tauorig / mu);
+        const float dbt_nd = clear * dbtc_nd + cloud * dbtmo_nd;
+        tdbt_nd = tdbt_nd * dbt_nd;
+        const float ztauo = ztauc + 0.0f;
+        const float dbtmo = __float_as_uint(ztauo) == __float_as_uint(ztauc) ? dbtc : exp_lookup(T, ztauo / mu);
+        ref = clear * c.ref + cloud * 0.0f;
+        refd = clear * c.refd + cloud * 0.0f;
+        tra = clear * c.tra + cloud * 1.0f;
+        trad = clear * c.trad + cloud * 1.0f;
+        dbt = clear * dbtc + cloud * dbtmo;
+      }
       stt[r].dn = make_float4(dbt, t_tdbt, t_tdn, t_rdnd);
       const float tdbt_next = t_tdbt * dbt;
       float tdn_next, rdnd_next;
@@ -1082,12 +1163,26 @@ __global__ void __launch_bounds__(kSweepThreads, 3) sw_sweep_kernel(Tables T, Sw
   SwLevel c = {make_float4(C.albedo, C.albedo, 0.0f, 0.0f), make_float4(0.0f, c_tdbt, c_tdn, c_rdnd)};
   SwLevel t = {make_float4(C.albedo, C.albedo, 0.0f, 0.0f), make_float4(0.0f, t_tdbt, t_tdn, t_rdnd)};
   if (clear_only) t = c;
+  // stack slot j (layer n - 1 - j) of both paths; a layer without cloud in
+  // this g-point has the total-sky mix clear * c + cloud * (0, 0, 1, 1)
+  auto load_slot = [&](int j, SwLevel &lc, SwLevel &lt) {
+    lc = stc[j];
+    if (clear_only) {
+      lt = lc;
+      return;
+    }
+    lt.dn = stt[j].dn;
+    if ((maskbase[static_cast<size_t>(n - 1 - j) * mstride] & bit) != 0u) {
+      lt.rt = stt[j].rt;
+    } else {
+      const float clear = 1.0f, cloud = 0.0f;
+      lt.rt = make_float4(clear * lc.rt.x + cloud * 0.0f, clear * lc.rt.y + cloud * 0.0f,
+                          clear * lc.rt.z + cloud * 1.0f, clear * lc.rt.w + cloud * 1.0f);
+    }
+  };
   for (int k = n; k >= 0; --k) {
     SwLevel nc = c, nt = t;
-    if (k > 0) {
-      nc = stc[k - 1];
-      if (!clear_only) nt = stt[k - 1];
-    }
+    if (k > 0) load_slot(k - 1, nc, nt);
     if (k < n) {
       const float zrc = 1.0f / (1.0f - rupdc * c.rt.y);
       const float nrupc = c.rt.x + c.rt.w * ((c.rt.z - c.dn.x) * rupdc + c.dn.x * rupc) * zrc;
@@ -1148,32 +1243,36 @@ size_t sw_record_floats(int nk, int chunk) {
   return (kSwColRecFloats + static_cast<size_t>(kSwRec) * (nk + 1)) * static_cast<size_t>(chunk);
 }
 
-cudaError_t launch_sw_columns(const Tables &T, const SwArgs &args, cudaStream_t stream) {
-  SwArgs a = args;
+cudaError_t launch_sw_chunk_optics(const Tables &T, const SwArgs &a, cudaStream_t stream) {
   const int threads = 128;
   const int n = a.nk + 1;
-  // The day count is known only on the device: chunks cover all ncol list
-  // slots; slots at or beyond the day count exit at once.
-  for (int first = 0; first < a.ncol; first += a.chunk_capacity) {
-    a.chunk_first = first;
-    a.chunk_count = a.ncol - first < a.chunk_capacity ? a.ncol - first : a.chunk_capacity;
-    sw_colprep_kernel<<<(a.chunk_count + 3) / 4, threads, 0, stream>>>(T, a);
-    cudaError_t e = cudaGetLastError();
+  sw_colprep_kernel<<<(a.chunk_count + 3) / 4, threads, 0, stream>>>(T, a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long layers = static_cast<long long>(a.chunk_count) * n;
+  sw_optics_kernel<<<static_cast<unsigned>((layers + threads - 1) / threads), threads, 0, stream>>>(T, a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  sw_source_kernel<<<dim3((a.chunk_count + threads - 1) / threads, kSwBands), threads, 0, stream>>>(T, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sw_chunk_sweep(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+  if (sizeof(SweepShared) > 48 * 1024) {  // a ring of more levels needs the opt-in
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const long long layers = static_cast<long long>(a.chunk_count) * n;
-    sw_optics_kernel<<<dim3(static_cast<unsigned>((layers + threads - 1) / threads), kSwBands), threads, 0,
-                       stream>>>(T, a);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    sw_source_kernel<<<dim3((a.chunk_count + threads - 1) / threads, kSwBands), threads, 0, stream>>>(T, a);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    sw_sweep_kernel<<<(a.chunk_count + kSweepCols - 1) / kSweepCols, kSweepThreads, sizeof(SweepShared), stream>>>(
-        T, a);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    if (dev < 64 && !((configured.load() >> dev) & 1ull)) {
+      e = cudaFuncSetAttribute(sw_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(sizeof(SweepShared)));
+      if (e != cudaSuccess) return e;
+      configured.fetch_or(1ull << dev);
+    }
   }
-  return cudaSuccess;
+  sw_sweep_kernel<<<(a.chunk_count + kSweepCols - 1) / kSweepCols, kSweepThreads, sizeof(SweepShared), stream>>>(T,
+                                                                                                               a);
+  return cudaGetLastError();
 }
 
 }  // namespace rrtmg
