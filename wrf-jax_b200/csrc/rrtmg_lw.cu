@@ -1496,34 +1496,42 @@ constexpr int kLwRing = 8;                                 // levels of radiance
 static_assert(kLwSweepThreads >= kLwSweepCols * kLwGpts && kLwSweepThreads % 32 == 0, "sweep block shape");
 
 struct LwSweepShared {
-  float ring[kLwRing][kLwSweepCols][2][kLwGpts];  // total, clear radiance of each g-point
-  float flux[kLwSweepCols][4][kMaxLay + 1];       // up total, up clear, down total, down clear per level
+  float ring[kLwRing][kLwSweepCols][2][kLwGpts];      // total, clear radiance of each g-point
+  float bands[kLwRing][kLwSweepCols][2][kLwBands];    // each band's radiance sum
+  float flux[kLwSweepCols][4][kMaxLay + 1];           // up total, up clear, down total, down clear per level
 };
 
-// Sums the ring's levels: chain (column, total/clear, level) adds each band's
-// radiances in g-point order, then the band terms (bandsum * 0.5) * delwave in
-// band order (band_step, lw:170-199), times fluxfac.
+// Sums the ring's levels in two rounds of independent chains: (column,
+// total/clear, level, band) adds the band's radiances in g-point order, then
+// (column, total/clear, level) adds the band terms (bandsum * 0.5) * delwave in
+// band order (band_step, lw:170-199) and multiplies by fluxfac.  The
+// operations and their order are those of one sequential sum per level.
 __device__ __forceinline__ void lw_flush(LwSweepShared &S, int count, int type0, int level0, int dir) {
   __syncthreads();
   const float pi = 3.1415926535897932384626433832795f;
   const float fluxfac = pi * 2.0e4f;
+  const int band_chains = kLwSweepCols * 2 * count * kLwBands;
+  for (int ch = threadIdx.x; ch < band_chains; ch += kLwSweepThreads) {
+    const int b = ch % kLwBands;
+    const int rest = ch / kLwBands;
+    const int j = rest % count;
+    const int cq = rest / count;  // column * 2 + total/clear
+    const float *v = S.ring[j][cq >> 1][cq & 1] + kGofsDev[b];
+    const int ngc = kNgcDev[b];
+    float bandsum = 0.0f;
+    for (int g = 0; g < ngc; ++g) bandsum = bandsum + v[g];
+    S.bands[j][cq >> 1][cq & 1][b] = bandsum;
+  }
+  __syncthreads();
   const int chains = kLwSweepCols * 2 * count;
   for (int ch = threadIdx.x; ch < chains; ch += kLwSweepThreads) {
     const int j = ch % count;
-    const int rest = ch / count;
-    const int q = rest & 1;
-    const int c = rest >> 1;
-    const float *v = S.ring[j][c][q];
+    const int cq = ch / count;
+    const float *bs = S.bands[j][cq >> 1][cq & 1];
     float total = 0.0f;
 #pragma unroll
-    for (int b = 0; b < kLwBands; ++b) {
-      float bandsum = 0.0f;
-      const float *vb = v + kGofsDev[b];
-      const int ngc = kNgcDev[b];
-      for (int g = 0; g < ngc; ++g) bandsum = bandsum + vb[g];
-      total = total + (bandsum * 0.5f) * kDelwave[b];
-    }
-    S.flux[c][type0 + q][level0 + dir * j] = total * fluxfac;
+    for (int b = 0; b < kLwBands; ++b) total = total + (bs[b] * 0.5f) * kDelwave[b];
+    S.flux[cq >> 1][type0 + (cq & 1)][level0 + dir * j] = total * fluxfac;
   }
   __syncthreads();
 }
