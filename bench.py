@@ -55,13 +55,28 @@ METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0
 # oracle columns timed for the CPU baseline: 100 rows of the domain, about 2-3 s
 # on 16 host threads (roughly 40 core-seconds of work)
 CPU_SAMPLE_COLUMNS = 42500
-# DRAM traffic per unit of the dominant kernels, from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch on the 256x256x50 case divided by its
-# units): sw_kernel 51.76 GB over 45,794 day columns, lw_group_kernel 5.22 GB
-# over 65,536 columns
-DRAM_BYTES_PER_DAY_COLUMN_SW = 1130231
-DRAM_BYTES_PER_COLUMN_LW = 79576
+# DRAM traffic per unit of the sweep kernels, from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch divided by its units): sw_sweep_kernel
+# 19.52 GB over 32,768 day columns (256 x 256 x 50 domain, one full chunk),
+# lw_sweep_kernel 2.27 GB over 16,384 columns (128 x 128 x 50 domain)
+DRAM_BYTES_PER_DAY_COLUMN_SW = 595700
+DRAM_BYTES_PER_COLUMN_LW = 138700
 L2_BYTES = 126 * 1024 * 1024
+# counted binary32 operations of the plain path per LW column and per SW day
+# column (tests/golden/make_flop_counts.py: the oracle's counting build on 10
+# rows of the 425 x 425 x 50 generator domain); read as data, nothing under
+# oracle/ runs here
+FLOP_COUNTS = REPO / "tests" / "golden" / "flop_counts.json"
+# FP32 SIMT peak of a B200 (148 SMs x 128 lanes x 2 flops per FMA x 1.965 GHz);
+# MEASURED_PEAKS.json has no FP32 figure.  The plain kernels are built without
+# FMA contraction (one instruction per add or multiply), so their issue-bound
+# ceiling is half of it.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+# compulsory HBM bytes of one column through both calls at nk levels: 12 mass-
+# level and 2 interface-level fields read, 4 heating fields written, 37 2-D
+# values in or out, binary32
+def plain_column_bytes(nk: int) -> int:
+    return (18 * nk + 37) * 4
 
 
 def _package():
@@ -218,7 +233,7 @@ def run_plain(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     _package()
-    from wrf_jax_b200 import rrtmg, synthetic
+    from wrf_jax_b200 import _capi, rrtmg, synthetic
 
     st = synthetic.make_columns(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nk"], seed=WORKLOAD["seed"] + rank)
     ncol = st.nx * st.ny
@@ -267,8 +282,10 @@ def run_plain(args):
     lw_t = statistics.median(a.elapsed_time(b) for a, b in lw_ms) / 1e3
     sw_t = statistics.median(a.elapsed_time(b) for a, b in sw_ms) / 1e3
     launch_ms = {}
-    for side, names in ((0, ("mcica_mask_kernel (LW)", "lw_group_kernel", "lw_finish_kernel")),
-                        (1, ("mcica_mask_kernel (SW)", "sw_daylist_kernel", "sw_kernel"))):
+    for side, names in ((0, ("mcica_mask_kernel (LW)", "lw optics (lw_colprep, lw_layer, lw_gas kernels)",
+                             "lw_sweep_kernel")),
+                        (1, ("mcica_mask_kernel (SW)",
+                             "sw optics (sw_daylist, sw_colprep, sw_optics, sw_source kernels)", "sw_sweep_kernel"))):
         buf = (ctypes.c_float * (3 * args.steps))()
         got = ctx.lib.rrtmg_timing_read(ctx.handle, side, buf, args.steps)
         if got != args.steps:
@@ -307,28 +324,44 @@ def run_plain(args):
     hbm, bf16, peak_kind = _peaks()
     nk = WORKLOAD["nk"]
     nlay_sw = nk + 1
+    sched = _capi.Schedule()
+    ctx.check(ctx.lib.rrtmg_get_schedule(ctx.handle, ctypes.byref(sched)))
+    lw_chunks = -(-ncol // sched.lw_chunk_columns)
+    sw_chunks = -(-ncol // sched.sw_chunk_columns)
+    gpu_launches = (1 + 4 * lw_chunks) + (2 + 4 * sw_chunks)
     nday = int((np.asarray(sw_host["coszr"]) > 0.0).sum())
-    # Dominant kernel and its algorithmic HBM bytes per launch.  sw_kernel, per
-    # day column: reads 12 (nx,nk,ny) fields (p3d t3d qv o3 cldfra qc qi qs
-    # re_cloud re_ice re_snow pi3d), 2 level fields (p8w t8w), 5 2-D fields and
-    # the McICA mask (4 words per layer); writes 2 (nx,nk,ny) heating rates and
-    # 16 2-D fields.  lw_group_kernel, per column and band group: reads 13
-    # (nx,nk,ny) fields, 2 level fields, 5 2-D fields and the mask (5 words per
-    # layer), writes its bands' level terms (4 per level and band).
-    dom = max(launch_ms, key=launch_ms.get)
-    if dom == "sw_kernel":
-        units = nday
-        unit_bytes = 4 * (12 * nk + 2 * (nk + 1) + 5 + 4 * nlay_sw + 2 * nk + 16)
-    else:
-        nlay_lw = ctx.lib.rrtmg_lw_nlayers(float(lw_host["p_top"]), nk)
-        units = ncol
-        unit_bytes = 9 * 4 * (13 * nk + 2 * (nk + 1) + 5 + 5 * nlay_lw) + 4 * 4 * (nk + 2) * 16
+    # The sweep kernels of the staged schedules and their HBM bytes per unit.
+    # sw_sweep_kernel, per day column: per layer each g-point's gas and
+    # Rayleigh depths and each band's cloud optics from the layer records
+    # (2 x 112 + 4 x 14 floats), its level stack written and read back (16
+    # floats per level and g-point, twice), the McICA mask (4 words per layer),
+    # pi3d and p8w for the heating, 2 heating fields and 16 2-D outputs.
+    # lw_sweep_kernel, per column: the layer records read in both sweeps
+    # (2 x 140 + 4 x 16 + 1 floats per layer, twice), the mask (5 words per
+    # layer, twice), pi3d and p8w, 2 heating fields and 15 2-D outputs.
+    nlay_lw = ctx.lib.rrtmg_lw_nlayers(float(lw_host["p_top"]), nk)
+    unit_bytes = {
+        "sw_sweep_kernel": 4 * (nlay_sw * (2 * 112 + 4 * 14) + 2 * 16 * (nlay_sw + 1) * 112 + 4 * nlay_sw
+                                + nk + (nk + 1) + 2 * nk + 16),
+        "lw_sweep_kernel": 4 * (2 * nlay_lw * (2 * 140 + 4 * 16 + 1) + 2 * 5 * nlay_lw + nk + (nk + 1) + 2 * nk + 15),
+    }
+    unit_count = {"sw_sweep_kernel": nday, "lw_sweep_kernel": ncol}
+    dom = max(("sw_sweep_kernel", "lw_sweep_kernel"), key=lambda k: launch_ms[k])
+    units = unit_count[dom]
     dom_s = launch_ms[dom] / 1e3
-    achieved = units * unit_bytes / dom_s / 1e9
+    achieved = units * unit_bytes[dom] / dom_s / 1e9
     # DRAM bytes per unit measured by ncu (dram__bytes_read.sum +
-    # dram__bytes_write.sum) on the 256x256x50 case, scaled to this launch
-    traffic_per_unit = {"sw_kernel": DRAM_BYTES_PER_DAY_COLUMN_SW, "lw_group_kernel": DRAM_BYTES_PER_COLUMN_LW}
-    traffic = traffic_per_unit[dom] * units if traffic_per_unit.get(dom) else None
+    # dram__bytes_write.sum of one launch on a smaller case, divided by its units)
+    traffic_per_unit = {"sw_sweep_kernel": DRAM_BYTES_PER_DAY_COLUMN_SW, "lw_sweep_kernel": DRAM_BYTES_PER_COLUMN_LW}
+    traffic = traffic_per_unit[dom] * units
+    plain_fp32 = None
+    if FLOP_COUNTS.exists():
+        fc = json.loads(FLOP_COUNTS.read_text())
+        lw_tf = fc["lw_flops_per_column"] * ncol / lw_t / 1e12
+        sw_tf = fc["sw_flops_per_day_column"] * nday / sw_t / 1e12
+        plain_fp32 = {"unit": "TFLOP/s", "peak": FP32_PEAK_TFLOPS, "lw_achieved": lw_tf, "lw_frac": lw_tf / FP32_PEAK_TFLOPS,
+                      "sw_achieved": sw_tf, "sw_frac": sw_tf / FP32_PEAK_TFLOPS,
+                      "flops": "counted binary32 operations per LW column / SW day column: " + fc["sample"]}
     line = {
         "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
@@ -340,12 +373,13 @@ def run_plain(args):
                    "lw_ms": lw_t * 1e3, "sw_ms": sw_t * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "kernel": dom,
-                     "kernel_ms": launch_ms[dom], "units_per_launch": units, "bytes_per_unit": unit_bytes,
+                     "kernel_ms": launch_ms[dom], "units_per_launch": units, "bytes_per_unit": unit_bytes[dom],
                      "peak_source": peak_kind,
-                     "note": "algorithmic HBM bytes / kernel time (CUDA events around the launch); "
-                             "the column kernels are latency and FP32-issue bound, not HBM bound"},
+                     "note": "staged-schedule HBM bytes of the sweep kernel (layer records, level stack, "
+                             "mask, I/O) / its time summed over the call's chunks (CUDA events)"},
+        "plain_fp32": plain_fp32,
         "launch_ms": launch_ms,
-        "gpu_launches": 6 * args.steps,  # LW: McICA, band groups, finish; SW: McICA, day list, columns
+        "gpu_launches": gpu_launches * args.steps,
         "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
     }
@@ -362,11 +396,10 @@ def run_plain(args):
 def _surrogate_launches(n_fallback: int, fused: bool) -> int:
     """Kernel launches of one surrogate step: features, the fused network
     kernel (or 4 GEMMs and a decode), compact; with fallback columns also one
-    batched gather and one scatter, the LW split schedule (McICA, column
-    set-up, layer optics, g-point sweep, finish) and the SW split schedule
-    (McICA, day list, column set-up, layer optics, solar source, g-point sweep,
-    g-point sums, finish)."""
-    return (3 if fused else 7) + (15 if n_fallback > 0 else 0)
+    batched gather and one scatter, the LW sweep schedule (McICA, column
+    set-up, layer set-up, gas optics, sweep) and the SW sweep schedule
+    (McICA, day list, column set-up, layer optics, solar source, sweep)."""
+    return (3 if fused else 7) + (13 if n_fallback > 0 else 0)
 
 
 def run_surrogate(args):
@@ -423,25 +456,73 @@ def run_surrogate(args):
     plain()
     for _ in range(max(3, args.warmup)):
         sur()
+    n_plain_steps = max(1, min(args.steps, 3))
+    from wrf_jax_b200 import rrtmg
+    lw_kw = {k: (d[k] if k in d else v) for k, v in st.lw_kwargs().items()}
+    sw_kw = {k: (d[k] if k in d else v) for k, v in st.sw_kwargs().items()}
     with ClockSampler(local) as clocks:
         el_sur, res = timed(sur, args.steps)
-        el_plain, (lw, sw) = timed(plain, max(1, min(args.steps, 3)))
-    n_plain_steps = max(1, min(args.steps, 3))
+        el_plain, (lw, sw) = timed(plain, n_plain_steps)
+        el_lw, _ = timed(lambda: rrtmg.rrtmg_lwrad_wrf_columns(**lw_kw), n_plain_steps)
+        el_sw, _ = timed(lambda: rrtmg.rrtmg_swrad_wrf_columns(**sw_kw), n_plain_steps)
     value = ws * ncol * args.steps / el_sur
     plain_value = ws * ncol * n_plain_steps / el_plain
 
-    # accuracy of the surrogate path against the plain kernels on the same columns
+    # accuracy of the surrogate path against the plain kernels on the same
+    # columns, LW over all columns and SW over the day columns (night SW is
+    # exactly zero on both paths)
     pi = d["pi3d"]
+    day = (d["coszr"] > 0.0)
+    nday = int(day.sum())
     hl, hs = S.heating_kday(res.rthratenlw, pi), S.heating_kday(res.rthratensw, pi)
     rl, rs = S.heating_kday(lw.rthratenlw, pi), S.heating_kday(sw.rthratensw, pi)
     heat_rmse = float(torch.sqrt(torch.cat([(hl - rl).flatten(), (hs - rs).flatten()]).pow(2).mean()))
     flux = torch.stack([res.glw - lw.glw, res.lwupb - lw.lwupb, res.swdnb - sw.swdnb, res.swupb - sw.swupb])
     flux_rmse = float(torch.sqrt((flux ** 2).mean()))
+    day3 = day[:, None, :].expand_as(hs)
+    accuracy = {
+        "lw_heating_rmse_kday": float(torch.sqrt((hl - rl).pow(2).mean())),
+        "sw_heating_rmse_kday_day_columns": float(torch.sqrt((hs - rs)[day3].pow(2).mean())),
+        "lw_surface_flux_rmse_wm2": float(torch.sqrt(torch.stack([res.glw - lw.glw, res.lwupb - lw.lwupb])
+                                                     .pow(2).mean())),
+        "sw_surface_flux_rmse_wm2_day_columns": float(torch.sqrt(torch.stack(
+            [(res.swdnb - sw.swdnb)[day], (res.swupb - sw.swupb)[day]]).pow(2).mean())),
+        "day_columns": nday,
+    }
+
+    # the plain kernels against the FP32 SIMT peak, with the counted
+    # operations per column, and against the HBM peak with the compulsory bytes
+    hbm, bf16, peak_kind = _peaks()
+    plain_roofline = None
+    if FLOP_COUNTS.exists():
+        fc = json.loads(FLOP_COUNTS.read_text())
+        lw_ms, sw_ms = el_lw / n_plain_steps * 1e3, el_sw / n_plain_steps * 1e3
+        lw_t = fc["lw_flops_per_column"] * ncol / (lw_ms / 1e3) / 1e12
+        sw_t = fc["sw_flops_per_day_column"] * nday / (sw_ms / 1e3) / 1e12
+        plain_ms = el_plain / n_plain_steps * 1e3
+        gbs = plain_column_bytes(wl["nk"]) * ncol / (plain_ms / 1e3) / 1e9
+        plain_roofline = {
+            "bound": "fp32", "unit": "TFLOP/s", "peak": FP32_PEAK_TFLOPS,
+            "peak_source": "nominal FP32 SIMT (148 SMs x 128 lanes x 2 x 1.965 GHz); the path runs without FMA, "
+                           "so its issue-bound ceiling is half the peak",
+            "lw": {"ms": lw_ms, "flops_per_column": fc["lw_flops_per_column"], "achieved": lw_t,
+                   "frac": lw_t / FP32_PEAK_TFLOPS},
+            "sw": {"ms": sw_ms, "flops_per_day_column": fc["sw_flops_per_day_column"], "day_columns": nday,
+                   "achieved": sw_t, "frac": sw_t / FP32_PEAK_TFLOPS},
+            "flop_counts": fc["sample"] + " (" + fc["workload"] + " generator)",
+            "hbm": {"bytes_per_column": plain_column_bytes(wl["nk"]), "achieved": gbs, "unit": "GB/s",
+                    "peak": hbm, "frac": gbs / hbm,
+                    "note": "compulsory I/O of both calls; the staged schedules move their layer records and "
+                            "the SW level stack through HBM as well (see profiles/)"},
+        }
 
     # the network alone (the tensor-core part) for the roofline: the fused
-    # kernel (four layers + decode), and for comparison the four unfused GEMMs
+    # kernel (four layers + decode), and for comparison the four unfused GEMMs.
+    # Algorithmic FLOPs count the network as specified (454 -> 3 x 512 -> 104
+    # outputs); the kernel computes padded 512-input and 128-output tiles.
     mpad = (ncol + 127) // 128 * 128
-    flops = 2.0 * mpad * sum(o * i for o, i in S.LAYER_SHAPES)
+    flops = 2.0 * ncol * (S.N_FEATURES * S.HIDDEN + 2 * S.HIDDEN * S.HIDDEN + S.HIDDEN * 104)
+    flops_padded = 2.0 * mpad * sum(o * i for o, i in S.LAYER_SHAPES)
     call = S.fused_kernel_call(model, st, d, energy_tol=tol)
     for _ in range(3):
         call()
@@ -457,7 +538,6 @@ def run_surrogate(args):
     gemm_ms = el_gemm / args.steps * 1e3
     del X, H, Y
     kernel_ms = fused_ms if fused else gemm_ms
-    hbm, bf16, peak_kind = _peaks()
     achieved = flops / (kernel_ms / 1e3) / 1e12
 
     # end to end with host inputs and host outputs through surrogate.infer_host
@@ -494,13 +574,14 @@ def run_surrogate(args):
                    "energy_gate_tol_wm2": tol, "weights": WEIGHTS.name},
         "plain_value": plain_value, "plain_ms_per_step": el_plain / n_plain_steps * 1e3,
         "speedup_vs_plain": value / plain_value,
-        "heating_rmse_kday": heat_rmse, "surface_flux_rmse_wm2": flux_rmse,
+        "heating_rmse_kday": heat_rmse, "surface_flux_rmse_wm2": flux_rmse, "accuracy": accuracy,
         "fallback_fraction": res.n_fallback / ncol,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                      "frac": achieved / bf16, "traffic": None,
                      "kernel": "mlp_kernel (4 layers + decode, fused)" if fused else "umma_gemm_kernel (4 GEMMs)",
-                     "kernel_ms": kernel_ms, "flops_per_launch": flops, "peak_source": peak_kind,
-                     "unfused_gemms_ms": gemm_ms, "fused_ms": fused_ms},
+                     "kernel_ms": kernel_ms, "flops_per_launch": flops, "padded_flops_per_launch": flops_padded,
+                     "peak_source": peak_kind, "unfused_gemms_ms": gemm_ms, "fused_ms": fused_ms},
+        "plain_roofline": plain_roofline,
         "gpu_launches": _surrogate_launches(res.n_fallback, fused) * args.steps,
         "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
