@@ -1,7 +1,9 @@
 """Surrogate training kernels on the GPU: gradients of one training step
 against the CPU oracle (oracle/surrogate_oracle.py), and a short training run
-showing what the trained network gains over the untrained one and over the
-plain kernels alone."""
+showing what the trained network gains over the untrained one (its
+climatological mean).  The trained network's accuracy against the plain
+kernels is tests/test_surrogate_accuracy.py; its speed is bench.py's
+surrogate line."""
 
 from __future__ import annotations
 
@@ -56,7 +58,7 @@ def test_training_step_gradients_match_cpu_oracle(torch_cuda):
         assert eb < 2e-2, (layer, eb)
 
 
-def test_short_training_beats_untrained_network_and_plain_speed(torch_cuda):
+def test_short_training_beats_untrained_network(torch_cuda):
     torch = torch_cuda
     from wrf_jax_b200 import surrogate as S, synthetic
 
