@@ -208,9 +208,26 @@ rrtmg_status rrtmg_sur_move_fields(const int *list, const int *count, int max_n,
 rrtmg_status rrtmg_gemm_set_tile(int bn);
 
 /* Synchronous: reads the sticky flag that a CTA of rrtmg_gemm_bf16 or
- * rrtmg_sur_mlp sets when it gives up waiting (2 s) for its copies or
- * tensor-core work; clears it when reset != 0. */
+ * rrtmg_sur_mlp sets when it gives up waiting for its copies or tensor-core
+ * work (it then drains what it started, frees its tensor memory and writes no
+ * output); clears it when reset != 0.  Returns RRTMG_TIMEOUT while the flag is
+ * set, RRTMG_OK otherwise. */
 rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag);
+
+/* Limit of each bounded mbarrier wait of rrtmg_gemm_bf16, in nanoseconds,
+ * passed to the kernel with every call; 0 restores the default of 2 s.
+ * Process-wide. */
+rrtmg_status rrtmg_gemm_set_wait_ns(unsigned long long wait_ns);
+
+/* Failure-detection test hook, off by default.  While enable != 0, every CTA
+ * of later rrtmg_gemm_bf16 calls withholds the tensor-core commit of its first
+ * K block: its wait for that block runs out after the wait limit, it waits for
+ * the commit of its second block (which covers the first block's MMAs), frees
+ * its tensor memory, writes no output and sets the flag rrtmg_gemm_error
+ * reports.  While it is on, calls with K / (64 * ksplit) no larger than the
+ * tile's pipeline stages (3 when N % 256 == 0 with the automatic tile, else
+ * 4) are rejected with RRTMG_BAD_ARG.  Process-wide. */
+rrtmg_status rrtmg_gemm_test_withhold_commit(int enable);
 
 #ifdef __cplusplus
 }

@@ -144,7 +144,8 @@ EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_l
            "rrtmg_lwrad_static_scratch", "rrtmg_lwrad_live", "rrtmg_swrad_live", "rrtmg_timing_enable",
            "rrtmg_timing_read", "rrtmg_set_schedule", "rrtmg_get_schedule", "rrtmg_lw_nlayers",
            "rrtmg_last_error", "rrtmg_status_string")
-SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile", "rrtmg_sur_features", "rrtmg_sur_targets",
+SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile", "rrtmg_gemm_set_wait_ns",
+                     "rrtmg_gemm_test_withhold_commit", "rrtmg_sur_features", "rrtmg_sur_targets",
                      "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
                      "rrtmg_sur_row_sum", "rrtmg_sur_reduce_splits", "rrtmg_sur_adam", "rrtmg_sur_decode",
                      "rrtmg_sur_compact", "rrtmg_sur_move_columns", "rrtmg_sur_timestamp",
@@ -198,6 +199,10 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.rrtmg_gemm_bf16.argtypes = [ctypes.POINTER(GemmArgs), ctypes.c_void_p]
     lib.rrtmg_gemm_error.restype = ctypes.c_int
     lib.rrtmg_gemm_error.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
+    lib.rrtmg_gemm_set_wait_ns.restype = ctypes.c_int
+    lib.rrtmg_gemm_set_wait_ns.argtypes = [ctypes.c_ulonglong]
+    lib.rrtmg_gemm_test_withhold_commit.restype = ctypes.c_int
+    lib.rrtmg_gemm_test_withhold_commit.argtypes = [ctypes.c_int]
     V, I, P, FL, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_float, ctypes.c_size_t
     sigs = {
         "rrtmg_sur_features": [ctypes.POINTER(SurFeaturesArgs), V],

@@ -1,6 +1,7 @@
 // C-ABI of the surrogate kernels.  See include/rrtmg_surrogate.h.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "../../include/rrtmg_surrogate.h"
@@ -10,6 +11,10 @@ using namespace rrtmg;
 
 namespace {
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;  // 2 s
+std::atomic<unsigned long long> g_wait_ns{kDefaultWaitNs};
+std::atomic<int> g_withhold_commit{0};
 }  // namespace
 
 extern "C" rrtmg_status rrtmg_gemm_bf16(const rrtmg_gemm_args *a, void *stream) {
@@ -50,6 +55,11 @@ extern "C" rrtmg_status rrtmg_gemm_bf16(const rrtmg_gemm_args *a, void *stream) 
   g.Ht = static_cast<__nv_bfloat16 *>(a->Ht); g.ldht = a->ldht;
   g.aux = a->aux; g.ldaux = a->ldaux;
   g.Z = a->Z; g.ldz = a->ldz;
+  g.wait_ns = g_wait_ns.load();
+  g.withhold_commit0 = g_withhold_commit.load();
+  // the hook needs a later commit to drain behind the withheld one and a wait
+  // on the withheld one inside the K loop: more K blocks than stages
+  if (g.withhold_commit0 && a->K / (64 * a->ksplit) <= gemm_stages(a->N)) return RRTMG_BAD_ARG;
   return launch_umma_gemm(g, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RRTMG_OK : RRTMG_CUDA;
 }
 
@@ -59,6 +69,16 @@ extern "C" rrtmg_status rrtmg_gemm_error(int reset, unsigned *flag) {
   if (gemm_error_flag(&g, reset != 0) != cudaSuccess || mlp_error_flag(&m, reset != 0) != cudaSuccess)
     return RRTMG_CUDA;
   *flag = g | m;
+  return *flag ? RRTMG_TIMEOUT : RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_gemm_set_wait_ns(unsigned long long wait_ns) {
+  g_wait_ns.store(wait_ns ? wait_ns : kDefaultWaitNs);
+  return RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_gemm_test_withhold_commit(int enable) {
+  g_withhold_commit.store(enable != 0);
   return RRTMG_OK;
 }
 

@@ -145,15 +145,20 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
             : "r"(tmem), "l"(adesc), "l"(bdesc), "r"(TL::kIdesc), "r"(accumulate)
             : "memory");
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&mbar[s]))
-                   : "memory");
+      // (the failure-detection test withholds block 0's commit: the wait for it
+      // below runs out, and block 1's commit, which covers every earlier MMA,
+      // still lets the CTA drain before it frees its tensor memory)
+      if (!(g.withhold_commit0 && kb == 0))
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar[s]))
+                     : "memory");
     }
     issued = kb + 1;
     const int next = kb + S - 1;
     if (next < nkb) {
       // stage next % S was last read by the MMAs of block kb - 1
-      if (kb >= 1 && !mbar_wait(smem_u32(&mbar[(kb - 1) % S]), static_cast<uint32_t>((kb - 1) / S) & 1u)) ok = false;
+      if (kb >= 1 && !mbar_wait(smem_u32(&mbar[(kb - 1) % S]), static_cast<uint32_t>((kb - 1) / S) & 1u, g.wait_ns))
+        ok = false;
       if (__syncthreads_or(!ok)) {
         if (tid == 0) fail_sh = 1;
         break;
@@ -163,7 +168,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(GemmArgs g) {
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
-  // wait for the last committed group (it covers every earlier MMA)
+  // wait for the last committed group (it covers every earlier MMA) before
+  // the tensor memory is freed; this drain keeps the default limit even when
+  // the pipeline waits above run with a shorter one
   if (issued > 0) {
     const int last = issued - 1;
     if (tid == 0 && !mbar_wait(smem_u32(&mbar[last % S]), static_cast<uint32_t>(last / S) & 1u)) fail_sh = 1;
@@ -266,9 +273,12 @@ int g_tile_choice = 0;  // 0 automatic, else 128 or 256
 
 void set_gemm_tile(int bn) { g_tile_choice = bn; }
 
+bool gemm_wide(int n) { return n % 256 == 0 && g_tile_choice != 128; }
+
+int gemm_stages(int n) { return gemm_wide(n) ? Tile<256>::kStages : Tile<128>::kStages; }
+
 cudaError_t launch_umma_gemm(const GemmArgs &g, cudaStream_t stream) {
-  const bool wide = g.N % 256 == 0 && g_tile_choice != 128;
-  return wide ? launch_tile<256>(g, stream) : launch_tile<128>(g, stream);
+  return gemm_wide(g.N) ? launch_tile<256>(g, stream) : launch_tile<128>(g, stream);
 }
 
 cudaError_t gemm_error_flag(unsigned *out, bool reset) {

@@ -48,11 +48,15 @@ struct GemmArgs {
   int ldht;
   const float *aux;   // kEpiDgelu: pre-activation Z [M][ldaux]
   int ldaux;
+  unsigned long long wait_ns;  // limit of each bounded mbarrier wait
+  int withhold_commit0;        // failure-detection test: skip the commit of K block 0
   float *Z;           // kEpiGelu: pre-activation output [M][ldz]
   int ldz;
 };
 
 cudaError_t launch_umma_gemm(const GemmArgs &g, cudaStream_t stream);
+// pipeline stages of the GEMM tile an N selects (the test hook's K bound)
+int gemm_stages(int n);
 
 using SurFeatureArgs = rrtmg_sur_features_args;
 using SurTargetArgs = rrtmg_sur_targets_args;

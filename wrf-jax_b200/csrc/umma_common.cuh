@@ -64,12 +64,12 @@ __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
   return done != 0;
 }
 
-// Waits for the given phase parity of an mbarrier; gives up after kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+// Waits for the given phase parity of an mbarrier; gives up after limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, uint64_t limit_ns = kWaitNs) {
   const uint64_t t0 = global_ns();
   while (true) {
     if (mbar_try(addr, parity)) return true;
-    if (global_ns() - t0 > kWaitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
 
