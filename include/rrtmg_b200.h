@@ -55,6 +55,16 @@ typedef struct {
     int has_reqc, has_reqi, has_reqs;                   /* effective-radius inputs present */
     int icloud;              /* 0: no cloud microphysics radii (SW runs clear) */
     int cldovrlp;            /* 0 clear, >= 1 McICA maximum-random overlap */
+    /* 0 (default): binary32 throughout, bit for bit the reference's results.
+     * 1: FP64 mode; no counterpart in the reference.  Two steps run in binary64:
+     * the SW delta-Eddington reflectance/transmittance (reftra,
+     * module_ra_rrtmg_sw.py:3490-3601) of every layer whose delta-scaled
+     * single-scattering albedo is >= 0.999 (the conservative branch, sw:2829,
+     * and the nearly conservative layers where g1^2 - g2^2 cancels) or whose
+     * optical depth is below 0.1 (where its terms cancel to O(tau)), and the
+     * flux-difference heating rate dF/dp (lw:5706-5709, sw:2285-2300) of the
+     * five highest model layers and every layer above them. */
+    int fp64_steps;
 } rrtmg_config;
 
 /* Keyword arrays of rrtmg_lwrad_wrf_columns (module_ra_rrtmg_lw.py:6789-6822).
@@ -75,12 +85,18 @@ typedef struct {
 } rrtmg_lw_out;
 
 /* Keyword arrays of rrtmg_swrad_wrf_columns (module_ra_rrtmg_sw.py:2386-2420).
- * Albedo fields for sf_surface_physics == 8 are not part of this path. */
+ * The four (nx, ny) albedo fields of the Noah-MP land model are optional: pass
+ * all four for sf_surface_physics == 8 (module_ra_rrtmg_sw.py:2519-2530), NULL
+ * otherwise.  With all four given, a column with xland < 1.5 takes its direct
+ * and diffuse surface albedos from alswvisdir / alswvisdif in bands 25-28 and
+ * from alswnirdir / alswnirdif in bands 16-24 and 29 (sw:2120-2127); the other
+ * columns, and every column without them, use `albedo` for both. */
 typedef struct {
     const float *p3d, *p8w, *pi3d, *t3d, *t8w, *tsk, *dz8w;
     const float *qv3d, *qc3d, *qi3d, *qs3d, *cldfra3d, *o33d;
     const float *albedo, *coszr, *xland, *xice, *snow;
     const float *re_cloud, *re_ice, *re_snow;
+    const float *alswvisdir, *alswvisdif, *alswnirdir, *alswnirdif;
 } rrtmg_sw_in;
 
 /* Fields of RrtmgSwWrfColumnResult (module_ra_rrtmg_sw.py:617-642). */
@@ -117,6 +133,25 @@ rrtmg_status rrtmg_lwrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrt
 rrtmg_status rrtmg_swrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in,
                               rrtmg_sw_out *out, const int *live_count, void *stream);
 
+/* LW / SW with the per-call scratch in a caller's workspace instead of the
+ * context's stream-ordered pool; no counterpart in the reference.  For
+ * callers whose framework owns device memory, such as an XLA custom call,
+ * which receives the workspace as one more result buffer from XLA's
+ * allocator.  rrtmg_lw_workspace_bytes / rrtmg_sw_workspace_bytes return the
+ * bytes a call with this config needs under the context's current schedule
+ * (0 for an invalid config); they also build the context's McICA jump table
+ * for the config's layer count, the one allocation a first call would
+ * otherwise make, so call them during set-up.  The workspace is device memory
+ * on the context's device, 256-byte aligned, at least that many bytes, and
+ * must not be used by anything else until the call's work on `stream` is
+ * done.  Results are those of rrtmg_lwrad / rrtmg_swrad bit for bit. */
+size_t rrtmg_lw_workspace_bytes(rrtmg_ctx *ctx, const rrtmg_config *cfg);
+size_t rrtmg_sw_workspace_bytes(rrtmg_ctx *ctx, const rrtmg_config *cfg);
+rrtmg_status rrtmg_lwrad_ws(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
+                            void *workspace, size_t workspace_bytes, void *stream);
+rrtmg_status rrtmg_swrad_ws(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
+                            void *workspace, size_t workspace_bytes, void *stream);
+
 /* LW with no allocation inside the call; no counterpart in the reference.
  * Same arguments and results as rrtmg_lwrad, but the McICA scratch lives in
  * fixed file-scope device arrays (32 MiB of mask words) instead of a per-call
@@ -127,6 +162,24 @@ rrtmg_status rrtmg_swrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrt
  * and streams of a device: calls that overlap in time on one device race. */
 rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_config *cfg,
                                         const rrtmg_lw_in *in, rrtmg_lw_out *out, void *stream);
+
+/* Per-column status of the last call (the per-column status of the C-ABI;
+ * the reference itself checks nothing at run time, so bad inputs propagate
+ * silently into its outputs).  While enabled on a context, every rrtmg_lwrad /
+ * rrtmg_swrad call ends with one more launch on its stream that writes a
+ * bitmask per column into the context's status array for that side (0 = LW,
+ * 1 = SW); the *_live and *_static_scratch calls do not.  Bits: */
+#define RRTMG_COL_NONFINITE_INPUT   0x1u  /* a NaN or infinity in an input of the column */
+#define RRTMG_COL_NONFINITE_OUTPUT  0x2u  /* a NaN or infinity in a result of the column */
+#define RRTMG_COL_PRESSURE_ORDER    0x4u  /* p8w not decreasing upward, or p3d outside its interfaces */
+#define RRTMG_COL_TEMPERATURE_RANGE 0x8u  /* t3d, t8w or tsk outside [160, 340) K: the tables clamp */
+#define RRTMG_COL_FRACTION_RANGE    0x10u /* cldfra, emiss or albedo outside [0, 1], or coszr > 1 */
+rrtmg_status rrtmg_column_status_enable(rrtmg_ctx *ctx, int enable);
+/* Copies the status words of the last enabled call of `side` into dev_status
+ * (device memory, ncol = nx * ny words of that call, column c = i * ny + j),
+ * asynchronously on `stream`, ordered after that call when both use the same
+ * stream.  RRTMG_BAD_ARG when no call was recorded or ncol differs. */
+rrtmg_status rrtmg_last_column_errors(rrtmg_ctx *ctx, int side, uint32_t *dev_status, int ncol, void *stream);
 
 /* Per-launch timing; no counterpart in the reference.  While enabled, every
  * rrtmg_lwrad / rrtmg_swrad call records CUDA events on its stream around its

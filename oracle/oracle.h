@@ -17,6 +17,15 @@
 
 #include <stdint.h>
 
+/* The type of the parts every build keeps in binary32: the McICA random
+ * stream and its cloud decisions, so that all builds sample the same
+ * subcolumns.  The binary64 build (fp64.h) defines it before it widens
+ * `float`. */
+#ifndef ORA_BINARY32_DEFINED
+#define ORA_BINARY32_DEFINED 1
+typedef float ora_binary32;
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -29,8 +38,8 @@ void ora_tables_free(ora_tables *t);
 const void *ora_table(const ora_tables *t, const char *name, int *n_out);
 
 /* ---- KISS random stream (common.py:964-1090) ----------------------------- */
-void ora_kiss_step(uint32_t s[4], float *ran);
-void ora_kiss_seeds(const float *pmid4, uint32_t s[4]);
+void ora_kiss_step(uint32_t s[4], ora_binary32 *ran);
+void ora_kiss_seeds(const ora_binary32 *pmid4, uint32_t s[4]);
 
 /* ---- WRF-layout batch inputs ------------------------------------------- */
 typedef struct {
@@ -46,6 +55,15 @@ typedef struct {
     float co2, n2o, ch4, cfc11, cfc12;   /* volume mixing ratios */
     float solcon;
     int has_reqc, has_reqi, has_reqs, icloud, cldovrlp;
+    /* 1: the two steps the GPU's FP64 mode evaluates in binary64 (SW reftra
+     * of layers whose delta-scaled single-scattering albedo is >= 0.999 or
+     * whose optical depth is below 0.1; the heating rate of every layer from
+     * the fifth-highest model layer up) are evaluated in binary64 here too;
+     * 0: binary32 throughout (the reference) */
+    int fp64_steps;
+    /* optional (ncol,) Noah-MP albedos for sf_surface_physics == 8 (all four or
+     * NULL): used for columns with xland < 1.5 (sw:2519-2530) */
+    const float *alswvisdir, *alswvisdif, *alswnirdir, *alswnirdif;
 } ora_in;
 
 typedef struct {

@@ -16,6 +16,7 @@ typedef struct {
     char name[48];
     uint32_t dtype, ndim, shape[4];
     uint64_t offset, nbytes;
+    uint64_t words;   /* nbytes / 4 as stored in the blob */
 } blob_entry;
 
 struct ora_tables {
@@ -30,7 +31,7 @@ const void *ora_table(const ora_tables *t, const char *name, int *n_out)
 {
     for (uint32_t i = 0; i < t->count; ++i) {
         if (strncmp(t->entries[i].name, name, 48) == 0) {
-            if (n_out) *n_out = (int)(t->entries[i].nbytes / 4);
+            if (n_out) *n_out = (int)t->entries[i].words;
             return t->raw + t->entries[i].offset;
         }
     }
@@ -39,6 +40,48 @@ const void *ora_table(const ora_tables *t, const char *name, int *n_out)
 }
 
 const ora_cache *ora_cache_of(const ora_tables *t) { return &t->cache; }
+
+#ifdef ORA_WIDE_TABLES
+/* Binary64 build: `float` is the 8-byte binary64 type, so every binary32
+ * entry (dtype 0) is copied once into an array of it (exact); other entries
+ * are copied as they are.  Entries start on 8-byte boundaries. */
+static int widen_tables(ora_tables *t)
+{
+    size_t total = 0;
+    for (uint32_t i = 0; i < t->count; ++i) {
+        const blob_entry *e = &t->entries[i];
+        const size_t bytes = e->dtype == 0 ? (size_t)e->words * sizeof(float) : (size_t)e->nbytes;
+        total += (bytes + 7) / 8 * 8;
+    }
+    unsigned char *wide = (unsigned char *)calloc(total ? total : 1, 1);
+    if (!wide) return -1;
+    size_t pos = 0;
+    for (uint32_t i = 0; i < t->count; ++i) {
+        blob_entry *e = &t->entries[i];
+        const unsigned char *src = t->raw + e->offset;
+        size_t bytes;
+        if (e->dtype == 0) {
+            float *dst = (float *)(wide + pos);
+            for (uint64_t k = 0; k < e->words; ++k) {
+                ora_binary32 v;
+                memcpy(&v, src + 4 * k, 4);
+                dst[k] = v;
+            }
+            bytes = (size_t)e->words * sizeof(float);
+        } else {
+            memcpy(wide + pos, src, (size_t)e->nbytes);
+            bytes = (size_t)e->nbytes;
+        }
+        e->offset = pos;
+        e->nbytes = bytes;
+        pos += (bytes + 7) / 8 * 8;
+    }
+    free(t->raw);
+    t->raw = wide;
+    t->size = total;
+    return 0;
+}
+#endif
 
 ora_tables *ora_tables_load(const char *path)
 {
@@ -68,7 +111,18 @@ ora_tables *ora_tables_load(const char *path)
         memcpy(t->entries[i].shape, p + 56, 16);
         memcpy(&t->entries[i].offset, p + 72, 8);
         memcpy(&t->entries[i].nbytes, p + 80, 8);
+        t->entries[i].words = t->entries[i].nbytes / 4;
+        if (t->entries[i].offset > t->size || t->entries[i].nbytes > t->size - t->entries[i].offset) {
+            ora_tables_free(t);
+            return NULL;
+        }
     }
+#ifdef ORA_WIDE_TABLES
+    if (widen_tables(t) != 0) {
+        ora_tables_free(t);
+        return NULL;
+    }
+#endif
     if (ora_cache_init(t, &t->cache) != 0) {
         ora_tables_free(t);
         return NULL;
@@ -138,7 +192,7 @@ void ora_o3data(const ora_cache *c, const float *plev, int nout, float *o3)
 /* ------------------------------------------------------------------------ */
 /* KISS generator (common:964-1005)                                          */
 /* ------------------------------------------------------------------------ */
-void ora_kiss_step(uint32_t s[4], float *ran)
+void ora_kiss_step(uint32_t s[4], ora_binary32 *ran)
 {
     s[0] = 69069u * s[0] + 1327217885u;
     uint32_t x = s[1];
@@ -149,14 +203,14 @@ void ora_kiss_step(uint32_t s[4], float *ran)
     s[2] = 18000u * (s[2] & 65535u) + (s[2] >> 16);
     s[3] = 30903u * (s[3] & 65535u) + (s[3] >> 16);
     uint32_t kiss = s[0] + s[1] + (s[2] << 16) + s[3];
-    float k = (float)(int32_t)kiss;
+    ora_binary32 k = (ora_binary32)(int32_t)kiss;
     *ran = k * 2.328306e-10f + 0.5f;
 }
 
-void ora_kiss_seeds(const float *pmid4, uint32_t s[4])
+void ora_kiss_seeds(const ora_binary32 *pmid4, uint32_t s[4])
 {
     for (int i = 0; i < 4; ++i) {
-        float frac = pmid4[i] - truncf(pmid4[i]);
+        ora_binary32 frac = pmid4[i] - truncf(pmid4[i]);
         s[i] = (uint32_t)(int32_t)(frac * 1000000000.0f);
     }
 }
@@ -164,27 +218,31 @@ void ora_kiss_seeds(const float *pmid4, uint32_t s[4])
 /* McICA maximum-random overlap (common:1092-1153) for one column.
  * cld: (nlay) cloud fraction.  cloudy: (nsub, nlay) output 0/1. */
 void ora_mcica_overlap2(const float *play, const float *cld_in, int nlay, int nsub,
-                        int change_seed, unsigned char *cloudy, float *cdf_work)
+                        int change_seed, unsigned char *cloudy, ora_binary32 *cdf_work)
 {
-    float pmid[4];
-    for (int i = 0; i < 4; ++i) pmid[i] = play[i] * 100.0f;
+    /* binary32 in every build: the layer pressures and cloud fractions are
+     * binary32 values (rounded to it in the binary64 build) */
+    ora_binary32 pmid[4];
+    for (int i = 0; i < 4; ++i) pmid[i] = (ora_binary32)play[i] * 100.0f;
     uint32_t s[4];
     ora_kiss_seeds(pmid, s);
-    float r;
+    ora_binary32 r;
     for (int i = 0; i < change_seed; ++i) ora_kiss_step(s, &r);
     for (int d = 0; d < nsub * nlay; ++d) {
         ora_kiss_step(s, &r);
         cdf_work[d] = r;          /* index = sub * nlay + lay */
     }
     for (int sub = 0; sub < nsub; ++sub) {
-        float *cdf = cdf_work + (size_t)sub * nlay;
+        ora_binary32 *cdf = cdf_work + (size_t)sub * nlay;
         for (int l = 1; l < nlay; ++l) {
-            float cprev = cld_in[l - 1] < 1.0e-20f ? 0.0f : cld_in[l - 1];
-            float thr = 1.0f - cprev;
+            const ora_binary32 cl = (ora_binary32)cld_in[l - 1];
+            ora_binary32 cprev = cl < 1.0e-20f ? 0.0f : cl;
+            ora_binary32 thr = 1.0f - cprev;
             cdf[l] = (cdf[l - 1] > thr) ? cdf[l - 1] : cdf[l] * thr;
         }
         for (int l = 0; l < nlay; ++l) {
-            float c = cld_in[l] < 1.0e-20f ? 0.0f : cld_in[l];
+            const ora_binary32 cl = (ora_binary32)cld_in[l];
+            ora_binary32 c = cl < 1.0e-20f ? 0.0f : cl;
             cloudy[(size_t)sub * nlay + l] = cdf[l] >= 1.0f - c;
         }
     }

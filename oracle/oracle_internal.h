@@ -70,7 +70,7 @@ int ora_lw_cache_init(const ora_tables *t, ora_lw_cache *c);
 int ora_sw_cache_init(const ora_tables *t, ora_sw_cache *c);
 void ora_o3data(const ora_cache *c, const float *plev, int nout, float *o3);
 void ora_mcica_overlap2(const float *play, const float *cld_in, int nlay, int nsub,
-                        int change_seed, unsigned char *cloudy, float *cdf_work);
+                        int change_seed, unsigned char *cloudy, ora_binary32 *cdf_work);
 void ora_cloud_flags(int has_reqc, int has_reqi, int has_reqs, int icloud,
                      int *inflg, int *iceflg, int *liqflg);
 void ora_cloud_paths(const ora_cache *c, const ora_in *in, int col, const float *tlay,
@@ -87,5 +87,19 @@ static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ?
 static inline int jrow(int r, int n) { if (r < 0) r += n; return clampi(r, 0, n - 1); }
 
 static inline float interpf(float lo, float hi, float f) { return lo + f * (hi - lo); }
+
+/* FP64 mode's heating rate of a layer (LW: lw:5702-5712, SW: sw:2285-2301
+ * with zdpgcp = heatfac / dp): the net fluxes at the layer's bottom (0) and
+ * top (1), their difference and the division by the pressure thickness are
+ * binary64 operations on the binary32 fluxes and pressures; one rounding to
+ * binary32 at the end.  up - dn is the LW net flux; the SW passes (dn, up). */
+static inline float ora_heating64(float heatfac, float up0, float dn0, float up1, float dn1,
+                                  float plev0, float plev1)
+{
+    const double f0 = (double)up0 - (double)dn0;
+    const double f1 = (double)up1 - (double)dn1;
+    const double dp = (double)plev0 - (double)plev1;
+    return (float)((double)heatfac * (f0 - f1) / dp);
+}
 
 #endif

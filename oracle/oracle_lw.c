@@ -99,6 +99,7 @@ int ora_lw_nlayers(double p_top, int nk)
 /* ------------------------------------------------------------------------ */
 typedef struct {
     int nlay, laytrop;
+    int fp64_from;   /* first layer whose heating is formed in binary64 (FP64 mode) */
     float play[MAX_LAY], plev[MAX_LAY + 1], tlay[MAX_LAY], tlev[MAX_LAY + 1];
     float h2o[MAX_LAY], o3[MAX_LAY], co2[MAX_LAY], ch4[MAX_LAY], n2o[MAX_LAY], o2[MAX_LAY];
     float cfc11[MAX_LAY], cfc12[MAX_LAY], cfc22[MAX_LAY], ccl4[MAX_LAY];
@@ -122,7 +123,7 @@ typedef struct {
     float ciwp[LW_NGPT][MAX_LAY], clwp[LW_NGPT][MAX_LAY], cswp[LW_NGPT][MAX_LAY];
     float taucmc[LW_NGPT][MAX_LAY];
     ora_cloud cloud;
-    float cdf_work[LW_NGPT * MAX_LAY];
+    ora_binary32 cdf_work[LW_NGPT * MAX_LAY];
     /* radiative transfer */
     float urad[MAX_LAY + 1][LW_NGPT], drad[MAX_LAY + 1][LW_NGPT];
     float clrurad[MAX_LAY + 1][LW_NGPT], clrdrad[MAX_LAY + 1][LW_NGPT];
@@ -138,6 +139,7 @@ static void lw_prepare(const ora_cache *C, const ora_in *in, int col, lw_col *S)
     const int nk = in->nk;
     const int nlay = ora_lw_nlayers(in->p_top, nk);
     S->nlay = nlay;
+    S->fp64_from = in->fp64_steps ? (nk > 5 ? nk - 5 : 0) : MAX_LAY + 1;
     const float *p3d = in->p3d + (size_t)col * nk;
     const float *t3d = in->t3d + (size_t)col * nk;
     const float *p8w = in->p8w + (size_t)col * (nk + 1);
@@ -1269,6 +1271,13 @@ static void lw_rtrnmc(const ora_lw_cache *L, lw_col *S)
         float dp = S->plev[l] - S->plev[l + 1];
         S->htr[l] = heatfac * (fnet0 - fnet1) / dp;
         S->htrc[l] = heatfac * (fnetc0 - fnetc1) / dp;
+        if (l >= S->fp64_from) {
+            /* FP64 mode: net fluxes, their difference and dF/dp in binary64 */
+            S->htr[l] = ora_heating64(heatfac, S->totuflux[l], S->totdflux[l], S->totuflux[l + 1],
+                                      S->totdflux[l + 1], S->plev[l], S->plev[l + 1]);
+            S->htrc[l] = ora_heating64(heatfac, S->totuclfl[l], S->totdclfl[l], S->totuclfl[l + 1],
+                                       S->totdclfl[l + 1], S->plev[l], S->plev[l + 1]);
+        }
     }
 }
 

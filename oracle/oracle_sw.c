@@ -76,6 +76,8 @@ int ora_sw_cache_init(const ora_tables *t, ora_sw_cache *c)
 /* ------------------------------------------------------------------------ */
 typedef struct {
     int nlay, laytrop;
+    int fp64_from;     /* first layer whose heating is formed in binary64 (FP64 mode) */
+    int fp64_reftra;   /* FP64 mode: reftra in binary64 when zwo >= 0.999 */
     float play[MAX_LAY], plev[MAX_LAY + 1], tlay[MAX_LAY], tlev[MAX_LAY + 1];
     float h2o[MAX_LAY], o3[MAX_LAY];
     float coldry[MAX_LAY], wkl[7][MAX_LAY], pdp[MAX_LAY], adjflux;
@@ -89,7 +91,7 @@ typedef struct {
     float ciwp[SW_NGPT][MAX_LAY], clwp[SW_NGPT][MAX_LAY], cswp[SW_NGPT][MAX_LAY];
     float taucmc[SW_NGPT][MAX_LAY], ssacmc[SW_NGPT][MAX_LAY], asmcmc[SW_NGPT][MAX_LAY], taormc[SW_NGPT][MAX_LAY];
     ora_cloud cloud;
-    float cdf_work[SW_NGPT * MAX_LAY];
+    ora_binary32 cdf_work[SW_NGPT * MAX_LAY];
     /* spectral flux sums, bottom-up levels */
     float bbfu[MAX_LAY + 1], bbfd[MAX_LAY + 1], bbcu[MAX_LAY + 1], bbcd[MAX_LAY + 1];
     float bbfddir[MAX_LAY + 1], bbcddir[MAX_LAY + 1];
@@ -101,6 +103,8 @@ static void sw_prepare(const ora_cache *C, const ora_in *in, int col, sw_col *S)
 {
     const int nk = in->nk, nlay = nk + 1;
     S->nlay = nlay;
+    S->fp64_from = in->fp64_steps ? (in->nk > 5 ? in->nk - 5 : 0) : MAX_LAY + 1;
+    S->fp64_reftra = in->fp64_steps;
     const float *p3d = in->p3d + (size_t)col * nk;
     const float *t3d = in->t3d + (size_t)col * nk;
     const float *p8w = in->p8w + (size_t)col * (nk + 1);
@@ -644,7 +648,87 @@ static inline float exp_lookup(const ora_sw_cache *W, float v)
 
 typedef struct { float ref, refd, tra, trad; } rt4;
 
-static rt4 reftra(const ora_sw_cache *W, int lrt, float zg, float mu, float zto1, float zw)
+/* FP64 mode (test of the GPU's binary64 variant): the Pade lookup of
+ * exp(-v) with binary64 arithmetic; the table is the same binary32 data. */
+static double exp_lookup64(const ora_sw_cache *W, double v)
+{
+    if (v <= 0.06) return (1.0 - v) + (0.5 * v) * v;
+    double tblind = v / ((double)W->bpade + v);
+    int it = clampi((int)((double)W->ntbl * tblind + 0.5), 0, W->ntbl);
+    return (double)W->pade_exp[it];
+}
+
+/* FP64 mode's reftra (sw:3490-3601) for a layer whose delta-scaled
+ * single-scattering albedo zwo is >= 0.999 or whose optical depth is below
+ * 0.1: every operation of both branches in binary64 on the binary32 inputs,
+ * the four results rounded once. */
+static rt4 reftra64(const ora_sw_cache *W, float zg_in, float mu_in, float zto1_in, float zw_in)
+{
+    const double zg = (double)zg_in, mu = (double)mu_in, zto1 = (double)zto1_in, zw = (double)zw_in;
+    const double eps = 1.0e-8, zwcrit = 0.9999995;
+    double ref, refd, tra, trad;
+    double zg3 = 3.0 * zg;
+    double g1 = (8.0 - zw * (5.0 + zg3)) * 0.25;
+    double g2 = 3.0 * (zw * (1.0 - zg)) * 0.25;
+    double g3 = (2.0 - zg3 * mu) * 0.25;
+    double g4 = 1.0 - g3;
+    double sr = zg != 1.0 ? zg / (1.0 - zg) : 0.0;
+    double denom = zg != 1.0 ? 1.0 - (1.0 - zw) * sr * sr : 1.0;
+    double zwo = (zw > 0.0 && denom != 0.0) ? zw / denom : 0.0;
+    double ze2 = zto1 / mu;
+    if (ze2 > 500.0) ze2 = 500.0;
+    double zem2 = exp_lookup64(W, ze2);
+    if (zwo >= zwcrit) {
+        double za = g1 * mu;
+        double za1 = za - g3;
+        double zgt = g1 * zto1;
+        ref = (zgt - za1 * (1.0 - zem2)) / (1.0 + zgt);
+        tra = 1.0 - ref;
+        refd = zgt / (1.0 + zgt);
+        trad = 1.0 - refd;
+        if (zem2 == 1.0) { ref = 0.0; tra = 1.0; refd = 0.0; trad = 1.0; }
+    } else {
+        double za1 = g1 * g4 + g2 * g3;
+        double za2 = g1 * g3 + g2 * g4;
+        double rad = g1 * g1 - g2 * g2;
+        double zrk = sqrt(rad > 0.0 ? rad : 0.0);
+        double zrp = zrk * mu;
+        double zrp1 = 1.0 + zrp, zrm1 = 1.0 - zrp, zrk2 = 2.0 * zrk;
+        double zrpp = 1.0 - zrp * zrp;
+        double zrkg = zrk + g1;
+        double zr1 = zrm1 * (za2 + zrk * g3);
+        double zr2 = zrp1 * (za2 - zrk * g3);
+        double zr3 = zrk2 * (g3 - za2 * mu);
+        double zr4 = zrpp * zrkg;
+        double zr5 = zrpp * (zrk - g1);
+        double zt1 = zrp1 * (za1 + zrk * g4);
+        double zt2 = zrm1 * (za1 - zrk * g4);
+        double zt3 = zrk2 * (g4 + za1 * mu);
+        double zbeta = (g1 - zrk) / zrkg;
+        double ze1 = zrk * zto1;
+        if (ze1 > 500.0) ze1 = 500.0;
+        double zem1 = exp_lookup64(W, ze1);
+        double zep1 = 1.0 / zem1;
+        double zep2 = 1.0 / zem2;
+        double zdenr = zr4 * zep1 + zr5 * zem1;
+        double zdent = zr4 * zep1 + zr5 * zem1;
+        if (zdenr >= -eps && zdenr <= eps) {
+            ref = eps;
+            tra = zem2;
+        } else {
+            ref = zw * (zr1 * zep1 - zr2 * zem1 - zr3 * zem2) / zdenr;
+            tra = zem2 - zem2 * zw * (zt1 * zep1 - zt2 * zem1 - zt3 * zep2) / zdent;
+        }
+        double zemm = zem1 * zem1;
+        double zdend = 1.0 / ((1.0 - zbeta * zemm) * zrkg);
+        refd = g2 * (1.0 - zemm) * zdend;
+        trad = zrk2 * zem1 * zdend;
+    }
+    rt4 r = {(float)ref, (float)refd, (float)tra, (float)trad};
+    return r;
+}
+
+static rt4 reftra(const ora_sw_cache *W, int fp64, int lrt, float zg, float mu, float zto1, float zw)
 {
     rt4 r = {0.0f, 0.0f, 1.0f, 1.0f};
     if (!lrt) return r;
@@ -657,6 +741,7 @@ static rt4 reftra(const ora_sw_cache *W, int lrt, float zg, float mu, float zto1
     float sr = zg != 1.0f ? zg / (1.0f - zg) : 0.0f;
     float denom = zg != 1.0f ? 1.0f - (1.0f - zw) * sr * sr : 1.0f;
     float zwo = (zw > 0.0f && denom != 0.0f) ? zw / denom : 0.0f;
+    if (fp64 && (zwo >= 0.999f || zto1 < 0.1f)) return reftra64(W, zg, mu, zto1, zw);
     if (zwo >= zwcrit) {
         float za = g1 * mu;
         float za1 = za - g3;
@@ -742,18 +827,34 @@ static void vrtqdr(int n, const float *pref, const float *prefd, const float *pt
     }
 }
 
+/* Direct (albp) and diffuse (albd) surface albedo of a band (0-based): the
+ * Noah-MP fields for columns with xland < 1.5 when all four are given
+ * (sw:2519-2530), visible in bands 25-28 and near infrared in bands 16-24 and
+ * 29 (sw:2120-2127); `albedo` otherwise. */
+static void sw_band_albedo(const ora_in *in, int col, int band, float *albp, float *albd)
+{
+    *albp = in->albedo[col];
+    *albd = in->albedo[col];
+    if (in->alswvisdir && in->alswvisdif && in->alswnirdir && in->alswnirdif && in->xland[col] < 1.5f) {
+        const int vis = band >= 9 && band <= 12;
+        *albp = vis ? in->alswvisdir[col] : in->alswnirdir[col];
+        *albd = vis ? in->alswvisdif[col] : in->alswnirdif[col];
+    }
+}
+
 static void sw_spcvmc(const ora_sw_cache *W, const ora_in *in, int col, sw_col *S, int clear_only)
 {
     const int n = S->nlay;
     const float mu = fmaxf(in->coszr[col], 1.0e-10f);
     const float repclc = 1.0e-12f;
-    const float albp = in->albedo[col], albd = in->albedo[col];
     /* accumulators, top-down levels */
     float sfu[MAX_LAY + 1], sfd[MAX_LAY + 1], scu[MAX_LAY + 1], scd[MAX_LAY + 1], sfdir[MAX_LAY + 1], scdir[MAX_LAY + 1];
     for (int k = 0; k <= n; ++k) { sfu[k] = 0; sfd[k] = 0; scu[k] = 0; scd[k] = 0; sfdir[k] = 0; scdir[k] = 0; }
     for (int g = 0; g < SW_NGPT; ++g) {
         int band = 0;
         while (g >= W->band[band].gofs + W->band[band].ngc) ++band;
+        float albp, albd;
+        sw_band_albedo(in, col, band, &albp, &albd);
         float zrefc[MAX_LAY + 1], zrefdc[MAX_LAY + 1], ztrac[MAX_LAY + 1], ztradc[MAX_LAY + 1];
         float zref[MAX_LAY + 1], zrefd[MAX_LAY + 1], ztra[MAX_LAY + 1], ztrad[MAX_LAY + 1];
         float zdbtc[MAX_LAY + 1], zdbt[MAX_LAY + 1], ztdbtc[MAX_LAY + 1], ztdbt[MAX_LAY + 1];
@@ -781,7 +882,7 @@ static void sw_spcvmc(const ora_sw_cache *W, const ora_in *in, int col, sw_col *
             float ztauc = (1.0f - zwf) * ztau;
             float zomcc = (zom - zwf) / (1.0f - zwf);
             float zgcc = (zgr - zf) / (1.0f - zf);
-            rt4 c = reftra(W, 1, zgcc, mu, ztauc, zomcc);
+            rt4 c = reftra(W, S->fp64_reftra, 1, zgcc, mu, ztauc, zomcc);
             zrefc[r] = c.ref; zrefdc[r] = c.refd; ztrac[r] = c.tra; ztradc[r] = c.trad;
             float dbtc = exp_lookup(W, ztauc / mu);
             zdbtc[r] = dbtc;
@@ -792,7 +893,7 @@ static void sw_spcvmc(const ora_sw_cache *W, const ora_in *in, int col, sw_col *
                 float zomco = ztauc * zomcc + tc * wc;
                 float zgco = (tc * wc * gc + ztauc * zomcc * zgcc) / zomco;
                 zomco = zomco / ztauo;
-                rt4 o = reftra(W, cloud > repclc, zgco, mu, ztauo, zomco);
+                rt4 o = reftra(W, S->fp64_reftra, cloud > repclc, zgco, mu, ztauo, zomco);
                 zref[r] = clear * c.ref + cloud * o.ref;
                 zrefd[r] = clear * c.refd + cloud * o.refd;
                 ztra[r] = clear * c.tra + cloud * o.tra;
@@ -837,6 +938,13 @@ static void sw_spcvmc(const ora_sw_cache *W, const ora_in *in, int col, sw_col *
         float c1 = S->bbcd[l + 1] - S->bbcu[l + 1], c0 = S->bbcd[l] - S->bbcu[l];
         S->swhr[l] = (n1 - n0) * zdpgcp;
         S->swhrc[l] = (c1 - c0) * zdpgcp;
+        if (l >= S->fp64_from) {
+            /* FP64 mode: net fluxes, their difference and dF/dp in binary64 */
+            S->swhr[l] = ora_heating64(heatfac, S->bbfu[l], S->bbfd[l], S->bbfu[l + 1], S->bbfd[l + 1],
+                                       S->plev[l], S->plev[l + 1]);
+            S->swhrc[l] = ora_heating64(heatfac, S->bbcu[l], S->bbcd[l], S->bbcu[l + 1], S->bbcd[l + 1],
+                                        S->plev[l], S->plev[l + 1]);
+        }
     }
     S->swhr[n - 1] = 0.0f;
     S->swhrc[n - 1] = 0.0f;

@@ -91,4 +91,7 @@ def case_kwargs(case: dict, side: str) -> dict:
         kw.update(albedo=inp["albedo"], coszr=inp["coszr"], solcon=float(inp["solcon"]),
                   co2vmr=float(inp["co2vmr"]), n2ovmr=float(inp["n2ovmr"]),
                   ch4vmr=float(inp["ch4vmr"]))
+        if "alswvisdir" in inp:  # Noah-MP albedos (sf_surface_physics = 8)
+            kw.update(sf_surface_physics=8, **{k: inp[k] for k in ("alswvisdir", "alswvisdif", "alswnirdir",
+                                                                    "alswnirdif")})
     return kw

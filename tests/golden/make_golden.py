@@ -49,7 +49,12 @@ CASES = (
     ("overcast_2x2x40", dict(nx=2, ny=2, nk=40, seed=8, cloud_p=1.0, night_fraction=0.0), {}),
     ("icloud0_2x2x44", dict(nx=2, ny=2, nk=44, seed=3, night_fraction=0.0), dict(icloud=0)),
     ("odd_1x3x17", dict(nx=1, ny=3, nk=17, seed=7, night_fraction=0.0), {}),
+    # Noah-MP albedos (sf_surface_physics = 8): half the columns with xland = 2
+    # (they keep `albedo`), the others take the four visible / near-infrared
+    # fields (module_ra_rrtmg_sw.py:2519-2530)
+    ("sf8_3x4x44", dict(nx=3, ny=4, nk=44, seed=9, night_fraction=0.0, fractional_clouds=True), dict(sf8=True)),
 )
+SF8_FIELDS = ("alswvisdir", "alswvisdif", "alswnirdir", "alswnirdif")
 
 
 def load_package():
@@ -77,9 +82,19 @@ def main(reference_root: str) -> None:
     out = {}
     for name, gen, over in CASES:
         st = synthetic.make_columns(**gen)
+        over = dict(over)
+        sf8 = over.pop("sf8", False)
+        if sf8:
+            rng = np.random.default_rng(99)
+            nx, ny = gen["nx"], gen["ny"]
+            st.fields["xland"] = np.where(rng.uniform(size=(nx, ny)) < 0.5, 1.0, 2.0).astype(np.float32)
+            for k in SF8_FIELDS:
+                st.fields[k] = rng.uniform(0.03, 0.5, size=(nx, ny)).astype(np.float32)
         lkw, skw = st.lw_kwargs(), st.sw_kwargs()
         lkw.update(over)
         skw.update(over)
+        if sf8:
+            skw.update(sf_surface_physics=8, **{k: st.fields[k] for k in SF8_FIELDS})
         for k, v in st.fields.items():
             out[f"{name}/in/{k}"] = v
         for k in ("p_top", "solcon", "co2vmr", "n2ovmr", "ch4vmr", "cfc11vmr", "cfc12vmr",

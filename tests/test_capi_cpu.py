@@ -30,7 +30,8 @@ def test_library_exports_every_declared_symbol(pkg):
     for header, exports in (("rrtmg_b200.h", _capi.EXPORTS), ("rrtmg_surrogate.h", _capi.SURROGATE_EXPORTS),
                             ("rrtmg_prologue.h", _capi.PROLOGUE_EXPORTS),
                             ("rrtmg_tendency.h", _capi.TENDENCY_EXPORTS),
-                            ("rrtmg_tables.h", _capi.TABLES_EXPORTS)):
+                            ("rrtmg_tables.h", _capi.TABLES_EXPORTS),
+                            ("rrtmg_xla_ffi.h", _capi.FFI_EXPORTS)):
         for name in _declared_symbols(header):
             assert hasattr(lib, name), name
         assert set(exports) == set(_declared_symbols(header))

@@ -13,7 +13,7 @@ from conftest import case_kwargs
 pytestmark = pytest.mark.gpu
 
 CASES = ("c0_4x4x44", "c1_3x5x50", "req_3x3x44", "fraccloud_ptop10_3x3x30", "allnight_2x3x44",
-         "clearsky_allday_3x2x44", "overcast_2x2x40", "icloud0_2x2x44", "odd_1x3x17")
+         "clearsky_allday_3x2x44", "overcast_2x2x40", "icloud0_2x2x44", "odd_1x3x17", "sf8_3x4x44")
 
 
 @pytest.fixture(scope="module")

@@ -18,7 +18,7 @@ class Config(ctypes.Structure):
                 ("co2vmr", ctypes.c_float), ("n2ovmr", ctypes.c_float), ("ch4vmr", ctypes.c_float),
                 ("cfc11vmr", ctypes.c_float), ("cfc12vmr", ctypes.c_float), ("solcon", ctypes.c_float),
                 ("has_reqc", ctypes.c_int), ("has_reqi", ctypes.c_int), ("has_reqs", ctypes.c_int),
-                ("icloud", ctypes.c_int), ("cldovrlp", ctypes.c_int)]
+                ("icloud", ctypes.c_int), ("cldovrlp", ctypes.c_int), ("fp64_steps", ctypes.c_int)]
 
 
 LW_IN_FIELDS = ("p3d", "p8w", "pi3d", "t3d", "t8w", "tsk", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d",
@@ -42,8 +42,12 @@ class LwOut(ctypes.Structure):
     _fields_ = [(n, _F) for n in LW_OUT_FIELDS]
 
 
+# optional Noah-MP albedos (sf_surface_physics == 8); NULL when not given
+SW_ALBEDO_FIELDS = ("alswvisdir", "alswvisdif", "alswnirdir", "alswnirdif")
+
+
 class SwIn(ctypes.Structure):
-    _fields_ = [(n, _F) for n in SW_IN_FIELDS]
+    _fields_ = [(n, _F) for n in SW_IN_FIELDS + SW_ALBEDO_FIELDS]
 
 
 class SwOut(ctypes.Structure):
@@ -143,7 +147,10 @@ STATUS = {0: "RRTMG_OK", 1: "RRTMG_BAD_ARG", 2: "RRTMG_UNSUPPORTED_OPTION", 3: "
 EXPORTS = ("rrtmg_create", "rrtmg_create_from_memory", "rrtmg_destroy", "rrtmg_lwrad", "rrtmg_swrad",
            "rrtmg_lwrad_static_scratch", "rrtmg_lwrad_live", "rrtmg_swrad_live", "rrtmg_timing_enable",
            "rrtmg_timing_read", "rrtmg_set_schedule", "rrtmg_get_schedule", "rrtmg_lw_nlayers",
-           "rrtmg_last_error", "rrtmg_status_string")
+           "rrtmg_last_error", "rrtmg_status_string", "rrtmg_column_status_enable", "rrtmg_last_column_errors",
+           "rrtmg_lw_workspace_bytes", "rrtmg_sw_workspace_bytes", "rrtmg_lwrad_ws", "rrtmg_swrad_ws")
+FFI_EXPORTS = ("rrtmg_ffi_lwrad", "rrtmg_ffi_swrad", "rrtmg_ffi_set_table_blob", "rrtmg_ffi_lw_workspace_bytes",
+               "rrtmg_ffi_sw_workspace_bytes")
 SURROGATE_EXPORTS = ("rrtmg_gemm_bf16", "rrtmg_gemm_error", "rrtmg_gemm_set_tile", "rrtmg_gemm_set_wait_ns",
                      "rrtmg_gemm_test_withhold_commit", "rrtmg_sur_features", "rrtmg_sur_targets",
                      "rrtmg_sur_column_stats", "rrtmg_sur_normalize", "rrtmg_sur_gather", "rrtmg_sur_loss_grad",
@@ -236,6 +243,8 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "rrtmg_blob_with_wrf_data": [ctypes.c_char_p] * 4,
         "rrtmg_create_with_wrf_data": [ctypes.c_char_p] * 3 + [I, ctypes.POINTER(ctypes.c_void_p)],
         "rrtmg_get_schedule": [V, ctypes.POINTER(Schedule)],
+        "rrtmg_column_status_enable": [V, I],
+        "rrtmg_last_column_errors": [V, I, P, I, V],
     }
     for name, argtypes in sigs.items():
         fn = getattr(lib, name)

@@ -20,8 +20,9 @@ BUILD = HERE / "_build"
 LIB = HERE / "librrtmg_b200.so"
 SOURCES = ("rrtmg_capi.cu", "rrtmg_mcica.cu", "rrtmg_lw.cu", "rrtmg_sw.cu", "surrogate_gemm.cu",
            "surrogate_ops.cu", "surrogate_capi.cu", "surrogate_mlp.cu", "rrtmg_prologue.cu",
-           "rrtmg_tendency.cu", "rrtmg_tables.cu")
-HEADERS = ("rrtmg_device.cuh", "rrtmg_kernels.h", "surrogate_kernels.h", "umma_common.cuh", "kiss_jump_host.h")
+           "rrtmg_tendency.cu", "rrtmg_tables.cu", "rrtmg_status.cu", "rrtmg_ffi.cu")
+HEADERS = ("rrtmg_device.cuh", "rrtmg_kernels.h", "surrogate_kernels.h", "umma_common.cuh", "kiss_jump_host.h",
+           "xla_ffi_abi.h")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
@@ -49,7 +50,8 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
                                              HERE.parent / "include" / "rrtmg_surrogate.h",
                                              HERE.parent / "include" / "rrtmg_prologue.h",
                                              HERE.parent / "include" / "rrtmg_tendency.h",
-                                             HERE.parent / "include" / "rrtmg_tables.h"]
+                                             HERE.parent / "include" / "rrtmg_tables.h",
+                                             HERE.parent / "include" / "rrtmg_xla_ffi.h"]
     objs = []
     jobs = []
     for src in SOURCES:

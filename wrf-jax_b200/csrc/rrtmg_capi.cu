@@ -55,6 +55,14 @@ struct rrtmg_ctx {
   std::vector<int> marks[2];
   int timing_next[2] = {0, 0};
   int timing_count[2] = {0, 0};
+  // per-column status (rrtmg_last_column_errors): one array per side, grown
+  // as needed; retired arrays stay allocated until destroy because queued
+  // status launches may still write them
+  bool colstatus = false;
+  uint32_t *status_buf[2] = {nullptr, nullptr};
+  size_t status_cap[2] = {0, 0};
+  int status_ncol[2] = {-1, -1};
+  std::vector<uint32_t *> retired_status;
   // radiation prologue: SVML sin/cos constants from the blob, and the CAM
   // ozone climatology (plev, lat, then the (12, latsiz, levsiz) table in one
   // allocation); replaced climatologies stay allocated until destroy because
@@ -455,6 +463,7 @@ rrtmg_status check_config(rrtmg_ctx *ctx, const rrtmg_config *cfg) {
   if (cfg->nk < 4) return fail(ctx, RRTMG_BAD_ARG, "nk must be at least 4 (McICA seeds read four layers)");
   if (static_cast<long long>(cfg->nx) * cfg->ny > (1ll << 30))
     return fail(ctx, RRTMG_BAD_ARG, "too many columns in one call");
+  if (cfg->fp64_steps != 0 && cfg->fp64_steps != 1) return fail(ctx, RRTMG_BAD_ARG, "fp64_steps must be 0 or 1");
   return RRTMG_OK;
 }
 
@@ -508,6 +517,8 @@ void rrtmg_destroy(rrtmg_ctx *ctx) {
   for (auto &kv : ctx->jumps) cudaFree(kv.second);
   cudaFree(ctx->ozone);
   for (float *p : ctx->retired_ozone) cudaFree(p);
+  for (uint32_t *p : ctx->status_buf) cudaFree(p);
+  for (uint32_t *p : ctx->retired_status) cudaFree(p);
   cudaFree(ctx->dev_blob);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   for (auto &side : ctx->events)
@@ -532,9 +543,94 @@ const char *rrtmg_status_string(rrtmg_status s) {
   return "unknown status";
 }
 
-// live: null, or a device count; columns at or past it are skipped.
+// When column status is enabled: the status array of `side` for ncol
+// columns (grown with cudaMalloc when needed), else null.
+static uint32_t *status_target(rrtmg_ctx *ctx, int side, int ncol, cudaError_t *err) {
+  *err = cudaSuccess;
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  if (!ctx->colstatus) return nullptr;
+  if (ctx->status_cap[side] < static_cast<size_t>(ncol)) {
+    uint32_t *fresh = nullptr;
+    *err = cudaMalloc(&fresh, sizeof(uint32_t) * static_cast<size_t>(ncol));
+    if (*err != cudaSuccess) return nullptr;
+    if (ctx->status_buf[side]) ctx->retired_status.push_back(ctx->status_buf[side]);
+    ctx->status_buf[side] = fresh;
+    ctx->status_cap[side] = static_cast<size_t>(ncol);
+  }
+  ctx->status_ncol[side] = ncol;
+  return ctx->status_buf[side];
+}
+
+// Per-call scratch: carved in order from a caller's workspace (each piece on
+// a 256-byte boundary), or taken from the context's stream-ordered pool and
+// returned to it by release().
+extern "C++" {
+struct CallScratch {
+  rrtmg_ctx *ctx;
+  cudaStream_t stream;
+  unsigned char *ws;
+  size_t ws_bytes, used = 0;
+  std::vector<void *> pooled;
+  CallScratch(rrtmg_ctx *c, cudaStream_t s, void *w, size_t wb)
+      : ctx(c), stream(s), ws(static_cast<unsigned char *>(w)), ws_bytes(wb) {}
+  static size_t aligned(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+  template <typename T>
+  cudaError_t take(T **p, size_t bytes) {
+    if (ws) {
+      if (aligned(used) + bytes > ws_bytes) return cudaErrorMemoryAllocation;
+      *p = reinterpret_cast<T *>(ws + aligned(used));
+      used = aligned(used) + bytes;
+      return cudaSuccess;
+    }
+    void *q = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&q, bytes, ctx->pool, stream);
+    if (e == cudaSuccess) {
+      pooled.push_back(q);
+      *p = static_cast<T *>(q);
+    }
+    return e;
+  }
+  cudaError_t release() {
+    cudaError_t first = cudaSuccess;
+    for (auto it = pooled.rbegin(); it != pooled.rend(); ++it) {
+      cudaError_t e = cudaFreeAsync(*it, stream);
+      if (first == cudaSuccess) first = e;
+    }
+    pooled.clear();
+    return first;
+  }
+};
+}  // extern "C++"
+
+// Scratch pieces of one call, in the order the calls take them.
+static size_t lw_chunk_columns(rrtmg_ctx *ctx, int ncol) {
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  return static_cast<size_t>(ncol < ctx->lw_chunk ? ncol : ctx->lw_chunk);
+}
+static size_t sw_chunk_columns(rrtmg_ctx *ctx, int ncol) {
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  return static_cast<size_t>(ncol < ctx->sw_chunk ? ncol : ctx->sw_chunk);
+}
+static size_t lw_workspace_bytes(rrtmg_ctx *ctx, const rrtmg_config *cfg) {
+  const int nlay = rrtmg_lw_nlayers(cfg->p_top, cfg->nk);
+  const size_t ncol = static_cast<size_t>(cfg->nx) * cfg->ny;
+  const size_t chunk = lw_chunk_columns(ctx, static_cast<int>(ncol));
+  return CallScratch::aligned(static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t)) +
+         CallScratch::aligned(lw_scratch_floats(nlay, static_cast<int>(chunk)) * sizeof(float));
+}
+static size_t sw_workspace_bytes(rrtmg_ctx *ctx, const rrtmg_config *cfg) {
+  const int nlay = cfg->nk + 1;
+  const size_t ncol = static_cast<size_t>(cfg->nx) * cfg->ny;
+  const size_t chunk = sw_chunk_columns(ctx, static_cast<int>(ncol));
+  return CallScratch::aligned(static_cast<size_t>(nlay) * kSwMaskWords * ncol * sizeof(uint32_t)) +
+         CallScratch::aligned((ncol + 1) * sizeof(int)) +
+         CallScratch::aligned(sw_record_floats(cfg->nk, static_cast<int>(chunk)) * sizeof(float));
+}
+
+// live: null, or a device count; columns at or past it are skipped.  ws: null
+// (scratch from the context's pool), or a caller's workspace of ws_bytes.
 static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
-                               void *stream_ptr, const int *live) {
+                               void *stream_ptr, const int *live, void *ws = nullptr, size_t ws_bytes = 0) {
   rrtmg_status st = check_config(ctx, cfg);
   if (st != RRTMG_OK) return st;
   if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
@@ -565,19 +661,16 @@ static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   uint32_t *mask = nullptr;
   float *scratch = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kLwMaskWords * ncol * sizeof(uint32_t);
-  int lw_chunk_setting;
-  {
-    std::lock_guard<std::mutex> lk(ctx->mutex);
-    lw_chunk_setting = ctx->lw_chunk;
-  }
-  const int chunk = ncol < lw_chunk_setting ? ncol : lw_chunk_setting;
-  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
-  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&scratch), lw_scratch_floats(nlay, chunk) * sizeof(float),
-                              ctx->pool, stream);
+  const int chunk = static_cast<int>(lw_chunk_columns(ctx, ncol));
+  if (ws && ws_bytes < lw_workspace_bytes(ctx, cfg))
+    return fail(ctx, RRTMG_BAD_ARG, "workspace smaller than rrtmg_lw_workspace_bytes");
+  CallScratch sc(ctx, stream, ws, ws_bytes);
+  e = sc.take(&mask, mask_bytes);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch (mcica mask)");
+  e = sc.take(&scratch, lw_scratch_floats(nlay, chunk) * sizeof(float));
   if (e != cudaSuccess) {
-    cudaFreeAsync(mask, stream);
-    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(lw layer records)");
+    sc.release();
+    return cuda_fail(ctx, e, "scratch (lw layer records)");
   }
 
   const int tslot = timing_slot(ctx, 0);
@@ -590,12 +683,12 @@ static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   e = launch_mcica(m, stream);
   timing_mark(ctx, 0, tslot, stream);
   if (e != cudaSuccess) {
-    cudaFreeAsync(scratch, stream);
-    cudaFreeAsync(mask, stream);
+    sc.release();
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
   LwArgs a{};
   a.live = live;
+  a.fp64_from = cfg->fp64_steps ? fp64_first_layer(cfg->nk) : kMaxLay + 1;
   a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
   a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.cfc11 = cfg->cfc11vmr; a.cfc12 = cfg->cfc12vmr;
   a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
@@ -621,16 +714,32 @@ static rrtmg_status lwrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
     if (e == cudaSuccess) e = launch_lw_chunk_sweep(ctx->tables, a, stream);
     timing_mark(ctx, 0, tslot, stream);
   }
-  cudaError_t ef = cudaFreeAsync(scratch, stream);
-  cudaError_t ef2 = cudaFreeAsync(mask, stream);
+  if (e == cudaSuccess && !live) {
+    cudaError_t es = cudaSuccess;
+    uint32_t *status = status_target(ctx, 0, ncol, &es);
+    if (es != cudaSuccess) e = es;
+    if (status) {
+      StatusArgs sa{};
+      sa.ncol = ncol; sa.nx = cfg->nx; sa.ny = cfg->ny; sa.nk = cfg->nk; sa.side = 0;
+      sa.has_req = cfg->has_reqc || cfg->has_reqi || cfg->has_reqs;
+      sa.in = a.in;
+      sa.rthraten = out->rthratenlw; sa.rthratenc = out->rthratenlwc;
+      const float *o2[8] = {out->lwupt, out->lwuptc, out->lwdnt, out->lwdntc, out->lwupb, out->lwupbc,
+                            out->lwdnb, out->lwdnbc};
+      for (int q = 0; q < 8; ++q) sa.out2d[q] = o2[q];
+      sa.n2d = 8;
+      sa.status = status;
+      e = launch_column_status(sa, stream);
+    }
+  }
+  cudaError_t ef = sc.release();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "lw kernel launch");
-  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(lw layer records)");
-  if (ef2 != cudaSuccess) return cuda_fail(ctx, ef2, "cudaFreeAsync(mcica mask)");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(lw scratch)");
   return RRTMG_OK;
 }
 
 static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
-                               void *stream_ptr, const int *live) {
+                               void *stream_ptr, const int *live, void *ws = nullptr, size_t ws_bytes = 0) {
   rrtmg_status st = check_config(ctx, cfg);
   if (st != RRTMG_OK) return st;
   if (!in || !out) return fail(ctx, RRTMG_BAD_ARG, "null input or output block");
@@ -661,13 +770,15 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   uint32_t *mask = nullptr;
   int *daylist = nullptr;
   const size_t mask_bytes = static_cast<size_t>(nlay) * kSwMaskWords * ncol * sizeof(uint32_t);
-  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&mask), mask_bytes, ctx->pool, stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(mcica mask)");
-  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&daylist), (static_cast<size_t>(ncol) + 1) * sizeof(int),
-                              ctx->pool, stream);
+  if (ws && ws_bytes < sw_workspace_bytes(ctx, cfg))
+    return fail(ctx, RRTMG_BAD_ARG, "workspace smaller than rrtmg_sw_workspace_bytes");
+  CallScratch sc(ctx, stream, ws, ws_bytes);
+  e = sc.take(&mask, mask_bytes);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch (mcica mask)");
+  e = sc.take(&daylist, (static_cast<size_t>(ncol) + 1) * sizeof(int));
   if (e != cudaSuccess) {
-    cudaFreeAsync(mask, stream);
-    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(day list)");
+    sc.release();
+    return cuda_fail(ctx, e, "scratch (day list)");
   }
   const int tslot = timing_slot(ctx, 1);
   timing_mark(ctx, 1, tslot, stream);
@@ -679,12 +790,13 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   e = launch_mcica(m, stream);
   timing_mark(ctx, 1, tslot, stream);
   if (e != cudaSuccess) {
-    cudaFreeAsync(daylist, stream);
-    cudaFreeAsync(mask, stream);
+    sc.release();
     return cuda_fail(ctx, e, "mcica kernel launch");
   }
   SwArgs a{};
   a.live = live;
+  a.fp64_from = cfg->fp64_steps ? fp64_first_layer(cfg->nk) : kMaxLay + 1;
+  a.fp64_reftra = cfg->fp64_steps != 0;
   a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
   a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.solcon = cfg->solcon;
   a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
@@ -694,6 +806,20 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
                        in->re_snow);
   a.in.albedo = in->albedo;
   a.in.coszr = in->coszr;
+  {
+    const int given = (in->alswvisdir != nullptr) + (in->alswvisdif != nullptr) + (in->alswnirdir != nullptr) +
+                      (in->alswnirdif != nullptr);
+    if (given != 0 && given != 4) {
+      sc.release();
+      return fail(ctx, RRTMG_BAD_ARG, "pass all four Noah-MP albedo fields or none");
+    }
+    if (given == 4) {
+      a.in.alswvisdir = in->alswvisdir;
+      a.in.alswvisdif = in->alswvisdif;
+      a.in.alswnirdir = in->alswnirdir;
+      a.in.alswnirdif = in->alswnirdif;
+    }
+  }
   a.mask = mask;
   a.rthraten = out->rthratensw; a.rthratenc = out->rthratenswc;
   a.upt = out->swupt; a.uptc = out->swuptc; a.dnt = out->swdnt; a.dntc = out->swdntc;
@@ -703,19 +829,12 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
   a.zero2[0] = out->swuptcln; a.zero2[1] = out->swdntcln; a.zero2[2] = out->swupbcln; a.zero2[3] = out->swdnbcln;
   a.nday = daylist + ncol;
   a.daylist = daylist;
-  int sw_chunk;
-  {
-    std::lock_guard<std::mutex> lk(ctx->mutex);
-    sw_chunk = ctx->sw_chunk;
-  }
-  a.chunk_capacity = ncol < sw_chunk ? ncol : sw_chunk;
+  a.chunk_capacity = static_cast<int>(sw_chunk_columns(ctx, ncol));
   float *records = nullptr;
-  e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&records),
-                              sw_record_floats(cfg->nk, a.chunk_capacity) * sizeof(float), ctx->pool, stream);
+  e = sc.take(&records, sw_record_floats(cfg->nk, a.chunk_capacity) * sizeof(float));
   if (e != cudaSuccess) {
-    cudaFreeAsync(daylist, stream);
-    cudaFreeAsync(mask, stream);
-    return cuda_fail(ctx, e, "cudaMallocFromPoolAsync(sw layer records)");
+    sc.release();
+    return cuda_fail(ctx, e, "scratch (sw layer records)");
   }
   a.records = records;
   // the day count is known only on the device: the chunks cover all ncol
@@ -730,15 +849,27 @@ static rrtmg_status swrad_impl(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rr
     if (e == cudaSuccess) e = launch_sw_chunk_sweep(ctx->tables, a, stream);
     timing_mark(ctx, 1, tslot, stream);
   }
-  {
-    cudaError_t es = cudaFreeAsync(records, stream);
-    if (e == cudaSuccess) e = es;
+  if (e == cudaSuccess && !live) {
+    cudaError_t es = cudaSuccess;
+    uint32_t *status = status_target(ctx, 1, ncol, &es);
+    if (es != cudaSuccess) e = es;
+    if (status) {
+      StatusArgs sa{};
+      sa.ncol = ncol; sa.nx = cfg->nx; sa.ny = cfg->ny; sa.nk = cfg->nk; sa.side = 1;
+      sa.has_req = cfg->has_reqc || cfg->has_reqi || cfg->has_reqs;
+      sa.in = a.in;
+      sa.rthraten = out->rthratensw; sa.rthratenc = out->rthratenswc;
+      const float *o2[8] = {out->swupt, out->swuptc, out->swdnt, out->swdntc, out->swupb, out->swupbc,
+                            out->swdnb, out->swdnbc};
+      for (int q = 0; q < 8; ++q) sa.out2d[q] = o2[q];
+      sa.n2d = 8;
+      sa.status = status;
+      e = launch_column_status(sa, stream);
+    }
   }
-  cudaError_t ef = cudaFreeAsync(daylist, stream);
-  cudaError_t ef2 = cudaFreeAsync(mask, stream);
+  cudaError_t ef = sc.release();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sw kernel launch");
-  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(day list)");
-  if (ef2 != cudaSuccess) return cuda_fail(ctx, ef2, "cudaFreeAsync(mcica mask)");
+  if (ef != cudaSuccess) return cuda_fail(ctx, ef, "cudaFreeAsync(sw scratch)");
   return RRTMG_OK;
 }
 
@@ -774,6 +905,42 @@ rrtmg_status rrtmg_swrad_live(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrt
                               const int *live_count, void *stream) {
   if (!device_count(live_count)) return fail(ctx, RRTMG_BAD_ARG, "live_count must be a device pointer");
   return swrad_impl(ctx, cfg, in, out, stream, live_count);
+}
+
+size_t rrtmg_lw_workspace_bytes(rrtmg_ctx *ctx, const rrtmg_config *cfg) {
+  if (check_config(ctx, cfg) != RRTMG_OK) return 0;
+  const int nlay = rrtmg_lw_nlayers(cfg->p_top, cfg->nk);
+  if (nlay > kMaxLay || nlay - cfg->nk > kMaxBuf || nlay < cfg->nk) return 0;
+  const KissJump *jumps = nullptr;  // built here, ahead of the first call
+  {
+    DeviceGuard guard(ctx->device);
+    if (guard.status() != cudaSuccess || get_jumps(ctx, nlay, kLwGpts, 150, &jumps) != RRTMG_OK) return 0;
+  }
+  return lw_workspace_bytes(ctx, cfg);
+}
+
+size_t rrtmg_sw_workspace_bytes(rrtmg_ctx *ctx, const rrtmg_config *cfg) {
+  if (check_config(ctx, cfg) != RRTMG_OK || cfg->nk + 1 > kMaxLay) return 0;
+  const KissJump *jumps = nullptr;
+  {
+    DeviceGuard guard(ctx->device);
+    if (guard.status() != cudaSuccess || get_jumps(ctx, cfg->nk + 1, kSwGpts, 1, &jumps) != RRTMG_OK) return 0;
+  }
+  return sw_workspace_bytes(ctx, cfg);
+}
+
+rrtmg_status rrtmg_lwrad_ws(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_lw_in *in, rrtmg_lw_out *out,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  if (!workspace) return fail(ctx, RRTMG_BAD_ARG, "null workspace");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(ctx, RRTMG_BAD_ARG, "workspace not 256-byte aligned");
+  return lwrad_impl(ctx, cfg, in, out, stream, nullptr, workspace, workspace_bytes);
+}
+
+rrtmg_status rrtmg_swrad_ws(rrtmg_ctx *ctx, const rrtmg_config *cfg, const rrtmg_sw_in *in, rrtmg_sw_out *out,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  if (!workspace) return fail(ctx, RRTMG_BAD_ARG, "null workspace");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(ctx, RRTMG_BAD_ARG, "workspace not 256-byte aligned");
+  return swrad_impl(ctx, cfg, in, out, stream, nullptr, workspace, workspace_bytes);
 }
 
 // rrtmg_lwrad_static_scratch: the LW call with its McICA scratch in fixed
@@ -885,6 +1052,7 @@ extern "C" rrtmg_status rrtmg_lwrad_static_scratch(rrtmg_ctx *ctx, const rrtmg_c
   e = launch_mcica(m, stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "mcica kernel launch");
   LwArgs a{};
+  a.fp64_from = cfg->fp64_steps ? fp64_first_layer(cfg->nk) : kMaxLay + 1;
   a.nx = cfg->nx; a.ny = cfg->ny; a.nk = cfg->nk; a.nlay = nlay; a.ncol = ncol;
   a.co2 = cfg->co2vmr; a.n2o = cfg->n2ovmr; a.ch4 = cfg->ch4vmr; a.cfc11 = cfg->cfc11vmr; a.cfc12 = cfg->cfc12vmr;
   a.has_reqc = cfg->has_reqc; a.has_reqi = cfg->has_reqi; a.has_reqs = cfg->has_reqs; a.icloud = cfg->icloud;
@@ -943,6 +1111,33 @@ extern "C" int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_ca
     for (int k = 0; k < 3; ++k) ms[q * 3 + k] = phase[k];
   }
   return count;
+}
+
+extern "C" rrtmg_status rrtmg_column_status_enable(rrtmg_ctx *ctx, int enable) {
+  if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
+  std::lock_guard<std::mutex> lk(ctx->mutex);
+  ctx->colstatus = enable != 0;
+  return RRTMG_OK;
+}
+
+extern "C" rrtmg_status rrtmg_last_column_errors(rrtmg_ctx *ctx, int side, uint32_t *dev_status, int ncol,
+                                                 void *stream_ptr) {
+  if (!ctx) return fail(nullptr, RRTMG_BAD_ARG, "null context");
+  if (side < 0 || side > 1 || !dev_status) return fail(ctx, RRTMG_BAD_ARG, "side must be 0 or 1, dev_status set");
+  const uint32_t *src = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mutex);
+    if (ctx->status_ncol[side] < 0 || !ctx->status_buf[side]) src = nullptr;
+    else if (ctx->status_ncol[side] == ncol) src = ctx->status_buf[side];
+  }
+  if (!src) return fail(ctx, RRTMG_BAD_ARG, "no column status recorded for this side and column count");
+  DeviceGuard guard(ctx->device);
+  cudaError_t e = guard.status();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  e = cudaMemcpyAsync(dev_status, src, sizeof(uint32_t) * static_cast<size_t>(ncol), cudaMemcpyDeviceToDevice,
+                      static_cast<cudaStream_t>(stream_ptr));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(column status)");
+  return RRTMG_OK;
 }
 
 extern "C" rrtmg_status rrtmg_set_schedule(rrtmg_ctx *ctx, const rrtmg_schedule *sch) {

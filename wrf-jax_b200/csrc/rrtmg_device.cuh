@@ -85,6 +85,22 @@ __device__ __forceinline__ float interpf(float lo, float hi, float f) { return l
 // (module_ra_rrtmg_common.py:70-82), identical to a binary32 division.
 __device__ __forceinline__ float pa_to_hpa(float p) { return p / 100.0f; }
 
+// First layer (bottom-up) whose heating rate the FP64 mode forms in binary64:
+// the fifth-highest model layer (nk - 5) and every layer above it.
+__host__ __device__ __forceinline__ int fp64_first_layer(int nk) { return nk > 5 ? nk - 5 : 0; }
+
+// FP64 mode's heating rate of a layer (LW lw:5702-5712, SW sw:2285-2301):
+// the net fluxes up - dn at the layer's bottom (0) and top (1), their
+// difference and the division by the pressure thickness are binary64
+// operations on the binary32 fluxes and level pressures, rounded once.
+__device__ __forceinline__ float heating64(float heatfac, float up0, float dn0, float up1, float dn1, float plev0,
+                                           float plev1) {
+  const double f0 = static_cast<double>(up0) - static_cast<double>(dn0);
+  const double f1 = static_cast<double>(up1) - static_cast<double>(dn1);
+  const double dp = static_cast<double>(plev0) - static_cast<double>(plev1);
+  return static_cast<float>(static_cast<double>(heatfac) * (f0 - f1) / dp);
+}
+
 // glibc 2.39 logf (e_logf.c, FMA build), including its special inputs.
 __device__ __forceinline__ float glibc_logf(const Tables &T, float x) {
   uint32_t ix = __float_as_uint(x);

@@ -27,6 +27,8 @@ struct ColumnInputs {
   const float *qv, *qc, *qi, *qs, *cldfra, *o3;
   const float *emiss, *albedo, *coszr, *xland, *xice, *snow;
   const float *re_cloud, *re_ice, *re_snow;
+  // SW only, optional (all four or none): Noah-MP albedos of xland < 1.5 columns
+  const float *alswvisdir, *alswvisdif, *alswnirdir, *alswnirdif;
 };
 
 struct LwArgs {
@@ -43,6 +45,7 @@ struct LwArgs {
   int chunk_capacity;   // columns per chunk of the sweep schedule
   int chunk_first, chunk_count;  // the chunk being launched
   const int *live;  // null, or a device count of leading columns to process
+  int fp64_from;    // FP64 mode: first layer with a binary64 heating rate; kMaxLay + 1 = off
 };
 
 // default columns per chunk of the LW sweep schedule (its scratch takes about
@@ -69,6 +72,8 @@ struct SwArgs {
   int chunk_capacity;  // day-list slots per chunk of the sweep schedule
   int chunk_first, chunk_count;  // the chunk being launched (set by launch_sw_columns)
   const int *live;     // null, or a device count of leading columns to process
+  int fp64_from;       // FP64 mode: first layer with a binary64 heating rate; kMaxLay + 1 = off
+  int fp64_reftra;     // FP64 mode: reftra in binary64 where zwo >= 0.999 or zto1 < 0.1
 };
 
 // default day-list slots per chunk of the SW sweep schedule (its records take
@@ -94,6 +99,18 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream);
 size_t sw_record_floats(int nk, int chunk);
 cudaError_t launch_sw_chunk_optics(const Tables &T, const SwArgs &a, cudaStream_t stream);
 cudaError_t launch_sw_chunk_sweep(const Tables &T, const SwArgs &a, cudaStream_t stream);
+
+// Per-column status of one LW (side 0) or SW (side 1) call: its inputs and
+// outputs (rrtmg_last_column_errors).
+struct StatusArgs {
+  int ncol, nx, ny, nk, side, has_req;
+  ColumnInputs in;
+  const float *rthraten, *rthratenc;
+  const float *out2d[8];
+  int n2d;
+  uint32_t *status;  // ncol words
+};
+cudaError_t launch_column_status(const StatusArgs &a, cudaStream_t stream);
 
 // Radiation prologue (cloud fraction, cos zenith, CAM ozone).  Constants of
 // the SVML sin/cos emulation in the reference's order (svml.sinf: 12,

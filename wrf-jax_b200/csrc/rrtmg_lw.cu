@@ -1212,8 +1212,12 @@ __global__ void __launch_bounds__(128) lw_kernel(Tables T, LwArgs a) {
       const float fnet0 = ufl_prev - dfl[l], fnet1 = ufl - dfl[l + 1];
       const float fnetc0 = uflc_prev - dflc[l], fnetc1 = uflc - dflc[l + 1];
       const float dp = L.plev0 - L.plev1;
-      const float htr = heatfac * (fnet0 - fnet1) / dp;
-      const float htrc = heatfac * (fnetc0 - fnetc1) / dp;
+      float htr = heatfac * (fnet0 - fnet1) / dp;
+      float htrc = heatfac * (fnetc0 - fnetc1) / dp;
+      if (l >= a.fp64_from) {
+        htr = heating64(heatfac, ufl_prev, dfl[l], ufl, dfl[l + 1], L.plev0, L.plev1);
+        htrc = heating64(heatfac, uflc_prev, dflc[l], uflc, dflc[l + 1], L.plev0, L.plev1);
+      }
       const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * C.ny);
       a.rthraten[rbase + static_cast<size_t>(l) * C.ny] = (htr / 86400.0f) / pi3d;
       a.rthratenc[rbase + static_cast<size_t>(l) * C.ny] = (htrc / 86400.0f) / pi3d;
@@ -1414,9 +1418,21 @@ __device__ __forceinline__ void gas_band(const Tables &T, const Layer &L, float4
   store_padded<ngc>(rec + (kLwRecFracs + pofs) / 4, fracs);
 }
 
-// thread = (layer, chunk column), grid.y = band
-__global__ void __launch_bounds__(128) lw_gas_kernel(Tables T, LwArgs a) {
-  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+// Blocks of (layer, chunk column) pairs taken kLwGasGroup at a time, each
+// group through all 16 bands before the next: the group's gas fields (44
+// words per pair, 11.5 MB) stay in L2 across its bands, and each band's code
+// runs on a full wave of blocks.
+constexpr int kLwGasGroup = 512;
+
+// thread = (layer, chunk column) of block `blk`; band from the block order above
+__global__ void __launch_bounds__(128) lw_gas_kernel(Tables T, LwArgs a, int nblk) {
+  const int group = blockIdx.x / (kLwGasGroup * kLwBands);
+  const int g0 = group * kLwGasGroup;
+  const int gsize = nblk - g0 < kLwGasGroup ? nblk - g0 : kLwGasGroup;
+  const int within = blockIdx.x - group * kLwGasGroup * kLwBands;
+  const int band = within / gsize;
+  const int blk = g0 + (within - band * gsize);
+  const long long idx = static_cast<long long>(blk) * blockDim.x + threadIdx.x;
   const int l = static_cast<int>(idx / a.chunk_count);
   const int lc = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
   if (l >= a.nlay || dead_column(a.live, a.chunk_first + lc)) return;
@@ -1431,7 +1447,7 @@ __global__ void __launch_bounds__(128) lw_gas_kernel(Tables T, LwArgs a) {
 #undef RRTMG_LW_GET
 #undef RRTMG_LW_GETI
   float4 *rec = reinterpret_cast<float4 *>(layer_records(a) + (static_cast<size_t>(lc) * a.nlay + l) * kLwRec);
-  switch (blockIdx.y) {
+  switch (band) {
     case 0: gas_band<0>(T, L, rec); break;
     case 1: gas_band<1>(T, L, rec); break;
     case 2: gas_band<2>(T, L, rec); break;
@@ -1665,8 +1681,12 @@ __global__ void __launch_bounds__(kLwSweepThreads, 3) lw_sweep_kernel(Tables T, 
     const float plev0 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l) * a.ny));
     const float plev1 = pa_to_hpa(ld(a.in.p8w + wbase + static_cast<size_t>(l + 1) * a.ny));
     const float dp = plev0 - plev1;
-    const float htr = heatfac * (fnet0 - fnet1) / dp;
-    const float htrc = heatfac * (fnetc0 - fnetc1) / dp;
+    float htr = heatfac * (fnet0 - fnet1) / dp;
+    float htrc = heatfac * (fnetc0 - fnetc1) / dp;
+    if (l >= a.fp64_from) {
+      htr = heating64(heatfac, fx[0][l], fx[2][l], fx[0][l + 1], fx[2][l + 1], plev0, plev1);
+      htrc = heating64(heatfac, fx[1][l], fx[3][l], fx[1][l + 1], fx[3][l + 1], plev0, plev1);
+    }
     const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * a.ny);
     a.rthraten[rbase + static_cast<size_t>(l) * a.ny] = (htr / 86400.0f) / pi3d;
     a.rthratenc[rbase + static_cast<size_t>(l) * a.ny] = (htrc / 86400.0f) / pi3d;
@@ -1714,7 +1734,7 @@ cudaError_t launch_lw_chunk_optics(const Tables &T, const LwArgs &a, cudaStream_
   lw_layer_kernel<<<blocks, threads, 0, stream>>>(T, a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  lw_gas_kernel<<<dim3(blocks, kLwBands), threads, 0, stream>>>(T, a);
+  lw_gas_kernel<<<blocks * kLwBands, threads, 0, stream>>>(T, a, static_cast<int>(blocks));
   return cudaGetLastError();
 }
 

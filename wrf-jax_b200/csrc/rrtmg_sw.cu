@@ -530,12 +530,101 @@ __device__ __forceinline__ float zero_over(float x) {
   return __int_as_float(__float_as_int(x) & static_cast<int>(0x80000000u));
 }
 
+// FP64 mode: the Pade lookup of exp(-v) (sw:2722-2760) with binary64
+// arithmetic; the table is the same binary32 data.
+__device__ __forceinline__ double exp_lookup64(const Tables &T, double v) {
+  if (v <= 0.06) return (1.0 - v) + (0.5 * v) * v;
+  const double tblind = v / (static_cast<double>(T.sw_bpade) + v);
+  const int it = clampi(static_cast<int>(static_cast<double>(T.sw_ntbl) * tblind + 0.5), 0, T.sw_ntbl);
+  return static_cast<double>(ld(T.sw_pade_exp + it));
+}
+
+// FP64 mode's reftra (sw:3490-3601) for a layer whose delta-scaled
+// single-scattering albedo zwo is >= 0.999 or whose optical depth zto1 is
+// below 0.1: both branches in binary64 on the binary32 inputs, the four
+// results rounded once.  Near zwo = 1 the general branch's g1 * g1 - g2 * g2
+// cancels (its binary32 relative error grows as 1 / (1 - zw)); for a thin
+// layer the O(1) terms of the reflectance and transmittance numerators cancel
+// to O(zto1), and in binary32 a layer of optical depth 5e-4 can come out with
+// a negative reflectance and 70% transmittance instead of 99.96%.
+__device__ __noinline__ RT4 reftra64(const Tables &T, float zg_in, float mu_in, float zto1_in, float zw_in) {
+  const double zg = zg_in, mu = mu_in, zto1 = zto1_in, zw = zw_in;
+  const double eps = 1.0e-8, zwcrit = 0.9999995;
+  double ref, refd, tra, trad;
+  const double zg3 = 3.0 * zg;
+  const double g1 = (8.0 - zw * (5.0 + zg3)) * 0.25;
+  const double g2 = 3.0 * (zw * (1.0 - zg)) * 0.25;
+  const double g3 = (2.0 - zg3 * mu) * 0.25;
+  const double g4 = 1.0 - g3;
+  const double sr = zg != 1.0 ? zg / (1.0 - zg) : 0.0;
+  const double denom = zg != 1.0 ? 1.0 - (1.0 - zw) * sr * sr : 1.0;
+  const double zwo = (zw > 0.0 && denom != 0.0) ? zw / denom : 0.0;
+  double ze2 = zto1 / mu;
+  if (ze2 > 500.0) ze2 = 500.0;
+  const double zem2 = exp_lookup64(T, ze2);
+  if (zwo >= zwcrit) {
+    const double za = g1 * mu;
+    const double za1 = za - g3;
+    const double zgt = g1 * zto1;
+    ref = (zgt - za1 * (1.0 - zem2)) / (1.0 + zgt);
+    tra = 1.0 - ref;
+    refd = zgt / (1.0 + zgt);
+    trad = 1.0 - refd;
+    if (zem2 == 1.0) { ref = 0.0; tra = 1.0; refd = 0.0; trad = 1.0; }
+  } else {
+    const double za1 = g1 * g4 + g2 * g3;
+    const double za2 = g1 * g3 + g2 * g4;
+    const double rad = g1 * g1 - g2 * g2;
+    const double zrk = sqrt(rad > 0.0 ? rad : 0.0);
+    const double zrp = zrk * mu;
+    const double zrp1 = 1.0 + zrp, zrm1 = 1.0 - zrp, zrk2 = 2.0 * zrk;
+    const double zrpp = 1.0 - zrp * zrp;
+    const double zrkg = zrk + g1;
+    const double zr1 = zrm1 * (za2 + zrk * g3);
+    const double zr2 = zrp1 * (za2 - zrk * g3);
+    const double zr3 = zrk2 * (g3 - za2 * mu);
+    const double zr4 = zrpp * zrkg;
+    const double zr5 = zrpp * (zrk - g1);
+    const double zt1 = zrp1 * (za1 + zrk * g4);
+    const double zt2 = zrm1 * (za1 - zrk * g4);
+    const double zt3 = zrk2 * (g4 + za1 * mu);
+    const double zbeta = (g1 - zrk) / zrkg;
+    double ze1 = zrk * zto1;
+    if (ze1 > 500.0) ze1 = 500.0;
+    const double zem1 = exp_lookup64(T, ze1);
+    const double zep1 = 1.0 / zem1;
+    const double zep2 = 1.0 / zem2;
+    const double zdenr = zr4 * zep1 + zr5 * zem1;
+    const double zdent = zr4 * zep1 + zr5 * zem1;
+    if (zdenr >= -eps && zdenr <= eps) {
+      ref = eps;
+      tra = zem2;
+    } else {
+      ref = zw * (zr1 * zep1 - zr2 * zem1 - zr3 * zem2) / zdenr;
+      tra = zem2 - zem2 * zw * (zt1 * zep1 - zt2 * zem1 - zt3 * zep2) / zdent;
+    }
+    const double zemm = zem1 * zem1;
+    const double zdend = 1.0 / ((1.0 - zbeta * zemm) * zrkg);
+    refd = g2 * (1.0 - zemm) * zdend;
+    trad = zrk2 * zem1 * zdend;
+  }
+  RT4 r;
+  r.ref = static_cast<float>(ref);
+  r.refd = static_cast<float>(refd);
+  r.tra = static_cast<float>(tra);
+  r.trad = static_cast<float>(trad);
+  return r;
+}
+
 // Delta-Eddington layer reflectance/transmittance (reftra_sw_columns,
 // sw:3490-3601) of a layer that scatters (the reference's lrt = true).
 // zto1_mu = zto1 / mu and ex_zto1_mu = exp_lookup(zto1_mu) come from the
 // caller, which needs the same quotient and lookup for its direct beam.
 // Divisions whose divisor is exactly 1 are skipped: their quotient is the
 // dividend, bit for bit.
+// kFp64: the FP64 mode, which hands layers with zwo >= 0.999 or zto1 < 0.1
+// to reftra64.
+template <bool kFp64>
 __device__ __forceinline__ RT4 reftra(const Tables &T, float zg, float mu, float zto1, float zw, float zto1_mu,
                                       float ex_zto1_mu) {
   RT4 r;
@@ -548,6 +637,9 @@ __device__ __forceinline__ RT4 reftra(const Tables &T, float zg, float mu, float
   const float sr = zg != 1.0f ? div_or_same(zg, 1.0f - zg) : 0.0f;
   const float denom = zg != 1.0f ? 1.0f - (1.0f - zw) * sr * sr : 1.0f;
   const float zwo = (zw > 0.0f && denom != 0.0f) ? div_or_same(zw, denom) : 0.0f;
+  if constexpr (kFp64) {
+    if (zwo >= 0.999f || zto1 < 0.1f) return reftra64(T, zg, mu, zto1, zw);
+  }
   if (zwo >= zwcrit) {
     const float za = g1 * mu;
     const float za1 = za - g3;
@@ -737,8 +829,12 @@ __device__ __forceinline__ void sw_layer_output(const SwArgs &a, const Col &C, i
   const float plev0 = pa_to_hpa(in3w(a.in.p8w, C, l));
   const float plev1 = pa_to_hpa(in3w(a.in.p8w, C, l + 1));
   const float zdpgcp = heatfac / (plev0 - plev1);
-  const float hr = (n1 - n0) * zdpgcp;
-  const float hrc = (c1 - c0) * zdpgcp;
+  float hr = (n1 - n0) * zdpgcp;
+  float hrc = (c1 - c0) * zdpgcp;
+  if (l >= a.fp64_from) {  // FP64 mode
+    hr = heating64(heatfac, fu[n - l], fd[n - l], fu[n - (l + 1)], fd[n - (l + 1)], plev0, plev1);
+    hrc = heating64(heatfac, cu[n - l], cd[n - l], cu[n - (l + 1)], cd[n - (l + 1)], plev0, plev1);
+  }
   const float pi3d = ld(a.in.pi3d + rbase + static_cast<size_t>(l) * C.ny);
   a.rthraten[rbase + static_cast<size_t>(l) * C.ny] = (hr / 86400.0f) / pi3d;
   a.rthratenc[rbase + static_cast<size_t>(l) * C.ny] = (hrc / 86400.0f) / pi3d;
@@ -994,6 +1090,7 @@ __device__ __forceinline__ void sweep_flush(SweepShared &S, int count, int ntype
 // reference skips (lrt = false).  The total-sky stack slot of such a layer is
 // not stored: the bottom-up pass re-forms it from the clear-sky slot with the
 // reference's mixing expression.
+template <bool kFp64>
 __global__ void __launch_bounds__(kSweepThreads, 4) sw_sweep_kernel(Tables T, SwArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SweepShared &S = *reinterpret_cast<SweepShared *>(smem_raw);
@@ -1071,7 +1168,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) sw_sweep_kernel(Tables T, Sw
     // ztauc is ztau exactly when d_w == 1
     const float v_c = d_w == 1.0f ? v_nd : ztauc / mu;
     const float dbtc = d_w == 1.0f ? dbtc_nd : exp_lookup(T, v_c);
-    const RT4 c = reftra(T, zgcc, mu, ztauc, zomcc, v_c, dbtc);
+    const RT4 c = reftra<kFp64>(T, zgcc, mu, ztauc, zomcc, v_c, dbtc);
     stc[r].rt = make_float4(c.ref, c.refd, c.tra, c.trad);
     stc[r].dn = make_float4(dbtc, c_tdbt, c_tdn, c_rdnd);
     // downward recurrence of vrtqdr (sw:3681-3702) for level r + 1
@@ -1104,7 +1201,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) sw_sweep_kernel(Tables T, Sw
         zomco = zomco / ztauo;
         const float v_o = ztauo / mu;
         const float dbtmo = exp_lookup(T, v_o);
-        const RT4 o = reftra(T, zgco, mu, ztauo, zomco, v_o, dbtmo);
+        const RT4 o = reftra<kFp64>(T, zgco, mu, ztauo, zomco, v_o, dbtmo);
         ref = clear * c.ref + cloud * o.ref;
         refd = clear * c.refd + cloud * o.refd;
         tra = clear * c.tra + cloud * o.tra;
@@ -1156,12 +1253,21 @@ __global__ void __launch_bounds__(kSweepThreads, 4) sw_sweep_kernel(Tables T, Sw
 
   // ---- bottom-up pass: upward adding and level fluxes (vrtqdr, sw:3655-3720)
   const int utypes[4] = {0, 1, 2, 3};
-  float rupc = C.albedo, rupdc = C.albedo;
-  float rupt = C.albedo, rupdt = C.albedo;
+  // surface albedos of this g-point's band: direct (albp) and diffuse (albd);
+  // the Noah-MP fields, when given, for columns with xland < 1.5 (sw:2519-2530):
+  // visible in bands 25-28, near infrared in 16-24 and 29 (sw:2120-2127)
+  float albp = C.albedo, albd = C.albedo;
+  if (a.in.alswvisdir && ld(a.in.xland + col) < 1.5f) {
+    const bool vis = band >= 9 && band <= 12;
+    albp = ld((vis ? a.in.alswvisdir : a.in.alswnirdir) + col);
+    albd = ld((vis ? a.in.alswvisdif : a.in.alswnirdif) + col);
+  }
+  float rupc = albp, rupdc = albd;
+  float rupt = albp, rupdt = albd;
   level0 = n;
   // surface level n: albedo reflection, no transmission; the recurrence's level-n values
-  SwLevel c = {make_float4(C.albedo, C.albedo, 0.0f, 0.0f), make_float4(0.0f, c_tdbt, c_tdn, c_rdnd)};
-  SwLevel t = {make_float4(C.albedo, C.albedo, 0.0f, 0.0f), make_float4(0.0f, t_tdbt, t_tdn, t_rdnd)};
+  SwLevel c = {make_float4(albp, albd, 0.0f, 0.0f), make_float4(0.0f, c_tdbt, c_tdn, c_rdnd)};
+  SwLevel t = {make_float4(albp, albd, 0.0f, 0.0f), make_float4(0.0f, t_tdbt, t_tdn, t_rdnd)};
   if (clear_only) t = c;
   // stack slot j (layer n - 1 - j) of both paths; a layer without cloud in
   // this g-point has the total-sky mix clear * c + cloud * (0, 0, 1, 1)
@@ -1257,22 +1363,27 @@ cudaError_t launch_sw_chunk_optics(const Tables &T, const SwArgs &a, cudaStream_
   return cudaGetLastError();
 }
 
-cudaError_t launch_sw_chunk_sweep(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+template <bool kFp64>
+static cudaError_t launch_sweep(const Tables &T, const SwArgs &a, cudaStream_t stream) {
   if (sizeof(SweepShared) > 48 * 1024) {  // a ring of more levels needs the opt-in
     static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 64 && !((configured.load() >> dev) & 1ull)) {
-      e = cudaFuncSetAttribute(sw_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      e = cudaFuncSetAttribute(sw_sweep_kernel<kFp64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                static_cast<int>(sizeof(SweepShared)));
       if (e != cudaSuccess) return e;
       configured.fetch_or(1ull << dev);
     }
   }
-  sw_sweep_kernel<<<(a.chunk_count + kSweepCols - 1) / kSweepCols, kSweepThreads, sizeof(SweepShared), stream>>>(T,
-                                                                                                               a);
+  sw_sweep_kernel<kFp64><<<(a.chunk_count + kSweepCols - 1) / kSweepCols, kSweepThreads, sizeof(SweepShared),
+                           stream>>>(T, a);
   return cudaGetLastError();
+}
+
+cudaError_t launch_sw_chunk_sweep(const Tables &T, const SwArgs &a, cudaStream_t stream) {
+  return a.fp64_reftra ? launch_sweep<true>(T, a, stream) : launch_sweep<false>(T, a, stream);
 }
 
 }  // namespace rrtmg

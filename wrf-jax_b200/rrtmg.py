@@ -142,6 +142,29 @@ class RrtmgContext:
                 raise NotImplementedError(msg)
             raise RrtmgError(st, msg)
 
+    # per-column status bits of rrtmg_last_column_errors (include/rrtmg_b200.h)
+    COL_NONFINITE_INPUT = 0x1
+    COL_NONFINITE_OUTPUT = 0x2
+    COL_PRESSURE_ORDER = 0x4
+    COL_TEMPERATURE_RANGE = 0x8
+    COL_FRACTION_RANGE = 0x10
+
+    def column_status(self, enable: bool = True) -> None:
+        """Record a per-column status bitmask after every LW / SW call on this
+        context (one extra launch per call) until disabled."""
+        self.check(self.lib.rrtmg_column_status_enable(self.handle, int(bool(enable))))
+
+    def last_column_errors(self, side: str, nx: int, ny: int, stream=None):
+        """Status words of the last recorded ``side`` ("lw" or "sw") call as an
+        (nx, ny) int32 CUDA tensor (the uint32 bits of include/rrtmg_b200.h)."""
+        import torch
+
+        out = torch.empty((nx, ny), dtype=torch.int32, device=f"cuda:{self.device}")
+        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        self.check(self.lib.rrtmg_last_column_errors(self.handle, 0 if side == "lw" else 1, out.data_ptr(),
+                                                     nx * ny, ctypes.c_void_p(s)))
+        return out
+
 
 _default_ctx: dict = {}
 _ctx_lock = threading.Lock()
@@ -177,24 +200,27 @@ def _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr, cfc11vmr, cfc12
 
 def lw_config(nx: int, ny: int, nk: int, *, p_top, yr, ghg_input=1, case_dir=None, co2vmr=None, n2ovmr=None,
               ch4vmr=None, cfc11vmr=None, cfc12vmr=None, icloud=1, has_reqc=1, has_reqi=1, has_reqs=1,
-              cldovrlp=2) -> "_capi.Config":
-    """rrtmg_config of an LW call: the scalar keywords of rrtmg_lwrad_wrf_columns."""
+              cldovrlp=2, fp64_steps=False) -> "_capi.Config":
+    """rrtmg_config of an LW call: the scalar keywords of rrtmg_lwrad_wrf_columns
+    (``fp64_steps``: the FP64 mode of include/rrtmg_b200.h; no counterpart in
+    the reference)."""
     co2, n2o, ch4, cfc11, cfc12 = _greenhouse(yr, ghg_input, case_dir, co2vmr, n2ovmr, ch4vmr,
                                               cfc11vmr, cfc12vmr, lw=True)
     return _capi.Config(nx=nx, ny=ny, nk=nk, p_top=float(p_top), co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4,
                         cfc11vmr=cfc11, cfc12vmr=cfc12, solcon=0.0, has_reqc=int(has_reqc),
                         has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
-                        cldovrlp=int(cldovrlp))
+                        cldovrlp=int(cldovrlp), fp64_steps=int(bool(fp64_steps)))
 
 
 def sw_config(nx: int, ny: int, nk: int, *, solcon, yr, ghg_input=1, co2vmr=None, n2ovmr=None, ch4vmr=None,
-              icloud=1, has_reqc=1, has_reqi=1, has_reqs=1, cldovrlp=2) -> "_capi.Config":
-    """rrtmg_config of an SW call: the scalar keywords of rrtmg_swrad_wrf_columns."""
+              icloud=1, has_reqc=1, has_reqi=1, has_reqs=1, cldovrlp=2, fp64_steps=False) -> "_capi.Config":
+    """rrtmg_config of an SW call: the scalar keywords of rrtmg_swrad_wrf_columns
+    (``fp64_steps`` as for lw_config)."""
     co2, n2o, ch4, _, _ = _greenhouse(yr, ghg_input, None, co2vmr, n2ovmr, ch4vmr, None, None, lw=False)
     return _capi.Config(nx=nx, ny=ny, nk=nk, p_top=0.0, co2vmr=co2, n2ovmr=n2o, ch4vmr=ch4, cfc11vmr=0.0,
                         cfc12vmr=0.0, solcon=float(np.float32(solcon)), has_reqc=int(has_reqc),
                         has_reqi=int(has_reqi), has_reqs=int(has_reqs), icloud=int(icloud),
-                        cldovrlp=int(cldovrlp))
+                        cldovrlp=int(cldovrlp), fp64_steps=int(bool(fp64_steps)))
 
 
 def _as_device(arrays: dict, device: int):
@@ -262,11 +288,14 @@ def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                             has_reqi=1, has_reqs=1, co2vmr=None, n2ovmr=None, ch4vmr=None, cfc11vmr=None,
                             cfc12vmr=None, lookup_tables=None, spectral=None, pade_tables=None,
                             cloud_tables=None, setcoef_tables=None, rounding_token=None,
-                            context: RrtmgContext | None = None, stream=None, out=None) -> RrtmgLwWrfColumnResult:
+                            context: RrtmgContext | None = None, stream=None, out=None,
+                            fp64_steps: bool = False) -> RrtmgLwWrfColumnResult:
     """B200 ``RRTMG_LWRAD`` (module_ra_rrtmg_lw.py:6789).  Table keywords are
     accepted for signature parity and ignored (the context owns the tables).
     ``out``: optional dict of preallocated float32 CUDA tensors, one per result
-    field, written in place (used for CUDA-graph capture)."""
+    field, written in place (used for CUDA-graph capture).  ``fp64_steps``:
+    heating rates of the five highest model layers formed in binary64 (the
+    FP64 mode; off by default, which reproduces the reference bit for bit)."""
     import torch
 
     del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables, setcoef_tables
@@ -284,7 +313,8 @@ def rrtmg_lwrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                       ("tsk", "emiss", "xland", "xice", "snow"))
         cfg = lw_config(nx, ny, nk, p_top=p_top, yr=yr, ghg_input=ghg_input, case_dir=case_dir, co2vmr=co2vmr,
                         n2ovmr=n2ovmr, ch4vmr=ch4vmr, cfc11vmr=cfc11vmr, cfc12vmr=cfc12vmr, icloud=icloud,
-                        has_reqc=has_reqc, has_reqi=has_reqi, has_reqs=has_reqs, cldovrlp=cldovrlp)
+                        has_reqc=has_reqc, has_reqi=has_reqi, has_reqs=has_reqs, cldovrlp=cldovrlp,
+                        fp64_steps=fp64_steps)
         outs = out if out is not None else {
             k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), dtype=torch.float32,
                            device=f"cuda:{ctx.device}") for k in _capi.LW_OUT_FIELDS}
@@ -307,34 +337,41 @@ def rrtmg_swrad_wrf_columns(*, p3d, p8w, pi3d, t3d, t8w, tsk, dz8w, qv3d, qc3d, 
                             sf_surface_physics=2, alswvisdir=None, alswvisdif=None, alswnirdir=None,
                             alswnirdif=None, co2vmr=None, n2ovmr=None, ch4vmr=None, lookup_tables=None,
                             spectral=None, pade_tables=None, cloud_tables=None, rounding_token=None,
-                            context: RrtmgContext | None = None, stream=None, out=None) -> RrtmgSwWrfColumnResult:
-    """B200 ``rrtmg_swrad`` (module_ra_rrtmg_sw.py:2386); ``out`` as for the LW call."""
+                            context: RrtmgContext | None = None, stream=None, out=None,
+                            fp64_steps: bool = False) -> RrtmgSwWrfColumnResult:
+    """B200 ``rrtmg_swrad`` (module_ra_rrtmg_sw.py:2386); ``out`` as for the LW
+    call.  ``fp64_steps``: the FP64 mode (reftra of nearly conservative layers
+    and the top layers' heating rates in binary64; off by default)."""
     import torch
 
     del idcor, julian, lookup_tables, spectral, pade_tables, cloud_tables
     _check_rounding_token(rounding_token)
-    if int(sf_surface_physics) == 8 and all(v is not None for v in (alswvisdir, alswvisdif, alswnirdir, alswnirdif)):
-        raise NotImplementedError("separate visible/near-IR albedos (sf_surface_physics=8) are not part of this path")
+    # Noah-MP albedos only when the reference uses them (sw:2521)
+    sf8 = int(sf_surface_physics) == 8 and all(v is not None for v in (alswvisdir, alswvisdif, alswnirdir,
+                                                                        alswnirdif))
     ctx = context or default_context()
     arrays = dict(p3d=p3d, p8w=p8w, pi3d=pi3d, t3d=t3d, t8w=t8w, tsk=tsk, dz8w=dz8w, qv3d=qv3d, qc3d=qc3d,
                   qi3d=qi3d, qs3d=qs3d, cldfra3d=cldfra3d, o33d=o33d, albedo=albedo, coszr=coszr,
                   xland=xland, xice=xice, snow=snow, re_cloud=re_cloud, re_ice=re_ice, re_snow=re_snow)
+    if sf8:
+        arrays.update(alswvisdir=alswvisdir, alswvisdif=alswvisdif, alswnirdir=alswnirdir, alswnirdif=alswnirdif)
     with torch.cuda.device(ctx.device):
         d, host = _as_device(arrays, ctx.device)
         nx, nk, ny = d["t3d"].shape
         _check_shapes(d, nx, nk, ny,
                       ("p3d", "pi3d", "t3d", "dz8w", "qv3d", "qc3d", "qi3d", "qs3d", "cldfra3d", "o33d",
                        "re_cloud", "re_ice", "re_snow"), ("p8w", "t8w"),
-                      ("tsk", "albedo", "coszr", "xland", "xice", "snow"))
+                      ("tsk", "albedo", "coszr", "xland", "xice", "snow")
+                      + (_capi.SW_ALBEDO_FIELDS if sf8 else ()))
         cfg = sw_config(nx, ny, nk, solcon=solcon, yr=yr, ghg_input=ghg_input, co2vmr=co2vmr, n2ovmr=n2ovmr,
                         ch4vmr=ch4vmr, icloud=icloud, has_reqc=has_reqc, has_reqi=has_reqi, has_reqs=has_reqs,
-                        cldovrlp=cldovrlp)
+                        cldovrlp=cldovrlp, fp64_steps=fp64_steps)
         outs = out if out is not None else {
             k: torch.empty((nx, nk, ny) if k.startswith("rthraten") else (nx, ny), dtype=torch.float32,
                            device=f"cuda:{ctx.device}") for k in _capi.SW_OUT_FIELDS}
         if out is not None:
             _check_outputs(out, _capi.SW_OUT_FIELDS, nx, nk, ny)
-        cin = _capi.SwIn(**{k: d[k].data_ptr() for k in _capi.SW_IN_FIELDS})
+        cin = _capi.SwIn(**{k: d[k].data_ptr() for k in _capi.SW_IN_FIELDS + (_capi.SW_ALBEDO_FIELDS if sf8 else ())})
         cout = _capi.SwOut(**{k: outs[k].data_ptr() for k in _capi.SW_OUT_FIELDS})
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         ctx.check(ctx.lib.rrtmg_swrad(ctx.handle, ctypes.byref(cfg), ctypes.byref(cin), ctypes.byref(cout),
