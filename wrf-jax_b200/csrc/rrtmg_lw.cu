@@ -1360,7 +1360,14 @@ __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
 }
 
 // thread = (layer, chunk column), columns fastest
-__global__ void __launch_bounds__(128) lw_layer_kernel(Tables T, LwArgs a) {
+// Resident blocks per SM the register allocation must allow (measured at
+// 425 x 425 x 50: without them the layer and gas kernels take 242 and 254
+// registers, two blocks per SM, and the LW optics take 42 ms instead of 27;
+// the sweep at 56 registers instead of 67 takes 27.7 ms instead of 32.9).
+constexpr int kLwLayerMinBlocks = 6;
+constexpr int kLwGasMinBlocks = 8;
+constexpr int kLwSweepMinBlocks = 4;
+__global__ void __launch_bounds__(128, kLwLayerMinBlocks) lw_layer_kernel(Tables T, LwArgs a) {
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int l = static_cast<int>(idx / a.chunk_count);
   const int lc = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
@@ -1425,7 +1432,7 @@ __device__ __forceinline__ void gas_band(const Tables &T, const Layer &L, float4
 constexpr int kLwGasGroup = 512;
 
 // thread = (layer, chunk column) of block `blk`; band from the block order above
-__global__ void __launch_bounds__(128) lw_gas_kernel(Tables T, LwArgs a, int nblk) {
+__global__ void __launch_bounds__(128, kLwGasMinBlocks) lw_gas_kernel(Tables T, LwArgs a, int nblk) {
   const int group = blockIdx.x / (kLwGasGroup * kLwBands);
   const int g0 = group * kLwGasGroup;
   const int gsize = nblk - g0 < kLwGasGroup ? nblk - g0 : kLwGasGroup;
@@ -1555,7 +1562,7 @@ __device__ __forceinline__ void lw_flush(LwSweepShared &S, int count, int type0,
 // Block = kLwSweepCols consecutive columns of the chunk.  A column past the
 // chunk or the live count repeats the block's first column so that every
 // thread takes the same barriers; its results are not written.
-__global__ void __launch_bounds__(kLwSweepThreads, 3) lw_sweep_kernel(Tables T, LwArgs a) {
+__global__ void __launch_bounds__(kLwSweepThreads, kLwSweepMinBlocks) lw_sweep_kernel(Tables T, LwArgs a) {
   __shared__ __align__(16) LwSweepShared S;
   const int lc0 = blockIdx.x * kLwSweepCols;
   if (lc0 >= a.chunk_count || dead_column(a.live, a.chunk_first + lc0)) return;  // whole block

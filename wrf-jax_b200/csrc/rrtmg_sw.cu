@@ -960,7 +960,12 @@ __device__ __forceinline__ void sw_band_record(const Tables &T, const SLayer &L,
 
 // thread = (layer, chunk slot), slots fastest: the layer set-up once, then the
 // records of all 14 bands.
-__global__ void __launch_bounds__(128) sw_optics_kernel(Tables T, SwArgs a) {
+// Resident blocks per SM the register allocation must allow (the optics
+// kernel at 80 registers instead of 128: 15.4 ms instead of 16.2 at 425 x 425
+// x 50; a fifth sweep block per SM spills and is slower).
+constexpr int kSwOpticsMinBlocks = 6;
+constexpr int kSwSweepMinBlocks = 4;
+__global__ void __launch_bounds__(128, kSwOpticsMinBlocks) sw_optics_kernel(Tables T, SwArgs a) {
   const int n = a.nk + 1;
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int l = static_cast<int>(idx / a.chunk_count);
@@ -1091,7 +1096,7 @@ __device__ __forceinline__ void sweep_flush(SweepShared &S, int count, int ntype
 // not stored: the bottom-up pass re-forms it from the clear-sky slot with the
 // reference's mixing expression.
 template <bool kFp64>
-__global__ void __launch_bounds__(kSweepThreads, 4) sw_sweep_kernel(Tables T, SwArgs a) {
+__global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_kernel(Tables T, SwArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SweepShared &S = *reinterpret_cast<SweepShared *>(smem_raw);
   const int nday = *a.nday;
