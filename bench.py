@@ -56,11 +56,11 @@ METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0
 # on 16 host threads (roughly 40 core-seconds of work)
 CPU_SAMPLE_COLUMNS = 42500
 # DRAM traffic per unit of the sweep kernels, from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch divided by its units): sw_sweep_kernel
-# 19.52 GB over 32,768 day columns (256 x 256 x 50 domain, one full chunk),
-# lw_sweep_kernel 2.27 GB over 16,384 columns (128 x 128 x 50 domain)
-DRAM_BYTES_PER_DAY_COLUMN_SW = 595700
-DRAM_BYTES_PER_COLUMN_LW = 138700
+# dram__bytes_write.sum of one launch divided by its units; the first launch
+# on the 256 x 256 x 50 domain, a full chunk): sw_sweep_kernel 19.75 GB over
+# 32,768 day columns, lw_sweep_kernel 2.374 GB over 16,384 columns
+DRAM_BYTES_PER_DAY_COLUMN_SW = 602800
+DRAM_BYTES_PER_COLUMN_LW = 144900
 L2_BYTES = 126 * 1024 * 1024
 # counted binary32 operations of the plain path per LW column and per SW day
 # column (tests/golden/make_flop_counts.py: the oracle's counting build on 10
