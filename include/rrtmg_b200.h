@@ -181,15 +181,16 @@ rrtmg_status rrtmg_column_status_enable(rrtmg_ctx *ctx, int enable);
  * stream.  RRTMG_BAD_ARG when no call was recorded or ncol differs. */
 rrtmg_status rrtmg_last_column_errors(rrtmg_ctx *ctx, int side, uint32_t *dev_status, int ncol, void *stream);
 
-/* Per-launch timing; no counterpart in the reference.  While enabled, every
- * rrtmg_lwrad / rrtmg_swrad call records CUDA events on its stream around its
- * three kernel launches (LW: McICA masks, band groups, finish; SW: McICA
- * masks, day-column compaction, column kernel), for up to 256 calls per side.
- * Domains of more than 131,072 columns run LW in column chunks; the band-
- * group duration then includes the finish kernels of all but the last chunk.
- * rrtmg_timing_read waits for the recorded calls and writes, oldest first,
- * three durations in milliseconds per call to ms[3 * i + k]; side 0 = LW,
- * 1 = SW.  It returns the number of calls written (at most max_calls), or -1. */
+/* Per-phase timing; no counterpart in the reference.  While enabled, every
+ * rrtmg_lwrad / rrtmg_swrad call records CUDA events on its stream between
+ * its phases, for up to 256 calls per side: the McICA masks, then per column
+ * chunk the optics launches (LW: column set-up, layer set-up, gas optics; SW:
+ * day list with the first chunk, column set-up, layer optics, solar source)
+ * and the sweep launch.  rrtmg_timing_read waits for the recorded calls and
+ * writes, oldest first, three durations in milliseconds per call to
+ * ms[3 * i + k]: McICA, the optics phases summed over the chunks, the sweeps
+ * summed; side 0 = LW, 1 = SW.  It returns the number of calls written (at
+ * most max_calls), or -1. */
 rrtmg_status rrtmg_timing_enable(rrtmg_ctx *ctx, int enable);
 int rrtmg_timing_read(rrtmg_ctx *ctx, int side, float *ms, int max_calls);
 
