@@ -1,5 +1,5 @@
 """CPU oracle (test infrastructure) of the radiation surrogate's MLP: forward
-and backward of the 4-layer GELU network in float64, with the BF16 roundings
+and backward of the 4-layer GELU (tanh form) network in float64, with the BF16 roundings
 placed where the GPU path stores BF16 (inputs, weights, hidden activations,
 output and hidden gradients).  Used only by tests to check the GPU gradients.
 """
@@ -19,15 +19,17 @@ def bf16(x: np.ndarray) -> np.ndarray:
     return rounded.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-_erf = np.vectorize(math.erf)
+_C = math.sqrt(2.0 / math.pi)
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in the tanh form (Hendrycks & Gimpel 2016), exact tanh."""
+    return 0.5 * z * (1.0 + np.tanh(_C * (z + 0.044715 * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_C * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _C * (1.0 + 3.0 * 0.044715 * z * z)
 
 
 def forward_backward(X, T, weights, biases, loss_w, scale):

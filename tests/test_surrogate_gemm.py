@@ -54,8 +54,10 @@ def test_gemm_gelu_epilogue(torch_cuda):
     assert surrogate.gemm_error() == 0
     zref = A.float() @ B.float().T + bias
     torch.testing.assert_close(Z, zref, rtol=1e-4, atol=1e-3)
-    href = torch.nn.functional.gelu(Z)
-    torch.testing.assert_close(H.float(), href, rtol=2 ** -8, atol=1e-6)
+    # GELU in the tanh form with the hardware tanh (relative error about
+    # 2^-11) and a BF16 result: within one BF16 unit of the exact tanh form
+    href = torch.nn.functional.gelu(Z, approximate="tanh")
+    torch.testing.assert_close(H.float(), href, rtol=2 ** -7, atol=2e-3)
     torch.testing.assert_close(Ht.float().T, H.float(), rtol=0, atol=0)
 
 
@@ -70,9 +72,12 @@ def test_gemm_dgelu_epilogue(torch_cuda):
     surrogate.gemm_bf16(A, B, epilogue=_capi.EPI_DGELU, aux=aux, H=H, Ht=Ht)
     torch.cuda.synchronize()
     z = aux.clone().requires_grad_(True)
-    torch.nn.functional.gelu(z).sum().backward()
-    ref = (A.float() @ B.float().T) * z.grad
-    torch.testing.assert_close(H.float(), ref, rtol=2 ** -7, atol=1e-4)
+    torch.nn.functional.gelu(z, approximate="tanh").sum().backward()
+    acc = A.float() @ B.float().T
+    ref = acc * z.grad
+    # GELU' with the hardware tanh (relative error about 2^-11 in tanh, so
+    # about 1e-3 absolute in GELU'), scaled by the accumulator, in BF16
+    torch.testing.assert_close(H.float(), ref, rtol=2 ** -7, atol=2e-3 * float(acc.abs().max()))
     torch.testing.assert_close(Ht.float().T, H.float(), rtol=0, atol=0)
 
 

@@ -134,26 +134,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Standard normal distribution function Phi(x) = erfc(-x / sqrt 2) / 2,
-// branch-free: erfc(z) for z = |x| / sqrt 2 by Abramowitz & Stegun, Handbook
-// of Mathematical Functions, formula 7.1.26 (Hastings' rational form,
-// |error| <= 1.5e-7), with the hardware reciprocal and base-2 exponential.
-__device__ __forceinline__ float normal_cdf(float x) {
-  const float z = fabsf(x) * 0.70710678118654752f;
-  const float t = __fdividef(1.0f, fmaf(0.3275911f, z, 1.0f));
-  float p = fmaf(t, 1.061405429f, -1.453152027f);
-  p = fmaf(t, p, 1.421413741f);
-  p = fmaf(t, p, -0.284496736f);
-  p = fmaf(t, p, 0.254829592f);
-  const float half_erfc = 0.5f * (t * p) * __expf(-(z * z));
-  return x >= 0.0f ? 1.0f - half_erfc : half_erfc;
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
-// GELU(x) = x Phi(x) (the erf form) and its derivative Phi(x) + x phi(x).
-__device__ __forceinline__ float gelu(float z) { return z * normal_cdf(z); }
+// GELU in the tanh form of Hendrycks & Gimpel (2016), 0.5 z (1 + tanh(u)),
+// u = sqrt(2/pi) (z + 0.044715 z^3), with the hardware tanh (one MUFU
+// operation), and its derivative 0.5 (1 + t) + 0.5 z (1 - t^2) du/dz.
+__device__ __forceinline__ float gelu(float z) {
+  const float h = 0.5f * z;
+  const float u = z * fmaf(0.0356774081f, z * z, 0.7978845608f);
+  return fmaf(h, tanh_approx(u), h);
+}
 
 __device__ __forceinline__ float gelu_grad(float z) {
-  return normal_cdf(z) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+  const float z2 = z * z;
+  const float t = tanh_approx(z * fmaf(0.0356774081f, z2, 0.7978845608f));
+  const float du = fmaf(0.1070322243f, z2, 0.7978845608f);
+  return fmaf(0.5f, t, 0.5f) + (0.5f * z) * fmaf(-t, t, 1.0f) * du;
 }
 
 }  // namespace umma
