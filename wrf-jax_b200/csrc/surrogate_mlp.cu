@@ -15,7 +15,12 @@
 //     owns lanes 32 (w mod 4) .. and one of three column groups), add the bias,
 //     apply GELU and write the BF16 result over the activation buffer as the
 //     next layer's A operand, each chunk's accumulator read in flight while
-//     the previous chunk is processed;
+//     the previous chunk is processed.  A hidden layer's two N halves are
+//     pipelined against the MMAs: the first half's GELU runs while the
+//     second half's MMAs still read the activation tile, so it is parked in
+//     tensor memory (packed BF16 pairs) and copied into K blocks 0-3 once the
+//     layer's MMAs are done; the next layer's MMAs over K blocks 0-3 then run
+//     while the epilogue turns the second half into K blocks 4-7;
 //   * after layer 3 two groups denormalize the outputs and write the WRF
 //     fields directly (LW group: LW heating, glw, lwupb; SW group: SW
 //     heating, swdnb, swupb), with the energy gate of rrtmg_sur_decode; their
@@ -78,10 +83,11 @@ __device__ __forceinline__ uint32_t load_bytes(int j) { return j < kLoadsHidden 
 
 struct Bars {
   uint64_t full[kStages], empty[kStages];
-  uint64_t act_full;   // feature tile landed (tx)
-  uint64_t act_free;   // layer-3 MMAs done reading the activation buffer (commit)
-  uint64_t acc_full;   // a layer's MMAs complete (commit)
-  uint64_t act_ready;  // epilogue wrote the next layer's A operand (12 warps)
+  uint64_t act_full;      // feature tile landed (tx)
+  uint64_t act_free;      // layer-3 MMAs done reading the activation buffer (commit)
+  uint64_t acc_full[2];   // a hidden layer's first / both halves' MMAs complete (commit)
+  uint64_t acc3_full;     // layer 3's MMAs complete (commit)
+  uint64_t act_ready[2];  // epilogue wrote K blocks 0-3 / 4-7 of the next A operand (12 warps)
   uint64_t tmem_free;  // decode read layer 3's accumulator (8 decode warps)
   uint64_t sw_done;    // SW half of the decode published its gate result (4 warps)
   uint64_t mma_done;   // drain at exit (commit)
@@ -186,9 +192,9 @@ __device__ __forceinline__ bool decode_row(const SurMlpArgs &a, uint32_t cb, int
   return decode_side<HALF>(a, col, y, y2a, y2b, ytop);
 }
 
-// 16 accumulator columns of this thread's row: + bias, GELU, BF16, written as
-// K = c .. c + 15 of the next layer's A operand (two 16-byte chunks).
-__device__ __forceinline__ void gelu_store(const uint32_t (&v)[16], const float *bias, int c, uint8_t *act, int r) {
+// 16 accumulator columns of this thread's row (K = c .. c + 15 of the next
+// layer): + bias, GELU, BF16 pairs.
+__device__ __forceinline__ void gelu_pack(const uint32_t (&v)[16], const float *bias, int c, uint32_t (&p)[8]) {
   const float4 *b4 = reinterpret_cast<const float4 *>(bias + c);
   float b[16];
 #pragma unroll
@@ -196,7 +202,6 @@ __device__ __forceinline__ void gelu_store(const uint32_t (&v)[16], const float 
     const float4 t = __ldg(b4 + q);
     b[4 * q] = t.x; b[4 * q + 1] = t.y; b[4 * q + 2] = t.z; b[4 * q + 3] = t.w;
   }
-  uint32_t p[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const float x0 = __uint_as_float(v[2 * j]) + b[2 * j];
@@ -204,6 +209,11 @@ __device__ __forceinline__ void gelu_store(const uint32_t (&v)[16], const float 
     const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu(x0), gelu(x1));
     p[j] = *reinterpret_cast<const uint32_t *>(&h2);
   }
+}
+
+// Eight BF16 pairs as K = c .. c + 15 of row r of the activation tile (two
+// 16-byte chunks in the swizzled layout).
+__device__ __forceinline__ void act_store(const uint32_t (&p)[8], int c, uint8_t *act, int r) {
   uint8_t *blk = act + (c / kKb) * kActBlock;
   const int kc = (c % kKb) / 8;
   *reinterpret_cast<uint4 *>(blk + swz(r, kc)) = make_uint4(p[0], p[1], p[2], p[3]);
@@ -236,8 +246,11 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
     }
     mbar_init(bar(bars.act_full), 1);
     mbar_init(bar(bars.act_free), 1);
-    mbar_init(bar(bars.acc_full), 1);
-    mbar_init(bar(bars.act_ready), kEpiWarps);
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(bar(bars.acc_full[h]), 1);
+      mbar_init(bar(bars.act_ready[h]), kEpiWarps);
+    }
+    mbar_init(bar(bars.acc3_full), 1);
     mbar_init(bar(bars.tmem_free), kDecodeWarps);
     mbar_init(bar(bars.sw_done), kDecodeWarps / 2);
     mbar_init(bar(bars.mma_done), 1);
@@ -289,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
     if (lane == 0) {
       constexpr uint32_t kIdescHidden = idesc_bf16(kRows, 256);
       constexpr uint32_t kIdescOut = idesc_bf16(kRows, kOutCols);
-      uint32_t li = 0, ready = 0;
+      uint32_t li = 0, ready[2] = {0, 0};
       int it = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
@@ -299,13 +312,18 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         for (int layer = 0; layer < 4 && ok; ++layer) {
-          if (layer > 0) {
-            if (!mbar_wait_or_abort(bar(bars.act_ready), ready & 1, &abort_sh)) {
-              ok = false;
-              break;
-            }
-            ++ready;
+          // the epilogue's K blocks 0-3 (act_ready[0]) and 4-7 (act_ready[1])
+          // of this layer's A operand; layer 3 also writes columns the
+          // epilogue's second half reads, so it waits for both first
+          auto wait_ready = [&](int h) {
+            if (!mbar_wait_or_abort(bar(bars.act_ready[h]), ready[h] & 1, &abort_sh)) return false;
+            ++ready[h];
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            return true;
+          };
+          if (layer == 3 && !(wait_ready(0) && wait_ready(1))) {
+            ok = false;
+            break;
           }
           const int halves = layer < 3 ? 2 : 1;
           for (int h = 0; h < halves && ok; ++h) {
@@ -319,6 +337,10 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
             const uint32_t d = tmem + (layer < 3 ? static_cast<uint32_t>(h) * 256u : kOutCol0);
             const uint32_t idesc = layer < 3 ? kIdescHidden : kIdescOut;
             for (int kb = 0; kb < kNkb; ++kb, ++li) {
+              if (layer > 0 && layer < 3 && h == 0 && (kb == 0 || kb == kNkb / 2) && !wait_ready(kb == 0 ? 0 : 1)) {
+                ok = false;
+                break;
+              }
               const int s = static_cast<int>(li % kStages);
               if (!mbar_wait_or_abort(bar(bars.full[s]), (li / kStages) & 1, &abort_sh)) {
                 ok = false;
@@ -331,9 +353,10 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
                 umma_bf16(d, smem_desc(ab + kk * 32), smem_desc(bb + kk * 32), idesc, (kb | kk) != 0 ? 1u : 0u);
               umma_commit(bar(bars.empty[s]));
             }
+            if (!ok) break;
+            umma_commit(bar(layer < 3 ? bars.acc_full[h] : bars.acc3_full));
           }
           if (!ok) break;
-          umma_commit(bar(bars.acc_full));
           if (layer == 3) umma_commit(bar(bars.act_free));
         }
       }
@@ -348,9 +371,27 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
     const int group = (warp - kEpiWarp0) >> 2;     // column group 0-2; decode side 0 / 1
     const int r = quarter * 32 + lane;             // tile row of this thread
     const uint32_t trow = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
-    uint32_t acc_uses = 0;
+    uint32_t acc_uses[2] = {0, 0};
     int it = 0;
     bool ok = true;
+    // 16-column chunks of each 256-column half: group 0 takes 0-5, group 1
+    // 6-10, group 2 11-15
+    const int ch0 = group == 0 ? 0 : (group == 1 ? 6 : 11);
+    const int ch1 = group == 0 ? 6 : (group == 1 ? 11 : 16);
+    auto wait_acc = [&](int h) {
+      if (!warp_wait(bar(bars.acc_full[h]), acc_uses[h] & 1, &abort_sh)) return false;
+      ++acc_uses[h];
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      return true;
+    };
+    // generic-proxy writes -> visible to the tensor cores; tensor-memory
+    // accesses done; then one arrival per warp
+    auto publish = [&](int h) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar(bars.act_ready[h]));
+    };
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
       const int col = tile * kRows + r;
       const bool live = col < a.ncol;
@@ -364,46 +405,78 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_kernel(SurMlpArgs a, int ntil
         for (int k = 0; k < levels; ++k)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(pp + base + static_cast<size_t>(k) * a.ny));
       }
+      // Per hidden layer: the first half's accumulator (columns 0-255) is
+      // ready while the second half's MMAs still read the activation tile,
+      // so its GELU result is parked in tensor memory, packed BF16 pairs in
+      // the group's own columns (chunk k at 16 ch0 + 8 (k - ch0), behind the
+      // columns still to be read); once the layer's MMAs are done it is
+      // copied into K blocks 0-3 of the tile (the next layer's first MMAs
+      // start on them) while the second half is processed into K blocks 4-7.
       for (int layer = 0; layer < 3 && ok; ++layer) {
-        if (!warp_wait(bar(bars.acc_full), acc_uses & 1, &abort_sh)) {
+        const float *bias = a.bias[layer];
+        if (!wait_acc(0)) {
           ok = false;
           break;
         }
-        ++acc_uses;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const float *bias = a.bias[layer];
-        // columns of this group: 176, 176 and 160 (11, 11 and 10 chunks of 16)
-        const int c0 = group * 176;
-        const int nch = group == 2 ? 10 : 11;
-        const uint32_t tl = trow + static_cast<uint32_t>(c0);
-        // the next chunk's accumulator read is in flight while this one is processed
-        uint32_t va[16], vb[16];
-        tmem_ld16(tl, va);
+        {
+          uint32_t va[16], vb[16], p[8];
+          tmem_ld16(trow + ch0 * 16, va);
 #pragma unroll 1
-        for (int ch = 0; ch < nch; ch += 2) {
-          tmem_ld_wait();
-          if (ch + 1 < nch) tmem_ld16(tl + (ch + 1) * 16, vb);
-          gelu_store(va, bias, c0 + ch * 16, act, r);
-          if (ch + 1 < nch) {
+          for (int ch = ch0; ch < ch1; ch += 2) {
             tmem_ld_wait();
-            if (ch + 2 < nch) tmem_ld16(tl + (ch + 2) * 16, va);
-            gelu_store(vb, bias, c0 + (ch + 1) * 16, act, r);
+            if (ch + 1 < ch1) tmem_ld16(trow + (ch + 1) * 16, vb);
+            gelu_pack(va, bias, ch * 16, p);
+            tmem_st8(trow + 16 * ch0 + 8 * (ch - ch0), p);
+            if (ch + 1 < ch1) {
+              tmem_ld_wait();
+              if (ch + 2 < ch1) tmem_ld16(trow + (ch + 2) * 16, va);
+              gelu_pack(vb, bias, (ch + 1) * 16, p);
+              tmem_st8(trow + 16 * ch0 + 8 * (ch + 1 - ch0), p);
+            }
+          }
+          tmem_st_wait();
+        }
+        if (!wait_acc(1)) {
+          ok = false;
+          break;
+        }
+        {
+          uint32_t p[8];
+#pragma unroll 1
+          for (int ch = ch0; ch < ch1; ++ch) {
+            tmem_ld8(trow + 16 * ch0 + 8 * (ch - ch0), p);
+            tmem_ld_wait();
+            act_store(p, ch * 16, act, r);
           }
         }
-        // generic-proxy writes -> visible to the tensor cores; accumulator reads done
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(bar(bars.act_ready));
+        publish(0);
+        {
+          const uint32_t th = trow + 256u;
+          uint32_t va[16], vb[16], p[8];
+          tmem_ld16(th + ch0 * 16, va);
+#pragma unroll 1
+          for (int ch = ch0; ch < ch1; ch += 2) {
+            tmem_ld_wait();
+            if (ch + 1 < ch1) tmem_ld16(th + (ch + 1) * 16, vb);
+            gelu_pack(va, bias, 256 + ch * 16, p);
+            act_store(p, 256 + ch * 16, act, r);
+            if (ch + 1 < ch1) {
+              tmem_ld_wait();
+              if (ch + 2 < ch1) tmem_ld16(th + (ch + 2) * 16, va);
+              gelu_pack(vb, bias, 256 + (ch + 1) * 16, p);
+              act_store(p, 256 + (ch + 1) * 16, act, r);
+            }
+          }
+        }
+        publish(1);
       }
       if (!ok) break;
-      // ---- layer 3: decode (groups 0 and 1; group 2 only keeps the phase) ----
-      if (!warp_wait(bar(bars.acc_full), acc_uses & 1, &abort_sh)) {
+      // ---- layer 3: decode (groups 0 and 1) ----
+      if (group >= 2) continue;
+      if (!warp_wait(bar(bars.acc3_full), it & 1, &abort_sh)) {
         ok = false;
         break;
       }
-      ++acc_uses;
-      if (group >= 2) continue;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t cb = trow + kOutCol0;
       if (group == 1) {

@@ -28,6 +28,11 @@ import numpy as np
 from . import _capi, rrtmg, surrogate as S, synthetic
 
 
+# cost of a plain column in surrogate columns (the surrogate path runs about
+# 150 times more columns per second than the plain kernels)
+PLAIN_COST = 150.0
+
+
 @dataclass
 class Member:
     name: str
@@ -90,6 +95,13 @@ class EnsembleRunner:
                          "rthratensw": torch.empty(nx, nk, ny, device="cuda")}
                 for k in ("glw", "lwupb", "swdnb", "swupb"):
                     m.out[k] = torch.empty(nx, ny, device="cuda")
+                # the member's own fallback domain (its count stays on the
+                # device, so the fallback is captured with the member)
+                lw_kw, sw_kw = m.st.lw_kwargs(), m.st.sw_kwargs()
+                m.buf["plan"] = S._FallbackPlan(
+                    nk, min(ncol, S.FALLBACK_CAPACITY),
+                    {k: lw_kw[k] for k in S._SCALAR_KEYS_LW if k in lw_kw},
+                    {k: sw_kw[k] for k in S._SCALAR_KEYS_SW if k in sw_kw})
 
     def set_streams(self, n: int) -> None:
         import torch
@@ -101,7 +113,10 @@ class EnsembleRunner:
         return sum(m.columns for m in self.members)
 
     # -- launches -----------------------------------------------------------------
-    def _launch_member(self, m: Member, stream) -> None:
+    def _launch_member(self, m: Member, stream, fallback: bool = False) -> None:
+        """Queue one member on `stream`; fallback: also the surrogate member's
+        own re-solve of the columns its gate rejects, with the count left on
+        the device (up to the member's fallback capacity)."""
         lib = _capi.load()
         sid = stream.cuda_stream
         if m.mode == "plain":
@@ -117,28 +132,40 @@ class EnsembleRunner:
         b["count"].zero_()
         S._check(lib.rrtmg_sur_compact(b["flags"].data_ptr(), m.columns, b["list"].data_ptr(),
                                        b["count"].data_ptr(), s), "compact")
+        if fallback:
+            S._solve_listed(b["plan"], lib, s, b["list"], b["count"], st.ny, m.d, m.out, None, live=True)
+
+    def launch_order(self) -> list[int]:
+        """Members cheapest first (shortest processing time first minimises the
+        mean completion time on one stream; with several streams the cheap
+        members finish while the expensive ones run).  Cost: columns, a plain
+        column weighted as PLAIN_COST surrogate columns."""
+        cost = [m.columns * (PLAIN_COST if m.mode == "plain" else 1.0) for m in self.members]
+        return sorted(range(len(self.members)), key=lambda i: cost[i])
 
     def _stamp(self, slot: int, stream) -> None:
         lib = _capi.load()
         S._check(lib.rrtmg_sur_timestamp(self.stamps[slot:].data_ptr(), ctypes.c_void_p(stream.cuda_stream)),
                  "timestamp")
 
-    def launch_all(self, stamp: bool = False) -> None:
-        """Every launch of one step except the merged fallback, spread over the
-        streams (fork from and join to the current stream).  With stamp, the GPU
-        timer is written at the start (slot 0) and after each domain (slot i+1)."""
+    def launch_all(self, stamp: bool = False, fallback: bool = False) -> None:
+        """Every launch of one step, spread over the streams (fork from and
+        join to the current stream); fallback: each surrogate member's own
+        device-counted fallback too (else the merged fallback runs after).
+        With stamp, the GPU timer is written at the start (slot 0) and after
+        each domain (slot i+1)."""
         import torch
         main = torch.cuda.current_stream()
         if stamp:
             self._stamp(0, main)
         fork = torch.cuda.Event()
         fork.record(main)
-        order = sorted(range(len(self.members)), key=lambda i: -self.members[i].columns)
+        order = self.launch_order()
         for q, i in enumerate(order):
             s = self.streams[q % len(self.streams)]
             s.wait_event(fork)
             with torch.cuda.stream(s):
-                self._launch_member(self.members[i], s)
+                self._launch_member(self.members[i], s, fallback=fallback)
                 if stamp:
                     self._stamp(i + 1, s)
         for s in self.streams:
@@ -195,43 +222,50 @@ class EnsembleRunner:
 
     # -- graph --------------------------------------------------------------------
     def capture(self) -> None:
-        """Warm up (table jumps, pools, kernel attributes), then capture one step."""
+        """Warm up (table jumps, pools, kernel attributes), then capture one
+        step: every member, each surrogate member's fallback included."""
         import torch
         for _ in range(2):
-            self.launch_all()
-            self.merged_fallback()
+            self.launch_all(fallback=True)
         torch.cuda.synchronize()
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
-            self.launch_all(stamp=True)
+            self.launch_all(stamp=True, fallback=True)
         torch.cuda.synchronize()
 
     def step_graph(self) -> dict:
-        """One replayed step plus the merged fallback; per-domain completion
-        times (ms from the step start) and the step time."""
+        """One replayed step; per-domain completion times (ms from the step
+        start, fallbacks included) and the step time.  A surrogate member
+        whose gate rejected more columns than its fallback capacity has them
+        all re-solved after the replay (on an exact-size domain), and its
+        completion is the end of that."""
         import torch
         if self.graph is None:
             self.capture()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         self.graph.replay()
-        n_fb = self.merged_fallback()
+        counts = [int(m.buf["count"].item()) if m.mode == "surrogate" else 0 for m in self.members]
+        over = [m for m, n in zip(self.members, counts) if m.mode == "surrogate" and n > m.buf["plan"].cap]
+        for m in over:
+            saved = self.members
+            self.members = [m]
+            self.merged_fallback()
+            self.members = saved
         self._stamp(len(self.members) + 1, torch.cuda.current_stream())
         end.record()
         torch.cuda.synchronize()
         total = start.elapsed_time(end)
         ts = self.stamps.cpu().tolist()
         t0, t_end = ts[0], ts[len(self.members) + 1]
-        lat = []
-        for i, m in enumerate(self.members):
-            # surrogate domains are complete once the merged fallback is done
-            t = t_end if (m.mode == "surrogate" and n_fb) else ts[i + 1]
-            lat.append((t - t0) / 1e6)
-        return dict(ms=total, latencies_ms=lat, fallback_columns=n_fb)
+        lat = [((t_end if m in over else ts[i + 1]) - t0) / 1e6 for i, m in enumerate(self.members)]
+        return dict(ms=total, latencies_ms=lat, fallback_columns=sum(counts))
 
     def step_sequential(self) -> dict:
-        """The baseline: one domain after another, each launched and finished
-        (its own fallback included) before the next starts."""
+        """The baseline: one domain after another in the members' order, each
+        launched and finished (its own fallback included) before the next
+        starts.  A domain's latency is its completion time since the step
+        started, as for the graph step."""
         import torch
         lat = []
         main = torch.cuda.current_stream()
@@ -239,8 +273,7 @@ class EnsembleRunner:
         t0.record()
         n_fb = 0
         for m in self.members:
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
+            b = torch.cuda.Event(enable_timing=True)
             self._launch_member(m, main)
             if m.mode == "surrogate":
                 saved = self.members
@@ -249,7 +282,7 @@ class EnsembleRunner:
                 self.members = saved
             b.record()
             torch.cuda.synchronize()
-            lat.append(a.elapsed_time(b))
+            lat.append(t0.elapsed_time(b))
         t1 = torch.cuda.Event(enable_timing=True)
         t1.record()
         torch.cuda.synchronize()
@@ -287,14 +320,12 @@ def autotune(runner: EnsembleRunner, *, log=None) -> dict:
 
     def measure(cfg):
         apply(cfg)
-        runner.launch_all()
-        runner.merged_fallback()
+        runner.launch_all(fallback=True)
         torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         for _ in range(2):
-            runner.launch_all()
-            runner.merged_fallback()
+            runner.launch_all(fallback=True)
         ev1.record()
         torch.cuda.synchronize()
         return ev0.elapsed_time(ev1) / 2

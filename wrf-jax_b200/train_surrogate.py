@@ -71,10 +71,13 @@ def evaluate(model, nx: int, ny: int, seed: int, energy_tol: float) -> dict:
 
 
 def calibrate_gate(model, nx: int, ny: int, seed: int, heating_target: float = 0.2, flux_target: float = 2.0,
-                   tolerances=(1e30, 20.0, 10.0, 5.0, 3.0, 2.0, 1.5, 1.0, 0.75, 0.5, 0.3, 0.2, 0.1, 0.05)) -> dict:
+                   tolerances=(1e30, 20.0, 10.0, 5.0, 3.0, 2.0, 1.5, 1.0, 0.75, 0.5, 0.3, 0.2, 0.1, 0.05),
+                   max_tol: float = 5.0) -> dict:
     """Energy-gate tolerance sweep on a calibration domain: the largest
-    tolerance whose surrogate+fallback heating and surface-flux RMSE against
-    the plain kernels meet the targets (0: every column falls back)."""
+    tolerance up to max_tol whose surrogate+fallback heating and surface-flux
+    RMSE against the plain kernels meet the targets (0: every column falls
+    back).  The ceiling keeps the energy-consistency check active; the sweep
+    still records the larger tolerances (1e30: no energy check)."""
     import torch
     from wrf_jax_b200 import surrogate as S, synthetic
 
@@ -92,10 +95,10 @@ def calibrate_gate(model, nx: int, ny: int, seed: int, heating_target: float = 0
         fl = float(torch.sqrt((flux ** 2).mean()))
         frac = res.n_fallback / (nx * ny)
         sweep.append(dict(energy_tol=tol, heating_rmse_kday=heat, surface_flux_rmse_wm2=fl, fallback_fraction=frac))
-        if heat <= heating_target and fl <= flux_target and chosen == 0.0:
+        if heat <= heating_target and fl <= flux_target and chosen == 0.0 and tol <= max_tol:
             chosen = tol
     return dict(energy_tol=chosen, heating_target_kday=heating_target, flux_target_wm2=flux_target,
-                calibration_domain=[nx, ny, seed], sweep=sweep)
+                calibration_domain=[nx, ny, seed], sweep=sweep, max_energy_tol=max_tol)
 
 
 def main(argv=None) -> int:
