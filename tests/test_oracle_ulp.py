@@ -14,7 +14,7 @@ This test moves each result by +-1 ulp in the oracle (a test knob,
   a 300-400 W/m2 flux is 3.05e-5 W/m2, and the heating of a layer is
   (g * 86400 / (cp * 100)) * dF / dp = 8.435 * dF / dp(hPa), so in the
   thinnest model layers near a 50 hPa top (a few hPa) a one-ulp change of
-  both bounding fluxes is already about 1e-4 K/day: the north star's 1e-4
+  both bounding fluxes is already about 1e-4 K/day: a 1e-4
   K/day heating tolerance is at the binary32 resolution of the fluxes there.
 
 The measured maxima are printed (pytest -s).

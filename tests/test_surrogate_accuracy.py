@@ -4,7 +4,7 @@ used seed 1 with widened perturbations, the gate calibration seed 3 and the
 benchmark seed 2), with its gate and plain-kernel fallback, against the plain
 kernels on the same columns.
 
-Bars: the north star's heating RMSE <= 0.2 K/day and surface-flux RMSE
+Bars: the specified heating RMSE <= 0.2 K/day and surface-flux RMSE
 <= 2 W/m2 over LW and SW together (every column), with at most 5 % of the
 columns sent to the fallback.  Each side alone is held to 0.2 K/day too (SW
 over the day columns only: night SW is exactly zero on both paths).  The SW

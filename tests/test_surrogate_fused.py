@@ -62,8 +62,10 @@ def _features(torch, model, st, d, x_layout, old_kernel=False):
     return X, flags
 
 
-@pytest.mark.parametrize("nx,ny", [(37, 29), (64, 50)])
+@pytest.mark.parametrize("nx,ny", [(37, 29), (64, 50), (40, 36), (17, 64), (6, 1000)])
 def test_feature_layouts_match_the_reference_kernel(torch_cuda, model, nx, ny):
+    """Warps of 32 columns that straddle west-east rows (ny = 29, 36, 50,
+    1000) or fall on row starts (ny = 64), and a partial last warp."""
     torch = torch_cuda
     from wrf_jax_b200 import surrogate as S, synthetic
     st = synthetic.make_columns(nx, ny, S.NK, seed=21)

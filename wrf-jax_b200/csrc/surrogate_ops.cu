@@ -221,12 +221,41 @@ __global__ void __launch_bounds__(kRowThreads) features_rows_kernel(SurFeatureAr
 
 // Features of a 50-level column with every index resolved at compile time:
 // word W (features 2W, 2W + 1) of the output row is one expansion of
-// RRTMG_FEAT_WORD(W), W = 0..255, so each load is a register pointer plus a
-// constant level offset, each statistics read a constant shared-memory slot,
-// and words leave four at a time as 16-byte chunks.  The compiler barrier
-// after each chunk keeps all 454 loads from being hoisted.  Values, rounding
-// and range flags are those of features_kernel.
+// RRTMG_FEAT_WORD(W), W = 0..255, so each load is a running field pointer,
+// each statistics read a constant shared-memory slot, and words leave four at
+// a time as 16-byte chunks.  A thread's chunks go to its row of the warp's
+// shared staging line (at the chunk's swizzled tile position); after each
+// 64-feature group the warp writes the 32 rows out as whole 128-byte lines
+// (feat_flush), so no line is left half written in L2 while the rest of its
+// row is computed.  Values, rounding and range flags are those of
+// features_kernel.
 constexpr int kFeatNk = 50;
+
+// Writes the warp's staging line (32 rows x 8 chunks of 64-feature group kb)
+// to X: lane = 4 x row + position pair, so each store instruction covers
+// whole 128-byte row lines.  Slot p of row r holds chunk p ^ (row & 7).
+template <bool kTiled>
+__device__ __forceinline__ void feat_flush(uint8_t *X, const uint4 *stage, size_t row0, int kb, int lane,
+                                           int nrows) {
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int r = t * 8 + (lane >> 2), p0 = (lane & 3) * 2;
+    if (r < nrows) {
+      const size_t row = row0 + r;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = p0 + h;
+        const uint4 v = stage[r * 8 + p];
+        if (kTiled)
+          *reinterpret_cast<uint4 *>(X + (row >> 7) * 131072u + kb * 16384 + (row & 127) * 128 + p * 16) = v;
+        else
+          *reinterpret_cast<uint4 *>(X + row * 1024 + (kb * 8 + (p ^ static_cast<int>(row & 7))) * 16) = v;
+      }
+    }
+  }
+  __syncwarp();
+}
 
 // One output word; a macro (not a function) so the 256 expansions stay in one
 // straight-line body with every array index a constant.
@@ -237,8 +266,10 @@ constexpr int kFeatNk = 50;
       float r0, r1;                                                                               \
       if constexpr (f_ < 8 * NK_) {                                                               \
         constexpr int F_ = f_ / NK_, k_ = f_ % NK_;                                               \
-        r0 = __ldg(pf[F_] + k_ * nys);                                                            \
-        r1 = __ldg(pf[F_] + (k_ + 1) * nys);                                                      \
+        if constexpr (k_ == 0) cur = pf[F_];                                                      \
+        r0 = __ldg(cur);                                                                          \
+        r1 = __ldg(cur + nys);                                                                    \
+        cur += 2 * nys;                                                                           \
         if constexpr (F_ == 1) {                                                                  \
           r0 = logf(r0);                                                                          \
           r1 = logf(r1);                                                                          \
@@ -246,10 +277,14 @@ constexpr int kFeatNk = 50;
       } else if constexpr (f_ < 9 * NK_) {                                                        \
         constexpr int k_ = f_ - 8 * NK_;                                                          \
         if constexpr (k_ == 0) {                                                                  \
-          _Pragma("unroll") for (int q_ = 0; q_ <= NK_; ++q_) pw[q_] = __ldg(p8 + q_ * nys);      \
+          cur = p8;                                                                               \
+          pbelow = __ldg(cur);                                                                    \
         }                                                                                         \
-        r0 = pw[k_] - pw[k_ + 1];                                                                 \
-        r1 = pw[k_ + 1] - pw[k_ + 2];                                                             \
+        const float pm_ = __ldg(cur + nys), pt_ = __ldg(cur + 2 * nys);                           \
+        cur += 2 * nys;                                                                           \
+        r0 = pbelow - pm_;                                                                        \
+        r1 = pm_ - pt_;                                                                           \
+        pbelow = pt_;                                                                             \
       } else {                                                                                    \
         constexpr int q_ = f_ - 9 * NK_;                                                          \
         r0 = __ldg(two[q_]);                                                                      \
@@ -265,11 +300,8 @@ constexpr int kFeatNk = 50;
     if constexpr (W_ % 4 == 3) {                                                                  \
       constexpr int q_ = W_ / 4;                                                                  \
       const uint4 v_ = make_uint4(ring[0], ring[1], ring[2], ring[3]);                            \
-      if (kTiled)                                                                                 \
-        *reinterpret_cast<uint4 *>(xrow + (q_ >> 3) * 16384 + rr * 128 + (((q_ & 7) ^ (rr & 7)) << 4)) = v_; \
-      else                                                                                        \
-        *reinterpret_cast<uint4 *>(xrow + q_ * 16) = v_;                                          \
-      asm volatile("" ::: "memory");                                                              \
+      line[(q_ & 7) ^ swz] = v_;                                                                  \
+      if constexpr (q_ % 8 == 7) feat_flush<kTiled>(X, stage, row0, q_ / 8, lane, nrows);         \
     }                                                                                             \
   }
 #define RRTMG_FEAT_W4(b) RRTMG_FEAT_WORD(b) RRTMG_FEAT_WORD((b) + 1) RRTMG_FEAT_WORD((b) + 2) RRTMG_FEAT_WORD((b) + 3)
@@ -280,12 +312,17 @@ template <bool kTiled>
 __global__ void __launch_bounds__(kRowThreads) features_nk50_kernel(SurFeatureArgs a) {
   constexpr int NK = kFeatNk, kNf = 9 * NK + 4;
   __shared__ float4 st[kNf];
+  __shared__ uint4 stages[kRowThreads / 32][32 * 8];  // per warp: 32 rows x one 128-byte line
   for (int f = threadIdx.x; f < kNf; f += blockDim.x)
     st[f] = make_float4(a.mean[f], a.rstd[f], a.lo ? a.lo[f] : -__int_as_float(0x7f800000),
                         a.hi ? a.hi[f] : __int_as_float(0x7f800000));
   __syncthreads();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncol) return;
+  const int lane = threadIdx.x & 31;
+  const int c_raw = blockIdx.x * blockDim.x + threadIdx.x;
+  const int warp_c0 = c_raw - lane;
+  if (warp_c0 >= a.ncol) return;  // the whole warp
+  const int nrows = min(32, a.ncol - warp_c0);
+  const int c = min(c_raw, a.ncol - 1);  // lanes past the end repeat the last column, unwritten
   const int ny = a.ny;
   const size_t nys = static_cast<size_t>(ny);
   const int i = c / ny, j = c - i * ny;
@@ -294,15 +331,17 @@ __global__ void __launch_bounds__(kRowThreads) features_nk50_kernel(SurFeatureAr
                               a.o3 + b3};
   const float *const p8 = a.p8w + bl;
   const float *const two[4] = {a.tsk + c, a.albedo + c, a.coszr + c, a.emiss + c};
-  const size_t row = static_cast<size_t>(a.row_offset) + c;
-  uint8_t *xrow = kTiled ? static_cast<uint8_t *>(a.X) + (row >> 7) * 131072u
-                         : static_cast<uint8_t *>(a.X) + row * a.ldx * 2;
-  const int rr = static_cast<int>(row & 127);
+  uint8_t *const X = static_cast<uint8_t *>(a.X);
+  const size_t row0 = static_cast<size_t>(a.row_offset) + warp_c0;
+  const int swz = static_cast<int>((row0 + lane) & 7);
+  uint4 *const stage = stages[threadIdx.x >> 5];
+  uint4 *const line = stage + lane * 8;
   unsigned oob = 0;
   uint32_t ring[4];
-  float pw[NK + 1];
+  const float *cur = nullptr;  // next level of the field being read
+  float pbelow = 0.0f;         // p8w at the lower interface of the next thickness pair
   RRTMG_FEAT_W64(0) RRTMG_FEAT_W64(64) RRTMG_FEAT_W64(128) RRTMG_FEAT_W64(192)
-  if (a.flags) a.flags[c] = oob;
+  if (a.flags && c_raw < a.ncol) a.flags[c] = oob;
 }
 #undef RRTMG_FEAT_W64
 #undef RRTMG_FEAT_W16
