@@ -308,8 +308,11 @@ __device__ __forceinline__ void feat_flush(uint8_t *X, const uint4 *stage, size_
 #define RRTMG_FEAT_W16(b) RRTMG_FEAT_W4(b) RRTMG_FEAT_W4((b) + 4) RRTMG_FEAT_W4((b) + 8) RRTMG_FEAT_W4((b) + 12)
 #define RRTMG_FEAT_W64(b) RRTMG_FEAT_W16(b) RRTMG_FEAT_W16((b) + 16) RRTMG_FEAT_W16((b) + 32) RRTMG_FEAT_W16((b) + 48)
 
+// 7 resident blocks (72 registers; the field pointers spill and come back
+// from L1): 0.56 ms at 1M columns against 0.71 ms at 6 blocks (80 registers)
+// and 0.58 ms at 8 (64 registers, more spills).
 template <bool kTiled>
-__global__ void __launch_bounds__(kRowThreads) features_nk50_kernel(SurFeatureArgs a) {
+__global__ void __launch_bounds__(kRowThreads, 7) features_nk50_kernel(SurFeatureArgs a) {
   constexpr int NK = kFeatNk, kNf = 9 * NK + 4;
   __shared__ float4 st[kNf];
   __shared__ uint4 stages[kRowThreads / 32][32 * 8];  // per warp: 32 rows x one 128-byte line

@@ -618,6 +618,7 @@ _FIELDS_2D = ("tsk", "emiss", "albedo", "coszr", "xland", "xice", "snow")
 
 
 _SIDE = {}
+_HIGH = {}
 
 
 def _side_stream():
@@ -626,6 +627,16 @@ def _side_stream():
     if dev not in _SIDE:
         _SIDE[dev] = torch.cuda.Stream(device=dev)
     return _SIDE[dev]
+
+
+def _high_stream():
+    """A stream of the device's highest priority: its blocks are dispatched
+    before those of default-priority streams as SMs free up."""
+    import torch
+    dev = torch.cuda.current_device()
+    if dev not in _HIGH:
+        _HIGH[dev] = torch.cuda.Stream(device=dev, priority=-100)  # clamped to the highest
+    return _HIGH[dev]
 
 
 _SCALAR_KEYS_LW = ("p_top", "yr", "co2vmr", "n2ovmr", "ch4vmr", "cfc11vmr", "cfc12vmr", "has_reqc", "has_reqi",
@@ -735,9 +746,9 @@ def _fallback(st, d: dict, flags, out: dict, before_scatter=None) -> int:
 
 def _solve_listed(plan, lib, s, lst, cnt, ny, d, out, before_scatter, *, live: bool, n: int | None = None) -> None:
     """Gather the listed columns into the plan's compact domain, run LW (side
-    stream) and SW (current stream) on it, scatter the results back.  live:
-    the domain has plan.cap slots and the count stays on the device; else
-    exactly n columns."""
+    stream) and SW (high-priority stream) on it, scatter the results back.
+    live: the domain has plan.cap slots and the count stays on the device;
+    else exactly n columns."""
     import torch
     m = plan.cap if live else n
     for i, k in enumerate(plan.nz):
@@ -747,26 +758,31 @@ def _solve_listed(plan, lib, s, lst, cnt, ny, d, out, before_scatter, *, live: b
     plan.cfg_lw.ny = m
     plan.cfg_sw.ny = m
     ctx = plan.ctx
-    # LW on a side stream overlaps SW on the current stream; both read the
-    # gathered fields, and the current stream waits for LW before the scatter.
-    main, side = torch.cuda.current_stream(), _side_stream()
+    # LW and SW on two streams forked from the current one; both read the
+    # gathered fields, and the current stream waits for both before the
+    # scatter.  SW, the longer chain at fallback sizes (its latency-bound
+    # sweep follows throughput-bound optics), runs at high priority so that
+    # LW's blocks fill the SMs its kernels leave free rather than delay it.
+    main, side, high = torch.cuda.current_stream(), _side_stream(), _high_stream()
     ready = torch.cuda.Event()
     ready.record(main)
     side.wait_event(ready)
-    side_s = ctypes.c_void_p(side.cuda_stream)
+    high.wait_event(ready)
+    side_s, high_s = ctypes.c_void_p(side.cuda_stream), ctypes.c_void_p(high.cuda_stream)
     if live:
         ctx.check(ctx.lib.rrtmg_lwrad_live(ctx.handle, ctypes.byref(plan.cfg_lw), ctypes.byref(plan.cin_lw),
                                            ctypes.byref(plan.cout_lw), ctypes.c_void_p(cnt.data_ptr()), side_s))
         ctx.check(ctx.lib.rrtmg_swrad_live(ctx.handle, ctypes.byref(plan.cfg_sw), ctypes.byref(plan.cin_sw),
-                                           ctypes.byref(plan.cout_sw), ctypes.c_void_p(cnt.data_ptr()), s))
+                                           ctypes.byref(plan.cout_sw), ctypes.c_void_p(cnt.data_ptr()), high_s))
     else:
         ctx.check(ctx.lib.rrtmg_lwrad(ctx.handle, ctypes.byref(plan.cfg_lw), ctypes.byref(plan.cin_lw),
                                       ctypes.byref(plan.cout_lw), side_s))
         ctx.check(ctx.lib.rrtmg_swrad(ctx.handle, ctypes.byref(plan.cfg_sw), ctypes.byref(plan.cin_sw),
-                                      ctypes.byref(plan.cout_sw), s))
-    done = torch.cuda.Event()
-    done.record(side)
-    main.wait_event(done)
+                                      ctypes.byref(plan.cout_sw), high_s))
+    for done_on in (side, high):
+        done = torch.cuda.Event()
+        done.record(done_on)
+        main.wait_event(done)
     if before_scatter is not None:
         main.wait_event(before_scatter)
     for i, (k, _, _) in enumerate(plan.scatter_src):
