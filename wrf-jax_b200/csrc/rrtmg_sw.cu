@@ -46,6 +46,18 @@ struct SLayer {
   float cldfrac, clwp, ciwp, cswp, rel, rei, res;
 };
 
+// The fields of SLayer, as the sweep schedule's layer kernel stores them
+// (one array per field, (layer, chunk slot) with slots fastest) for the
+// band-parallel optics kernel.
+#define RRTMG_SW_LAYER_FLOATS(X)                                                                           \
+  X(pavel) X(tavel) X(pdp) X(fac00) X(fac01) X(fac10) X(fac11) X(colh2o) X(colco2) X(colo3) X(colch4)      \
+  X(colo2) X(colmol) X(selffac) X(selffrac) X(forfac) X(forfrac) X(cldfrac) X(clwp) X(ciwp) X(cswp) X(rel) \
+  X(rei) X(res)
+#define RRTMG_SW_LAYER_INTS(X) X(jp) X(jt) X(jt1) X(indself) X(indfor) X(trop)
+#define RRTMG_SW_COUNT(name) +1
+constexpr int kSwLayerFields = 1 RRTMG_SW_LAYER_FLOATS(RRTMG_SW_COUNT) RRTMG_SW_LAYER_INTS(RRTMG_SW_COUNT);  // + cloud-water flag
+#undef RRTMG_SW_COUNT
+
 __device__ __forceinline__ float in3(const float *p, const Col &C, int k) {
   return ld(p + (static_cast<size_t>(C.i) * C.nk + k) * C.ny + C.j);
 }
@@ -870,10 +882,12 @@ __device__ __forceinline__ void sw_column_outputs(const SwArgs &a, const Col &C,
 // per chunk:
 //   sw_colprep_kernel  warp = day slot: the column set-up once (laytrop by a
 //                      warp vote over the layers);
-//   sw_optics_kernel   thread = (day slot, layer, band): the band's gas and
-//                      Rayleigh depths of every g-point, its cloud optics, the
-//                      spectral interpolation its solar source uses, and jp,
-//                      into a layer record;
+//   sw_layer_kernel    thread = (day slot, layer): the layer set-up into
+//                      layer fields, and jp into the layer record;
+//   sw_optics_kernel   thread = (day slot, layer), block = one band: the
+//                      band's gas and Rayleigh depths of every g-point, its
+//                      cloud optics and the spectral interpolation its solar
+//                      source uses, into the layer record;
 //   sw_source_kernel   thread = (day slot, band): the band's solar source;
 //   sw_sweep_kernel    block = kSweepCols day slots x 112 g-points, thread =
 //                      one g-point: the top-down pass (delta-Eddington layers,
@@ -882,7 +896,8 @@ __device__ __forceinline__ void sw_column_outputs(const SwArgs &a, const Col &C,
 //                      per-level spectral sums in g-point order in shared
 //                      memory, then heating and the 2-D outputs.
 // Records: per chunk slot a column record, then nlay layer records of kSwRec
-// floats (1,376 bytes per layer, 70 KB per day column at nk = 50).  Each
+// floats (1,376 bytes per layer, 70 KB per day column at nk = 50), then the
+// kSwLayerFields layer fields (124 bytes per layer).  Each
 // band's g-points start on a 16-byte boundary (kPadOfs) so the optics kernel
 // writes whole float4s: taug at [0, 128), taur at [128, 256), the cloud optics
 // (tau, ssa, asm, unscaled tau) of band B at 256 + 4 B, the solar-source
@@ -903,6 +918,11 @@ constexpr size_t kSwColRecFloats = (sizeof(SwColRec) + 15) / 16 * 4;
 __device__ __forceinline__ SwColRec *sw_colrecs(const SwArgs &a) { return reinterpret_cast<SwColRec *>(a.records); }
 __device__ __forceinline__ float *sw_layrecs(const SwArgs &a) {
   return a.records + kSwColRecFloats * static_cast<size_t>(a.chunk_capacity);
+}
+// the layer fields of the chunk: field f of (layer l, slot u) at
+// [(f * (nk + 1) + l) * chunk_capacity + u]
+__device__ __forceinline__ float *sw_layfields(const SwArgs &a) {
+  return sw_layrecs(a) + static_cast<size_t>(kSwRec) * (a.nk + 1) * a.chunk_capacity;
 }
 
 // A warp per day column; the lanes take the layers of the laytrop count.
@@ -958,44 +978,92 @@ __device__ __forceinline__ void sw_band_record(const Tables &T, const SLayer &L,
   spec[2 * B + 1] = sp.fs;
 }
 
-// thread = (layer, chunk slot), slots fastest: the layer set-up once, then the
-// records of all 14 bands.
-// Resident blocks per SM the register allocation must allow (the optics
-// kernel at 80 registers instead of 128: 15.4 ms instead of 16.2 at 425 x 425
-// x 50; a fifth sweep block per SM spills and is slower).
-constexpr int kSwOpticsMinBlocks = 6;
-constexpr int kSwSweepMinBlocks = 4;
-__global__ void __launch_bounds__(128, kSwOpticsMinBlocks) sw_optics_kernel(Tables T, SwArgs a) {
+// sw_layer_kernel: thread = (layer, chunk slot), slots fastest: the layer
+// set-up (make_layer) and cldprmc_sw's activity test once, stored as layer
+// fields, and the layer's jp into its record.
+__global__ void __launch_bounds__(128) sw_layer_kernel(Tables T, SwArgs a) {
   const int n = a.nk + 1;
   const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int l = static_cast<int>(idx / a.chunk_count);
   const int u = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
   if (l >= n || a.chunk_first + u >= *a.nday) return;
   const Col C = sw_colrecs(a)[u].C;
-  float4 *rec = reinterpret_cast<float4 *>(sw_layrecs(a) + (static_cast<size_t>(u) * n + l) * kSwRec);
   const SLayer L = make_layer(T, a, C, l);
   // the activity test of cldprmc_sw (sw:1409-1440), the same for every band
   const float cswp = C.iceflg == 5 ? L.cswp : 0.0f;
   const bool cloud_water = a.icld != 0 && ((L.ciwp + L.clwp) + cswp) >= 1.0e-20f;
-  float spec[2 * kSwBands];
-  sw_band_record<0>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<1>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<2>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<3>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<4>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<5>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<6>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<7>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<8>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<9>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<10>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<11>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<12>(T, L, cloud_water, C.iceflg, rec, spec);
-  sw_band_record<13>(T, L, cloud_water, C.iceflg, rec, spec);
-#pragma unroll
-  for (int q = 0; q < kSwBands / 2; ++q)
-    rec[kSwRecSpec / 4 + q] = make_float4(spec[4 * q], spec[4 * q + 1], spec[4 * q + 2], spec[4 * q + 3]);
+  float *fld = sw_layfields(a) + static_cast<size_t>(l) * a.chunk_capacity + u;
+  const size_t fstride = static_cast<size_t>(n) * a.chunk_capacity;
+  int f = 0;
+#define RRTMG_SW_PUT(name) fld[static_cast<size_t>(f++) * fstride] = L.name;
+#define RRTMG_SW_PUTI(name) fld[static_cast<size_t>(f++) * fstride] = __int_as_float(L.name);
+  RRTMG_SW_LAYER_FLOATS(RRTMG_SW_PUT)
+  RRTMG_SW_LAYER_INTS(RRTMG_SW_PUTI)
+#undef RRTMG_SW_PUT
+#undef RRTMG_SW_PUTI
+  fld[static_cast<size_t>(f) * fstride] = __int_as_float(cloud_water ? 1 : 0);
+  float4 *rec = reinterpret_cast<float4 *>(sw_layrecs(a) + (static_cast<size_t>(u) * n + l) * kSwRec);
   rec[kSwRecJp / 4] = make_float4(__int_as_float(L.jp), 0.0f, 0.0f, 0.0f);
+}
+
+// sw_optics_kernel: one band per block.  Blocks of (layer, chunk slot) pairs
+// are taken kSwOpticsGroup at a time through all 14 bands, so that a group's
+// layer fields (about 8 MB) are read from L2 by the later bands; each block
+// runs one band's code only.
+// Resident blocks per SM the register allocation must allow: 6 (80
+// registers); at 8 (64 registers, with spills) the 425 x 425 x 50 step took
+// 118 ms instead of 103.
+constexpr int kSwOpticsGroup = 512;
+constexpr int kSwOpticsMinBlocks = 6;
+constexpr int kSwSweepMinBlocks = 4;
+__global__ void __launch_bounds__(128, kSwOpticsMinBlocks) sw_optics_kernel(Tables T, SwArgs a, int nblk) {
+  const int group = blockIdx.x / (kSwOpticsGroup * kSwBands);
+  const int g0 = group * kSwOpticsGroup;
+  const int gsize = nblk - g0 < kSwOpticsGroup ? nblk - g0 : kSwOpticsGroup;
+  const int within = blockIdx.x - group * kSwOpticsGroup * kSwBands;
+  const int band = within / gsize;
+  const int blk = g0 + (within - band * gsize);
+  const int n = a.nk + 1;
+  const long long idx = static_cast<long long>(blk) * blockDim.x + threadIdx.x;
+  const int l = static_cast<int>(idx / a.chunk_count);
+  const int u = static_cast<int>(idx - static_cast<long long>(l) * a.chunk_count);
+  if (l >= n || a.chunk_first + u >= *a.nday) return;
+  const float *fld = sw_layfields(a) + static_cast<size_t>(l) * a.chunk_capacity + u;
+  const size_t fstride = static_cast<size_t>(n) * a.chunk_capacity;
+  SLayer L;
+  int f = 0;
+#define RRTMG_SW_GET(name) L.name = fld[static_cast<size_t>(f++) * fstride];
+#define RRTMG_SW_GETI(name) L.name = __float_as_int(fld[static_cast<size_t>(f++) * fstride]);
+  RRTMG_SW_LAYER_FLOATS(RRTMG_SW_GET)
+  RRTMG_SW_LAYER_INTS(RRTMG_SW_GETI)
+#undef RRTMG_SW_GET
+#undef RRTMG_SW_GETI
+  const bool cloud_water = __float_as_int(fld[static_cast<size_t>(f) * fstride]) != 0;
+  const int iceflg = sw_colrecs(a)[u].C.iceflg;
+  float *rec = sw_layrecs(a) + (static_cast<size_t>(u) * n + l) * kSwRec;
+  float spec[2 * kSwBands];
+#define RRTMG_SW_OPT(B)                                                                                    \
+  {                                                                                                        \
+    sw_band_record<B>(T, L, cloud_water, iceflg, reinterpret_cast<float4 *>(rec), spec);                   \
+    *reinterpret_cast<float2 *>(rec + kSwRecSpec + 2 * (B)) = make_float2(spec[2 * (B)], spec[2 * (B) + 1]); \
+  }
+  switch (band) {
+    case 0: RRTMG_SW_OPT(0); break;
+    case 1: RRTMG_SW_OPT(1); break;
+    case 2: RRTMG_SW_OPT(2); break;
+    case 3: RRTMG_SW_OPT(3); break;
+    case 4: RRTMG_SW_OPT(4); break;
+    case 5: RRTMG_SW_OPT(5); break;
+    case 6: RRTMG_SW_OPT(6); break;
+    case 7: RRTMG_SW_OPT(7); break;
+    case 8: RRTMG_SW_OPT(8); break;
+    case 9: RRTMG_SW_OPT(9); break;
+    case 10: RRTMG_SW_OPT(10); break;
+    case 11: RRTMG_SW_OPT(11); break;
+    case 12: RRTMG_SW_OPT(12); break;
+    default: RRTMG_SW_OPT(13); break;
+  }
+#undef RRTMG_SW_OPT
 }
 
 #define RRTMG_SW_BAND_SWITCH(band, CALL) \
@@ -1351,7 +1419,7 @@ cudaError_t launch_sw_daylist(const SwArgs &a, cudaStream_t stream) {
 }
 
 size_t sw_record_floats(int nk, int chunk) {
-  return (kSwColRecFloats + static_cast<size_t>(kSwRec) * (nk + 1)) * static_cast<size_t>(chunk);
+  return (kSwColRecFloats + static_cast<size_t>(kSwRec + kSwLayerFields) * (nk + 1)) * static_cast<size_t>(chunk);
 }
 
 cudaError_t launch_sw_chunk_optics(const Tables &T, const SwArgs &a, cudaStream_t stream) {
@@ -1361,7 +1429,11 @@ cudaError_t launch_sw_chunk_optics(const Tables &T, const SwArgs &a, cudaStream_
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const long long layers = static_cast<long long>(a.chunk_count) * n;
-  sw_optics_kernel<<<static_cast<unsigned>((layers + threads - 1) / threads), threads, 0, stream>>>(T, a);
+  const long long blocks = (layers + threads - 1) / threads;
+  sw_layer_kernel<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(T, a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  sw_optics_kernel<<<static_cast<unsigned>(blocks * kSwBands), threads, 0, stream>>>(T, a, static_cast<int>(blocks));
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   sw_source_kernel<<<dim3((a.chunk_count + threads - 1) / threads, kSwBands), threads, 0, stream>>>(T, a);
