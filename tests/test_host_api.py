@@ -54,3 +54,16 @@ def test_infer_host_rejects_pageable_buffers(pkg):
     out = {k: torch.empty((2, S.NK, 3) if k.startswith("rthraten") else (2, 3)) for k in S.OUTPUT_FIELDS}
     with pytest.raises(ValueError):
         S.infer_host(None, st, host, out)
+
+
+@pytest.mark.parametrize("nx,slabs", [(1000, 8), (425, 8), (9, 8), (3, 8), (2, 8), (1, 8), (100, 3), (100, 2),
+                                      (100, 1)])
+def test_host_pipeline_slabs_cover_the_rows_once(pkg, nx, slabs):
+    from wrf_jax_b200 import surrogate as S
+    b = S._slab_bounds(nx, slabs)
+    assert b[0][0] == 0 and b[-1][1] == nx
+    assert all(i1 > i0 for i0, i1 in b) and all(b[q][1] == b[q + 1][0] for q in range(len(b) - 1))
+    assert len(b) <= min(slabs, nx)
+    if nx >= 4 * slabs and slabs >= 3:  # the last two slabs taper to a half and a quarter
+        sizes = [i1 - i0 for i0, i1 in b]
+        assert sizes[-1] < sizes[-2] < sizes[0]

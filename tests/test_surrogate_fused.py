@@ -155,7 +155,7 @@ def test_infer_host_equals_device_path(torch_cuda, model):
     torch.cuda.synchronize()
     host = {k: torch.from_numpy(v).pin_memory() for k, v in st.fields.items()}
     out = {k: torch.empty(tuple(getattr(ref, k).shape), pin_memory=True) for k in S.OUTPUT_FIELDS}
-    for slabs in (3, 1):
+    for slabs in (8, 3, 1):  # 8: tapered last slabs (6 x 6 rows, then 3 and 1)
         for t in out.values():
             t.fill_(float("nan"))
         n = S.infer_host(model, st, host, out, energy_tol=1.0, slabs=slabs)

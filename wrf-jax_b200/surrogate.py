@@ -495,6 +495,19 @@ def _host_workspace(nx: int, nk: int, ny: int, rows: int) -> dict:
     return ws
 
 
+def _slab_bounds(nx: int, slabs: int) -> list:
+    """West-east row ranges of the host pipeline's slabs: equal slabs, the
+    last two at a half and a quarter of the others; no empty slab."""
+    slabs = max(1, min(int(slabs), nx))
+    weights = [1.0] * slabs if slabs < 3 else [1.0] * (slabs - 2) + [0.5, 0.25]
+    total, acc, edges = sum(weights), 0.0, [0]
+    for w in weights[:-1]:
+        acc += w
+        edges.append(int(round(nx * acc / total)))
+    edges.append(nx)
+    return [(i0, i1) for i0, i1 in zip(edges, edges[1:]) if i1 > i0]
+
+
 def infer_host(model: SurrogateModel, st, host: dict, out: dict, *, energy_tol: float = 5.0, slabs: int = 8,
                fallback: bool = True) -> int:
     """Surrogate radiation with host inputs and outputs, pipelined over the
@@ -505,9 +518,12 @@ def infer_host(model: SurrogateModel, st, host: dict, out: dict, *, energy_tol: 
     west-east rows on one copy stream, each slab's network runs as soon as it
     has landed and its outputs return on a second copy stream; the fallback
     then reads the other inputs of its columns from host memory in place and
-    writes its columns' outputs back to host memory in place.  Results are
-    those of infer() on device fields.  Returns the number of fallback columns;
-    the outputs are complete on return."""
+    writes its columns' outputs back to host memory in place.  The last two
+    slabs are a half and a quarter of the others, which shortens the part of
+    the step left after the last transfer (the last slab's network and the
+    return of its outputs).  Results are those of infer() on device fields.
+    Returns the number of fallback columns; the outputs are complete on
+    return."""
     import torch
     if st.nk != NK:
         raise ValueError(f"the surrogate is built for {NK} levels, got {st.nk}")
@@ -516,8 +532,7 @@ def infer_host(model: SurrogateModel, st, host: dict, out: dict, *, energy_tol: 
                 and t.dtype == torch.float32):
             raise ValueError(f"{name} must be a contiguous page-locked CPU float32 tensor")
     nx, ny, nk = st.nx, st.ny, st.nk
-    slabs = max(1, min(int(slabs), nx))
-    bounds = [(nx * q // slabs, nx * (q + 1) // slabs) for q in range(slabs)]
+    bounds = _slab_bounds(nx, slabs)
     ws = _host_workspace(nx, nk, ny, max(i1 - i0 for i0, i1 in bounds))
     main, h2d, d2h = torch.cuda.current_stream(), ws["h2d"], ws["d2h"]
     dev, dout, flags = ws["d"], ws["out"], ws["flags"]
@@ -532,6 +547,7 @@ def infer_host(model: SurrogateModel, st, host: dict, out: dict, *, energy_tol: 
             ev.record(h2d)
             landed.append(ev)
     s = _stream()
+    n_fb = 0
     for (i0, i1), ev in zip(bounds, landed):
         main.wait_event(ev)
         d_slab = {k: v[i0:i1] for k, v in dev.items()}
@@ -543,8 +559,10 @@ def infer_host(model: SurrogateModel, st, host: dict, out: dict, *, energy_tol: 
         with torch.cuda.stream(d2h):
             for k in OUTPUT_FIELDS:
                 out[k][i0:i1].copy_(dout[k][i0:i1], non_blocking=True)
-    n_fb = 0
     if fallback:
+        # the fallback reads its columns' other inputs from host memory in
+        # place; a slab's fallback ahead of the later slabs' transfers gained
+        # nothing (the last one is latency-bound and stays exposed)
         returned = torch.cuda.Event()
         returned.record(d2h)
         src = {k: (dev[k] if k in dev else host[k]) for k in host}
