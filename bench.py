@@ -328,7 +328,10 @@ def run_plain(args):
     ctx.check(ctx.lib.rrtmg_get_schedule(ctx.handle, ctypes.byref(sched)))
     lw_chunks = -(-ncol // sched.lw_chunk_columns)
     sw_chunks = -(-ncol // sched.sw_chunk_columns)
-    gpu_launches = (1 + 4 * lw_chunks) + (2 + 4 * sw_chunks)
+    # LW: McICA, then per chunk column set-up, layer set-up, gas optics, sweep;
+    # SW: McICA, day list, then per chunk column set-up, layer set-up, band
+    # optics, solar source, sweep
+    gpu_launches = (1 + 4 * lw_chunks) + (2 + 5 * sw_chunks)
     nday = int((np.asarray(sw_host["coszr"]) > 0.0).sum())
     # The sweep kernels of the staged schedules and their HBM bytes per unit.
     # sw_sweep_kernel, per day column: per layer each g-point's gas and
@@ -395,11 +398,16 @@ def run_plain(args):
 
 def _surrogate_launches(n_fallback: int, fused: bool) -> int:
     """Kernel launches of one surrogate step: features, the fused network
-    kernel (or 4 GEMMs and a decode), compact; with fallback columns also one
-    batched gather and one scatter, the LW sweep schedule (McICA, column
-    set-up, layer set-up, gas optics, sweep) and the SW sweep schedule
-    (McICA, day list, column set-up, layer optics, solar source, sweep)."""
-    return (3 if fused else 7) + (13 if n_fallback > 0 else 0)
+    kernel (or 4 GEMMs and a decode), compact; then the fallback's batched
+    gather and scatter, the LW sweep schedule (McICA, column set-up, layer
+    set-up, gas optics, sweep) and the SW sweep schedule (McICA, day list,
+    column set-up, layer set-up, band optics, solar source, sweep), queued
+    with the rejected count left on the device whatever it is; all of the
+    fallback once more on a domain of the exact size when more columns are
+    rejected than its capacity."""
+    from wrf_jax_b200 import surrogate as S
+    per_solve = 2 + 5 + 7
+    return (3 if fused else 7) + per_solve + (per_solve if n_fallback > S.FALLBACK_CAPACITY else 0)
 
 
 def run_surrogate(args):
