@@ -716,23 +716,45 @@ __device__ __forceinline__ void sw_source(const Tables &T, const Col &C, JpFn jp
   const int layreffr = K.layreffr;
   int ls = -1;
   bool found = false;
+  // The searches read jp in batches of kJpBatch layers so that the record
+  // loads overlap; each stops where its condition can no longer hold (below
+  // laytrop for the lower-atmosphere bands, from laytrop up for 17 and 28).
+  constexpr int kJpBatch = 8;
   if constexpr (bn == 18 || bn == 19 || bn == 21 || bn == 22 || bn == 24) {
     // first troposphere crossing of layreffr, one layer up, capped at laytrop-1
-    for (int l = 0; l < n && !found; ++l) {
-      const int jl = jp(l);
-      const int next = l + 1 < n ? jp(l + 1) : jl;
-      if (l < C.laytrop && jl < layreffr && next >= layreffr) {
-        found = true;
-        ls = (l + 1 < C.laytrop - 1) ? l + 1 : C.laytrop - 1;
+    const int lend = C.laytrop < n ? C.laytrop : n;
+    for (int l0 = 0; l0 < lend && !found; l0 += kJpBatch) {
+      int jb[kJpBatch + 1];
+#pragma unroll
+      for (int q = 0; q <= kJpBatch; ++q) jb[q] = l0 + q < n ? jp(l0 + q) : 0;
+#pragma unroll
+      for (int q = 0; q < kJpBatch; ++q) {
+        const int l = l0 + q;
+        if (l < lend && !found) {
+          const int jl = jb[q];
+          const int next = l + 1 < n ? jb[q + 1] : jl;
+          if (jl < layreffr && next >= layreffr) {
+            found = true;
+            ls = (l + 1 < C.laytrop - 1) ? l + 1 : C.laytrop - 1;
+          }
+        }
       }
     }
     if (!found) ls = C.laytrop - 1;
   }
   if constexpr (bn == 17 || bn == 28) {
-    for (int l = 1; l < n && !found; ++l) {
-      if (l >= C.laytrop && jp(l - 1) < layreffr && jp(l) >= layreffr) {
-        found = true;
-        ls = l;
+    const int lbeg = C.laytrop > 1 ? C.laytrop : 1;
+    for (int l0 = lbeg; l0 < n && !found; l0 += kJpBatch) {
+      int jb[kJpBatch + 1];  // jp(l0 - 1 + q)
+#pragma unroll
+      for (int q = 0; q <= kJpBatch; ++q) jb[q] = l0 - 1 + q < n ? jp(l0 - 1 + q) : 0;
+#pragma unroll
+      for (int q = 0; q < kJpBatch; ++q) {
+        const int l = l0 + q;
+        if (l < n && !found && jb[q] < layreffr && jb[q + 1] >= layreffr) {
+          found = true;
+          ls = l;
+        }
       }
     }
     if (!found) ls = n - 1;
