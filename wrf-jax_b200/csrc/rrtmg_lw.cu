@@ -120,7 +120,13 @@ __device__ float retab_interp(const Tables &T, float temp, int hi) {
 }
 
 // Column set-up: buffer layers above the model top (lw:6633-6786).
-__device__ void column_setup(const Tables &T, const LwArgs &a, Col &C) {
+// kWarp: called by the 32 lanes of a warp for one column, each lane taking
+// every 32nd buffer level (temperature) and buffer layer (ozone) into the
+// warp's shared arrays s_tlev / s_o3, which every lane then reads back; the
+// values are those of the one-thread form.
+template <bool kWarp = false>
+__device__ void column_setup(const Tables &T, const LwArgs &a, Col &C, int lane = 0, float *s_tlev = nullptr,
+                             float *s_o3 = nullptr) {
   const int nk = C.nk, nlay = C.nlay, nbuf = C.nbuf;
   C.plev_b[0] = pa_to_hpa(in3w(a.in.p8w, C, nk));
   for (int m = 1; m <= nbuf; ++m) C.plev_b[m] = C.plev_b[m - 1] - 4.0f;
@@ -138,20 +144,32 @@ __device__ void column_setup(const Tables &T, const LwArgs &a, Col &C) {
     return w * (t1 - t0) + t0;
   };
   const float offset = in3w(a.in.t8w, C, nk - 1) - varint(pa_to_hpa(in3w(a.in.p8w, C, nk - 1)));
-  for (int m = 0; m <= nbuf; ++m) C.tlev_b[m] = varint(C.plev_b[m]) + offset;
-  // tlay[lev-1] = (tlev[lev] + tlev[lev-1]) / 2 for lev = nk .. nlay
-  C.tlay_b[0] = 0.5f * (C.tlev_b[0] + in3w(a.in.t8w, C, nk - 1));
-  for (int m = 1; m <= nbuf; ++m) C.tlay_b[m] = 0.5f * (C.tlev_b[m] + C.tlev_b[m - 1]);
+  if constexpr (kWarp) {
+    for (int m = lane; m <= nbuf; m += 32) s_tlev[m] = varint(C.plev_b[m]) + offset;
+  } else {
+    for (int m = 0; m <= nbuf; ++m) C.tlev_b[m] = varint(C.plev_b[m]) + offset;
+  }
   // ozone above the model top (lw:6766-6786)
   const float amdo = 0.603461f;
   const float o3base = in3(a.in.o3, C, nk - 1) -
                        o3data_layer(T, pa_to_hpa(in3w(a.in.p8w, C, nk - 1)), C.plev_b[0]) * amdo;
-  for (int m = 0; m < nbuf; ++m) {
+  auto o3_layer = [&](int m) {
     const float mmr = o3data_layer(T, C.plev_b[m], C.plev_b[m + 1]) * amdo;
     float top = o3base + mmr;
     if (top <= 0.0f) top = mmr;
-    C.o3_b[m] = top;
+    return top;
+  };
+  if constexpr (kWarp) {
+    for (int m = lane; m < nbuf; m += 32) s_o3[m] = o3_layer(m);
+    __syncwarp();
+    for (int m = 0; m <= nbuf; ++m) C.tlev_b[m] = s_tlev[m];
+    for (int m = 0; m < nbuf; ++m) C.o3_b[m] = s_o3[m];
+  } else {
+    for (int m = 0; m < nbuf; ++m) C.o3_b[m] = o3_layer(m);
   }
+  // tlay[lev-1] = (tlev[lev] + tlev[lev-1]) / 2 for lev = nk .. nlay
+  C.tlay_b[0] = 0.5f * (C.tlev_b[0] + in3w(a.in.t8w, C, nk - 1));
+  for (int m = 1; m <= nbuf; ++m) C.tlay_b[m] = 0.5f * (C.tlev_b[m] + C.tlev_b[m - 1]);
   (void)nlay;
 }
 
@@ -1320,11 +1338,12 @@ __device__ __forceinline__ bool load_mask(const LwArgs &a, int l, int col, uint3
   return any != 0u;
 }
 
-// A warp per column: the lanes take the layers of the column integrals, whose
-// sums are then taken in layer order from shared memory (the operations and
-// order of column_prologue).
+// A warp per column: the lanes take the buffer levels of the column set-up
+// and the layers of the column integrals, whose sums are then taken in layer
+// order from shared memory (the operations and order of column_prologue).
 __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
   __shared__ float s_cd[4][kMaxLay], s_wk[4][kMaxLay];
+  __shared__ float s_tlev[4][kMaxBuf + 1], s_o3[4][kMaxBuf];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lc = blockIdx.x * 4 + w;
   if (lc >= a.chunk_count || dead_column(a.live, a.chunk_first + lc)) return;  // whole warps
@@ -1332,7 +1351,7 @@ __global__ void __launch_bounds__(128) lw_colprep_kernel(Tables T, LwArgs a) {
   ColRec r;
   Col &C = r.C;
   column_head(a, col, C);
-  column_setup(T, a, C);
+  column_setup<true>(T, a, C, lane, s_tlev[w], s_o3[w]);
   const int nlay = C.nlay;
   int trop_count = 0;
   bool cloud = false;
