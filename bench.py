@@ -100,7 +100,12 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """nvidia-smi clock/throttle samples during the timed region.  The sampler
+    is started, and its first sample awaited, before the region: nvidia-smi's
+    start-up attaches to the driver, which can hold up CUDA calls of other
+    processes for a while (the plain bench's enqueues stalled by hundreds of
+    ms with the sampler started inside the region).  The first sample, taken
+    before the region, is left out of the summary."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -118,6 +123,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
+        if self.proc is not None:
+            import select
+            ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+            if ready:
+                self.proc.stdout.readline()  # the warm-up sample
         return self
 
     def __exit__(self, *exc):
