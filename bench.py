@@ -72,6 +72,14 @@ FLOP_COUNTS = REPO / "tests" / "golden" / "flop_counts.json"
 # FMA contraction (one instruction per add or multiply), so their issue-bound
 # ceiling is half of it.
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+# DRAM bytes of one fused-kernel launch per column: dram__bytes_read.sum +
+# dram__bytes_write.sum of one mlp_kernel launch on 500,000 columns (ncu, the
+# 500 x 1000 x 50 surrogate bench; its 512 MB of feature tiles exceed L2),
+# 719,976,960 + 190,990,080 bytes: the reads are the compulsory 1,440 bytes per
+# column (feature tile, pi3d, p8w, coszr, flags), the writes just under the
+# outputs' 420 (the last ones still in L2 when the kernel ends).  Every byte
+# is per column, so a launch's traffic is this times its columns.
+MLP_DRAM_BYTES_PER_COLUMN = (719_976_960 + 190_990_080) / 500_000
 # compulsory HBM bytes of one column through both calls at nk levels: 12 mass-
 # level and 2 interface-level fields read, 4 heating fields written, 37 2-D
 # values in or out, binary32
@@ -595,7 +603,10 @@ def run_surrogate(args):
         "heating_rmse_kday": heat_rmse, "surface_flux_rmse_wm2": flux_rmse, "accuracy": accuracy,
         "fallback_fraction": res.n_fallback / ncol,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                     "frac": achieved / bf16, "traffic": None,
+                     "frac": achieved / bf16,
+                     "traffic": MLP_DRAM_BYTES_PER_COLUMN * ncol if fused else None,
+                     "traffic_source": ("ncu DRAM bytes of one launch on 500,000 columns, scaled to the launch's "
+                                        "columns" if fused else None),
                      "kernel": "mlp_kernel (4 layers + decode, fused)" if fused else "umma_gemm_kernel (4 GEMMs)",
                      "kernel_ms": kernel_ms, "flops_per_launch": flops, "padded_flops_per_launch": flops_padded,
                      "peak_source": peak_kind, "unfused_gemms_ms": gemm_ms, "fused_ms": fused_ms},
