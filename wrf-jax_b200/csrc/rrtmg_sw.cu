@@ -542,6 +542,12 @@ __device__ __forceinline__ float zero_over(float x) {
   return __int_as_float(__float_as_int(x) & static_cast<int>(0x80000000u));
 }
 
+// The four components of x and y have the same bit patterns.
+__device__ __forceinline__ bool same_bits(float4 x, float4 y) {
+  return ((__float_as_uint(x.x) ^ __float_as_uint(y.x)) | (__float_as_uint(x.y) ^ __float_as_uint(y.y)) |
+          (__float_as_uint(x.z) ^ __float_as_uint(y.z)) | (__float_as_uint(x.w) ^ __float_as_uint(y.w))) == 0u;
+}
+
 // FP64 mode: the Pade lookup of exp(-v) (sw:2722-2760) with binary64
 // arithmetic; the table is the same binary32 data.
 __device__ __forceinline__ double exp_lookup64(const Tables &T, double v) {
@@ -1140,6 +1146,7 @@ constexpr int kRing = 8;                              // levels of terms per ord
 struct SweepShared {
   float ring[kRing][kSweepCols][4][kSwGpts];
   float sums[kSweepCols][6][kMaxLev];  // type: fu, fd, cu, cd, fdir, cdir; level top-down
+  uint32_t slotbits[2][kMaxLay / 32][kSweepThreads];  // per thread: cloudy slots, total = clear slots
 };
 
 // One level of one adding path, as the bottom-up pass reads it back: the
@@ -1215,6 +1222,12 @@ __global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_ker
 
   // per-thread stack of the top-down pass, read back bottom-up
   SwLevel stc[kMaxLev], stt[kMaxLev];
+  // per stack slot r, bit r & 31 of word r >> 5 (gathered in registers, 32
+  // slots at a time, then kept in shared memory): the g-point layer is cloudy
+  // (its total-sky reftra results are stored), and the slot's total-sky
+  // values equal the clear-sky ones bit for bit (no total-sky slot is stored;
+  // the bottom-up pass reuses the clear-sky slot and reads no mask word)
+  uint32_t cloudy_bits = 0, same_word = 0;
 
   // ---- top-down pass: layer optics, direct beam, downward adding (sw:6887-7041)
   const int dtypes[2] = {4, 5};
@@ -1264,8 +1277,13 @@ __global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_ker
     const float v_c = d_w == 1.0f ? v_nd : ztauc / mu;
     const float dbtc = d_w == 1.0f ? dbtc_nd : exp_lookup(T, v_c);
     const RT4 c = reftra<kFp64>(T, zgcc, mu, ztauc, zomcc, v_c, dbtc);
-    stc[r].rt = make_float4(c.ref, c.refd, c.tra, c.trad);
+    const float4 c_rt = make_float4(c.ref, c.refd, c.tra, c.trad);
+    stc[r].rt = c_rt;
     stc[r].dn = make_float4(dbtc, c_tdbt, c_tdn, c_rdnd);
+    // the total-sky carry equals the clear-sky one bit for bit (first half of
+    // the test whether this slot's total-sky values need storing)
+    const bool carry_same =
+        same_bits(make_float4(0.0f, t_tdbt, t_tdn, t_rdnd), make_float4(0.0f, c_tdbt, c_tdn, c_rdnd));
     // downward recurrence of vrtqdr (sw:3681-3702) for level r + 1
     {
       const float tdbt_next = c_tdbt * dbtc;
@@ -1303,6 +1321,7 @@ __global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_ker
         trad = clear * c.trad + cloud * o.trad;
         dbt = clear * dbtc + cloud * dbtmo;
         stt[r].rt = make_float4(ref, refd, tra, trad);
+        cloudy_bits |= 1u << (r & 31);
       } else {
         // no cloud in this g-point layer: taor = tcld = 0, so tauorig and
         // ztauo are ztau and ztauc plus zero, and the cloudy reftra is the
@@ -1320,7 +1339,13 @@ __global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_ker
         trad = clear * c.trad + cloud * 1.0f;
         dbt = clear * dbtc + cloud * dbtmo;
       }
-      stt[r].dn = make_float4(dbt, t_tdbt, t_tdn, t_rdnd);
+      const float4 t_dn = make_float4(dbt, t_tdbt, t_tdn, t_rdnd);
+      if (!cldb && carry_same && __float_as_uint(dbt) == __float_as_uint(dbtc) &&
+          same_bits(make_float4(ref, refd, tra, trad), c_rt)) {
+        same_word |= 1u << (r & 31);
+      } else {
+        stt[r].dn = t_dn;
+      }
       const float tdbt_next = t_tdbt * dbt;
       float tdn_next, rdnd_next;
       if (r == 0) {
@@ -1336,6 +1361,12 @@ __global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_ker
       t_rdnd = rdnd_next;
     } else {
       tdbt_nd = tdbtc_nd;
+    }
+    if ((r & 31) == 31 || r == n - 1) {
+      S.slotbits[0][r >> 5][threadIdx.x] = cloudy_bits;
+      S.slotbits[1][r >> 5][threadIdx.x] = same_word;
+      cloudy_bits = 0;
+      same_word = 0;
     }
     S.ring[filled][cslot][0][G] = tdbt_nd * zincflx;
     S.ring[filled][cslot][1][G] = tdbtc_nd * zincflx;
@@ -1368,12 +1399,12 @@ __global__ void __launch_bounds__(kSweepThreads, kSwSweepMinBlocks) sw_sweep_ker
   // this g-point has the total-sky mix clear * c + cloud * (0, 0, 1, 1)
   auto load_slot = [&](int j, SwLevel &lc, SwLevel &lt) {
     lc = stc[j];
-    if (clear_only) {
+    if (clear_only || ((S.slotbits[1][j >> 5][threadIdx.x] >> (j & 31)) & 1u) != 0u) {
       lt = lc;
       return;
     }
     lt.dn = stt[j].dn;
-    if ((maskbase[static_cast<size_t>(n - 1 - j) * mstride] & bit) != 0u) {
+    if (((S.slotbits[0][j >> 5][threadIdx.x] >> (j & 31)) & 1u) != 0u) {
       lt.rt = stt[j].rt;
     } else {
       const float clear = 1.0f, cloud = 0.0f;
