@@ -20,6 +20,12 @@ coupling, accumulation into t_tendf) on 1000 x 51 x 1000 memory arrays.
 the inputs and the device->host copies of the outputs are inside the timed
 region.
 
+On one GPU the default line also carries `ensemble`: the ragged-ensemble
+workload (`--workload ensemble`: 12 domains, half surrogate, one CUDA-graph
+replay per step against the same domains launched one after another), run in
+a child process after the surrogate measurement (`--no-ensemble` leaves it
+out).
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload surrogate|plain] [--impl reference]
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own domain (weak
@@ -57,9 +63,9 @@ METRIC = "LW+SW columns/s on 1 B200: surrogate vs plain RRTMG @ heating RMSE≤0
 CPU_SAMPLE_COLUMNS = 42500
 # DRAM traffic per unit of the sweep kernels, from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch divided by its units; the first launch
-# on the 256 x 256 x 50 domain, a full chunk): sw_sweep_kernel 19.75 GB over
+# on the 256 x 256 x 50 domain, a full chunk): sw_sweep_kernel 15.62 GB over
 # 32,768 day columns, lw_sweep_kernel 2.374 GB over 16,384 columns
-DRAM_BYTES_PER_DAY_COLUMN_SW = 602800
+DRAM_BYTES_PER_DAY_COLUMN_SW = 476700
 DRAM_BYTES_PER_COLUMN_LW = 144900
 L2_BYTES = 126 * 1024 * 1024
 # counted binary32 operations of the plain path per LW column and per SW day
@@ -354,15 +360,18 @@ def run_plain(args):
     # The sweep kernels of the staged schedules and their HBM bytes per unit.
     # sw_sweep_kernel, per day column: per layer each g-point's gas and
     # Rayleigh depths and each band's cloud optics from the layer records
-    # (2 x 112 + 4 x 14 floats), its level stack written and read back (16
-    # floats per level and g-point, twice), the McICA mask (4 words per layer),
-    # pi3d and p8w for the heating, 2 heating fields and 16 2-D outputs.
+    # (2 x 112 + 4 x 14 floats), the clear-sky half of its level stack written
+    # and read back (8 floats per level and g-point, twice), the McICA mask (4
+    # words per layer), pi3d and p8w for the heating, 2 heating fields and 16
+    # 2-D outputs.  The total-sky stack slots, stored only where the g-point
+    # layer is cloudy or its total-sky values differ from the clear-sky ones,
+    # are data-dependent and not counted: a lower bound on the bytes moved.
     # lw_sweep_kernel, per column: the layer records read in both sweeps
     # (2 x 140 + 4 x 16 + 1 floats per layer, twice), the mask (5 words per
     # layer, twice), pi3d and p8w, 2 heating fields and 15 2-D outputs.
     nlay_lw = ctx.lib.rrtmg_lw_nlayers(float(lw_host["p_top"]), nk)
     unit_bytes = {
-        "sw_sweep_kernel": 4 * (nlay_sw * (2 * 112 + 4 * 14) + 2 * 16 * (nlay_sw + 1) * 112 + 4 * nlay_sw
+        "sw_sweep_kernel": 4 * (nlay_sw * (2 * 112 + 4 * 14) + 2 * 8 * (nlay_sw + 1) * 112 + 4 * nlay_sw
                                 + nk + (nk + 1) + 2 * nk + 16),
         "lw_sweep_kernel": 4 * (2 * nlay_lw * (2 * 140 + 4 * 16 + 1) + 2 * 5 * nlay_lw + nk + (nk + 1) + 2 * nk + 15),
     }
@@ -619,10 +628,39 @@ def run_surrogate(args):
         v, th, desc, dt = cpu_baseline(int(os.environ.get("RRTMG_CPU_SAMPLE_COLUMNS", str(CPU_SAMPLE_COLUMNS))),
                                        workload=wl)
         line["cpu_baseline"] = {"value": v, "unit": "columns/s", "cores": th, "kind": "port", "sample": desc}
+    if rank == 0 and ws == 1 and not args.no_ensemble:
+        line["ensemble"] = ensemble_leg()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+ENSEMBLE_KEYS = ("value", "ms_per_step", "sequential_value", "sequential_ms_per_step", "latency_p50_ms",
+                 "latency_p99_ms", "sequential_latency_p50_ms", "sequential_latency_p99_ms", "fallback_columns",
+                 "autotune_trials", "clocks")
+
+
+def ensemble_leg(steps: int = 3, warmup: int = 3, timeout_s: int = 420) -> dict:
+    """The ragged-ensemble workload (`--workload ensemble`) run in a child
+    process on the same GPU after the surrogate measurement, summarised for the
+    default line: graph-replay and sequential columns/s and per-domain
+    completion latencies.  A failure is reported in the summary, not raised."""
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--workload", "ensemble", "--steps", str(steps),
+           "--warmup", str(warmup)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, cwd=str(REPO))
+    except subprocess.TimeoutExpired:
+        return {"error": f"ensemble run exceeded {timeout_s} s"}
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr or r.stdout).strip().splitlines()[-1:] or [""]
+        return {"error": f"ensemble run exited {r.returncode}: {tail[0][:200]}"}
+    d = json.loads(lines[-1])
+    out = {"workload": d["config"]["workload"], "unit": "columns/s", "columns_per_step": d["config"]["columns_per_step"],
+           "schedule": d["config"]["schedule"], "steps": steps, "warmup": warmup}
+    out.update({k: d[k] for k in ENSEMBLE_KEYS if k in d})
+    return out
 
 
 def run_ensemble(args):
@@ -923,6 +961,8 @@ def main():
     ap.add_argument("--nk", type=int, default=None)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--unfused", action="store_true", help="surrogate network as 4 GEMMs + decode kernel")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="leave out the ragged-ensemble leg of the default line (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args, SURROGATE_WORKLOAD if args.workload == "surrogate" else WORKLOAD)
